@@ -1,0 +1,247 @@
+"""beyond-rpa_b200: B200 (sm_100a) Cholesky-vector RPA hot path.
+
+Thin ctypes binding of the C ABI in include/rpa_b200.h (librpa_b200.so, built
+in-tree by build.py).  The binding only marshals arguments: every array is
+passed to the library as a pointer (numpy arrays as host pointers, torch CUDA
+tensors as device pointers) and all compute runs in the CUDA library.  There
+is no CPU fallback: if the library or a B200 is missing, calls raise.
+
+Python names follow the reference routines they stand in for:
+  pi_u            rpa_THC_PiU (src/rpa/rpa_THC.f90:215-282)
+  ec_from_pi      rpa_CC_EcRPA_Analytic (src/rpa/rpa_CC.f90:412-471)
+  ec_rpa          rpa_THC_PiU + rpa_CC_EcRPA_Analytic as chained in
+                  rpa_THC_MBPT3 (src/rpa/rpa_THC.f90:106-108)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "librpa_b200.so"
+HEADER = HERE.parent / "include" / "rpa_b200.h"
+
+RPA_OK = 0
+RPA_ERR_INVALID_ARG = 1
+RPA_ERR_NOT_SPD = 2
+RPA_ERR_NONFINITE = 3
+RPA_ERR_OOM = 4
+RPA_ERR_CUDA = 5
+RPA_ERR_TIMEOUT = 6
+RPA_ERR_NO_DEVICE = 7
+RPA_ERR_NOT_CONVERGED = 8
+
+PREC_FP64 = 0
+PREC_SPLIT_BF16 = 1
+_PREC = {"fp64": PREC_FP64, "split": PREC_SPLIT_BF16, "split_bf16": PREC_SPLIT_BF16,
+         PREC_FP64: PREC_FP64, PREC_SPLIT_BF16: PREC_SPLIT_BF16}
+
+_i64 = ctypes.c_int64
+_dbl = ctypes.c_double
+_vp = ctypes.c_void_p
+_lib = None
+
+
+class RPAError(RuntimeError):
+    def __init__(self, status: int, detail: str = ""):
+        self.status = status
+        msg = _status_string(status)
+        super().__init__(f"{msg} (status {status})" + (f": {detail}" if detail else ""))
+
+
+def _status_string(status: int) -> str:
+    lib = load_library()
+    return lib.rpa_b200_status_string(int(status)).decode()
+
+
+def load_library(path: str | os.PathLike | None = None):
+    """Load librpa_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f"{p} is missing: run `python beyond-rpa_b200/build.py` first")
+    lib = ctypes.CDLL(str(p))
+    lib.rpa_b200_create.argtypes = [ctypes.POINTER(_vp), _i64, _i64]
+    lib.rpa_b200_destroy.argtypes = [_vp]
+    lib.rpa_b200_status_string.argtypes = [ctypes.c_int]
+    lib.rpa_b200_status_string.restype = ctypes.c_char_p
+    lib.rpa_b200_last_error.argtypes = [_vp]
+    lib.rpa_b200_last_error.restype = ctypes.c_char_p
+    lib.rpa_b200_last_timings.argtypes = [_vp, _vp, _i64]
+    lib.rpa_b200_last_launches.argtypes = [_vp]
+    lib.rpa_b200_last_launches.restype = _i64
+    lib.rpa_b200_set_stream.argtypes = [_vp, _vp]
+    lib.rpa_b200_pi.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _dbl, _i64, _vp, _i64]
+    lib.rpa_b200_ec_from_pi.argtypes = [_vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp]
+    lib.rpa_b200_ec.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _dbl, _i64, _vp, _vp]
+    lib.rpa_b200_freq_grid.argtypes = [_i64, _i64, _vp, _dbl, _dbl, _dbl, _i64, _vp, _vp, _vp]
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def freq_grid(orb_energies, nocc, nvirt, nfixed=0, core_thresh=-3.0, target_error=1e-6, target_rel_error=1e-3):
+    """Frequency points and weights (rpa_b200_freq_grid; host code, no GPU needed)."""
+    lib = load_library()
+    e = np.ascontiguousarray(orb_energies, dtype=np.float64)
+    if e.size != nocc + nvirt:
+        raise ValueError("orb_energies must hold NOcc + NVirt values")
+    x = np.zeros(64)
+    w = np.zeros(64)
+    n = ctypes.c_int64()
+    st = lib.rpa_b200_freq_grid(int(nocc), int(nvirt), e.ctypes.data, float(core_thresh), float(target_error),
+                                float(target_rel_error), int(nfixed), x.ctypes.data, w.ctypes.data,
+                                ctypes.byref(n))
+    if st != RPA_OK:
+        raise RPAError(st, "rpa_b200_freq_grid")
+    return x[: n.value].copy(), w[: n.value].copy()
+
+
+def declared_functions() -> list[str]:
+    """Function names declared by include/rpa_b200.h."""
+    import re
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(rpa_b200_\w+)\s*\(", text, re.M)))
+
+
+# ----------------------------------------------------------------------------- marshalling
+
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
+class _Arg:
+    """Pointer + leading dimension of an array argument (keeps the owner alive)."""
+
+    def __init__(self, ptr, ld=None, owner=None):
+        self.ptr, self.ld, self.owner = ptr, ld, owner
+
+
+def _vec(x):
+    if _is_torch(x):
+        if str(x.dtype) != "torch.float64" or not x.is_contiguous():
+            raise ValueError("vector arguments must be contiguous float64")
+        return _Arg(x.data_ptr(), owner=x)
+    a = np.ascontiguousarray(x, dtype=np.float64)
+    return _Arg(a.ctypes.data, owner=a)
+
+
+def _colmajor(x, nrows):
+    """(nrows x ncols) column-major view: returns pointer and leading dimension."""
+    if _is_torch(x):
+        import torch
+        if x.dtype != torch.float64 or x.dim() != 2 or x.shape[0] != nrows:
+            raise ValueError("expected a float64 (NQ, nov) tensor")
+        if x.stride(0) != 1:
+            raise ValueError("R must be column-major: stride(0) == 1 (use R_t.T of a contiguous (nov, NQ) tensor)")
+        return _Arg(x.data_ptr(), ld=max(x.stride(1), nrows), owner=x)
+    a = np.asarray(x, dtype=np.float64)
+    if a.ndim != 2 or a.shape[0] != nrows:
+        raise ValueError("expected an (NQ, nov) array")
+    if not a.flags.f_contiguous:
+        a = np.asfortranarray(a)
+    return _Arg(a.ctypes.data, ld=nrows, owner=a)
+
+
+class Handle:
+    """A librpa_b200 handle bound to one GPU (rpa_b200_create / rpa_b200_destroy)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        h = _vp()
+        st = self.lib.rpa_b200_create(ctypes.byref(h), int(device), 0)
+        if st != RPA_OK:
+            raise RPAError(st, "rpa_b200_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.rpa_b200_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != RPA_OK:
+            raise RPAError(st, self.lib.rpa_b200_last_error(self._h).decode())
+
+    def timings(self):
+        """Phase times (ms) of the last call, CUDA events on the call's stream."""
+        out = (ctypes.c_double * 6)()
+        self._check(self.lib.rpa_b200_last_timings(self._h, ctypes.cast(out, _vp), 6))
+        return {"staging_ms": out[0], "pi_ms": out[1], "logdet_ms": out[2], "other_ms": out[3],
+                "contraction_ms": out[4], "split_ms": out[5]}
+
+    def launches(self):
+        """Kernels launched by the library during the last call."""
+        return int(self.lib.rpa_b200_last_launches(self._h))
+
+    def set_stream(self, stream=None):
+        """Run calls on a cudaStream_t (e.g. torch.cuda.current_stream().cuda_stream)."""
+        self._check(self.lib.rpa_b200_set_stream(self._h, stream))
+
+    # ------------------------------------------------------------------ Pi(u)
+    def pi_u(self, R, eps_o, eps_v, freqs, alpha=4.0, prec="split", out=None):
+        """PiU(:,:,u) for every frequency; returns (K, NQ, NQ) (numpy unless `out` is given)."""
+        nq = int(R.shape[0])
+        no, nv, K = len(eps_o), len(eps_v), len(freqs)
+        r = _colmajor(R, nq)
+        eo, ev, fr = _vec(eps_o), _vec(eps_v), _vec(freqs)
+        if out is None:
+            out = np.empty((K, nq, nq), dtype=np.float64)
+        optr = out.data_ptr() if _is_torch(out) else out.ctypes.data
+        self._check(self.lib.rpa_b200_pi(self._h, nq, no, nv, r.ptr, r.ld, eo.ptr, ev.ptr, K, fr.ptr,
+                                         float(alpha), _PREC[prec], optr, nq))
+        return out
+
+    # ------------------------------------------------------------------ energies
+    def ec_from_pi(self, pi, weights):
+        """E_c and E(u) from (K, NQ, NQ) Pi(u) matrices (lower triangles read)."""
+        K, nq = int(pi.shape[0]), int(pi.shape[1])
+        if _is_torch(pi):
+            p = _Arg(pi.contiguous().data_ptr(), owner=pi.contiguous())
+        else:
+            a = np.ascontiguousarray(pi, dtype=np.float64)
+            p = _Arg(a.ctypes.data, owner=a)
+        w = _vec(weights)
+        ec = ctypes.c_double()
+        eu = np.zeros(K)
+        self._check(self.lib.rpa_b200_ec_from_pi(self._h, nq, K, p.ptr, nq, w.ptr, ctypes.byref(ec),
+                                                 eu.ctypes.data))
+        return ec.value, eu
+
+    def ec_rpa(self, R, eps_o, eps_v, freqs, weights, alpha=4.0, prec="split"):
+        """Fused Pi build + energy: returns (E_c, E(u))."""
+        nq = int(R.shape[0])
+        no, nv, K = len(eps_o), len(eps_v), len(freqs)
+        r = _colmajor(R, nq)
+        eo, ev, fr, w = _vec(eps_o), _vec(eps_v), _vec(freqs), _vec(weights)
+        ec = ctypes.c_double()
+        eu = np.zeros(K)
+        self._check(self.lib.rpa_b200_ec(self._h, nq, no, nv, r.ptr, r.ld, eo.ptr, ev.ptr, K, fr.ptr, w.ptr,
+                                         float(alpha), _PREC[prec], ctypes.byref(ec), eu.ctypes.data))
+        return ec.value, eu
+
+
+def build(force: bool = False):
+    """Compile librpa_b200.so in-tree (nvcc, sm_100a)."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("_rpa_b200_build", HERE / "build.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.build(force=force)

@@ -1,0 +1,145 @@
+// FP64 lower-triangle SYRK on the FP64 tensor-core path (mma.sync m8n8k4 f64).
+//
+// Two uses:
+//  * plain-FP64 Pi(u):  C = sum_k A(:,k) alpha c_u(k) A(:,k)^T  with
+//    c_u(k) = D(k)/(D(k)^2 + u^2) -- the FP64 form of rpa_THC_PiU_BlockAlgo
+//    (src/rpa/rpa_THC.f90:313-339), lower triangle only (the reference's
+//    full DGEMM computes both halves);
+//  * the trailing update of the blocked Cholesky (C -= P P^T).
+// A is column-major (rows contiguous), exactly the Cholesky-vector layout
+// R(Q, ai) and the panel layout of a column-major lower Cholesky factor.
+// CTA tile 64 x 64, 4 warps in 2 x 2, warp tile 32 x 32 (4 x 4 DMMA tiles),
+// 16-deep K chunks double-buffered through shared memory.
+#include "kernels.h"
+
+namespace rpa {
+
+namespace {
+constexpr int BM = 64;
+constexpr int BK = 16;
+constexpr int LDS = BM + 8;  // 72 doubles: fragment loads hit each bank pair twice (optimal)
+constexpr int kThreads = 128;
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void tri_decode(int b, int& tm, int& tn) {
+  int t = (int)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
+  while ((t + 1) * (t + 2) / 2 <= b) ++t;
+  while (t * (t + 1) / 2 > b) --t;
+  tm = t;
+  tn = b - t * (t + 1) / 2;
+}
+
+template <bool kScaled>
+__global__ void __launch_bounds__(kThreads) dsyrk_lower_kernel(const DsyrkArgs a) {
+  __shared__ double As[2][BK][LDS];
+  __shared__ double Bs[2][BK][LDS];
+  __shared__ double sS[2][BK];
+
+  int tm, tn;
+  tri_decode(blockIdx.x, tm, tn);
+  const int z = blockIdx.y;
+  const double* A = a.A + (int64_t)z * a.strideA;
+  double* C = a.C + (int64_t)z * a.strideC;
+  const int m0 = tm * BM, n0 = tn * BM;
+  const int t = threadIdx.x;
+  const int lane = t & 31, warp = t >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  const double u2 = kScaled ? a.u2[z] : 0.0;
+
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+  double ra[8], rb[8];
+  auto gload = [&](int64_t k0) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int idx = t + kThreads * i;
+      const int col = idx / BM, row = idx % BM;
+      const int64_t k = k0 + col;
+      const bool kin = k < a.kdim;
+      ra[i] = (kin && m0 + row < a.n) ? A[(int64_t)(m0 + row) + a.lda * k] : 0.0;
+      rb[i] = (kin && n0 + row < a.n) ? A[(int64_t)(n0 + row) + a.lda * k] : 0.0;
+    }
+  };
+  auto sstore = [&](int buf, int64_t k0) {
+    if (kScaled && t < BK) {
+      const int64_t k = k0 + t;
+      double s = 0.0;
+      if (k < a.kdim) {
+        const double d = a.D[k];
+        s = a.alpha * d / (d * d + u2);
+      }
+      sS[buf][t] = s;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int idx = t + kThreads * i;
+      const int col = idx / BM, row = idx % BM;
+      As[buf][col][row] = ra[i];
+      Bs[buf][col][row] = rb[i];
+    }
+  };
+
+  const int64_t nch = (a.kdim + BK - 1) / BK;
+  gload(0);
+  sstore(0, 0);
+  __syncthreads();
+  for (int64_t c = 0; c < nch; ++c) {
+    const int buf = (int)(c & 1);
+    if (c + 1 < nch) gload((c + 1) * BK);
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 4) {
+      const int kr = kk + (lane & 3);
+      double af[4], bf[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) af[i] = As[buf][kr][wm * 32 + i * 8 + (lane >> 2)];
+      const double s = kScaled ? sS[buf][kr] : 1.0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bf[j] = Bs[buf][kr][wn * 32 + j * 8 + (lane >> 2)] * s;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+    }
+    if (c + 1 < nch) sstore(buf ^ 1, (c + 1) * BK);
+    __syncthreads();
+  }
+
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int row = m0 + wm * 32 + i * 8 + (lane >> 2);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+#pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        const int col = n0 + wn * 32 + j * 8 + 2 * (lane & 3) + v;
+        if (row < a.n && col < a.n && row >= col) {
+          double* p = C + (int64_t)row + a.ldc * (int64_t)col;
+          if (kScaled) *p = acc[i][j][v];
+          else *p -= acc[i][j][v];
+        }
+      }
+    }
+  }
+}
+}  // namespace
+
+cudaError_t launch_dsyrk_lower(const DsyrkArgs& a, cudaStream_t stream) {
+  if (a.n <= 0 || a.batch <= 0) return cudaSuccess;
+  const int T = (a.n + BM - 1) / BM;
+  dim3 grid((unsigned)(T * (T + 1) / 2), (unsigned)a.batch);
+  if (a.D) dsyrk_lower_kernel<true><<<grid, kThreads, 0, stream>>>(a);
+  else dsyrk_lower_kernel<false><<<grid, kThreads, 0, stream>>>(a);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+}  // namespace rpa

@@ -1,0 +1,189 @@
+// Imaginary-frequency quadrature for the RPA energy (host code).
+//
+// Transformed ("Casimir-Polder") Gauss-Legendre grid on (0, inf):
+//   u_k = a (1 + t_k)/(1 - t_k),  w_k = 2 a w_GL,k / (1 - t_k)^2,
+// with the scale a chosen by a scan over [0.1, 15] (15000 points) minimising
+// the RMSD of sum_k w_k/(D^2+u_k^2) against pi/(2D) over a 100-bin histogram
+// of the orbital-energy differences D, and n the smallest point count in
+// [8, 64] meeting the RMSD and max-relative-error targets.  Restates
+// rpa_OptimizeFreqQuad / rpa_OptQuadScaling / rpa_FreqQuadError
+// (src/rpa/OptFreqQuad.f90:12-169), quad_CasimirPolder
+// (src/rpa/quadratures.f90:570-643) and rpa_DaiHistogram / rpa_NCore
+// (src/rpa/OrbDiffHist.f90:42-146).  The Gauss-Legendre nodes come from a
+// Newton iteration on theta = arccos(t) with the three-term Legendre
+// recurrence (as quad_GaussLegendre, quadratures.f90:418-509, does).
+#include <cmath>
+#include <vector>
+
+#include "../../include/rpa_b200.h"
+
+namespace {
+
+const double kPiG = 3.14159265358979323846;
+
+void legendre(int n, double x, double& pn, double& pn1) {
+  double pb = 0.0, pa = 1.0;
+  for (int a = 1; a <= n; ++a) {
+    const double pc = pb;
+    pb = pa;
+    pa = (2.0 * a - 1.0) / a * x * pb - (a - 1.0) / a * pc;
+  }
+  pn = pa;
+  pn1 = pb;
+}
+
+// All n nodes (ascending) and weights of Gauss-Legendre on (-1, 1).
+bool gauss_legendre(int n, std::vector<double>& x, std::vector<double>& w) {
+  x.assign(n, 0.0);
+  w.assign(n, 0.0);
+  bool ok = true;
+  for (int k = 1; k <= n; ++k) {
+    double th = kPiG * (k - 0.25) / (n + 0.5);
+    bool conv = false;
+    for (int it = 0; it < 100; ++it) {
+      const double c = std::cos(th);
+      double pn, pn1;
+      legendre(n, c, pn, pn1);
+      const double dth = n * (c * pn - pn1) / std::sin(th);
+      const double nt = th - pn / dth;
+      const bool done = std::fabs(nt - th) < 1.0e-14;
+      th = nt;
+      if (done) {
+        conv = true;
+        break;
+      }
+    }
+    ok = ok && conv;
+    const double c = std::cos(th);
+    double pn, pn1;
+    legendre(n, c, pn, pn1);
+    const double dth = n * (c * pn - pn1) / std::sin(th);
+    x[n - k] = c;  // cos is decreasing in theta: store ascending
+    w[n - k] = 2.0 / (dth * dth);
+  }
+  return ok;
+}
+
+struct Hist {
+  std::vector<double> d, wt;
+};
+
+bool histogram(const double* e, int64_t nocc, int64_t nvirt, double core_thresh, int nbins, Hist& h) {
+  int64_t nc = 0;
+  for (int64_t k = 0; k < nocc; ++k) {
+    if (e[k] < core_thresh) ++nc;
+    else break;
+  }
+  if (nc >= nocc) return false;
+  const int64_t i0 = nc, i1 = nocc - 1, a0 = nocc, a1 = nocc + nvirt - 1;
+  const double dmin = e[a0] - e[i1];
+  const double dmax = e[a1] - e[i0];
+  if (!(dmin > 0.0)) return false;
+  const double width = (dmax - dmin) / nbins;
+  h.d.resize(nbins);
+  h.wt.assign(nbins, 0.0);
+  for (int k = 0; k < nbins; ++k) h.d[k] = dmin + k * width;
+  std::vector<int64_t> cnt(nbins, 0);
+  int64_t total = 0;
+  for (int64_t i = i0; i <= i1; ++i)
+    for (int64_t a = a0; a <= a1; ++a) {
+      const double d = e[a] - e[i];
+      const double x = (d - (dmin + width / 2.0)) / width;
+      int64_t k = 1 + (int64_t)(x >= 0 ? std::floor(x + 0.5) : -std::floor(-x + 0.5));  // Fortran nint
+      if (k < 1) k = 1;
+      if (k > nbins) k = nbins;
+      ++cnt[k - 1];
+      ++total;
+    }
+  for (int k = 0; k < nbins; ++k) h.wt[k] = std::fabs((double)cnt[k] / (double)total);
+  return true;
+}
+
+void quad_error(const std::vector<double>& u, const std::vector<double>& w, const Hist& h, double& rel,
+                double& rmsd) {
+  rel = 0.0;
+  double err2 = 0.0;
+  for (size_t l = 0; l < h.d.size(); ++l) {
+    if (!(h.wt[l] > 0.0)) continue;
+    const double d = h.d[l];
+    const double exact = kPiG / (2.0 * d);
+    double approx = 0.0;
+    for (size_t k = 0; k < u.size(); ++k) approx += w[k] / (d * d + u[k] * u[k]);
+    rel = std::fmax(rel, std::fabs((approx - exact) / exact));
+    err2 += h.wt[l] * (approx - exact) * (approx - exact);
+  }
+  rmsd = std::sqrt(err2);
+}
+
+bool opt_scaling(int n, const Hist& h, std::vector<double>& u, std::vector<double>& w, double& rel, double& rmsd) {
+  std::vector<double> t, wgl;
+  if (!gauss_legendre(n, t, wgl)) return false;
+  std::vector<double> u0(n), w0(n);
+  for (int k = 0; k < n; ++k) {
+    u0[k] = (1.0 + t[k]) / (1.0 - t[k]);
+    w0[k] = 2.0 * wgl[k] / ((1.0 - t[k]) * (1.0 - t[k]));
+  }
+  const double amin = 0.1, amax = 15.0;
+  const int nscan = 15000;
+  double best = HUGE_VAL, best_rel = 0.0, best_a = 0.0;
+  std::vector<double> uu(n), ww(n);
+  for (int k = 0; k < nscan; ++k) {
+    const double a = amin + (amax - amin) * (double)k / (double)(nscan - 1);
+    for (int j = 0; j < n; ++j) {
+      uu[j] = a * u0[j];
+      ww[j] = a * w0[j];
+    }
+    double r, e;
+    quad_error(uu, ww, h, r, e);
+    if (e < best) {
+      best = e;
+      best_rel = r;
+      best_a = a;
+    }
+  }
+  u.resize(n);
+  w.resize(n);
+  for (int j = 0; j < n; ++j) {
+    u[j] = best_a * u0[j];
+    w[j] = best_a * w0[j];
+  }
+  rel = best_rel;
+  rmsd = best;
+  return true;
+}
+
+}  // namespace
+
+extern "C" int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* OrbEnergies, double CoreOrbThresh,
+                                  double TargetError, double TargetRelError, int64_t NFixed, double* Freqs,
+                                  double* FreqWeights, int64_t* NFreqs) {
+  if (NOcc < 1 || NVirt < 1 || !OrbEnergies || !Freqs || !FreqWeights || !NFreqs) return RPA_ERR_INVALID_ARG;
+  if (NFixed < 0 || NFixed > 64) return RPA_ERR_INVALID_ARG;
+  for (int64_t k = 0; k < NOcc + NVirt; ++k)
+    if (!std::isfinite(OrbEnergies[k])) return RPA_ERR_NONFINITE;
+  Hist h;
+  if (!histogram(OrbEnergies, NOcc, NVirt, CoreOrbThresh, 100, h)) return RPA_ERR_INVALID_ARG;
+  std::vector<double> u, w;
+  double rel = 0.0, rmsd = 0.0;
+  int n = 0;
+  if (NFixed > 0) {
+    n = (int)NFixed;
+    if (!opt_scaling(n, h, u, w, rel, rmsd)) return RPA_ERR_NOT_CONVERGED;
+  } else {
+    bool conv = false;
+    for (n = 8; n <= 64; ++n) {
+      if (!opt_scaling(n, h, u, w, rel, rmsd)) return RPA_ERR_NOT_CONVERGED;
+      if (rmsd < TargetError && rel < TargetRelError) {
+        conv = true;
+        break;
+      }
+    }
+    if (!conv) return RPA_ERR_NOT_CONVERGED;
+  }
+  for (int k = 0; k < n; ++k) {
+    Freqs[k] = u[k];
+    FreqWeights[k] = w[k];
+  }
+  *NFreqs = n;
+  return RPA_OK;
+}

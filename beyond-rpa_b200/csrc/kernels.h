@@ -1,0 +1,105 @@
+// Internal launch interface between the C-ABI host layer (capi.cu) and the
+// sm_100a kernels.  Not installed; the public ABI is include/rpa_b200.h.
+#pragma once
+#include <cstdint>
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+
+#include "rpa_common.cuh"
+
+namespace rpa {
+
+// Kernel launches issued by this host thread (read and reset by the C-ABI layer).
+extern thread_local int64_t g_launches;
+
+// Frequencies handled by one scale/split launch (register-resident diagonal sums).
+constexpr int kMaxKgLaunch = 16;
+
+struct FreqGroup {
+  int n;                       // number of frequencies in this launch
+  double u2[kMaxKgLaunch];     // u_k^2
+};
+
+struct SplitPlan {
+  int qtiles = 0;
+  int nsplit = 0;
+  int64_t ai_per_split = 0;
+};
+
+SplitPlan plan_scale_split(int NQ, int64_t nov, int num_sms);
+
+// X_k = sqrt(alpha c_k) R split into bf16 hi/lo rows (Q-major rows, ai
+// contiguous, row pitch `pitch`, frequency stride `kstride` elements), plus
+// the exact FP64 diagonal diag[k*NQ + Q] = sum_ai X_k(Q,ai)^2.
+cudaError_t launch_scale_split(const double* R, int64_t ldR, int NQ, int64_t nov, const double* D,
+                               const FreqGroup& fg, double alpha, __nv_bfloat16* Xhi, __nv_bfloat16* Xlo,
+                               int64_t pitch, int64_t kstride, double* diag_part, double* diag,
+                               const SplitPlan& plan, cudaStream_t stream);
+
+// ---------------------------------------------------------------- tcgen05 SYRK
+struct SyrkTcArgs {
+  int NQ;
+  int64_t nov;
+  int kg;            // frequencies in this launch
+  double* Pi;        // output, lower triangle of Pi_k written (incl. diagonal)
+  int64_t ldPi;
+  int64_t piStride;  // elements between consecutive Pi_k
+  const double* diag;  // exact diagonal [kg][NQ]
+  int* err;
+};
+// Tensor maps: 3-D (ai, Q, k) bf16 views of X_hi / X_lo; A maps use a
+// 128-row box, B maps a 256-row box, 32 ai per box, 64-byte swizzle.
+cudaError_t launch_syrk_split_bf16(const CUtensorMap* tmA_hi, const CUtensorMap* tmA_lo, const CUtensorMap* tmB_hi,
+                                   const CUtensorMap* tmB_lo, const SyrkTcArgs& a, int num_sms,
+                                   cudaStream_t stream);
+constexpr int kSyrkTcTM = 128;
+constexpr int kSyrkTcTN = 256;
+constexpr int kSyrkTcTK = 32;
+
+// ---------------------------------------------------------------- FP64 (DMMA)
+// C(lower) = alpha_scale * sum_k A(m,k) s(k) A(n,k) over k < kdim, or
+// C(lower) -= sum_k A(m,k) A(n,k) (subtract mode).  A is column-major with
+// leading dimension lda (rows contiguous).  Batched over `batch` matrices:
+// A + z*strideA, C + z*strideC, and for scaled mode frequency z uses
+// s(k) = alpha * D(k) / (D(k)^2 + u2[z]).
+struct DsyrkArgs {
+  const double* A;
+  int64_t lda;
+  int64_t strideA;
+  double* C;
+  int64_t ldc;
+  int64_t strideC;
+  int n;          // order of C
+  int64_t kdim;   // contraction length
+  int batch;
+  // scaled mode
+  const double* D;  // nullptr -> subtract mode
+  double alpha;
+  double u2[64];
+};
+cudaError_t launch_dsyrk_lower(const DsyrkArgs& a, cudaStream_t stream);
+
+// ---------------------------------------------------------------- log-det
+// Batched lower Cholesky of nmat matrices (column-major, ld, stride),
+// on entry A = 1 + Pi (lower triangle), on exit L; Ldiag[z*n + i] = L_ii.
+cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag, int* err,
+                                  cudaStream_t stream);
+// tr[z] = sum_i A_z(i,i) (double-double, deterministic); then A_z(i,i) += 1.
+// If `diag` is non-null the diagonal is first overwritten with diag[z*n+i].
+cudaError_t launch_trace_shift(double* A, int64_t ld, int64_t stride, int n, int nmat, const double* diag,
+                               double* tr_dd, cudaStream_t stream);
+// logdet[z] = 2 sum_i log(Ldiag[z*n+i]) in double-double.
+cudaError_t launch_logdet_sum(const double* Ldiag, int n, int nmat, double* logdet_dd, cudaStream_t stream);
+// D(ai) = eps_v(a) - eps_o(i), ai = a + nv*i.
+cudaError_t launch_dai(const double* eps_o, const double* eps_v, int64_t no, int64_t nv, double* D,
+                       cudaStream_t stream);
+// Copy lower triangle to upper (full symmetric square) for nmat matrices.
+cudaError_t launch_symmetrize(double* A, int64_t ld, int64_t stride, int n, int nmat, cudaStream_t stream);
+// Count non-finite entries of a device array (result accumulated into *count).
+cudaError_t launch_count_nonfinite(const double* x, int64_t n, int* count, cudaStream_t stream);
+// Strided 2-D copy of a column-major matrix block (device to device).
+cudaError_t launch_copy_lower(const double* src, int64_t lds, int64_t strideS, double* dst, int64_t ldd,
+                              int64_t strideD, int n, int nmat, cudaStream_t stream);
+
+}  // namespace rpa

@@ -1,0 +1,251 @@
+// FP64 log-det of 1 + Pi(u) by a batched, blocked, right-looking lower
+// Cholesky, and the double-double trace / log sums of the energy.
+//
+// The reference takes ln|det(1+Pi)| from the diagonal of a Householder QR
+// (real_LogDet, src/linear-algebra/real_linalg.f90:793-825, DGEQRF) and sums
+// log|R_kk| and Tr Pi in REAL(16) (rpa_CC_EcRPA_Analytic,
+// src/rpa/rpa_CC.f90:440-453).  1 + Pi is symmetric positive definite
+// (Pi = R diag(alpha c) R^T with c > 0), so ln det = 2 sum ln L_kk of its
+// Cholesky factor equals the QR value; the sums here are double-double.
+// A non-positive pivot is reported as an error, never as a NaN energy.
+#include "kernels.h"
+
+namespace rpa {
+
+namespace {
+constexpr int NB = 64;  // Cholesky block size
+
+// Factor the NB x NB diagonal block of each matrix in shared memory.
+__global__ void __launch_bounds__(256) potrf_diag_kernel(double* A, int64_t ld, int64_t stride, int n, int j0,
+                                                         double* Ldiag, int* err) {
+  __shared__ double L[NB][NB + 1];
+  const int z = blockIdx.x;
+  double* Az = A + (int64_t)z * stride;
+  const int nbe = min(NB, n - j0);
+  const int t = threadIdx.x;
+  for (int idx = t; idx < NB * NB; idx += blockDim.x) {
+    const int r = idx % NB, c = idx / NB;
+    L[r][c] = (r >= c && r < nbe && c < nbe) ? Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] : 0.0;
+  }
+  __syncthreads();
+  for (int j = 0; j < nbe; ++j) {
+    if (t == 0) {
+      double d = L[j][j];
+      if (!(d > 0.0)) {  // also catches NaN
+        atomicCAS(err, 0, (int)kDevNotSPD);
+        d = 1.0;
+      }
+      L[j][j] = sqrt(d);
+    }
+    __syncthreads();
+    const double inv = 1.0 / L[j][j];
+    for (int r = j + 1 + t; r < nbe; r += blockDim.x) L[r][j] *= inv;
+    __syncthreads();
+    const int m = nbe - j - 1;
+    for (int idx = t; idx < m * m; idx += blockDim.x) {
+      const int r = j + 1 + idx % m, c = j + 1 + idx / m;
+      if (r >= c) L[r][c] -= L[r][j] * L[c][j];
+    }
+    __syncthreads();
+  }
+  for (int idx = t; idx < NB * NB; idx += blockDim.x) {
+    const int r = idx % NB, c = idx / NB;
+    if (r >= c && r < nbe && c < nbe) Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] = L[r][c];
+  }
+  for (int j = t; j < nbe; j += blockDim.x) Ldiag[(int64_t)z * n + j0 + j] = L[j][j];
+}
+
+// Panel solve: rows below the diagonal block, X L_jj^T = A_panel.
+__global__ void __launch_bounds__(128) trsm_panel_kernel(double* A, int64_t ld, int64_t stride, int n, int j0) {
+  __shared__ double Ls[NB][NB + 1];
+  __shared__ double inv[NB];
+  const int z = blockIdx.y;
+  double* Az = A + (int64_t)z * stride;
+  const int t = threadIdx.x;
+  for (int idx = t; idx < NB * NB; idx += blockDim.x) {
+    const int r = idx % NB, c = idx / NB;
+    Ls[r][c] = (r >= c) ? Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] : 0.0;
+  }
+  __syncthreads();
+  if (t < NB) inv[t] = 1.0 / Ls[t][t];
+  __syncthreads();
+  const int r = j0 + NB + blockIdx.x * blockDim.x + t;
+  if (r >= n) return;
+  double x[NB];
+#pragma unroll
+  for (int c = 0; c < NB; ++c) x[c] = Az[(int64_t)r + ld * (int64_t)(j0 + c)];
+#pragma unroll
+  for (int c = 0; c < NB; ++c) {
+    double s = x[c];
+#pragma unroll
+    for (int m = 0; m < c; ++m) s -= x[m] * Ls[c][m];
+    x[c] = s * inv[c];
+  }
+#pragma unroll
+  for (int c = 0; c < NB; ++c) Az[(int64_t)r + ld * (int64_t)(j0 + c)] = x[c];
+}
+
+// Deterministic block reduction of double-double values (blockDim = 256).
+__device__ dd block_reduce_dd(dd v) {
+  __shared__ double sh[256], sl[256];
+  sh[threadIdx.x] = v.hi;
+  sl[threadIdx.x] = v.lo;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      dd o = dd_add_dd({sh[threadIdx.x], sl[threadIdx.x]}, {sh[threadIdx.x + s], sl[threadIdx.x + s]});
+      sh[threadIdx.x] = o.hi;
+      sl[threadIdx.x] = o.lo;
+    }
+    __syncthreads();
+  }
+  return {sh[0], sl[0]};
+}
+
+__global__ void __launch_bounds__(256) trace_shift_kernel(double* A, int64_t ld, int64_t stride, int n,
+                                                          const double* diag, double* tr_dd) {
+  const int z = blockIdx.x;
+  double* Az = A + (int64_t)z * stride;
+  dd acc{0.0, 0.0};
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double* p = Az + (int64_t)i * (ld + 1);
+    double v = diag ? diag[(int64_t)z * n + i] : *p;
+    acc = dd_add(acc, v);
+    *p = v + 1.0;
+  }
+  dd r = block_reduce_dd(acc);
+  if (threadIdx.x == 0) {
+    tr_dd[2 * z] = r.hi;
+    tr_dd[2 * z + 1] = r.lo;
+  }
+}
+
+__global__ void __launch_bounds__(256) logdet_sum_kernel(const double* Ldiag, int n, double* out_dd) {
+  const int z = blockIdx.x;
+  dd acc{0.0, 0.0};
+  for (int i = threadIdx.x; i < n; i += blockDim.x) acc = dd_add(acc, 2.0 * log(Ldiag[(int64_t)z * n + i]));
+  dd r = block_reduce_dd(acc);
+  if (threadIdx.x == 0) {
+    out_dd[2 * z] = r.hi;
+    out_dd[2 * z + 1] = r.lo;
+  }
+}
+
+__global__ void dai_kernel(const double* eps_o, const double* eps_v, int64_t no, int64_t nv, double* D) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= no * nv) return;
+  const int64_t i = idx / nv, a = idx - i * nv;
+  D[idx] = eps_v[a] - eps_o[i];
+}
+
+__global__ void symmetrize_kernel(double* A, int64_t ld, int64_t stride, int n) {
+  __shared__ double tile[32][33];
+  const int z = blockIdx.z;
+  double* Az = A + (int64_t)z * stride;
+  const int bx = blockIdx.x, by = blockIdx.y;  // destination tile: rows by*32, cols bx*32 (upper: rows < cols)
+  if (by > bx) return;
+  // read source tile (rows bx*32.., cols by*32..) which lies in the lower triangle
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int r = bx * 32 + threadIdx.x, c = by * 32 + j;
+    tile[j][threadIdx.x] = (r < n && c < n) ? Az[(int64_t)r + ld * c] : 0.0;
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int r = by * 32 + threadIdx.x, c = bx * 32 + j;  // destination (r, c) = source (c, r)
+    if (r < n && c < n && r < c) Az[(int64_t)r + ld * c] = tile[threadIdx.x][j];
+  }
+}
+
+__global__ void count_nonfinite_kernel(const double* x, int64_t n, int* count) {
+  int local = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (!isfinite(x[i])) ++local;
+  if (local) atomicAdd(count, local);
+}
+
+__global__ void copy_lower_kernel(const double* src, int64_t lds, int64_t strideS, double* dst, int64_t ldd,
+                                  int64_t strideD, int n) {
+  const int z = blockIdx.z;
+  const int c = blockIdx.y;
+  const double* s = src + (int64_t)z * strideS + lds * c;
+  double* d = dst + (int64_t)z * strideD + ldd * c;
+  for (int r = c + blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) d[r] = s[r];
+}
+}  // namespace
+
+cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag, int* err,
+                                  cudaStream_t stream) {
+  for (int j0 = 0; j0 < n; j0 += NB) {
+    potrf_diag_kernel<<<nmat, 256, 0, stream>>>(A, ld, stride, n, j0, Ldiag, err);
+    ++g_launches;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int below = n - j0 - NB;
+    if (below <= 0) break;
+    trsm_panel_kernel<<<dim3((below + 127) / 128, nmat), 128, 0, stream>>>(A, ld, stride, n, j0);
+    ++g_launches;
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    DsyrkArgs u{};
+    u.A = A + (int64_t)(j0 + NB) + ld * (int64_t)j0;
+    u.lda = ld;
+    u.strideA = stride;
+    u.C = A + (int64_t)(j0 + NB) + ld * (int64_t)(j0 + NB);
+    u.ldc = ld;
+    u.strideC = stride;
+    u.n = below;
+    u.kdim = NB;
+    u.batch = nmat;
+    u.D = nullptr;
+    e = launch_dsyrk_lower(u, stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_trace_shift(double* A, int64_t ld, int64_t stride, int n, int nmat, const double* diag,
+                               double* tr_dd, cudaStream_t stream) {
+  trace_shift_kernel<<<nmat, 256, 0, stream>>>(A, ld, stride, n, diag, tr_dd);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_logdet_sum(const double* Ldiag, int n, int nmat, double* logdet_dd, cudaStream_t stream) {
+  logdet_sum_kernel<<<nmat, 256, 0, stream>>>(Ldiag, n, logdet_dd);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dai(const double* eps_o, const double* eps_v, int64_t no, int64_t nv, double* D,
+                       cudaStream_t stream) {
+  const int64_t n = no * nv;
+  if (n == 0) return cudaSuccess;
+  dai_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(eps_o, eps_v, no, nv, D);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_symmetrize(double* A, int64_t ld, int64_t stride, int n, int nmat, cudaStream_t stream) {
+  const int T = (n + 31) / 32;
+  symmetrize_kernel<<<dim3(T, T, nmat), dim3(32, 8), 0, stream>>>(A, ld, stride, n);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_count_nonfinite(const double* x, int64_t n, int* count, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  int64_t blocks = (n + 255) / 256;
+  if (blocks > 4096) blocks = 4096;
+  count_nonfinite_kernel<<<(unsigned)blocks, 256, 0, stream>>>(x, n, count);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_copy_lower(const double* src, int64_t lds, int64_t strideS, double* dst, int64_t ldd,
+                              int64_t strideD, int n, int nmat, cudaStream_t stream) {
+  copy_lower_kernel<<<dim3((n + 255) / 256, n, nmat), 256, 0, stream>>>(src, lds, strideS, dst, ldd, strideD, n);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+}  // namespace rpa

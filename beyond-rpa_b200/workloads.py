@@ -1,0 +1,82 @@
+"""Seeded synthetic RPA inputs with the shapes of the measured workloads.
+
+There is no network and no SCF/Cholesky stack here, so inputs are synthetic:
+occupied energies ~ U[occ_range], virtual energies log-uniform in virt_range,
+R(Q, ai) ~ N(0,1) * scale * exp(-Q/decay), rescaled so that the largest
+eigenvalue of Pi(0) equals `lam0` (a physical coupling strength).
+R is generated on the GPU (torch) as a column-major (NQ, nov) view.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+# name -> (NQ, NOcc, NVirt, K, generator kwargs)
+SINGLE_SYSTEM = {
+    # single-system split-BF16 vs FP64 workload: N_occ=64, N_virt=1024, NQ=4096, 16 points
+    "single_4096": (4096, 64, 1024, 16, dict(occ_range=(-1.2, -0.3), virt_range=(0.02, 5.0), decay=512.0,
+                                             scale=0.05, lam0=0.8)),
+    # seeded twin of the water dimer (10 occ incl. 2 core, 72 virt, NQ = 400, 12 points)
+    "water_dimer_twin": (400, 8, 72, 12, dict(occ_range=(-1.3, -0.4), virt_range=(0.03, 4.0), decay=50.0,
+                                              scale=1.0, lam0=0.8)),
+    # adjoint workload shapes
+    "adjoint_2560": (2560, 48, 640, 16, dict(occ_range=(-1.3, -0.4), virt_range=(0.03, 4.0), decay=320.0,
+                                             scale=1.0, lam0=0.8)),
+    # beyond-RPA large case shapes
+    "large_8192": (8192, 128, 2048, 20, dict(occ_range=(-1.3, -0.4), virt_range=(0.03, 4.0), decay=1024.0,
+                                             scale=1.0, lam0=0.8)),
+}
+
+
+@dataclass
+class SyntheticSystem:
+    R: object            # torch (NQ, nov) column-major view on the device, or numpy
+    eps_o: np.ndarray
+    eps_v: np.ndarray
+    freqs: np.ndarray
+    weights: np.ndarray
+
+    @property
+    def nq(self):
+        return int(self.R.shape[0])
+
+
+def orbital_energies(no, nv, seed, occ_range, virt_range):
+    rng = np.random.default_rng(seed)
+    eo = np.sort(rng.uniform(occ_range[0], occ_range[1], no))
+    ev = np.sort(np.exp(rng.uniform(math.log(virt_range[0]), math.log(virt_range[1]), nv)))
+    return eo, ev
+
+
+def lambda_max_pi0(R, d, alpha=4.0, iters=40, seed=0):
+    """Largest eigenvalue of Pi(0) = alpha R diag(1/D) R^T (power iteration, torch)."""
+    import torch
+    g = torch.Generator(device=R.device).manual_seed(seed)
+    v = torch.randn(R.shape[0], generator=g, device=R.device, dtype=R.dtype)
+    lam = 0.0
+    for _ in range(iters):
+        w = alpha * (R @ ((R.T @ v) / d))
+        lam = float(torch.linalg.norm(w))
+        v = w / lam
+    return lam
+
+
+def make_single_system(name="single_4096", seed=0, device="cuda", K=None):
+    """Build one synthetic system on `device` with its optimised frequency grid."""
+    import torch
+    from . import freq_grid
+    nq, no, nv, k_default, kw = SINGLE_SYSTEM[name]
+    K = K or k_default
+    eo, ev = orbital_energies(no, nv, seed, kw["occ_range"], kw["virt_range"])
+    nov = no * nv
+    g = torch.Generator(device=device).manual_seed(seed + 1)
+    Rt = torch.randn((nov, nq), generator=g, device=device, dtype=torch.float64)  # (ai, Q) rows -> R = Rt.T
+    Rt *= kw["scale"] * torch.exp(-torch.arange(nq, device=device, dtype=torch.float64) / kw["decay"])[None, :]
+    R = Rt.T
+    d = torch.from_numpy((ev[:, None] - eo[None, :]).reshape(-1, order="F")).to(device)
+    lam = lambda_max_pi0(R, d)
+    Rt *= math.sqrt(kw["lam0"] / lam)
+    x, w = freq_grid(np.concatenate([eo, ev]), no, nv, nfixed=K)
+    return SyntheticSystem(R=R, eps_o=eo, eps_v=ev, freqs=x, weights=w)

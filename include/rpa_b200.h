@@ -1,0 +1,127 @@
+/*
+ * librpa_b200 -- C ABI of the B200 (sm_100a) Cholesky-vector RPA hot path.
+ *
+ * Conventions (chosen to match the Fortran reference, modrzejewski/beyond-rpa,
+ * compiled with -fdefault-integer-8 / -i8):
+ *   - every dimension and flag is int64_t (Fortran default INTEGER = 8 bytes);
+ *   - every matrix is column-major with an explicit leading dimension;
+ *   - Cholesky vectors R(Q, ai) with ai = a + NVirt*(i-1) (a fastest), i.e.
+ *     the Rkai(NCholesky, NVirt*NOcc) arrays of src/rpa/rpa_THC.f90:362 and
+ *     src/rpa/rpa_core_MO.f90:395;
+ *   - array arguments may point to host memory (pageable or pinned) or to
+ *     device memory of the handle's GPU; the library detects which
+ *     (cudaPointerGetAttributes) and stages host data itself;
+ *   - scalar outputs (energies) are host pointers;
+ *   - every call is synchronous on return and returns an rpa_status.
+ * Errors: the Fortran reference stops with `error stop` after msg(...,
+ * MSG_ERROR); this ABI returns a non-zero status instead, and the Fortran
+ * shim maps it back to msg + error stop.
+ * A handle must not be shared by two host threads at the same time.
+ */
+#ifndef RPA_B200_H
+#define RPA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum rpa_status {
+  RPA_OK = 0,
+  RPA_ERR_INVALID_ARG = 1,  /* bad dimension, NULL pointer, unsupported mode   */
+  RPA_ERR_NOT_SPD = 2,      /* 1+Pi(u) not positive definite (Cholesky pivot) */
+  RPA_ERR_NONFINITE = 3,    /* NaN/Inf in an input or result                 */
+  RPA_ERR_OOM = 4,          /* device allocation failed                       */
+  RPA_ERR_CUDA = 5,         /* CUDA runtime / driver error                    */
+  RPA_ERR_TIMEOUT = 6,      /* a bounded device-side wait expired             */
+  RPA_ERR_NO_DEVICE = 7,    /* no sm_100 GPU visible                          */
+  RPA_ERR_NOT_CONVERGED = 8 /* quadrature / eigen-solver did not converge     */
+} rpa_status;
+
+/* Precision of the Pi(u) contraction. */
+#define RPA_PREC_FP64 0      /* plain FP64 (FP64 tensor-core DMMA)                 */
+#define RPA_PREC_SPLIT_BF16 1 /* X = hi + lo (bf16), 3 tcgen05 products, FP32 acc,
+                                 exact FP64 diagonal                               */
+
+typedef struct rpa_b200_handle rpa_b200_handle;
+
+/* Create / destroy a handle bound to one GPU (`device` = CUDA ordinal).
+ * The handle owns a stream, a grow-only device workspace and the TMA
+ * descriptors.  flags: reserved, pass 0.                                    */
+int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags);
+int rpa_b200_destroy(rpa_b200_handle* handle);
+const char* rpa_b200_status_string(int status);
+/* Human-readable detail of the last failing call on this handle. */
+const char* rpa_b200_last_error(const rpa_b200_handle* handle);
+/* Time (ms, CUDA events on the handle's stream) of the last call:
+ * out[0] = staging (H2D copies, input screening), out[1] = Pi build,
+ * out[2] = log-det (Cholesky + sums), out[3] = the rest (result copies),
+ * out[4] = the Pi contraction kernel alone, out[5] = the scale/split pass. */
+int rpa_b200_last_timings(const rpa_b200_handle* handle, double* out, int64_t n);
+/* Number of kernels this library launched during the last call.           */
+int64_t rpa_b200_last_launches(const rpa_b200_handle* handle);
+/* Run subsequent calls on `stream` (a cudaStream_t of the handle's device;
+ * NULL restores the handle's own stream).  Calls still synchronise the
+ * stream before returning.                                                 */
+int rpa_b200_set_stream(rpa_b200_handle* handle, void* stream);
+
+/*
+ * Pi(u) matrices:  PiU(:,:,u) = alpha * sum_ai R(:,ai) Chi_u(ai) R(:,ai)^T,
+ * Chi_u(ai) = D(ai) / (D(ai)^2 + u^2), D(ai) = VirtEnergies(a) - OccEnergies(i).
+ * Replaces rpa_THC_PiU / rpa_THC_PiU_BlockAlgo / rpa_THC_ChiRkai
+ * (src/rpa/rpa_THC.f90:215-371) and rpa_GPiUG_MO (src/rpa/rpa_core_MO.f90:347-406).
+ * alpha = 4 closed shell, 2 per spin for open shell (rpa_THC.f90:258-268).
+ * PiU: NQ x NQ x NFreqs, leading dimension ldPi >= NQ, full symmetric square
+ * on return (as the reference's DGEMM produces).
+ */
+int rpa_b200_pi(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R, int64_t ldR,
+                const double* OccEnergies, const double* VirtEnergies, int64_t NFreqs, const double* Freqs,
+                double alpha, int64_t prec, double* PiU, int64_t ldPi);
+
+/*
+ * RPA correlation energy from given Pi(u) matrices:
+ *   Ec = 1/(2 pi) sum_u w_u [ln det(1 + Pi(u)) - Tr Pi(u)],
+ * log-det by FP64 Cholesky, traces and sums in double-double.
+ * Replaces rpa_CC_EcRPA_Analytic (src/rpa/rpa_CC.f90:412-471) with
+ * real_LogDet (src/linear-algebra/real_linalg.f90:776-825) and the energy loop
+ * of rpa_FreqIntegral_MO (src/rpa/rpa.f90:1338-1380).
+ * Only the lower triangle of each PiU(:,:,u) is read.  Eu (NFreqs, may be
+ * NULL) receives E(u) = ln det(1+Pi(u)) - Tr Pi(u).
+ */
+int rpa_b200_ec_from_pi(rpa_b200_handle* h, int64_t NQ, int64_t NFreqs, const double* PiU, int64_t ldPi,
+                        const double* FreqWeights, double* Ec, double* Eu);
+
+/*
+ * Fused Pi build + energy (Pi never leaves the GPU): the chain
+ * rpa_THC_PiU -> rpa_CC_EcRPA_Analytic of rpa_THC_MBPT3
+ * (src/rpa/rpa_THC.f90:106-108) and rpa_CC_PiU -> rpa_CC_EcRPA_Analytic of
+ * rpa_CC_Energy_2 (src/rpa/rpa_CC.f90:781-785).
+ */
+int rpa_b200_ec(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R, int64_t ldR,
+                const double* OccEnergies, const double* VirtEnergies, int64_t NFreqs, const double* Freqs,
+                const double* FreqWeights, double alpha, int64_t prec, double* Ec, double* Eu);
+
+/*
+ * Imaginary-frequency quadrature (host code, no GPU needed): transformed
+ * Gauss-Legendre points u_k = a(1+t_k)/(1-t_k), weights 2 a w_k/(1-t_k)^2,
+ * with a scanned over [0.1, 15] (15000 points) to minimise the RMSD of
+ * sum_k w_k/(D^2+u_k^2) against pi/(2D) over a 100-bin histogram of the
+ * active D(ai).  Replaces rpa_OptimizeFreqQuad / rpa_OptQuadScaling /
+ * rpa_FreqQuadError (src/rpa/OptFreqQuad.f90:12-169), quad_CasimirPolder
+ * (src/rpa/quadratures.f90:570-643), rpa_DaiHistogram and rpa_NCore
+ * (src/rpa/OrbDiffHist.f90:42-146).
+ * OrbEnergies: NOcc occupied then NVirt virtual energies, each ascending;
+ * occupied orbitals below CoreOrbThresh (reference default -3 Eh) are frozen.
+ * NFixed > 0: exactly NFixed points; NFixed = 0: the smallest n in [8, 64]
+ * with RMSD < TargetError and max relative error < TargetRelError
+ * (reference defaults 1e-6 and 1e-3).  Freqs / FreqWeights need room for 64.
+ */
+int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* OrbEnergies, double CoreOrbThresh,
+                       double TargetError, double TargetRelError, int64_t NFixed, double* Freqs,
+                       double* FreqWeights, int64_t* NFreqs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RPA_B200_H */

@@ -1,0 +1,580 @@
+"""FP64 CPU oracle for the Cholesky-vector RPA hot path.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker: it is imported by
+``tests/``, by ``__graft_entry__.smoke()`` and by the ``cpu_baseline`` /
+``--impl reference`` legs of ``bench.py``, and by nothing else.  The product
+path (``beyond-rpa_b200/``) never imports, links or executes it.
+
+It restates, in numpy/scipy (ILP64 OpenBLAS/LAPACK, the same BLAS/LAPACK
+routines the Fortran reference calls through MKL), the math of
+modrzejewski/beyond-rpa for this path.  Every function cites the reference
+file:line it follows (paths relative to the reference project root).
+
+Parity status: **parity unpinned by the reference's own tests.**  The
+reference ships no test suite, golden vectors or output logs, and it cannot
+be compiled here (Fortran 2008 + MKL + coarrays; no gfortran in the image).
+The restatement is pinned instead by the reference's built-in identities:
+  (i)   E_c(log-det of Pi) == E_c(T2 eigen-decomposition), rpa_T2_EigRPA
+        (src/rpa/rpa_CC_Doubles.f90:987-1009);
+  (ii)  the small-coupling limit R -> eps*R equals the direct-MP2 formula of
+        rpa_PT_Order2 (src/rpa/rpa_PT_Terms.f90:66) up to the frequency
+        quadrature error;
+  (iii) log-det by QR (the reference's DGEQRF) == Cholesky == sum ln(1+lambda);
+  (iv)  exactness of the frequency grid on 1/(D^2+u^2)
+        (src/rpa/OptFreqQuad.f90:125-169);
+  (v)   size consistency of many-body-expansion differences
+        (src/rpa/rpa_driver.f90:381-433).
+The checks live in tests/test_oracle.py and the fixtures in tests/golden/.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.linalg
+import scipy.linalg.lapack as lapack
+
+PI = math.pi
+# src/rpa/rpa_definitions.f90:109-110
+RPA_MIN_NFREQS = 8
+RPA_MAX_NFREQS = 64
+# src/rpa/rpa_definitions.f90:295-296,301,305,356,428,480
+TARGET_ERROR_FREQ = 1.0e-6
+TARGET_REL_ERROR_FREQ = 1.0e-3
+CORE_ORB_THRESH = -3.0
+SMALL_EIGENVAL_CUTOFF_T2 = 1.0e-10
+MAX_BATCH_DIM_T2 = 100
+GUESS_NVECS_T2 = 3.0
+T2_CUTOFF_THRESH = 1.0e-4
+# src/rpa/rpa_THC.f90:464 (THC_BlockDim)
+THC_BLOCK_DIM = 500
+# src/rpa/rpa_definitions.f90: T2 cutoff types (RPA_T2_CUTOFF_*)
+T2_CUTOFF_EIG = 0
+T2_CUTOFF_EIG_DIV_MAXEIG = 1
+T2_CUTOFF_EIG_DIV_NELECTRON = 2
+T2_CUTOFF_SUM_REJECTED = 3
+
+
+# --------------------------------------------------------------------------
+# Orbital-energy bookkeeping
+# --------------------------------------------------------------------------
+
+def ncore(orb_energies, nocc, core_thresh=CORE_ORB_THRESH):
+    """Frozen-core count. rpa_NCore, src/rpa/OrbDiffHist.f90:126-146."""
+    n = 0
+    for k in range(nocc):
+        if orb_energies[k] < core_thresh:
+            n += 1
+        else:
+            break
+    return n
+
+
+def dai(eps_o, eps_v):
+    """D(a,i) = e_a - e_i in the reference's ai = a + NVirt*(i-1) order.
+
+    rpa_CC_D, src/rpa/rpa_CC_Doubles.f90:348-366 (a is the fast index)."""
+    eps_o = np.asarray(eps_o, np.float64)
+    eps_v = np.asarray(eps_v, np.float64)
+    return (eps_v[:, None] - eps_o[None, :]).reshape(-1, order="F")
+
+
+def dai_histogram(orb_energies, nocc, nvirt, core_thresh=CORE_ORB_THRESH,
+                  dai_max_thresh=np.inf, nbins=100):
+    """Histogram of orbital-energy differences used by the grid optimiser.
+
+    rpa_DaiHistogram, src/rpa/OrbDiffHist.f90:42-123."""
+    e = np.asarray(orb_energies, np.float64)
+    nc = ncore(e, nocc, core_thresh)
+    if nc >= nocc:
+        vals = np.zeros(nbins)
+        vals[0] = np.finfo(np.float64).max
+        vals[-1] = 0.0
+        return vals, -np.ones(nbins)
+    i0, i1 = nc, nocc - 1
+    a0, a1 = nocc, nocc + nvirt - 1
+    dmin = e[a0] - e[i1]
+    dmax = min(dai_max_thresh, e[a1] - e[i0])
+    if not dmin > 0.0:
+        raise ValueError("Found invalid orbital energy gap. Cannot decompose energy denominators.")
+    width = (dmax - dmin) / nbins
+    vals = dmin + np.arange(nbins) * width
+    d = (e[a0:a1 + 1][None, :] - e[i0:i1 + 1][:, None]).ravel()
+    d = d[d <= dai_max_thresh]
+    # nint() is round-half-away-from-zero in Fortran
+    x = (d - (dmin + width / 2.0)) / width
+    k = 1 + np.where(x >= 0, np.floor(x + 0.5), -np.floor(-x + 0.5)).astype(np.int64)
+    k = np.clip(k, 1, nbins)
+    count = np.bincount(k - 1, minlength=nbins).astype(np.float64)
+    return vals, np.abs(count / count.sum())
+
+
+# --------------------------------------------------------------------------
+# Frequency quadrature (transformed Gauss-Legendre, "Casimir-Polder")
+# --------------------------------------------------------------------------
+
+def gauss_legendre(n, max_abs_error=1.0e-14):
+    """All n Gauss-Legendre roots (ascending) and weights on (-1,1).
+
+    Follows quad_GaussLegendre, src/rpa/quadratures.f90:418-509: Newton
+    iteration on theta = arccos(x) with the three-term Legendre recurrence
+    (LegendrePolynomial, quadratures.f90:309-328) and weights
+    w = 2 / (dP_n/dtheta)^2.  The initial guesses here are the classical
+    theta_k = pi (k - 1/4)/(n + 1/2) (the reference uses the Tricomi and
+    Gatteschi asymptotic guesses of the same roots); the converged roots agree
+    to the Newton tolerance."""
+    k = np.arange(1, n + 1, dtype=np.float64)
+    theta = PI * (k - 0.25) / (n + 0.5)
+
+    def legendre(x):
+        pb = np.zeros_like(x)
+        pa = np.ones_like(x)
+        for a in range(1, n + 1):
+            pc = pb
+            pb = pa
+            pa = (2 * a - 1.0) / a * x * pb - (a - 1.0) / a * pc
+        return pa, pb
+
+    for _ in range(100):
+        x = np.cos(theta)
+        pa, pb = legendre(x)
+        p_theta = n * (x * pa - pb) / np.sin(theta)
+        new = theta - pa / p_theta
+        done = np.all(np.abs(new - theta) < max_abs_error)
+        theta = new
+        if done:
+            break
+    x = np.cos(theta)
+    pa, pb = legendre(x)
+    p_theta = n * (x * pa - pb) / np.sin(theta)
+    w = 2.0 / p_theta ** 2
+    order = np.argsort(x)
+    return x[order], w[order]
+
+
+def casimir_polder(n, alpha=0.5):
+    """Semi-infinite GL quadrature x = a(1+t)/(1-t), w = 2 a w_GL/(1-t)^2.
+
+    quad_CasimirPolder, src/rpa/quadratures.f90:570-643 (points ascending)."""
+    t, wgl = gauss_legendre(n)
+    x = alpha * (1.0 + t) / (1.0 - t)
+    w = 2.0 * wgl * alpha / (1.0 - t) ** 2
+    return x, w
+
+
+def freq_quad_error(freqs, weights, dai_values, dai_weights):
+    """(MaxRelError, RMSD) of sum_k w_k/(d^2+u_k^2) vs pi/(2d).
+
+    rpa_FreqQuadError, src/rpa/OptFreqQuad.f90:125-169.  dai_values and
+    dai_weights are (NBins, NDaiSets)."""
+    dv = np.atleast_2d(np.asarray(dai_values, np.float64).T).T
+    dw = np.atleast_2d(np.asarray(dai_weights, np.float64).T).T
+    rel = np.zeros(dv.shape[1])
+    err2 = np.zeros(dv.shape[1])
+    for s in range(dv.shape[1]):
+        m = dw[:, s] > 0.0
+        d = dv[m, s]
+        exact = PI / (2.0 * d)
+        approx = (weights[None, :] / (d[:, None] ** 2 + freqs[None, :] ** 2)).sum(axis=1)
+        if d.size:
+            rel[s] = np.max(np.abs((approx - exact) / exact))
+            err2[s] = np.sum(dw[m, s] * (approx - exact) ** 2)
+    return float(rel.max()), float(math.sqrt(err2.max()))
+
+
+def opt_quad_scaling(n, dai_values, dai_weights, min_alpha=0.1, max_alpha=15.0, nscan=15000):
+    """Scan of the scale alpha minimising the RMSD.
+
+    rpa_OptQuadScaling, src/rpa/OptFreqQuad.f90:75-122 (first minimum wins,
+    strict '<' comparison)."""
+    x0, w0 = casimir_polder(n, 1.0)
+    dv = np.atleast_2d(np.asarray(dai_values, np.float64).T).T
+    dw = np.atleast_2d(np.asarray(dai_weights, np.float64).T).T
+    alphas = min_alpha + (max_alpha - min_alpha) * np.arange(nscan) / (nscan - 1)
+    best = (np.inf, 0.0, 0.0)
+    err2 = np.zeros((nscan, dv.shape[1]))
+    rel = np.zeros((nscan, dv.shape[1]))
+    for s in range(dv.shape[1]):
+        m = dw[:, s] > 0.0
+        d = dv[m, s]
+        exact = PI / (2.0 * d)
+        for c0 in range(0, nscan, 1000):
+            a = alphas[c0:c0 + 1000]
+            u = a[:, None] * x0[None, :]
+            w = a[:, None] * w0[None, :]
+            approx = np.einsum("ak,abk->ab", w, 1.0 / (d[None, :, None] ** 2 + u[:, None, :] ** 2))
+            err2[c0:c0 + 1000, s] = ((approx - exact[None, :]) ** 2 * dw[m, s][None, :]).sum(axis=1)
+            rel[c0:c0 + 1000, s] = np.abs((approx - exact[None, :]) / exact[None, :]).max(axis=1)
+    rmsd = np.sqrt(err2.max(axis=1))
+    maxrel = rel.max(axis=1)
+    for k in range(nscan):
+        if rmsd[k] < best[0]:
+            best = (rmsd[k], maxrel[k], alphas[k])
+    a = best[2]
+    return a * x0, a * w0, a, best[1], best[0]
+
+
+def optimize_freq_quad(dai_values, dai_weights, target_error=TARGET_ERROR_FREQ,
+                       target_rel_error=TARGET_REL_ERROR_FREQ,
+                       min_n=RPA_MIN_NFREQS, max_n=RPA_MAX_NFREQS):
+    """Smallest n whose optimally scaled grid meets both targets.
+
+    rpa_OptimizeFreqQuad, src/rpa/OptFreqQuad.f90:12-72."""
+    for n in range(min_n, max_n + 1):
+        x, w, a, rel, rmsd = opt_quad_scaling(n, dai_values, dai_weights)
+        if rmsd < target_error and rel < target_rel_error:
+            return x, w
+    raise RuntimeError("Quadrature did not converge to specified accuracy")
+
+
+# --------------------------------------------------------------------------
+# Pi(u) build
+# --------------------------------------------------------------------------
+
+def chi_factor(d, freq):
+    """Chi = D/(D^2 + u^2). rpa_THC_ChiRkai, src/rpa/rpa_THC.f90:360-370."""
+    return d / (d * d + freq * freq)
+
+
+def pi_matrices(R, eps_o, eps_v, freqs, alpha=4.0, block_dim=THC_BLOCK_DIM):
+    """Pi(:,:,u) = alpha * sum_ai R(:,ai) Chi_u(ai) R(:,ai)^T, full square FP64.
+
+    rpa_THC_PiU / rpa_THC_PiU_BlockAlgo, src/rpa/rpa_THC.f90:215-340:
+    ai columns in blocks of THC_BlockDim, for every frequency
+    W = Chi*R_blk (rpa_THC_ChiRkai) then DGEMM Pi += alpha R_blk W^T
+    (real_abT_x, beta = 1).  alpha = 4 closed shell, 2 per spin open shell
+    (rpa_THC.f90:258-268)."""
+    R = np.asarray(R, np.float64)
+    nq, nov = R.shape
+    d = dai(eps_o, eps_v)
+    assert d.size == nov
+    K = len(freqs)
+    pi = np.zeros((K, nq, nq))
+    for t in range(0, nov, block_dim):
+        blk = R[:, t:t + block_dim]
+        db = d[t:t + block_dim]
+        for u in range(K):
+            W = blk * chi_factor(db, freqs[u])[None, :]
+            pi[u] += alpha * (blk @ W.T)
+    return pi
+
+
+# --------------------------------------------------------------------------
+# Energy: ln det(1+Pi) - Tr Pi, frequency quadrature
+# --------------------------------------------------------------------------
+
+def logdet_qr(A):
+    """ln|det A| via DGEQRF and sum ln|R_kk| accumulated exactly.
+
+    real_LogDet, src/linear-algebra/real_linalg.f90:793-825.  The reference
+    accumulates log(|a_kk|) in REAL(16); here the logs are FP64 and their
+    sum is exactly rounded (math.fsum), which agrees to well below 1e-14."""
+    qr, tau, work, info = lapack.dgeqrf(np.array(A, np.float64, order="F"))
+    if info != 0:
+        raise RuntimeError(f"DGEQRF returned error code {info}")
+    return math.fsum(np.log(np.abs(np.diag(qr))).tolist())
+
+
+def logdet_cholesky(A):
+    """2 sum ln L_kk (identity (iii) against logdet_qr)."""
+    L = np.linalg.cholesky(A)
+    return 2.0 * math.fsum(np.log(np.diag(L)).tolist())
+
+
+def ec_rpa_analytic(pi, weights, logdet=logdet_qr):
+    """E_c = 1/(2 pi) sum_u w_u [ln det(1+Pi_u) - Tr Pi_u] and the E(u) list.
+
+    rpa_CC_EcRPA_Analytic, src/rpa/rpa_CC.f90:412-471 (traces and E(u) in
+    REAL(16): exactly rounded sums here)."""
+    K = pi.shape[0]
+    eu = np.zeros(K)
+    terms = []
+    for u in range(K):
+        W = pi[u]
+        tr = math.fsum(np.diag(W).tolist())
+        A = W + np.eye(W.shape[0])
+        ld = logdet(A)
+        eu[u] = ld - tr
+        terms.append(eu[u] * weights[u] / (2.0 * PI))
+    return math.fsum(terms), eu
+
+
+def ec_rpa(R, eps_o, eps_v, freqs, weights, alpha=4.0):
+    """Pi build + analytic energy (the fused path the boundary replaces)."""
+    pi = pi_matrices(R, eps_o, eps_v, freqs, alpha)
+    return ec_rpa_analytic(pi, weights)
+
+
+def direct_mp2(R, eps_o, eps_v):
+    """Direct (ring) MP2: 2 sum_{ai,bj} (ai|bj)^2 / (e_i + e_j - e_a - e_b).
+
+    rpa_PT_Order2 direct term, src/rpa/rpa_PT_Terms.f90:66 (closed shell,
+    spatial orbitals).  E_c(RPA) of eps*R tends to this times eps^4."""
+    d = dai(eps_o, eps_v)
+    V = R.T @ R
+    return 2.0 * float(np.sum(V * V / (-(d[:, None] + d[None, :]))))
+
+
+# --------------------------------------------------------------------------
+# Pi eigen-decomposition, direct-ring T2, EigRPA
+# --------------------------------------------------------------------------
+
+def diagonalize_pi(pi):
+    """Ascending eigenpairs of every Pi(u). rpa_CC_Diagonalize_PiU,
+    src/rpa/rpa_CC.f90:1108-1129 (symmetric_eigenproblem)."""
+    w, v = np.linalg.eigh(pi)
+    return w, v
+
+
+def _apply_I(M, R, d, freqs, fweights, pi_vals, pi_vecs, lam):
+    """I(lambda) M = -sum_u w_u/(4 pi) Chi_u R^T Q_u diag(l/(1+l pi_u)) Q_u^T R Chi_u M.
+
+    rpa_CC_IM_v5, src/rpa/rpa_CC_Doubles.f90:369-422, with
+    Chi_u = -4 D/(D^2+u^2) (rpa_CC_Chi, 276-292)."""
+    out = np.zeros_like(M)
+    for u in range(len(freqs)):
+        chi = -(4.0 * d) / (d * d + freqs[u] ** 2)
+        Q = pi_vecs[u]
+        RChiM = R @ (chi[:, None] * M)
+        MTChiRTQ = RChiM.T @ Q
+        MTChiRTQ *= (lam / (1.0 + lam * pi_vals[u]))[None, :]
+        MTChiRTQWQT = MTChiRTQ @ Q.T
+        out += (-fweights[u] / (4.0 * PI)) * (chi[:, None] * (R.T @ MTChiRTQWQT.T))
+    return out
+
+
+def _normalize_columns(M):
+    """rpa_CC_NormalizeColumns, src/rpa/rpa_CC_Doubles.f90:80-91."""
+    return M / np.linalg.norm(M, axis=0)[None, :]
+
+
+def t2_direct_ring(R, eps_o, eps_v, freqs, fweights, pi_vals, pi_vecs, omega,
+                   lam=1.0, small_cutoff=SMALL_EIGENVAL_CUTOFF_T2,
+                   cutoff_thresh=T2_CUTOFF_THRESH, cutoff_type=T2_CUTOFF_EIG,
+                   common_thresh=-1.0, nocc=None):
+    """Direct-ring T2 = U diag(A) U^T by randomised range finding.
+
+    rpa_THC_CC_T2, src/rpa/rpa_CC_Doubles.f90:645-984 (sharp cutoff branch):
+      IOmega = normalize(I(l) normalize(Omega))           (747-763)
+      S = IOmega^T IOmega, EVD, keep eigenvalues > 1e-10  (770-781)
+      T = IOmega S_vecs / sqrt(S_vals)                     (786-795)
+      TIT = T^T I T, EVD, A = a/(2(a+1))                   (797-808)
+      cutoff |A| <= K, K = T2CutoffThresh (supersystem) or the common
+      threshold of the supersystem (subsystems)            (855-945)
+      U = T TIT_vecs(:, 1:NT)                              (973-975)
+    omega holds the guess vectors (nov x G): the reference draws them from
+    gfortran's random_number stream, which is not reproducible outside
+    gfortran, so parity is at the level of the converged subspace.
+    Returns (A, U, K)."""
+    d = dai(eps_o, eps_v)
+    G = omega.shape[1]
+    IOmega = np.zeros_like(omega)
+    for q0 in range(0, G, MAX_BATCH_DIM_T2):
+        Om = _normalize_columns(omega[:, q0:q0 + MAX_BATCH_DIM_T2])
+        IOmega[:, q0:q0 + MAX_BATCH_DIM_T2] = _normalize_columns(
+            _apply_I(Om, R, d, freqs, fweights, pi_vals, pi_vecs, lam))
+    S = IOmega.T @ IOmega
+    s_vals, s_vecs = np.linalg.eigh(S)
+    nt = 0
+    for i in range(G - 1, -1, -1):
+        if s_vals[i] > small_cutoff:
+            nt += 1
+        else:
+            break
+    W = s_vecs[:, G - nt:] / np.sqrt(s_vals[G - nt:])[None, :]
+    T = IOmega @ W
+    TIT = T.T @ _apply_I(T, R, d, freqs, fweights, pi_vals, pi_vecs, lam)
+    TIT = 0.5 * (TIT + TIT.T)
+    a, vecs = np.linalg.eigh(TIT)
+    A = 0.5 * (a / (a + 1.0))
+    if common_thresh < 0.0:
+        if cutoff_type == T2_CUTOFF_EIG:
+            K = cutoff_thresh
+        elif cutoff_type == T2_CUTOFF_EIG_DIV_MAXEIG:
+            K = cutoff_thresh * np.max(np.abs(A))
+        elif cutoff_type == T2_CUTOFF_EIG_DIV_NELECTRON:
+            K = cutoff_thresh / (nocc * 2)
+        elif cutoff_type == T2_CUTOFF_SUM_REJECTED:
+            K = 0.0
+            for i in range(len(A) - 1):
+                if abs(A[i + 1:].sum()) < cutoff_thresh:
+                    K = abs(A[i + 1])
+                    break
+        else:
+            raise ValueError("Invalid value of T2CutoffThresh")
+    else:
+        K = common_thresh
+    keep = 0
+    for i in range(len(A)):
+        if abs(A[i]) > K:
+            keep = i + 1
+        else:
+            break
+    if keep == 0:
+        raise RuntimeError("Invalid T2CutoffThresh: no eigenvectors left after cutoff")
+    U = T @ vecs[:, :keep]
+    return A[:keep].copy(), U, K
+
+
+def t2_eig_rpa(U, A, R):
+    """EigRPA(mu) = 2 A_mu ||R U_mu||^2.
+
+    rpa_T2_EigRPA, src/rpa/rpa_CC_Doubles.f90:987-1009; the sum is stored as
+    RPA_ENERGY_T2_DIRECT_RING (src/rpa/rpa_THC.f90:126)."""
+    RU = R @ U
+    return 2.0 * A * np.sum(RU * RU, axis=0)
+
+
+def exchange_sosex(V, A, R, nocc, nvirt, alpha=1.0, s2_operator=False):
+    """E_x = -alpha sum_{abij} (aj|bi) T_aibj.
+
+    rpa_CC_Exchange_SOSEX + rpa_CC_EcExchange1,
+    src/rpa/rpa_CC_Exchange.f90:36-116.  V is (NT, NVirt, NOcc) (the
+    NVecsT2 x nov row layout of that routine), R is (NQ, NVirt, NOcc);
+    B = A/(1-4A^2) when the S2 operator is requested."""
+    nq = R.shape[0]
+    nt = V.shape[0]
+    Rr = R.reshape(nq, nvirt, nocc, order="F")
+    Vr = V.reshape(nt, nvirt, nocc, order="F")
+    B = A / (1.0 - 4.0 * A * A) if s2_operator else A
+    e = []
+    for j in range(nocc):
+        for i in range(j, nocc):
+            Wij = Rr[:, :, i] @ Vr[:, :, j].T
+            if i != j:
+                Wji = Rr[:, :, j] @ Vr[:, :, i].T
+                e.append(-2.0 * float(np.sum(Wji * Wij * B[None, :])))
+            else:
+                e.append(-float(np.sum(Wij * Wij * B[None, :])))
+    return alpha * math.fsum(e)
+
+
+# --------------------------------------------------------------------------
+# Adjoint (no reference counterpart): dE_c/dR, dE_c/de
+# --------------------------------------------------------------------------
+
+def ec_grad(R, eps_o, eps_v, freqs, weights, alpha=4.0):
+    """Analytic gradient of E_c = 1/(2pi) sum_u w_u [ln det(1+Pi_u) - Tr Pi_u].
+
+    The reference has no gradients; this is the FP64 reference gradient:
+      dE/dR(:,ai) = 1/(2pi) sum_u w_u 2 alpha c_u(ai) M_u R(:,ai),
+      M_u = (1+Pi_u)^-1 - 1;
+      dE/dD(ai)  = 1/(2pi) sum_u w_u alpha R(:,ai)^T M_u R(:,ai) dc_u/dD,
+      dc/dD = (u^2 - D^2)/(D^2+u^2)^2; dD(ai)/de_a = 1, dD(ai)/de_i = -1."""
+    nq, nov = R.shape
+    no, nv = len(eps_o), len(eps_v)
+    d = dai(eps_o, eps_v)
+    pi = pi_matrices(R, eps_o, eps_v, freqs, alpha)
+    dR = np.zeros_like(R)
+    dD = np.zeros(nov)
+    for u in range(len(freqs)):
+        c = chi_factor(d, freqs[u])
+        M = np.linalg.inv(np.eye(nq) + pi[u]) - np.eye(nq)
+        MR = M @ R
+        f = weights[u] / (2.0 * PI)
+        dR += f * 2.0 * alpha * c[None, :] * MR
+        dcdD = (freqs[u] ** 2 - d * d) / (d * d + freqs[u] ** 2) ** 2
+        dD += f * alpha * np.sum(R * MR, axis=0) * dcdD
+    dD2 = dD.reshape(nv, no, order="F")
+    return dR, -dD2.sum(axis=0), dD2.sum(axis=1)
+
+
+# --------------------------------------------------------------------------
+# Many-body-expansion differences
+# --------------------------------------------------------------------------
+
+def eint_2body(e_ab, e_a, e_b):
+    """rpa_Eint2Body, src/rpa/rpa_driver.f90:381-386 (REAL(16) -> exact sums)."""
+    return math.fsum([e_ab, -e_a, -e_b])
+
+
+def eint_nadd3(e):
+    """3-body nonadditive energy from the 7 subsystem energies
+    [ABC, AB, AC, BC, A, B, C]. rpa_EintNadd, src/rpa/rpa_driver.f90:389-400."""
+    abc, ab, ac, bc, a, b, c = e
+    return math.fsum([abc, -ab, -ac, -bc, a, b, c])
+
+
+# --------------------------------------------------------------------------
+# Seeded synthetic inputs with the shapes of the measured workloads
+# --------------------------------------------------------------------------
+
+@dataclass
+class RPASystem:
+    R: np.ndarray            # (NQ, nov) FP64, ai = a + nv*i
+    eps_o: np.ndarray        # active occupied energies (no)
+    eps_v: np.ndarray        # virtual energies (nv)
+    freqs: np.ndarray = field(default=None)
+    weights: np.ndarray = field(default=None)
+    alpha: float = 4.0
+
+    @property
+    def nq(self):
+        return self.R.shape[0]
+
+    @property
+    def no(self):
+        return len(self.eps_o)
+
+    @property
+    def nv(self):
+        return len(self.eps_v)
+
+
+def lambda_max_pi0(R, d, alpha=4.0, iters=60, seed=0):
+    """Largest eigenvalue of Pi(0) = alpha R diag(1/D) R^T by power iteration."""
+    rng = np.random.default_rng(seed)
+    v = rng.standard_normal(R.shape[0])
+    lam = 0.0
+    for _ in range(iters):
+        w = alpha * (R @ ((R.T @ v) / d))
+        lam = float(np.linalg.norm(w))
+        v = w / lam
+    return lam
+
+
+def make_system(nq, no, nv, seed, occ_range=(-1.3, -0.4), virt_range=(0.03, 4.0),
+                decay=50.0, scale=1.0, lam0=None, ncore_orbs=0):
+    """Seeded synthetic twin: occ e ~ U[occ_range], virt e log-uniform in
+    virt_range, R ~ N(0,1)*scale*exp(-Q/decay); optionally rescaled so that
+    lambda_max(Pi(0)) = lam0.  Extra core orbitals (e < -3 Eh) are generated
+    and frozen by rpa_NCore when ncore_orbs > 0; only active ones are kept."""
+    rng = np.random.default_rng(seed)
+    eo = np.sort(rng.uniform(occ_range[0], occ_range[1], no))
+    lo, hi = np.log(virt_range[0]), np.log(virt_range[1])
+    ev = np.sort(np.exp(rng.uniform(lo, hi, nv)))
+    if ncore_orbs:
+        core = np.sort(rng.uniform(-21.0, -19.0, ncore_orbs))
+        allocc = np.concatenate([core, eo])
+        nc = ncore(np.concatenate([allocc, ev]), len(allocc))
+        eo = allocc[nc:]
+    R = rng.standard_normal((nq, no * nv)) * scale
+    R *= np.exp(-np.arange(nq) / decay)[:, None]
+    if lam0 is not None:
+        lm = lambda_max_pi0(R, dai(eo, ev))
+        R *= math.sqrt(lam0 / lm)
+    return RPASystem(R=R, eps_o=eo, eps_v=ev)
+
+
+def grid_for(sys_, n=None):
+    """Frequency grid for a system: histogram -> optimised grid (n fixed or
+    chosen by the convergence targets)."""
+    e = np.concatenate([sys_.eps_o, sys_.eps_v])
+    vals, wts = dai_histogram(e, sys_.no, sys_.nv)
+    if n is None:
+        return optimize_freq_quad(vals, wts)
+    x, w, *_ = opt_quad_scaling(n, vals, wts)
+    return x, w
+
+
+# --------------------------------------------------------------------------
+# Split-BF16 emulation (used to size the precision budget of the tensor-core path)
+# --------------------------------------------------------------------------
+
+def to_bf16(x):
+    """Round float64 -> float32 -> bf16 (round to nearest even), as float64."""
+    f = np.asarray(x, np.float32)
+    b = f.view(np.uint32).astype(np.uint64)
+    b = (b + 0x7FFF + ((b >> 16) & 1)) & 0xFFFF0000
+    return b.astype(np.uint32).view(np.float32).astype(np.float64)

@@ -1,0 +1,60 @@
+"""CPU tests of the C-ABI library: it loads, and exports every entry point
+include/rpa_b200.h declares.  No compute call is made without a GPU."""
+import ctypes
+
+import numpy as np
+
+import pytest
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    lib = pkg.load_library()
+    names = pkg.declared_functions()
+    assert "rpa_b200_ec" in names and "rpa_b200_pi" in names
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_status_strings(pkg):
+    lib = pkg.load_library()
+    assert lib.rpa_b200_status_string(pkg.RPA_OK) == b"success"
+    assert b"positive definite" in lib.rpa_b200_status_string(pkg.RPA_ERR_NOT_SPD)
+    assert lib.rpa_b200_status_string(999) == b"unknown status"
+
+
+def test_create_without_gpu_reports_no_device(pkg):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    lib = pkg.load_library()
+    h = ctypes.c_void_p()
+    assert lib.rpa_b200_create(ctypes.byref(h), 0, 0) == pkg.RPA_ERR_NO_DEVICE
+    assert not h.value
+    with pytest.raises(pkg.RPAError):
+        pkg.Handle(0)
+
+
+def test_null_handle_is_rejected(pkg):
+    lib = pkg.load_library()
+    assert lib.rpa_b200_destroy(None) == pkg.RPA_OK
+    assert lib.rpa_b200_ec_from_pi(None, 4, 1, None, 4, None, None, None) == pkg.RPA_ERR_INVALID_ARG
+
+
+def test_freq_grid_matches_oracle(pkg, oracle):
+    # host-side grid generator of the library vs the oracle restatement
+    s = oracle.make_system(10, 12, 150, 5, occ_range=(-1.2, -0.3), virt_range=(0.02, 5.0), ncore_orbs=2)
+    core = np.array([-20.3, -19.7])
+    e = np.concatenate([core, s.eps_o, s.eps_v])
+    for nfixed in (12, 16):
+        x, w = pkg.freq_grid(e, len(core) + s.no, s.nv, nfixed=nfixed)
+        xr, wr = oracle.grid_for(s, nfixed)
+        assert np.allclose(x, xr, rtol=1e-12) and np.allclose(w, wr, rtol=1e-12)
+    x, w = pkg.freq_grid(e, len(core) + s.no, s.nv)
+    xr, wr = oracle.grid_for(s)
+    assert len(x) == len(xr) and np.allclose(x, xr, rtol=1e-12)
+
+
+def test_freq_grid_rejects_bad_gap(pkg):
+    e = np.array([-1.0, 0.5, 0.2, 1.0])  # HOMO above LUMO
+    with pytest.raises(pkg.RPAError):
+        pkg.freq_grid(e, 2, 2)

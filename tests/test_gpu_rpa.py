@@ -1,0 +1,150 @@
+"""GPU parity tests of the Pi(u) build and the RPA energy through the C ABI,
+against the FP64 oracle and its golden fixtures.
+
+Tolerances (stated per north-star precision budget):
+  FP64 path:   Pi entries 1e-12 relative to max|Pi|; E_c 1e-10 Eh.
+  split-BF16:  Pi off-diagonal 3e-5 relative to max|Pi| (bf16 hi/lo, FP32
+               accumulation), diagonal exact to 1e-12 relative; E_c 1e-6 Eh.
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle import rpa_oracle as O
+
+pytestmark = pytest.mark.gpu
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "oracle_golden.json").read_text())
+
+
+def golden_system(name):
+    from tests.golden.make_golden import system
+    return system(name)
+
+
+def rel_err(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+@pytest.mark.parametrize("name", ["ragged", "tiny", "water_dimer_twin"])
+def test_pi_fp64_matches_oracle(handle, name):
+    s, x, w = golden_system(name)
+    ref = O.pi_matrices(s.R, s.eps_o, s.eps_v, x)
+    got = handle.pi_u(s.R, s.eps_o, s.eps_v, x, prec="fp64")
+    assert rel_err(got, ref) < 1e-12
+    assert np.array_equal(got, np.transpose(got, (0, 2, 1)))
+
+
+@pytest.mark.parametrize("name", ["ragged", "tiny", "water_dimer_twin", "scaled_c2"])
+def test_pi_split_matches_oracle(handle, name):
+    s, x, w = golden_system(name)
+    ref = O.pi_matrices(s.R, s.eps_o, s.eps_v, x)
+    got = handle.pi_u(s.R, s.eps_o, s.eps_v, x, prec="split")
+    assert rel_err(got, ref) < 3e-5
+    for k in range(len(x)):
+        assert rel_err(np.diag(got[k]), np.diag(ref[k])) < 1e-12
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN))
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("split", 1e-6)])
+def test_ec_matches_golden(handle, name, prec, tol):
+    g = GOLDEN[name]
+    s, x, w = golden_system(name)
+    ec, eu = handle.ec_rpa(s.R, s.eps_o, s.eps_v, x, w, prec=prec)
+    assert abs(ec - g["Ec"]) < tol
+    eu_tol = 1e-9 if prec == "fp64" else 2e-5
+    assert np.max(np.abs(eu - np.array(g["Eu"]))) < eu_tol
+
+
+def test_ec_from_pi_matches_qr_logdet(handle):
+    s, x, w = golden_system("water_dimer_twin")
+    pi = O.pi_matrices(s.R, s.eps_o, s.eps_v, x)
+    ref, ref_eu = O.ec_rpa_analytic(pi, w)
+    ec, eu = handle.ec_from_pi(pi, w)
+    assert abs(ec - ref) < 1e-11
+    assert np.max(np.abs(eu - ref_eu)) < 1e-10
+
+
+def test_device_pointers_match_host(handle):
+    import torch
+    s, x, w = golden_system("ragged")
+    host = handle.ec_rpa(s.R, s.eps_o, s.eps_v, x, w, prec="split")
+    Rt = torch.from_numpy(np.ascontiguousarray(s.R.T)).cuda()  # (nov, NQ) contiguous -> R = Rt.T column-major
+    dev = handle.ec_rpa(Rt.T, torch.from_numpy(s.eps_o).cuda(), torch.from_numpy(s.eps_v).cuda(),
+                        torch.from_numpy(x).cuda(), torch.from_numpy(w).cuda(), prec="split")
+    assert dev[0] == host[0]
+    out = torch.empty((len(x), s.nq, s.nq), dtype=torch.float64, device="cuda")
+    handle.pi_u(Rt.T, s.eps_o, s.eps_v, x, prec="fp64", out=out)
+    ref = O.pi_matrices(s.R, s.eps_o, s.eps_v, x)
+    assert rel_err(out.cpu().numpy(), ref) < 1e-12
+
+
+def test_leading_dimension_larger_than_nq(handle):
+    s, x, w = golden_system("ragged")
+    big = np.zeros((s.nq + 13, s.R.shape[1]), order="F")
+    big[: s.nq] = s.R
+    import torch
+    Rt = torch.from_numpy(np.ascontiguousarray(big.T)).cuda()
+    view = Rt.T[: s.nq]  # stride(1) = NQ + 13
+    ec, _ = handle.ec_rpa(view, s.eps_o, s.eps_v, x, w, prec="fp64")
+    assert abs(ec - GOLDEN["ragged"]["Ec"]) < 1e-10
+
+
+def test_repeated_calls_are_deterministic(handle):
+    s, x, w = golden_system("scaled_c2")
+    a = handle.ec_rpa(s.R, s.eps_o, s.eps_v, x, w, prec="split")
+    b = handle.ec_rpa(s.R, s.eps_o, s.eps_v, x, w, prec="split")
+    assert a[0] == b[0] and np.array_equal(a[1], b[1])
+
+
+def test_multi_tile_split_against_fp64(handle):
+    # several 128 x 256 tiles, nov not a multiple of 32, K > 16 (two frequency groups)
+    s = O.make_system(1000, 9, 227, 31, decay=150.0, lam0=0.8)
+    x, w = O.casimir_polder(20, 0.8)
+    e64, _ = handle.ec_rpa(s.R, s.eps_o, s.eps_v, x, w, prec="fp64")
+    esp, _ = handle.ec_rpa(s.R, s.eps_o, s.eps_v, x, w, prec="split")
+    assert abs(e64 - esp) < 1e-6
+    p64 = handle.pi_u(s.R, s.eps_o, s.eps_v, x[:3], prec="fp64")
+    psp = handle.pi_u(s.R, s.eps_o, s.eps_v, x[:3], prec="split")
+    assert rel_err(psp, p64) < 3e-5
+
+
+# ----------------------------------------------------------------------------- errors
+
+def test_nonfinite_input_is_reported(handle, pkg):
+    s, x, w = golden_system("tiny")
+    R = s.R.copy()
+    R[3, 5] = np.nan
+    with pytest.raises(pkg.RPAError) as e:
+        handle.ec_rpa(R, s.eps_o, s.eps_v, x, w)
+    assert e.value.status == pkg.RPA_ERR_NONFINITE
+
+
+def test_invalid_gap_is_reported(handle, pkg):
+    s, x, w = golden_system("tiny")
+    eo = s.eps_o.copy()
+    eo[-1] = s.eps_v[0] + 0.1
+    with pytest.raises(pkg.RPAError) as e:
+        handle.ec_rpa(s.R, eo, s.eps_v, x, w)
+    assert e.value.status == pkg.RPA_ERR_INVALID_ARG
+
+
+def test_not_spd_is_reported(handle, pkg):
+    pi = np.zeros((2, 70, 70))
+    pi[0] = np.eye(70) * 0.1
+    pi[1] = np.eye(70) * 0.1
+    pi[1, 65, 65] = -1.5  # 1 + Pi has a negative eigenvalue
+    with pytest.raises(pkg.RPAError) as e:
+        handle.ec_from_pi(pi, np.array([0.5, 0.5]))
+    assert e.value.status == pkg.RPA_ERR_NOT_SPD
+    # the handle stays usable afterwards
+    ec, eu = handle.ec_from_pi(pi[:1], np.array([1.0]))
+    assert np.isfinite(ec)
+
+
+def test_bad_dimensions_are_rejected(handle, pkg):
+    s, x, w = golden_system("tiny")
+    with pytest.raises(pkg.RPAError) as e:
+        handle.ec_rpa(s.R, s.eps_o, s.eps_v, np.zeros(65), np.zeros(65))
+    assert e.value.status == pkg.RPA_ERR_INVALID_ARG
