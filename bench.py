@@ -36,7 +36,7 @@ import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 METRIC = "RPA E_c/s & Π-build TFLOP/s: split-BF16 vs FP64 on 1 B200 at |ΔE|≤1e-7 Eh"
-WORKLOAD = "single_4096"
+WORKLOAD = "single_4096"  # default measured workload; --workload selects another (e.g. single_2048 to profile)
 
 
 def load_package():
@@ -171,10 +171,12 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     pkg = load_package()
     from beyond_rpa_b200.workloads import make_single_system, SINGLE_SYSTEM
+    WORKLOAD = args.workload
     nq, no, nv, K, _ = SINGLE_SYSTEM[WORKLOAD]
     nov = no * nv
     h = pkg.Handle(local)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()  # the library and the timing events share this stream
+    torch.cuda.set_stream(stream)
     h.set_stream(stream.cuda_stream)
     s = make_single_system(WORKLOAD, seed=1000 + rank)
     torch.cuda.synchronize()
@@ -221,6 +223,14 @@ def run_ours(args):
     t_ms = max_over_ranks(e0.elapsed_time(e1))
     value = world * args.steps / (t_ms / 1e3)
 
+    if args.no_extras:
+        if rank == 0:
+            print(json.dumps({"workload": WORKLOAD, "ms_per_step": t_ms / args.steps, "Ec": ecs[-1],
+                              "phase_ms": {"contraction": statistics.mean(contraction),
+                                           "scale_split": statistics.mean(split),
+                                           "logdet": statistics.mean(logdet)}}), flush=True)
+        h.close()
+        return
     # end-to-end through the public API with host (pinned) inputs
     Rh_t = torch.empty((nov, nq), dtype=torch.float64, pin_memory=True)
     Rh_t.copy_(s.R.T)
@@ -338,6 +348,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default=WORKLOAD, help="single-system workload name (beyond-rpa_b200/workloads.py)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="profiling runs: print only the timed leg (no e2e, FP64-form or CPU legs)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -39,10 +40,22 @@ struct rpa_b200_handle {
   cudaEvent_t ev[5] = {};
   double timings[6] = {0, 0, 0, 0, 0, 0};
   int64_t launches = 0;
+  int seg_chunks = 16;  // 512-column accumulation segments of the tensor-core SYRK
   // per-call event pairs around the scale/split pass and the contraction kernel
   std::vector<cudaEvent_t> pool;
   size_t pool_used = 0;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> split_ev, tc_ev;
+  // CUDA graphs of the blocked Cholesky launch sequence, keyed by its arguments
+  struct CholGraph {
+    double* A;
+    int64_t ld, stride;
+    int n, nmat;
+    double* Ldiag;
+    cudaStream_t stream;
+    cudaGraphExec_t exec;
+    int64_t launches;
+  };
+  std::vector<CholGraph> chol_graphs;
 };
 
 namespace {
@@ -287,10 +300,53 @@ int build_pi(rpa_b200_handle* h, const Validated& v, const double* Rd, int64_t l
     a.piStride = (int64_t)NQ * NQ;
     a.diag = diag;
     a.err = h->err_dev;
+    a.seg_chunks = h->seg_chunks;
     RPA_CUDA(h, rpa::launch_syrk_split_bf16(&mAh, &mAl, &mBh, &mBl, a, h->num_sms, h->stream));
     RPA_CUDA(h, cudaEventRecord(e2, h->stream));
     h->tc_ev.push_back({e1, e2});
   }
+  return RPA_OK;
+}
+
+// Blocked Cholesky of nmat matrices through a cached CUDA graph (the launch
+// sequence depends only on the arguments; ~6 launches per 64 columns would
+// otherwise leave the GPU idle between the small late-step kernels).
+int cholesky(rpa_b200_handle* h, double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag) {
+  for (auto& g : h->chol_graphs) {
+    if (g.A == A && g.ld == ld && g.stride == stride && g.n == n && g.nmat == nmat && g.Ldiag == Ldiag &&
+        g.stream == h->stream) {
+      RPA_CUDA(h, cudaGraphLaunch(g.exec, h->stream));
+      rpa::g_launches += g.launches;
+      return RPA_OK;
+    }
+  }
+  const int64_t before = rpa::g_launches;
+  cudaGraph_t graph = nullptr;
+  if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+    cudaError_t e = rpa::launch_cholesky_lower(A, ld, stride, n, nmat, Ldiag, h->err_dev, h->stream);
+    cudaError_t e2 = cudaStreamEndCapture(h->stream, &graph);
+    const int64_t count = rpa::g_launches - before;
+    rpa::g_launches = before;
+    cudaGraphExec_t exec = nullptr;
+    if (e == cudaSuccess && e2 == cudaSuccess && graph &&
+        cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+      cudaGraphDestroy(graph);
+      if (h->chol_graphs.size() >= 8) {
+        cudaGraphExecDestroy(h->chol_graphs.front().exec);
+        h->chol_graphs.erase(h->chol_graphs.begin());
+      }
+      h->chol_graphs.push_back({A, ld, stride, n, nmat, Ldiag, h->stream, exec, count});
+      RPA_CUDA(h, cudaGraphLaunch(exec, h->stream));
+      rpa::g_launches += count;
+      return RPA_OK;
+    }
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+  } else {
+    cudaGetLastError();
+  }
+  // capture unavailable on this stream: launch the same kernels directly
+  RPA_CUDA(h, rpa::launch_cholesky_lower(A, ld, stride, n, nmat, Ldiag, h->err_dev, h->stream));
   return RPA_OK;
 }
 
@@ -303,8 +359,8 @@ int energy_from_workspace(rpa_b200_handle* h, int NQ, int K, const std::vector<d
   double* ld = tr + 2 * K;
   RPA_CUDA(h, rpa::launch_trace_shift(Pi, NQ, (int64_t)NQ * NQ, NQ, K, nullptr, tr, h->stream));
   RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
-  RPA_CUDA(h, rpa::launch_cholesky_lower(Pi, NQ, (int64_t)NQ * NQ, NQ, K, static_cast<double*>(h->Ldiag.p),
-                                         h->err_dev, h->stream));
+  int cs = cholesky(h, Pi, NQ, (int64_t)NQ * NQ, NQ, K, static_cast<double*>(h->Ldiag.p));
+  if (cs != RPA_OK) return cs;
   RPA_CUDA(h, rpa::launch_logdet_sum(static_cast<double*>(h->Ldiag.p), NQ, K, ld, h->stream));
   RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
   std::vector<double> host(4 * (size_t)K);
@@ -392,6 +448,7 @@ int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) {
     return RPA_ERR_CUDA;
   }
   h->stream = h->own_stream;
+  if (const char* sc = std::getenv("RPA_B200_SEG_CHUNKS")) h->seg_chunks = std::atoi(sc);
   for (auto& e : h->ev) cudaEventCreate(&e);
   cudaDriverEntryPointQueryResult q;
   void* fn = nullptr;
@@ -417,6 +474,7 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : h->pool) cudaEventDestroy(e);
+  for (auto& g : h->chol_graphs) cudaGraphExecDestroy(g.exec);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   delete h;
   return RPA_OK;

@@ -26,22 +26,29 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-__device__ __forceinline__ void tri_decode(int b, int& tm, int& tn) {
-  int t = (int)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
-  while ((t + 1) * (t + 2) / 2 <= b) ++t;
-  while (t * (t + 1) / 2 > b) --t;
-  tm = t;
-  tn = b - t * (t + 1) / 2;
+// Tile b of the lower trapezoid of a T x T tile grid restricted to the first
+// Tc tile columns, enumerated column by column: column tn holds rows tn..T-1.
+__device__ __forceinline__ void trap_decode(int b, int T, int Tc, int& tm, int& tn) {
+  // tiles before column c: c*T - c*(c-1)/2
+  int lo = 0, hi = Tc - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (mid * T - mid * (mid - 1) / 2 <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  tn = lo;
+  tm = tn + (b - (tn * T - tn * (tn - 1) / 2));
 }
 
 template <bool kScaled>
-__global__ void __launch_bounds__(kThreads) dsyrk_lower_kernel(const DsyrkArgs a) {
+__global__ void __launch_bounds__(kThreads) dsyrk_lower_kernel(const DsyrkArgs a, const int T, const int Tc) {
   __shared__ double As[2][BK][LDS];
   __shared__ double Bs[2][BK][LDS];
   __shared__ double sS[2][BK];
 
   int tm, tn;
-  tri_decode(blockIdx.x, tm, tn);
+  trap_decode(blockIdx.x, T, Tc, tm, tn);
+  const int ncols = a.ncols > 0 ? a.ncols : a.n;
   const int z = blockIdx.y;
   const double* A = a.A + (int64_t)z * a.strideA;
   double* C = a.C + (int64_t)z * a.strideC;
@@ -121,7 +128,7 @@ __global__ void __launch_bounds__(kThreads) dsyrk_lower_kernel(const DsyrkArgs a
 #pragma unroll
       for (int v = 0; v < 2; ++v) {
         const int col = n0 + wn * 32 + j * 8 + 2 * (lane & 3) + v;
-        if (row < a.n && col < a.n && row >= col) {
+        if (row < a.n && col < ncols && row >= col) {
           double* p = C + (int64_t)row + a.ldc * (int64_t)col;
           if (kScaled) *p = acc[i][j][v];
           else *p -= acc[i][j][v];
@@ -135,9 +142,12 @@ __global__ void __launch_bounds__(kThreads) dsyrk_lower_kernel(const DsyrkArgs a
 cudaError_t launch_dsyrk_lower(const DsyrkArgs& a, cudaStream_t stream) {
   if (a.n <= 0 || a.batch <= 0) return cudaSuccess;
   const int T = (a.n + BM - 1) / BM;
-  dim3 grid((unsigned)(T * (T + 1) / 2), (unsigned)a.batch);
-  if (a.D) dsyrk_lower_kernel<true><<<grid, kThreads, 0, stream>>>(a);
-  else dsyrk_lower_kernel<false><<<grid, kThreads, 0, stream>>>(a);
+  const int nc = (a.ncols > 0 && a.ncols < a.n) ? a.ncols : a.n;
+  const int Tc = (nc + BM - 1) / BM;
+  const int64_t tiles = (int64_t)Tc * T - (int64_t)Tc * (Tc - 1) / 2;
+  dim3 grid((unsigned)tiles, (unsigned)a.batch);
+  if (a.D) dsyrk_lower_kernel<true><<<grid, kThreads, 0, stream>>>(a, T, Tc);
+  else dsyrk_lower_kernel<false><<<grid, kThreads, 0, stream>>>(a, T, Tc);
   ++g_launches;
   return cudaGetLastError();
 }

@@ -47,6 +47,7 @@ struct SyrkTcArgs {
   int64_t piStride;  // elements between consecutive Pi_k
   const double* diag;  // exact diagonal [kg][NQ]
   int* err;
+  int seg_chunks;    // 32-column chunks per accumulation segment (<= 0: no segmentation)
 };
 // Tensor maps: 3-D (ai, Q, k) bf16 views of X_hi / X_lo; A maps use a
 // 128-row box, B maps a 256-row box, 32 ai per box, 64-byte swizzle.
@@ -70,7 +71,8 @@ struct DsyrkArgs {
   double* C;
   int64_t ldc;
   int64_t strideC;
-  int n;          // order of C
+  int n;          // rows of C (order of the lower triangle)
+  int ncols;      // columns of C updated (<= n; 0 means n): lower trapezoid
   int64_t kdim;   // contraction length
   int batch;
   // scaled mode

@@ -16,6 +16,9 @@ namespace {
 constexpr int NB = 64;  // Cholesky block size
 
 // Factor the NB x NB diagonal block of each matrix in shared memory.
+// Column j is used unscaled in step j (update of the columns right of it by
+// a_rj a_cj / d_j) and scaled by 1/sqrt(d_j) in step j+1, when nobody reads
+// it any more: one barrier per column.
 __global__ void __launch_bounds__(256) potrf_diag_kernel(double* A, int64_t ld, int64_t stride, int n, int j0,
                                                          double* Ldiag, int* err) {
   __shared__ double L[NB][NB + 1];
@@ -28,26 +31,42 @@ __global__ void __launch_bounds__(256) potrf_diag_kernel(double* A, int64_t ld, 
     L[r][c] = (r >= c && r < nbe && c < nbe) ? Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] : 0.0;
   }
   __syncthreads();
+  bool bad = false;
   for (int j = 0; j < nbe; ++j) {
-    if (t == 0) {
-      double d = L[j][j];
-      if (!(d > 0.0)) {  // also catches NaN
-        atomicCAS(err, 0, (int)kDevNotSPD);
-        d = 1.0;
-      }
-      L[j][j] = sqrt(d);
+    double d = L[j][j];
+    if (!(d > 0.0)) {  // also catches NaN; keep going with a unit pivot, report the error
+      bad = true;
+      d = 1.0;
     }
-    __syncthreads();
-    const double inv = 1.0 / L[j][j];
-    for (int r = j + 1 + t; r < nbe; r += blockDim.x) L[r][j] *= inv;
-    __syncthreads();
+    const double inv = 1.0 / d;
+    // scale the previous column (nobody reads it in this step)
+    if (j > 0) {
+      double dp = L[j - 1][j - 1];
+      if (!(dp > 0.0)) dp = 1.0;
+      const double s = rsqrt(dp);
+      for (int r = j + t; r < nbe; r += blockDim.x) L[r][j - 1] *= s;
+    }
     const int m = nbe - j - 1;
     for (int idx = t; idx < m * m; idx += blockDim.x) {
       const int r = j + 1 + idx % m, c = j + 1 + idx / m;
-      if (r >= c) L[r][c] -= L[r][j] * L[c][j];
+      if (r >= c) L[r][c] -= L[r][j] * L[c][j] * inv;
     }
     __syncthreads();
   }
+  {  // scale the last column and take the square roots of the pivots
+    const int j = nbe - 1;
+    double dp = L[j][j];
+    if (!(dp > 0.0)) dp = 1.0;
+    if (t == 0) L[j][j] = sqrt(dp);
+  }
+  __syncthreads();
+  for (int j = t; j < nbe - 1; j += blockDim.x) {
+    double d = L[j][j];
+    if (!(d > 0.0)) d = 1.0;
+    L[j][j] = sqrt(d);
+  }
+  if (bad && t == 0) atomicCAS(err, 0, (int)kDevNotSPD);
+  __syncthreads();
   for (int idx = t; idx < NB * NB; idx += blockDim.x) {
     const int r = idx % NB, c = idx / NB;
     if (r >= c && r < nbe && c < nbe) Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] = L[r][c];
@@ -173,31 +192,58 @@ __global__ void copy_lower_kernel(const double* src, int64_t lds, int64_t stride
 }
 }  // namespace
 
+// Two-level blocked right-looking Cholesky: 64-wide column panels (diagonal
+// factorization + panel solve + update of the rest of the 256-wide outer
+// block), then one rank-256 update of the trailing matrix per outer block.
+constexpr int NB2 = 256;
+
 cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag, int* err,
                                   cudaStream_t stream) {
-  for (int j0 = 0; j0 < n; j0 += NB) {
-    potrf_diag_kernel<<<nmat, 256, 0, stream>>>(A, ld, stride, n, j0, Ldiag, err);
-    ++g_launches;
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    const int below = n - j0 - NB;
-    if (below <= 0) break;
-    trsm_panel_kernel<<<dim3((below + 127) / 128, nmat), 128, 0, stream>>>(A, ld, stride, n, j0);
-    ++g_launches;
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+  for (int J0 = 0; J0 < n; J0 += NB2) {
+    const int J1 = min(n, J0 + NB2);
+    for (int j0 = J0; j0 < J1; j0 += NB) {
+      potrf_diag_kernel<<<nmat, 256, 0, stream>>>(A, ld, stride, n, j0, Ldiag, err);
+      ++g_launches;
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+      const int below = n - j0 - NB;
+      if (below <= 0) break;
+      trsm_panel_kernel<<<dim3((below + 127) / 128, nmat), 128, 0, stream>>>(A, ld, stride, n, j0);
+      ++g_launches;
+      e = cudaGetLastError();
+      if (e != cudaSuccess) return e;
+      const int ncols = J1 - (j0 + NB);  // columns of this outer block right of the panel
+      if (ncols <= 0) continue;
+      DsyrkArgs u{};
+      u.A = A + (int64_t)(j0 + NB) + ld * (int64_t)j0;
+      u.lda = ld;
+      u.strideA = stride;
+      u.C = A + (int64_t)(j0 + NB) + ld * (int64_t)(j0 + NB);
+      u.ldc = ld;
+      u.strideC = stride;
+      u.n = below;
+      u.ncols = ncols;
+      u.kdim = NB;
+      u.batch = nmat;
+      u.D = nullptr;
+      e = launch_dsyrk_lower(u, stream);
+      if (e != cudaSuccess) return e;
+    }
+    const int trail = n - J1;
+    if (trail <= 0) break;
     DsyrkArgs u{};
-    u.A = A + (int64_t)(j0 + NB) + ld * (int64_t)j0;
+    u.A = A + (int64_t)J1 + ld * (int64_t)J0;
     u.lda = ld;
     u.strideA = stride;
-    u.C = A + (int64_t)(j0 + NB) + ld * (int64_t)(j0 + NB);
+    u.C = A + (int64_t)J1 + ld * (int64_t)J1;
     u.ldc = ld;
     u.strideC = stride;
-    u.n = below;
-    u.kdim = NB;
+    u.n = trail;
+    u.ncols = trail;
+    u.kdim = J1 - J0;
     u.batch = nmat;
     u.D = nullptr;
-    e = launch_dsyrk_lower(u, stream);
+    cudaError_t e = launch_dsyrk_lower(u, stream);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;

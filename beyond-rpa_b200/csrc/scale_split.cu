@@ -17,18 +17,24 @@ namespace rpa {
 namespace {
 constexpr int kTQ = 32;        // Q rows per CTA
 constexpr int kTA = 128;       // ai columns per chunk
-constexpr int kThreads = 256;  // 8 warps; warp w owns columns w, w+8, ...
-constexpr int kPerThread = kTA / 8;  // 16 columns per thread
-constexpr int kOutPitch = kTA + 8;   // bf16 elements per staged row (272 B)
+constexpr int kThreads = 256;  // 8 warps; warp w owns the ai pairs w, w+8, ..., w+56
+constexpr int kPairs = kTA / 2;
+constexpr int kPairsPerThread = kPairs / 8;  // 8 pairs = 16 columns per thread
+constexpr int kWordPitch = kPairs + 1;       // 65 words: conflict-free transposed staging
 
-__global__ void __launch_bounds__(kThreads) scale_split_kernel(
+__device__ __forceinline__ uint32_t bf162_bits(__nv_bfloat162 v) {
+  return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__global__ void __launch_bounds__(kThreads, 3) scale_split_kernel(
     const double* __restrict__ R, int64_t ldR, int NQ, int64_t nov, const double* __restrict__ D,
     FreqGroup fg, double alpha, __nv_bfloat16* __restrict__ Xhi, __nv_bfloat16* __restrict__ Xlo, int64_t pitch,
     int64_t kstride, double* __restrict__ diag_part, int64_t ai_per_split) {
-  __shared__ double sfac[kMaxKgLaunch][kTA];
-  __shared__ __align__(16) __nv_bfloat16 ohi[kTQ][kOutPitch];
-  __shared__ __align__(16) __nv_bfloat16 olo[kTQ][kOutPitch];
-  __shared__ double red[8][kTQ];
+  extern __shared__ double dyn_smem[];
+  auto sfac = reinterpret_cast<double(*)[kTA]>(dyn_smem);                          // [kMaxKgLaunch][kTA]
+  auto sdiag = reinterpret_cast<double(*)[kMaxKgLaunch][kTQ]>(dyn_smem + kMaxKgLaunch * kTA);  // [8][k][q]
+  auto ohi = reinterpret_cast<uint32_t(*)[kWordPitch]>(dyn_smem + kMaxKgLaunch * kTA + 8 * kMaxKgLaunch * kTQ);
+  auto olo = ohi + kTQ;  // per-warp partial diagonal sums above need no atomics
 
   const int t = threadIdx.x;
   const int qi = t & 31;
@@ -39,12 +45,10 @@ __global__ void __launch_bounds__(kThreads) scale_split_kernel(
   const int64_t a_begin = (int64_t)blockIdx.y * ai_per_split;
   const int64_t a_end = min(nov, a_begin + ai_per_split);
 
-  double dsum[kMaxKgLaunch];
-#pragma unroll
-  for (int k = 0; k < kMaxKgLaunch; ++k) dsum[k] = 0.0;
+  for (int k = 0; k < kMaxKgLaunch; ++k) sdiag[wa][k][qi] = 0.0;
 
   for (int64_t a0 = a_begin; a0 < a_end; a0 += kTA) {
-    // scaling factors of this chunk, FP64
+    // scaling factors sqrt(alpha D/(D^2+u^2)) of this chunk, FP64
     for (int idx = t; idx < kg * kTA; idx += kThreads) {
       const int k = idx / kTA, aj = idx % kTA;
       const int64_t a = a0 + aj;
@@ -55,60 +59,59 @@ __global__ void __launch_bounds__(kThreads) scale_split_kernel(
       }
       sfac[k][aj] = f;
     }
-    double r[kPerThread];
+    // R(q, a): a warp reads 32 consecutive Q of one column (coalesced)
+    double r[2 * kPairsPerThread];
 #pragma unroll
-    for (int i = 0; i < kPerThread; ++i) {
-      const int64_t a = a0 + wa + 8 * i;
-      r[i] = (q < NQ && a < a_end) ? __ldg(R + (int64_t)q + ldR * a) : 0.0;
-    }
+    for (int p = 0; p < kPairsPerThread; ++p)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int64_t a = a0 + 2 * (wa + 8 * p) + e;
+        r[2 * p + e] = (q < NQ && a < a_end) ? __ldg(R + (int64_t)q + ldR * a) : 0.0;
+      }
     __syncthreads();
 #pragma unroll 1
     for (int k = 0; k < kg; ++k) {
       double s = 0.0;
 #pragma unroll
-      for (int i = 0; i < kPerThread; ++i) {
-        const int aj = wa + 8 * i;
-        const double x = r[i] * sfac[k][aj];
-        const __nv_bfloat16 h = __double2bfloat16(x);
-        const __nv_bfloat16 l = __double2bfloat16(x - (double)__bfloat162float(h));
-        s = fma(x, x, s);
-        ohi[qi][aj] = h;
-        olo[qi][aj] = l;
+      for (int p = 0; p < kPairsPerThread; ++p) {
+        const int pw = wa + 8 * p;
+        const double x0 = r[2 * p] * sfac[k][2 * pw];
+        const double x1 = r[2 * p + 1] * sfac[k][2 * pw + 1];
+        s = fma(x0, x0, s);
+        s = fma(x1, x1, s);
+        // hi = bf16(x), lo = bf16(x - hi); x - hi is exact in FP32
+        const float f0 = (float)x0, f1 = (float)x1;
+        const __nv_bfloat162 h2 = __floats2bfloat162_rn(f0, f1);
+        const float2 hf = __bfloat1622float2(h2);
+        const __nv_bfloat162 l2 = __floats2bfloat162_rn(f0 - hf.x, f1 - hf.y);
+        ohi[qi][pw] = bf162_bits(h2);
+        olo[qi][pw] = bf162_bits(l2);
       }
-      // register-resident accumulator selected by a uniform branch
-#pragma unroll
-      for (int kk = 0; kk < kMaxKgLaunch; ++kk)
-        if (kk == k) dsum[kk] += s;
+      sdiag[wa][k][qi] += s;  // owned by this thread alone
       __syncthreads();
-      // rows of 16-byte vectors: 32 rows x 16 vectors per array
-      for (int v = t; v < kTQ * (kTA / 8); v += kThreads) {
-        const int row = v / (kTA / 8);
-        const int col = (v % (kTA / 8)) * 8;
-        const int64_t a = a0 + col;
+      // a warp stores 32 words (64 columns) of one row per instruction (128 B)
+      for (int idx = t; idx < kTQ * kPairs; idx += kThreads) {
+        const int row = idx / kPairs, w = idx % kPairs;
+        const int64_t a = a0 + 2 * w;
         if (q0 + row < NQ && a < nov) {
           const int64_t off = (int64_t)k * kstride + (int64_t)(q0 + row) * pitch + a;
-          *reinterpret_cast<uint4*>(Xhi + off) = *reinterpret_cast<const uint4*>(&ohi[row][col]);
-          *reinterpret_cast<uint4*>(Xlo + off) = *reinterpret_cast<const uint4*>(&olo[row][col]);
+          *reinterpret_cast<uint32_t*>(Xhi + off) = ohi[row][w];
+          *reinterpret_cast<uint32_t*>(Xlo + off) = olo[row][w];
         }
       }
       __syncthreads();
     }
   }
   // deterministic reduction of the 8 column owners of each row
-  for (int k = 0; k < kg; ++k) {
-    double v = 0.0;
+  __syncthreads();
+  for (int idx = t; idx < kg * kTQ; idx += kThreads) {
+    const int k = idx / kTQ, row = idx % kTQ;
+    if (q0 + row < NQ) {
+      double acc = 0.0;
 #pragma unroll
-    for (int kk = 0; kk < kMaxKgLaunch; ++kk)
-      if (kk == k) v = dsum[kk];
-    red[wa][qi] = v;
-    __syncthreads();
-    if (wa == 0 && q < NQ) {
-      double s = 0.0;
-#pragma unroll
-      for (int w = 0; w < 8; ++w) s += red[w][qi];
-      diag_part[((int64_t)blockIdx.y * kg + k) * NQ + q] = s;
+      for (int w = 0; w < 8; ++w) acc += sdiag[w][k][row];
+      diag_part[((int64_t)blockIdx.y * kg + k) * NQ + q0 + row] = acc;
     }
-    __syncthreads();
   }
 }
 
@@ -123,10 +126,12 @@ __global__ void diag_reduce_kernel(const double* __restrict__ diag_part, int nsp
 }  // namespace
 
 SplitPlan plan_scale_split(int NQ, int64_t nov, int num_sms) {
+  // Enough CTAs for ~16 waves of 2 resident CTAs per SM, so that the last
+  // partial wave costs little.
   SplitPlan p;
   p.qtiles = (NQ + kTQ - 1) / kTQ;
   const int64_t chunks = (nov + kTA - 1) / kTA;
-  int64_t want = (4 * (int64_t)num_sms + p.qtiles - 1) / p.qtiles;
+  int64_t want = (32 * (int64_t)num_sms + p.qtiles - 1) / p.qtiles;
   if (want < 1) want = 1;
   if (want > chunks) want = chunks;
   const int64_t chunks_per = (chunks + want - 1) / want;
@@ -136,12 +141,17 @@ SplitPlan plan_scale_split(int NQ, int64_t nov, int num_sms) {
   return p;
 }
 
+constexpr size_t kSplitSmem =
+    sizeof(double) * (kMaxKgLaunch * kTA + 8 * kMaxKgLaunch * kTQ) + sizeof(uint32_t) * 2 * kTQ * kWordPitch;
+
 cudaError_t launch_scale_split(const double* R, int64_t ldR, int NQ, int64_t nov, const double* D,
                                const FreqGroup& fg, double alpha, __nv_bfloat16* Xhi, __nv_bfloat16* Xlo,
                                int64_t pitch, int64_t kstride, double* diag_part, double* diag,
                                const SplitPlan& plan, cudaStream_t stream) {
   dim3 grid(plan.qtiles, plan.nsplit);
-  scale_split_kernel<<<grid, kThreads, 0, stream>>>(R, ldR, NQ, nov, D, fg, alpha, Xhi, Xlo, pitch, kstride,
+  cudaError_t e0 = cudaFuncSetAttribute(scale_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmem);
+  if (e0 != cudaSuccess) return e0;
+  scale_split_kernel<<<grid, kThreads, kSplitSmem, stream>>>(R, ldR, NQ, nov, D, fg, alpha, Xhi, Xlo, pitch, kstride,
                                                      diag_part, plan.ai_per_split);
   ++g_launches;
   cudaError_t e = cudaGetLastError();

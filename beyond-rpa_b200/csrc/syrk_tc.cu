@@ -8,15 +8,22 @@
 // 313-339, DGEMM real_abT_x of a 500-column block, repeated per frequency),
 // done as one lower-triangle SYRK per frequency over all ai at once.
 //
-// Persistent kernel, one CTA per SM, 192 threads:
+// Persistent kernel, one CTA per SM, 576 threads:
 //   warp 0      TMA producer (one elected lane)
 //   warp 1      TMEM allocator + MMA issuer (one elected lane)
-//   warps 2..5  epilogue: TMEM -> registers -> FP64 global stores
+//   warps 2..17 epilogue: TMEM -> registers -> FP64 global stores
+//               (warp w reads TMEM lanes 32*(w%4).. and 64 accumulator columns)
 // Work unit = (frequency k, 128-row tile tm, 256-column tile tn) with
-// tm*128 + 127 >= tn*256 (touches the lower triangle).  The 128 x 256 FP32
-// accumulator lives in TMEM; two accumulators (512 columns) let the epilogue
-// of one unit overlap the main loop of the next.  Smem pipeline: 4 stages of
-// {A_hi, A_lo (128x32), B_hi, B_lo (256x32)} bf16, 64-byte swizzle.
+// tm*128 + 127 >= tn*256 (touches the lower triangle).  Segmented
+// accumulation: the ai range of a unit is cut into segments of
+// `seg_chunks` x 32 columns; each segment accumulates into a fresh 128 x 256
+// FP32 TMEM accumulator (two of them, 512 columns, alternate), and the
+// epilogue warps add the segment partials in IEEE FP32 registers.  The
+// tensor-core accumulator rounds toward zero, so its relative bias grows
+// with the accumulation depth; segmenting bounds that depth (at NQ = 4096,
+// nov = 65536 an unsegmented accumulator biases E_c by ~1e-5 Eh).
+// Smem pipeline: 4 stages of {A_hi, A_lo (128x32), B_hi, B_lo (256x32)}
+// bf16, 64-byte swizzle.
 #include "kernels.h"
 
 namespace rpa {
@@ -27,10 +34,24 @@ constexpr int kStages = 4;
 constexpr int kATileBytes = TM * TK * 2;  // 8 KB
 constexpr int kBTileBytes = TN * TK * 2;  // 16 KB
 constexpr int kStageBytes = 2 * kATileBytes + 2 * kBTileBytes;  // 48 KB
-constexpr int kThreads = 192;
+constexpr int kThreads = 576;
+constexpr int kEpiWarps = 16;
+constexpr int kEpiCols = TN / 4;  // accumulator columns per epilogue warp
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kIdesc = umma_idesc_bf16_f32(TM, TN);
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align slack*/ + 256 /*barriers*/;
+
+// 32 lanes x 8 consecutive 32-bit TMEM columns per warp, added into acc[0..7]
+// (first == true: assigned).
+__device__ __forceinline__ void tmem_ld_add_x8(uint32_t taddr, float* acc, bool first) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc[i] = first ? __uint_as_float(r[i]) : acc[i] + __uint_as_float(r[i]);
+}
 
 struct UnitCoord {
   int k, tm, tn;
@@ -56,7 +77,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     syrk_split_bf16_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
                            const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
                            const SyrkTcArgs args, const int nblocks, const int ntm, const int nunits,
-                           const int nchunks) {
+                           const int nchunks, const int seg_chunks) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
@@ -77,7 +98,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b], 4);
+      mbar_init(&acc_empty[b], kEpiWarps);
     }
     mbar_init(drain, 1);
     fence_mbar_init();
@@ -104,8 +125,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       // ------------------------------------------------------------ producer
       int stage = 0;
       uint32_t phase = 0;
-      int issued_parity[kStages];
-      for (int s = 0; s < kStages; ++s) issued_parity[s] = -1;
+      uint32_t issued = 0, issued_par = 0;  // per-stage bit masks: issued, parity of the last issue
       bool ok = true;
       for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
         const UnitCoord c = decode_unit(u, nblocks, ntm);
@@ -120,7 +140,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           tma_load_3d(a_lo(stage), &tmA_lo, &full[stage], x, c.tm * TM, c.k);
           tma_load_3d(b_hi(stage), &tmB_hi, &full[stage], x, c.tn * TN, c.k);
           tma_load_3d(b_lo(stage), &tmB_lo, &full[stage], x, c.tn * TN, c.k);
-          issued_parity[stage] = (int)phase;
+          issued |= 1u << stage;
+          issued_par = (issued_par & ~(1u << stage)) | (phase << stage);
           if (++stage == kStages) {
             stage = 0;
             phase ^= 1u;
@@ -129,46 +150,52 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       // make sure no bulk copy is still landing in shared memory at exit
       for (int s = 0; s < kStages; ++s)
-        if (issued_parity[s] >= 0) mbar_wait(&full[s], (uint32_t)issued_parity[s], err, kDevTimeoutDrain);
+        if (issued & (1u << s)) mbar_wait(&full[s], (issued_par >> s) & 1u, err, kDevTimeoutDrain);
     }
   } else if (warp == 1) {
     if (lane == 0) {
       // ------------------------------------------------------------ MMA issuer
       int stage = 0;
       uint32_t phase = 0;
-      int it = 0;
+      int it = 0;  // segment counter (selects the TMEM accumulator)
       bool ok = true;
-      for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++it) {
-        const int b = it & 1;
-        const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
-        if (!mbar_wait(&acc_empty[b], acc_phase ^ 1u, err, kDevTimeoutAccEmpty)) break;
-        tc_fence_after();
-        const uint32_t d_tmem = tmem_base + (uint32_t)(b * TN);
-        for (int ch = 0; ch < nchunks; ++ch) {
-          if (!mbar_wait(&full[stage], phase, err, kDevTimeoutTmaFull)) {
+      for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+        for (int c0 = 0; c0 < nchunks && ok; c0 += seg_chunks, ++it) {
+          const int b = it & 1;
+          const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
+          if (!mbar_wait(&acc_empty[b], acc_phase ^ 1u, err, kDevTimeoutAccEmpty)) {
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t ah = smem_u32(a_hi(stage)), al = smem_u32(a_lo(stage));
-          const uint32_t bh = smem_u32(b_hi(stage)), bl = smem_u32(b_lo(stage));
+          const uint32_t d_tmem = tmem_base + (uint32_t)(b * TN);
+          const int c1 = min(nchunks, c0 + seg_chunks);
+          for (int ch = c0; ch < c1; ++ch) {
+            if (!mbar_wait(&full[stage], phase, err, kDevTimeoutTmaFull)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const uint32_t ah = smem_u32(a_hi(stage)), al = smem_u32(a_lo(stage));
+            const uint32_t bh = smem_u32(b_hi(stage)), bl = smem_u32(b_lo(stage));
 #pragma unroll
-          for (int kk = 0; kk < TK / 16; ++kk) {
-            const uint32_t off = (uint32_t)(kk * 32);  // 16 bf16 = 32 bytes along K
-            const uint64_t dah = umma_desc_k_sw64(ah + off), dal = umma_desc_k_sw64(al + off);
-            const uint64_t dbh = umma_desc_k_sw64(bh + off), dbl = umma_desc_k_sw64(bl + off);
-            tc_mma_bf16(d_tmem, dah, dbh, kIdesc, (ch > 0 || kk > 0) ? 1u : 0u);
-            tc_mma_bf16(d_tmem, dah, dbl, kIdesc, 1u);
-            tc_mma_bf16(d_tmem, dal, dbh, kIdesc, 1u);
+            for (int kk = 0; kk < TK / 16; ++kk) {
+              const uint32_t off = (uint32_t)(kk * 32);  // 16 bf16 = 32 bytes along K
+              const uint64_t dah = umma_desc_k_sw64(ah + off), dal = umma_desc_k_sw64(al + off);
+              const uint64_t dbh = umma_desc_k_sw64(bh + off), dbl = umma_desc_k_sw64(bl + off);
+              tc_mma_bf16(d_tmem, dah, dbh, kIdesc, (ch > c0 || kk > 0) ? 1u : 0u);
+              tc_mma_bf16(d_tmem, dah, dbl, kIdesc, 1u);
+              tc_mma_bf16(d_tmem, dal, dbh, kIdesc, 1u);
+            }
+            tc_commit(&empty[stage]);
+            if (++stage == kStages) {
+              stage = 0;
+              phase ^= 1u;
+            }
           }
-          tc_commit(&empty[stage]);
-          if (++stage == kStages) {
-            stage = 0;
-            phase ^= 1u;
-          }
+          if (!ok) break;
+          tc_commit(&acc_full[b]);
         }
-        if (!ok) break;
-        tc_commit(&acc_full[b]);
       }
       // drain: wait until every issued MMA has completed before TMEM is freed
       tc_commit(drain);
@@ -176,37 +203,47 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   } else {
     // -------------------------------------------------------------- epilogue
-    const int quarter = warp & 3;  // TMEM lanes quarter*32 .. +31
+    const int quarter = warp & 3;            // TMEM lanes quarter*32 .. +31
+    const int colq = (warp - 2) >> 2;        // accumulator columns colq*64 .. +63
     int it = 0;
-    for (int u = blockIdx.x; u < nunits; u += gridDim.x, ++it) {
-      const int b = it & 1;
-      const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
-      if (!mbar_wait(&acc_full[b], acc_phase, err, kDevTimeoutAccFull)) break;
-      tc_fence_after();
+    bool ok = true;
+    float run[kEpiCols];
+    for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
       const UnitCoord c = decode_unit(u, nblocks, ntm);
       const int m = c.tm * TM + quarter * 32 + lane;
       const int warp_max_m = c.tm * TM + quarter * 32 + 31;
-      double* Pk = args.Pi + (int64_t)c.k * args.piStride;
-      const double* dk = args.diag + (int64_t)c.k * args.NQ;
-      const double dm = (m < args.NQ) ? dk[m] : 0.0;
-#pragma unroll 1
-      for (int cc = 0; cc < TN; cc += 32) {
-        const int n0 = c.tn * TN + cc;
-        if (n0 > warp_max_m || n0 >= args.NQ) break;  // warp-uniform: rest is above the diagonal
-        float v[32];
-        tmem_ld_32x32b_x32(tmem_base + (uint32_t)(b * TN + cc) + ((uint32_t)(quarter * 32) << 16), v);
-        if (m < args.NQ) {
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int n = n0 + j;
-            if (n < m) Pk[(int64_t)m + (int64_t)n * args.ldPi] = (double)v[j];
-            else if (n == m) Pk[(int64_t)m + (int64_t)n * args.ldPi] = dm;
-          }
+      const int nbase = c.tn * TN + colq * kEpiCols;
+      for (int c0 = 0; c0 < nchunks; c0 += seg_chunks, ++it) {
+        const int b = it & 1;
+        const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
+        if (!mbar_wait(&acc_full[b], acc_phase, err, kDevTimeoutAccFull)) {
+          ok = false;
+          break;
         }
+        tc_fence_after();
+#pragma unroll
+        for (int cc = 0; cc < kEpiCols / 8; ++cc) {
+          const int n0 = nbase + cc * 8;
+          if (n0 <= warp_max_m && n0 < args.NQ)  // warp-uniform: skip columns above the diagonal
+            tmem_ld_add_x8(tmem_base + (uint32_t)(b * TN + colq * kEpiCols + cc * 8) + ((uint32_t)(quarter * 32) << 16),
+                           &run[cc * 8], c0 == 0);
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&acc_empty[b]);
       }
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&acc_empty[b]);
+      if (!ok) break;
+      if (m < args.NQ && nbase <= m) {
+        double* p = args.Pi + (int64_t)c.k * args.piStride + (int64_t)m + (int64_t)nbase * args.ldPi;
+        const int jd = m - nbase;  // column index of the diagonal element (may be >= kEpiCols)
+#pragma unroll
+        for (int j = 0; j < kEpiCols; ++j) {
+          if (j < jd) *p = (double)run[j];
+          p += args.ldPi;
+        }
+        if (jd < kEpiCols) args.Pi[(int64_t)c.k * args.piStride + (int64_t)m * (args.ldPi + 1)] =
+            args.diag[(int64_t)c.k * args.NQ + m];
+      }
     }
   }
   tc_fence_before();
@@ -228,16 +265,13 @@ cudaError_t launch_syrk_split_bf16(const CUtensorMap* tmA_hi, const CUtensorMap*
   const int nunits = nblocks * a.kg;
   const int nchunks = (int)((a.nov + TK - 1) / TK);
   if (nunits == 0 || nchunks == 0) return cudaSuccess;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e =
-        cudaFuncSetAttribute(syrk_split_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
+  cudaError_t e =
+      cudaFuncSetAttribute(syrk_split_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+  if (e != cudaSuccess) return e;
   const int grid = nunits < num_sms ? nunits : num_sms;
+  int seg_chunks = a.seg_chunks > 0 ? a.seg_chunks : nchunks;
   syrk_split_bf16_kernel<<<grid, kThreads, kSmemBytes, stream>>>(*tmA_hi, *tmA_lo, *tmB_hi, *tmB_lo, a, nblocks,
-                                                                  ntm, nunits, nchunks);
+                                                                  ntm, nunits, nchunks, seg_chunks);
   ++g_launches;
   return cudaGetLastError();
 }

@@ -18,6 +18,9 @@ SINGLE_SYSTEM = {
     # single-system split-BF16 vs FP64 workload: N_occ=64, N_virt=1024, NQ=4096, 16 points
     "single_4096": (4096, 64, 1024, 16, dict(occ_range=(-1.2, -0.3), virt_range=(0.02, 5.0), decay=512.0,
                                              scale=0.05, lam0=0.8)),
+    # a quarter-size single system (NQ = 2048, nov = 16384): profiling case that fits an ncu capture
+    "single_2048": (2048, 32, 512, 16, dict(occ_range=(-1.2, -0.3), virt_range=(0.02, 5.0), decay=256.0,
+                                            scale=0.05, lam0=0.8)),
     # seeded twin of the water dimer (10 occ incl. 2 core, 72 virt, NQ = 400, 12 points)
     "water_dimer_twin": (400, 8, 72, 12, dict(occ_range=(-1.3, -0.4), virt_range=(0.03, 4.0), decay=50.0,
                                               scale=1.0, lam0=0.8)),
