@@ -33,6 +33,7 @@ RPA_ERR_CUDA = 5
 RPA_ERR_TIMEOUT = 6
 RPA_ERR_NO_DEVICE = 7
 RPA_ERR_NOT_CONVERGED = 8
+RPA_ERR_TOO_LARGE = 9
 
 PREC_FP64 = 0
 PREC_SPLIT_BF16 = 1
@@ -80,6 +81,7 @@ def load_library(path: str | os.PathLike | None = None):
     lib.rpa_b200_ec_from_pi.argtypes = [_vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp]
     lib.rpa_b200_ec.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _dbl, _i64, _vp, _vp]
     lib.rpa_b200_freq_grid.argtypes = [_i64, _i64, _vp, _dbl, _dbl, _dbl, _i64, _vp, _vp, _vp]
+    lib.rpa_b200_ec_from_pi_noalloc.argtypes = [_i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp]
     if path is None:
         _lib = lib
     return lib

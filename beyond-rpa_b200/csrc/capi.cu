@@ -491,6 +491,7 @@ const char* rpa_b200_status_string(int status) {
     case RPA_ERR_TIMEOUT: return "device-side wait timed out";
     case RPA_ERR_NO_DEVICE: return "no sm_100 device";
     case RPA_ERR_NOT_CONVERGED: return "not converged";
+    case RPA_ERR_TOO_LARGE: return "problem exceeds the fixed scratch of the allocation-free entry point";
     default: return "unknown status";
   }
 }

@@ -36,7 +36,9 @@ typedef enum rpa_status {
   RPA_ERR_CUDA = 5,         /* CUDA runtime / driver error                    */
   RPA_ERR_TIMEOUT = 6,      /* a bounded device-side wait expired             */
   RPA_ERR_NO_DEVICE = 7,    /* no sm_100 GPU visible                          */
-  RPA_ERR_NOT_CONVERGED = 8 /* quadrature / eigen-solver did not converge     */
+  RPA_ERR_NOT_CONVERGED = 8, /* quadrature / eigen-solver did not converge    */
+  RPA_ERR_TOO_LARGE = 9      /* problem exceeds the fixed scratch of
+                                rpa_b200_ec_from_pi_noalloc                    */
 } rpa_status;
 
 /* Precision of the Pi(u) contraction. */
@@ -120,6 +122,31 @@ int rpa_b200_ec(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, con
 int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* OrbEnergies, double CoreOrbThresh,
                        double TargetError, double TargetRelError, int64_t NFixed, double* Freqs,
                        double* FreqWeights, int64_t* NFreqs);
+
+/*
+ * Allocation-free energy from given Pi(u) matrices.  No counterpart in the
+ * reference: it exists for callers that cannot allocate GPU memory (a host
+ * whose device memory belongs to a pool or arena it cannot grow, or code
+ * running while the device-memory footprint must not change).  Same result
+ * and arguments as rpa_b200_ec_from_pi, but no handle and no device
+ * allocation: the working storage is one fixed array of
+ * RPA_B200_NOALLOC_SCRATCH_BYTES (32 MiB) inside the library, which every GPU
+ * that loads the library holds until process exit.
+ *   - Limit: NFreqs*NQ*NQ + NFreqs*NQ + 4*NFreqs + 1 doubles must fit in the
+ *     array (NQ = 512 with NFreqs <= 15; NQ = 400 with NFreqs <= 26);
+ *     otherwise RPA_ERR_TOO_LARGE is returned before any GPU work.
+ *   - PiU and FreqWeights may be host or device pointers; Ec/Eu are host.
+ *   - stream: a cudaStream_t of `device`, or NULL for the default stream; the
+ *     call synchronises it before returning.
+ *   - All calls on a device share the array (contents persist between calls;
+ *     the call clears what must start at zero).  Calls that overlap on the GPU
+ *     race on it: serialise them.
+ *   - The first call on a device looks the array's address up once
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ */
+#define RPA_B200_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+int rpa_b200_ec_from_pi_noalloc(int64_t device, void* stream, int64_t NQ, int64_t NFreqs, const double* PiU,
+                                int64_t ldPi, const double* FreqWeights, double* Ec, double* Eu);
 
 #ifdef __cplusplus
 }
