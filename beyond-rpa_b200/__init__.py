@@ -82,6 +82,9 @@ def load_library(path: str | os.PathLike | None = None):
     lib.rpa_b200_ec.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _dbl, _i64, _vp, _vp]
     lib.rpa_b200_freq_grid.argtypes = [_i64, _i64, _vp, _dbl, _dbl, _dbl, _i64, _vp, _vp, _vp]
     lib.rpa_b200_ec_from_pi_noalloc.argtypes = [_i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp]
+    lib.rpa_b200_dring_t2.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _dbl, _i64, _i64,
+                                      _vp, ctypes.c_uint64, _dbl, _dbl, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _vp]
+    lib.rpa_b200_exchange_sosex.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _dbl, _i64, _vp]
     if path is None:
         _lib = lib
     return lib
@@ -108,7 +111,7 @@ def declared_functions() -> list[str]:
     """Function names declared by include/rpa_b200.h."""
     import re
     text = HEADER.read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(rpa_b200_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int64_t|int|const char\*)\s+(rpa_b200_\w+)\s*\(", text, re.M)))
 
 
 # ----------------------------------------------------------------------------- marshalling
@@ -226,6 +229,54 @@ class Handle:
         self._check(self.lib.rpa_b200_ec_from_pi(self._h, nq, K, p.ptr, nq, w.ptr, ctypes.byref(ec),
                                                  eu.ctypes.data))
         return ec.value, eu
+
+    # ------------------------------------------------------------------ beyond RPA
+    def dring_t2(self, R, eps_o, eps_v, freqs, weights, alpha=4.0, prec="fp64", guess=None, n_guess=None, seed=0,
+                 small_cutoff=1e-10, cutoff_thresh=1e-4, cutoff_type=0, common_thresh=-1.0, max_vecs=None):
+        """Direct-ring T2 = U diag(A) U^T (rpa_b200_dring_t2).  guess: (nov, G) guess vectors or None.
+
+        Returns dict(A, U (nov x NT), EigRPA, NT, common_thresh, Ec)."""
+        nq = int(R.shape[0])
+        no, nv, K = len(eps_o), len(eps_v), len(freqs)
+        nov = no * nv
+        r = _colmajor(R, nq)
+        eo, ev, fr, w = _vec(eps_o), _vec(eps_v), _vec(freqs), _vec(weights)
+        if guess is not None:
+            gm = _colmajor(guess, nov)
+            G = int(guess.shape[1])
+            gptr = gm.ptr
+        else:
+            gm = None
+            G = int(n_guess if n_guess is not None else min(int(np.ceil(3.0 * nq)), nov))
+            gptr = None
+        cap = int(max_vecs or G)
+        A = np.zeros(cap)
+        eig = np.zeros(cap)
+        U = np.zeros((nov, cap), order="F")
+        nt = ctypes.c_int64()
+        ct = ctypes.c_double(common_thresh)
+        ec = ctypes.c_double()
+        self._check(self.lib.rpa_b200_dring_t2(self._h, nq, no, nv, r.ptr, r.ld, eo.ptr, ev.ptr, K, fr.ptr, w.ptr,
+                                               float(alpha), _PREC[prec], G, gptr, int(seed), float(small_cutoff),
+                                               float(cutoff_thresh), int(cutoff_type), ctypes.byref(ct), cap,
+                                               A.ctypes.data, U.ctypes.data, nov, ctypes.byref(nt),
+                                               eig.ctypes.data, ctypes.byref(ec)))
+        n = nt.value
+        return {"A": A[:n].copy(), "U": np.asfortranarray(U[:, :n]), "EigRPA": eig[:n].copy(), "NT": n,
+                "common_thresh": ct.value, "Ec": ec.value}
+
+    def exchange_sosex(self, R, nocc, nvirt, U, A, alpha=1.0, s2_operator=False):
+        """SOSEX exchange energy -alpha sum (aj|bi) T_aibj (rpa_b200_exchange_sosex)."""
+        nq = int(R.shape[0])
+        nov = nocc * nvirt
+        r = _colmajor(R, nq)
+        u = _colmajor(U, nov)
+        a = _vec(A)
+        ex = ctypes.c_double()
+        self._check(self.lib.rpa_b200_exchange_sosex(self._h, nq, nocc, nvirt, r.ptr, r.ld, int(U.shape[1]), u.ptr,
+                                                     u.ld, a.ptr, float(alpha), int(bool(s2_operator)),
+                                                     ctypes.byref(ex)))
+        return ex.value
 
     def ec_rpa(self, R, eps_o, eps_v, freqs, weights, alpha=4.0, prec="split"):
         """Fused Pi build + energy: returns (E_c, E(u))."""

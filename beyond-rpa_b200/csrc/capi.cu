@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -34,6 +35,8 @@ struct rpa_b200_handle {
   cudaStream_t own_stream = nullptr;  // the handle's own stream
   std::string last_error;
   DevBuf R, D, eps, Xhi, Xlo, diag_part, diag, Pi, Ldiag, ddbuf;
+  // direct-ring T2 / exchange workspace
+  DevBuf tZ, tOm, tIOm, tP, tS, tV, tT, tTIT, tVt, tW, tU, tRU, tSmall, tRot, tPerm;
   int* err_dev = nullptr;    // device error word
   int* count_dev = nullptr;  // non-finite counter
   PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -385,6 +388,196 @@ int energy_from_workspace(rpa_b200_handle* h, int NQ, int K, const std::vector<d
   return RPA_OK;
 }
 
+
+// ------------------------------------------------------------------ direct-ring T2
+// I(1) M = -(1/4pi) sum_k Z_k^T (Z_k M),  Z_k = sqrt(w_k) L_k^{-1} R diag(chi_k),
+// chi_k = -alpha D/(D^2+u_k^2), L_k the Cholesky factor of 1 + Pi_k (kept in h->Pi
+// by the energy step).  This is rpa_CC_IM_v5 (src/rpa/rpa_CC_Doubles.f90:369-422)
+// with Q diag(1/(1+pi)) Q^T = (1+Pi)^{-1} = L^{-T} L^{-1}: no eigen-decomposition
+// of Pi(u) is needed for lambda = 1.
+struct T2Ctx {
+  int NQ, K;
+  int64_t nov;
+  const double* R;
+  int64_t ldR;
+  double alpha;
+  std::vector<double> u2, w;
+  int zk;             // frequencies per Z group
+  bool z_resident;    // all groups built once
+};
+
+int build_z_group(rpa_b200_handle* h, const T2Ctx& c, int g0, int n, double* Z) {
+  rpa::ChiGroup cg{};
+  cg.n = n;
+  cg.alpha = c.alpha;
+  for (int k = 0; k < n; ++k) {
+    cg.u2[k] = c.u2[g0 + k];
+    cg.sqrtw[k] = std::sqrt(c.w[g0 + k]);
+  }
+  const int64_t ldz = (int64_t)n * c.NQ;
+  RPA_CUDA(h, rpa::launch_chi_scale(c.R, c.ldR, c.NQ, c.nov, static_cast<const double*>(h->D.p), cg, Z, ldz,
+                                    h->stream));
+  // L_k^{-1} on rows k*NQ.. of Z (batched over the group's frequencies)
+  const double* L = static_cast<const double*>(h->Pi.p) + (int64_t)g0 * c.NQ * c.NQ;
+  RPA_CUDA(h, rpa::launch_trsm_lower_left(L, c.NQ, (int64_t)c.NQ * c.NQ, Z, ldz, c.NQ, c.NQ, (int)c.nov, n,
+                                          h->stream));
+  return RPA_OK;
+}
+
+// out (nov x ncols, ld nov) = I M (M: nov x ncols, ld nov)
+int apply_I(rpa_b200_handle* h, const T2Ctx& c, const double* M, int ncols, double* out) {
+  double* Z = static_cast<double*>(h->tZ.p);
+  double* P = static_cast<double*>(h->tP.p);
+  bool first = true;
+  for (int g0 = 0; g0 < c.K; g0 += c.zk) {
+    const int n = std::min(c.zk, c.K - g0);
+    const int64_t ldz = (int64_t)n * c.NQ;
+    double* Zg = c.z_resident ? Z + (int64_t)g0 * c.NQ * c.nov : Z;
+    if (!c.z_resident) {
+      int s = build_z_group(h, c, g0, n, Zg);
+      if (s != RPA_OK) return s;
+    }
+    rpa::GemmF64Args g{};
+    g.M = (int)ldz;
+    g.N = ncols;
+    g.K = c.nov;
+    g.A = Zg;
+    g.a_m = 1;
+    g.a_k = ldz;
+    g.B = M;
+    g.b_k = 1;
+    g.b_n = c.nov;
+    g.C = P;
+    g.ldc = ldz;
+    g.alpha = 1.0;
+    g.beta = 0.0;
+    g.batch = 1;
+    RPA_CUDA(h, rpa::launch_gemm_f64(g, h->stream));
+    rpa::GemmF64Args g2{};
+    g2.M = (int)c.nov;
+    g2.N = ncols;
+    g2.K = ldz;
+    g2.A = Zg;
+    g2.a_m = ldz;
+    g2.a_k = 1;
+    g2.B = P;
+    g2.b_k = 1;
+    g2.b_n = ldz;
+    g2.C = out;
+    g2.ldc = c.nov;
+    g2.alpha = -1.0 / (4.0 * kPi);
+    g2.beta = first ? 0.0 : 1.0;
+    g2.batch = 1;
+    RPA_CUDA(h, rpa::launch_gemm_f64(g2, h->stream));
+    first = false;
+  }
+  return RPA_OK;
+}
+
+// Normalise the columns of X (rows x cols, ld rows) on the device.
+int normalize_columns(rpa_b200_handle* h, double* X, int64_t rows, int cols) {
+  double* nrm = static_cast<double*>(h->tSmall.p);
+  RPA_CUDA(h, rpa::launch_col_sqnorm(X, rows, cols, rows, nrm, h->stream));
+  RPA_CUDA(h, rpa::launch_scale_cols(X, rows, cols, rows, nrm, true, h->stream));
+  return RPA_OK;
+}
+
+// Symmetric eigen-decomposition of A (n x n, ld n) by parallel Jacobi sweeps:
+// on return V holds the eigenvectors (unsorted), evals the eigenvalues and
+// order the permutation that sorts them ascending.
+int jacobi_eig(rpa_b200_handle* h, double* A, double* V, int n, std::vector<double>& evals, std::vector<int>& order) {
+  RPA_CUDA(h, rpa::launch_set_identity(V, n, n, h->stream));
+  double4* rot = static_cast<double4*>(h->tRot.p);
+  double* red = static_cast<double*>(h->tSmall.p);
+  // one sweep = (m-1) rounds x 2 kernels: captured once, replayed per sweep
+  cudaGraphExec_t exec = nullptr;
+  const int64_t before = rpa::g_launches;
+  int64_t per_sweep = 0;
+  {
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+      cudaError_t e = rpa::launch_jacobi_sweep(A, n, V, n, n, rot, h->stream);
+      cudaError_t e2 = cudaStreamEndCapture(h->stream, &graph);
+      per_sweep = rpa::g_launches - before;
+      rpa::g_launches = before;
+      if (e != cudaSuccess || e2 != cudaSuccess || !graph || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+        exec = nullptr;
+      if (graph) cudaGraphDestroy(graph);
+    }
+    cudaGetLastError();
+  }
+  bool converged = false;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double od[2];
+    RPA_CUDA(h, rpa::launch_offdiag(A, n, n, red, h->stream));
+    RPA_CUDA(h, cudaMemcpyAsync(od, red, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (!(std::isfinite(od[0]) && std::isfinite(od[1]))) break;
+    if (std::sqrt(od[0]) <= 1e-14 * std::sqrt(od[0] + od[1]) || od[0] == 0.0) {
+      converged = true;
+      break;
+    }
+    if (exec) {
+      RPA_CUDA(h, cudaGraphLaunch(exec, h->stream));
+      rpa::g_launches += per_sweep;
+    } else {
+      RPA_CUDA(h, rpa::launch_jacobi_sweep(A, n, V, n, n, rot, h->stream));
+    }
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (!converged) return fail(h, RPA_ERR_NOT_CONVERGED, "Jacobi eigensolver did not converge (n=%d)", n);
+  evals.resize(n);
+  RPA_CUDA(h, cudaMemcpy2DAsync(evals.data(), sizeof(double), A, (size_t)(n + 1) * sizeof(double), sizeof(double),
+                                (size_t)n, cudaMemcpyDeviceToHost, h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  order.resize(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return evals[a] < evals[b]; });
+  return RPA_OK;
+}
+
+// dst(:, j) = src(:, cols[j]) * scale[j] on the device (cols/scale from the host)
+int gather(rpa_b200_handle* h, const double* src, int64_t rows, double* dst, const std::vector<int>& cols,
+           const std::vector<double>* scale) {
+  const int nc = (int)cols.size();
+  if (nc == 0) return RPA_OK;
+  int* perm = static_cast<int*>(h->tPerm.p);
+  double* sc = static_cast<double*>(h->tSmall.p);
+  RPA_CUDA(h, cudaMemcpyAsync(perm, cols.data(), (size_t)nc * sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  if (scale)
+    RPA_CUDA(h, cudaMemcpyAsync(sc, scale->data(), (size_t)nc * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  RPA_CUDA(h, rpa::launch_gather_cols(src, rows, dst, rows, rows, nc, perm, scale ? sc : nullptr, h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));  // host vectors must outlive the copies
+  return RPA_OK;
+}
+
+rpa::GemmF64Args gemm_nn(int M, int N, int64_t K, const double* A, int64_t lda, const double* B, int64_t ldb,
+                         double* C, int64_t ldc) {
+  rpa::GemmF64Args g{};
+  g.M = M;
+  g.N = N;
+  g.K = K;
+  g.A = A;
+  g.a_m = 1;
+  g.a_k = lda;
+  g.B = B;
+  g.b_k = 1;
+  g.b_n = ldb;
+  g.C = C;
+  g.ldc = ldc;
+  g.alpha = 1.0;
+  g.beta = 0.0;
+  g.batch = 1;
+  return g;
+}
+rpa::GemmF64Args gemm_tn(int M, int N, int64_t K, const double* A, int64_t lda, const double* B, int64_t ldb,
+                         double* C, int64_t ldc) {
+  rpa::GemmF64Args g = gemm_nn(M, N, K, A, lda, B, ldb, C, ldc);
+  g.a_m = lda;
+  g.a_k = 1;
+  return g;
+}
+
 float elapsed(cudaEvent_t a, cudaEvent_t b) {
   float ms = 0.f;
   if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
@@ -467,7 +660,9 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->own_stream) cudaStreamSynchronize(h->own_stream);
-  for (DevBuf* b : {&h->R, &h->D, &h->eps, &h->Xhi, &h->Xlo, &h->diag_part, &h->diag, &h->Pi, &h->Ldiag, &h->ddbuf})
+  for (DevBuf* b : {&h->R, &h->D, &h->eps, &h->Xhi, &h->Xlo, &h->diag_part, &h->diag, &h->Pi, &h->Ldiag, &h->ddbuf,
+                    &h->tZ, &h->tOm, &h->tIOm, &h->tP, &h->tS, &h->tV, &h->tT, &h->tTIT, &h->tVt, &h->tW, &h->tU,
+                    &h->tRU, &h->tSmall, &h->tRot, &h->tPerm})
     release(*b);
   if (h->err_dev) cudaFree(h->err_dev);
   if (h->count_dev) cudaFree(h->count_dev);
@@ -595,6 +790,239 @@ int rpa_b200_ec(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, con
   if ((s = build_pi(h, v, Rd, ldd, alpha, prec))) return s;
   if ((s = energy_from_workspace(h, v.NQ, v.K, v.weights, Ec, Eu))) return s;
   RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+  finish_timings(h);
+  return RPA_OK;
+}
+
+
+int rpa_b200_dring_t2(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R, int64_t ldR,
+                      const double* OccEnergies, const double* VirtEnergies, int64_t NFreqs, const double* Freqs,
+                      const double* FreqWeights, double alpha, int64_t prec, int64_t GuessNVecs, const double* Omega,
+                      uint64_t seed, double SmallEigenvalsCutoff, double CutoffThresh, int64_t CutoffType,
+                      double* CommonThresh, int64_t MaxNVecsT2, double* A, double* U, int64_t ldU,
+                      int64_t* NVecsT2, double* EigRPA, double* Ec) {
+  int s = begin_call(h);
+  if (s != RPA_OK) return s;
+  Validated v;
+  if ((s = validate_common(h, NQ, NOcc, NVirt, R, ldR, OccEnergies, VirtEnergies, NFreqs, Freqs, alpha, prec, v)))
+    return s;
+  if (!FreqWeights || !CommonThresh || !A || !U || !NVecsT2 || !EigRPA || MaxNVecsT2 < 1 || GuessNVecs < 1 ||
+      ldU < NOcc * NVirt)
+    return fail(h, RPA_ERR_INVALID_ARG, "invalid T2 output arguments");
+  if (CutoffType < 0 || CutoffType > 3) return fail(h, RPA_ERR_INVALID_ARG, "unknown T2 cutoff type");
+  if ((s = fetch_small(h, FreqWeights, NFreqs, v.weights))) return s;
+  const double* Rd;
+  int64_t ldd;
+  if ((s = stage_R(h, v, R, ldR, &Rd, &ldd))) return s;
+  RPA_CUDA(h, cudaEventRecord(h->ev[1], h->stream));
+  if ((s = build_pi(h, v, Rd, ldd, alpha, prec))) return s;
+  double ec = 0.0;
+  if ((s = energy_from_workspace(h, v.NQ, v.K, v.weights, &ec, nullptr))) return s;  // leaves L_k in h->Pi
+  if (Ec) *Ec = ec;
+
+  T2Ctx c;
+  c.NQ = v.NQ;
+  c.K = v.K;
+  c.nov = v.nov;
+  c.R = Rd;
+  c.ldR = ldd;
+  c.alpha = alpha;
+  for (int k = 0; k < v.K; ++k) {
+    c.u2.push_back(v.freqs[k] * v.freqs[k]);
+    c.w.push_back(v.weights[k]);
+  }
+  const int G = (int)GuessNVecs;
+  const int64_t nov = v.nov;
+  size_t freeB = 0, totalB = 0;
+  RPA_CUDA(h, cudaMemGetInfo(&freeB, &totalB));
+  const size_t zAll = (size_t)v.K * v.NQ * nov * 8;
+  const size_t fixed = (size_t)nov * G * 8 * 3 + (size_t)G * G * 8 * 2;
+  c.z_resident = zAll + fixed < (size_t)(0.8 * (double)(freeB + h->tZ.bytes));
+  c.zk = c.z_resident ? v.K : std::max(1, (int)std::min<size_t>(v.K, (size_t)(0.4 * freeB) / ((size_t)v.NQ * nov * 8)));
+  RPA_CUDA(h, ensure(h->tZ, (size_t)c.zk * v.NQ * nov * 8 * (c.z_resident ? 1 : 1)));
+  if (c.z_resident) RPA_CUDA(h, ensure(h->tZ, zAll));
+  RPA_CUDA(h, ensure(h->tP, (size_t)c.zk * v.NQ * G * 8));
+  RPA_CUDA(h, ensure(h->tOm, (size_t)nov * G * 8));
+  RPA_CUDA(h, ensure(h->tIOm, (size_t)nov * G * 8));
+  RPA_CUDA(h, ensure(h->tS, (size_t)G * G * 8));
+  RPA_CUDA(h, ensure(h->tV, (size_t)G * G * 8));
+  RPA_CUDA(h, ensure(h->tSmall, (size_t)std::max<int64_t>(G, 64) * 8 + 64));
+  RPA_CUDA(h, ensure(h->tRot, (size_t)(G / 2 + 2) * sizeof(double4)));
+  RPA_CUDA(h, ensure(h->tPerm, (size_t)G * sizeof(int)));
+  if (c.z_resident)
+    for (int g0 = 0; g0 < v.K; g0 += c.zk)
+      if ((s = build_z_group(h, c, g0, std::min(c.zk, v.K - g0), static_cast<double*>(h->tZ.p)))) return s;
+
+  // guess vectors (rpa_CC_Doubles.f90:746-763): given, or uniform [-1/2, 1/2) from the seed
+  double* Om = static_cast<double*>(h->tOm.p);
+  double* IOm = static_cast<double*>(h->tIOm.p);
+  if (Omega) {
+    RPA_CUDA(h, cudaMemcpyAsync(Om, Omega, (size_t)nov * G * 8, cudaMemcpyDefault, h->stream));
+  } else {
+    RPA_CUDA(h, rpa::launch_fill_uniform(Om, nov, G, nov, seed, h->stream));
+  }
+  if ((s = normalize_columns(h, Om, nov, G))) return s;
+  if ((s = apply_I(h, c, Om, G, IOm))) return s;
+  if ((s = normalize_columns(h, IOm, nov, G))) return s;
+  // S = IOm^T IOm, eigenvalues above the linear-dependency cutoff (771-795)
+  double* S = static_cast<double*>(h->tS.p);
+  double* Vs = static_cast<double*>(h->tV.p);
+  RPA_CUDA(h, rpa::launch_gemm_f64(gemm_tn(G, G, nov, IOm, nov, IOm, nov, S, G), h->stream));
+  RPA_CUDA(h, rpa::launch_symmetrize_avg(S, G, G, h->stream));
+  std::vector<double> sval;
+  std::vector<int> sord;
+  if ((s = jacobi_eig(h, S, Vs, G, sval, sord))) return s;
+  int NT = 0;
+  for (int i = G - 1; i >= 0; --i) {
+    if (sval[sord[i]] > SmallEigenvalsCutoff) ++NT;
+    else break;
+  }
+  if (NT == 0) return fail(h, RPA_ERR_NOT_CONVERGED, "no T2 guess direction above the linear-dependency cutoff");
+  std::vector<int> wcols(NT);
+  std::vector<double> wscale(NT);
+  for (int j = 0; j < NT; ++j) {
+    wcols[j] = sord[G - NT + j];
+    wscale[j] = 1.0 / std::sqrt(sval[wcols[j]]);
+  }
+  RPA_CUDA(h, ensure(h->tW, (size_t)G * NT * 8));
+  RPA_CUDA(h, ensure(h->tT, (size_t)nov * NT * 8));
+  double* W = static_cast<double*>(h->tW.p);
+  double* T = static_cast<double*>(h->tT.p);
+  if ((s = gather(h, Vs, G, W, wcols, &wscale))) return s;
+  RPA_CUDA(h, rpa::launch_gemm_f64(gemm_nn((int)nov, NT, G, IOm, nov, W, G, T, nov), h->stream));
+  // Rayleigh-Ritz: TIT = T^T I T (rpa_CC_MIM_v5, 425-488), eigenpairs (797-808)
+  double* IT = Om;  // guess vectors no longer needed
+  if ((s = apply_I(h, c, T, NT, IT))) return s;
+  RPA_CUDA(h, ensure(h->tTIT, (size_t)NT * NT * 8));
+  RPA_CUDA(h, ensure(h->tVt, (size_t)NT * NT * 8));
+  double* TIT = static_cast<double*>(h->tTIT.p);
+  double* Vt = static_cast<double*>(h->tVt.p);
+  RPA_CUDA(h, rpa::launch_gemm_f64(gemm_tn(NT, NT, nov, T, nov, IT, nov, TIT, NT), h->stream));
+  RPA_CUDA(h, rpa::launch_symmetrize_avg(TIT, NT, NT, h->stream));
+  std::vector<double> aval;
+  std::vector<int> aord;
+  if ((s = jacobi_eig(h, TIT, Vt, NT, aval, aord))) return s;
+  std::vector<double> Aall(NT);
+  for (int i = 0; i < NT; ++i) {
+    const double a = aval[aord[i]];
+    Aall[i] = 0.5 * (a / (a + 1.0));
+  }
+  // eigenvalue cutoff (rpa_THC_CC_T2, 855-945); supersystem when *CommonThresh < 0
+  double K = 0.0;
+  if (*CommonThresh < 0.0) {
+    switch (CutoffType) {
+      case 0: K = CutoffThresh; break;
+      case 1: {
+        double mx = 0.0;
+        for (double a : Aall) mx = std::max(mx, std::fabs(a));
+        K = CutoffThresh * mx;
+        break;
+      }
+      case 2: K = CutoffThresh / (double)(NOcc * 2); break;
+      case 3: {
+        K = 0.0;
+        for (int i = 0; i + 1 < NT; ++i) {
+          double sum = 0.0;
+          for (int j = i + 1; j < NT; ++j) sum += Aall[j];
+          if (std::fabs(sum) < CutoffThresh) {
+            K = std::fabs(Aall[i + 1]);
+            break;
+          }
+        }
+        break;
+      }
+    }
+  } else {
+    K = *CommonThresh;
+  }
+  int keep = 0;
+  for (int i = 0; i < NT; ++i) {
+    if (std::fabs(Aall[i]) > K) keep = i + 1;
+    else break;
+  }
+  if (keep == 0) return fail(h, RPA_ERR_NOT_CONVERGED, "Invalid T2CutoffThresh: no eigenvectors left after cutoff");
+  if (keep > MaxNVecsT2) return fail(h, RPA_ERR_INVALID_ARG, "%d T2 eigenvectors exceed MaxNVecsT2", keep);
+  std::vector<int> tcols(aord.begin(), aord.begin() + keep);
+  if ((s = gather(h, Vt, NT, W, tcols, nullptr))) return s;  // W reused: NT x keep
+  RPA_CUDA(h, ensure(h->tU, (size_t)nov * keep * 8));
+  double* Ud = static_cast<double*>(h->tU.p);
+  RPA_CUDA(h, rpa::launch_gemm_f64(gemm_nn((int)nov, keep, NT, T, nov, W, NT, Ud, nov), h->stream));
+  // EigRPA(mu) = 2 A_mu |R U_mu|^2 (rpa_T2_EigRPA, 987-1009)
+  RPA_CUDA(h, ensure(h->tRU, (size_t)v.NQ * keep * 8));
+  double* RU = static_cast<double*>(h->tRU.p);
+  RPA_CUDA(h, rpa::launch_gemm_f64(gemm_nn(v.NQ, keep, nov, Rd, ldd, Ud, nov, RU, v.NQ), h->stream));
+  double* nrm = static_cast<double*>(h->tSmall.p);
+  RPA_CUDA(h, rpa::launch_col_sqnorm(RU, v.NQ, keep, v.NQ, nrm, h->stream));
+  std::vector<double> n2(keep);
+  RPA_CUDA(h, cudaMemcpyAsync(n2.data(), nrm, (size_t)keep * 8, cudaMemcpyDeviceToHost, h->stream));
+  const cudaMemcpyKind kind = is_device_ptr(U) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  RPA_CUDA(h, cudaMemcpy2DAsync(U, (size_t)ldU * 8, Ud, (size_t)nov * 8, (size_t)nov * 8, (size_t)keep, kind,
+                                h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  if ((s = check_device_error(h))) return s;
+  for (int i = 0; i < keep; ++i) {
+    A[i] = Aall[i];
+    EigRPA[i] = 2.0 * Aall[i] * n2[i];
+  }
+  *NVecsT2 = keep;
+  if (*CommonThresh < 0.0) *CommonThresh = K;
+  finish_timings(h);
+  return RPA_OK;
+}
+
+int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R,
+                            int64_t ldR, int64_t NVecsT2, const double* U, int64_t ldU, const double* A, double Alpha,
+                            int64_t S2Operator, double* Ex) {
+  int s = begin_call(h);
+  if (s != RPA_OK) return s;
+  const int64_t nov = NOcc * NVirt;
+  if (NQ < 1 || NOcc < 1 || NVirt < 1 || NVecsT2 < 1 || ldR < NQ || ldU < nov || !R || !U || !A || !Ex)
+    return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_exchange_sosex");
+  const int NT = (int)NVecsT2;
+  std::vector<double> Ah;
+  if ((s = fetch_small(h, A, NT, Ah))) return s;
+  std::vector<double> B(NT);
+  for (int m = 0; m < NT; ++m) {
+    B[m] = S2Operator ? Ah[m] / (1.0 - 4.0 * Ah[m] * Ah[m]) : Ah[m];
+    if (!std::isfinite(B[m])) return fail(h, RPA_ERR_NONFINITE, "non-finite T2 eigenvalue");
+  }
+  // stage R and U on the device
+  const double* Rd = R;
+  int64_t ldr = ldR;
+  if (!is_device_ptr(R)) {
+    RPA_CUDA(h, ensure(h->R, (size_t)NQ * nov * 8));
+    RPA_CUDA(h, cudaMemcpy2DAsync(h->R.p, (size_t)NQ * 8, R, (size_t)ldR * 8, (size_t)NQ * 8, (size_t)nov,
+                                  cudaMemcpyHostToDevice, h->stream));
+    Rd = static_cast<const double*>(h->R.p);
+    ldr = NQ;
+  }
+  const double* Ud = U;
+  int64_t ldu = ldU;
+  if (!is_device_ptr(U)) {
+    RPA_CUDA(h, ensure(h->tU, (size_t)nov * NT * 8));
+    RPA_CUDA(h, cudaMemcpy2DAsync(h->tU.p, (size_t)nov * 8, U, (size_t)ldU * 8, (size_t)nov * 8, (size_t)NT,
+                                  cudaMemcpyHostToDevice, h->stream));
+    Ud = static_cast<const double*>(h->tU.p);
+    ldu = nov;
+  }
+  const int64_t np = rpa::sosex_partials((int)NQ, (int)NOcc, NT);
+  RPA_CUDA(h, ensure(h->tSmall, (size_t)(NT + np) * 8));
+  double* Bd = static_cast<double*>(h->tSmall.p);
+  double* part = Bd + NT;
+  RPA_CUDA(h, cudaMemcpyAsync(Bd, B.data(), (size_t)NT * 8, cudaMemcpyHostToDevice, h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[1], h->stream));
+  int64_t npart = 0;
+  RPA_CUDA(h, rpa::launch_sosex(Rd, ldr, (int)NQ, (int)NOcc, (int)NVirt, Ud, ldu, NT, Bd, part, &npart, h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
+  std::vector<double> hp((size_t)npart);
+  RPA_CUDA(h, cudaMemcpyAsync(hp.data(), part, (size_t)npart * 8, cudaMemcpyDeviceToHost, h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  dd acc{0.0, 0.0};
+  for (double x : hp) acc = rpa::dd_add(acc, x);
+  *Ex = -Alpha * (acc.hi + acc.lo);
   finish_timings(h);
   return RPA_OK;
 }

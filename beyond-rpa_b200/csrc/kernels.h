@@ -104,4 +104,56 @@ cudaError_t launch_count_nonfinite(const double* x, int64_t n, int* count, cudaS
 cudaError_t launch_copy_lower(const double* src, int64_t lds, int64_t strideS, double* dst, int64_t ldd,
                               int64_t strideD, int n, int nmat, cudaStream_t stream);
 
+// ---------------------------------------------------------------- generic FP64 GEMM
+// C_b(m,n) = alpha * rowscale(m) * sum_k A_b(m,k) kscale_b(k) B_b(k,n) + beta * C_b(m,n)
+struct GemmF64Args {
+  int M, N;
+  int64_t K;
+  const double* A;
+  int64_t a_m, a_k, sA;  // element strides of A (one of a_m, a_k should be 1)
+  const double* B;
+  int64_t b_k, b_n, sB;
+  double* C;
+  int64_t ldc, sC;       // C column-major
+  double alpha, beta;
+  const double* kscale;  // optional, per k (stride ks_stride per batch)
+  int64_t ks_stride;
+  const double* rowscale;  // optional, per m
+  int batch;
+};
+cudaError_t launch_gemm_f64(const GemmF64Args& g, cudaStream_t stream);
+
+// ---------------------------------------------------------------- T2 chain
+// Batched forward substitution L_b X_b = B_b in place (L lower, column-major).
+cudaError_t launch_trsm_lower_left(const double* L, int64_t ldl, int64_t sL, double* X, int64_t ldx, int64_t sX,
+                                   int n, int ncols, int batch, cudaStream_t stream);
+// One sweep (m-1 rounds) of the parallel two-sided Jacobi method: A <- J^T A J, V <- V J.
+cudaError_t launch_jacobi_sweep(double* A, int64_t lda, double* V, int64_t ldv, int n, double4* rot,
+                                cudaStream_t stream);
+cudaError_t launch_offdiag(const double* A, int64_t lda, int n, double* out, cudaStream_t stream);
+cudaError_t launch_set_identity(double* V, int64_t ldv, int n, cudaStream_t stream);
+cudaError_t launch_fill_uniform(double* X, int64_t rows, int64_t cols, int64_t ldx, uint64_t seed,
+                                cudaStream_t stream);
+cudaError_t launch_col_sqnorm(const double* X, int64_t rows, int64_t cols, int64_t ldx, double* out,
+                              cudaStream_t stream);
+cudaError_t launch_scale_cols(double* X, int64_t rows, int64_t cols, int64_t ldx, const double* s, bool inv_sqrt,
+                              cudaStream_t stream);
+struct ChiGroup {
+  int n;
+  double alpha;
+  double u2[64];
+  double sqrtw[64];
+};
+cudaError_t launch_chi_scale(const double* R, int64_t ldR, int NQ, int64_t nov, const double* D, const ChiGroup& cg,
+                             double* Y, int64_t ldy, cudaStream_t stream);
+cudaError_t launch_gather_cols(const double* src, int64_t lds, double* dst, int64_t ldd, int64_t rows, int64_t cols,
+                               const int* perm, const double* colscale, cudaStream_t stream);
+cudaError_t launch_symmetrize_avg(double* A, int64_t lda, int n, cudaStream_t stream);
+
+// SOSEX pair contraction: partial[tile] of -sum_{i>=j} (2 - delta_ij) sum_{Q,mu} B_mu W_ij W_ji,
+// W_ij = R(:, :, i) U(:, :, j)^T; partials reduced on the host in fixed order.
+cudaError_t launch_sosex(const double* R, int64_t ldR, int NQ, int no, int nv, const double* U, int64_t ldU, int NT,
+                         const double* Bmu, double* partial, int64_t* npartial, cudaStream_t stream);
+int64_t sosex_partials(int NQ, int no, int NT);
+
 }  // namespace rpa

@@ -1,0 +1,358 @@
+// Device kernels of the direct-ring T2 chain (rpa_THC_CC_T2 / rpa_CC_T2_v5,
+// src/rpa/rpa_CC_Doubles.f90:491-984):
+//   * batched blocked forward substitution L X = B (the (1 + Pi_u)^{-1}
+//     factors of rpa_CC_IM_v5 come from the Cholesky factors of the energy);
+//   * a parallel two-sided Jacobi eigensolver (FP64) for the Gram matrix of
+//     the guess vectors and the Rayleigh-Ritz matrix T^T I T
+//     (symmetric_eigenproblem calls at rpa_CC_Doubles.f90:771, 805);
+//   * guess-vector generation, column normalisation (rpa_CC_NormalizeColumns,
+//     rpa_CC_Doubles.f90:80-91), scalings, gathers and column norms.
+#include "kernels.h"
+
+namespace rpa {
+
+namespace {
+
+// ----------------------------------------------------------------- TRSM
+constexpr int TB = 64;     // block of the blocked substitution
+constexpr int TCOLS = 64;  // right-hand sides per CTA
+
+// X_b(j0:j0+nb, cols) <- L_b(j0:j0+nb, j0:j0+nb)^{-1} X_b(j0:j0+nb, cols)
+constexpr size_t kTrsmSmem = sizeof(double) * (TB * (TB + 1) + TB * (TCOLS + 1));
+
+__global__ void __launch_bounds__(TCOLS) trsm_diag_kernel(const double* L, int64_t ldl, int64_t sL, double* X,
+                                                          int64_t ldx, int64_t sX, int n, int ncols, int j0) {
+  extern __shared__ double trsm_smem[];
+  auto Ls = reinterpret_cast<double(*)[TB + 1]>(trsm_smem);
+  auto Xs = reinterpret_cast<double(*)[TCOLS + 1]>(trsm_smem + TB * (TB + 1));
+  const int b = blockIdx.y;
+  const double* Lb = L + (int64_t)b * sL;
+  double* Xb = X + (int64_t)b * sX;
+  const int nb = min(TB, n - j0);
+  const int c0 = blockIdx.x * TCOLS;
+  const int t = threadIdx.x;
+  for (int idx = t; idx < TB * TB; idx += blockDim.x) {
+    const int r = idx % TB, c = idx / TB;
+    Ls[r][c] = (r < nb && c <= r) ? Lb[(int64_t)(j0 + r) + ldl * (j0 + c)] : 0.0;
+  }
+  for (int idx = t; idx < TB * TCOLS; idx += blockDim.x) {
+    const int r = idx % TB, c = idx / TB;  // a warp reads contiguous rows of one column
+    Xs[r][c] = (r < nb && c0 + c < ncols) ? Xb[(int64_t)(j0 + r) + ldx * (c0 + c)] : 0.0;
+  }
+  __syncthreads();
+  // thread t solves column t
+  for (int r = 0; r < nb; ++r) {
+    double s = Xs[r][t];
+    for (int m = 0; m < r; ++m) s -= Ls[r][m] * Xs[m][t];
+    Xs[r][t] = s / Ls[r][r];
+  }
+  __syncthreads();
+  for (int idx = t; idx < TB * TCOLS; idx += blockDim.x) {
+    const int r = idx % TB, c = idx / TB;
+    if (r < nb && c0 + c < ncols) Xb[(int64_t)(j0 + r) + ldx * (c0 + c)] = Xs[r][c];
+  }
+}
+
+// ----------------------------------------------------------------- Jacobi
+__device__ __forceinline__ int rr_index(int j, int r, int m) { return j == 0 ? 0 : 1 + (j - 1 + r) % (m - 1); }
+
+// Rotation (c, s) of every pair of round r, from the current matrix.
+__global__ void jacobi_params_kernel(const double* A, int64_t lda, int n, int m, int r, double4* rot) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m / 2) return;
+  int p = rr_index(k, r, m), q = rr_index(m - 1 - k, r, m);
+  if (p > q) {
+    const int x = p;
+    p = q;
+    q = x;
+  }
+  double c = 1.0, s = 0.0;
+  if (q < n) {
+    const double app = A[(int64_t)p * (lda + 1)], aqq = A[(int64_t)q * (lda + 1)];
+    const double apq = A[(int64_t)p + lda * q];
+    if (fabs(apq) > 1e-300 && fabs(apq) > 1e-18 * sqrt(fabs(app * aqq))) {
+      const double tau = (aqq - app) / (2.0 * apq);
+      const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+      c = 1.0 / sqrt(1.0 + tt * tt);
+      s = tt * c;
+    }
+  }
+  rot[k] = make_double4(c, s, (double)p, (double)q);
+}
+
+// A <- J^T A J for the 2x2 blocks (pair P, pair Q); V <- V J.
+// blockIdx.y < m/2: A block rows; blockIdx.y == m/2: V (all n rows, pair Q).
+__global__ void jacobi_apply_kernel(double* A, int64_t lda, double* V, int64_t ldv, int n, int m,
+                                    const double4* rot) {
+  const int half = m / 2;
+  const int Pk = blockIdx.x * blockDim.x + threadIdx.x;
+  const int Qk = blockIdx.y;
+  if (blockIdx.z == 0) {
+    if (Pk >= half) return;
+    const double4 P = rot[Pk], Q = rot[Qk];
+    const int p1 = (int)P.z, p2 = (int)P.w, q1 = (int)Q.z, q2 = (int)Q.w;
+    if (p2 >= n || q2 >= n) {
+      // a dummy index (odd n): rotate only the real one
+      if (p2 >= n && q2 >= n) return;
+      if (p2 >= n) {  // rows: only p1 exists; columns rotate
+        const double x1 = A[(int64_t)p1 + lda * q1], x2 = A[(int64_t)p1 + lda * q2];
+        A[(int64_t)p1 + lda * q1] = Q.x * x1 - Q.y * x2;
+        A[(int64_t)p1 + lda * q2] = Q.y * x1 + Q.x * x2;
+      } else {  // columns: only q1 exists; rows rotate
+        const double x1 = A[(int64_t)p1 + lda * q1], x2 = A[(int64_t)p2 + lda * q1];
+        A[(int64_t)p1 + lda * q1] = P.x * x1 - P.y * x2;
+        A[(int64_t)p2 + lda * q1] = P.y * x1 + P.x * x2;
+      }
+      return;
+    }
+    // X = [[a11, a12], [a21, a22]] over rows (p1, p2), columns (q1, q2)
+    const double a11 = A[(int64_t)p1 + lda * q1], a12 = A[(int64_t)p1 + lda * q2];
+    const double a21 = A[(int64_t)p2 + lda * q1], a22 = A[(int64_t)p2 + lda * q2];
+    // X J_Q : col q1' = c x_q1 - s x_q2 ; col q2' = s x_q1 + c x_q2
+    const double b11 = Q.x * a11 - Q.y * a12, b12 = Q.y * a11 + Q.x * a12;
+    const double b21 = Q.x * a21 - Q.y * a22, b22 = Q.y * a21 + Q.x * a22;
+    // J_P^T (X J_Q) : row p1' = c r_p1 - s r_p2 ; row p2' = s r_p1 + c r_p2
+    A[(int64_t)p1 + lda * q1] = P.x * b11 - P.y * b21;
+    A[(int64_t)p1 + lda * q2] = P.x * b12 - P.y * b22;
+    A[(int64_t)p2 + lda * q1] = P.y * b11 + P.x * b21;
+    A[(int64_t)p2 + lda * q2] = P.y * b12 + P.x * b22;
+  } else {
+    // V J_Q over all rows i = Pk (grid covers n rows)
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double4 Q = rot[Qk];
+    const int q1 = (int)Q.z, q2 = (int)Q.w;
+    if (q2 >= n) return;
+    const double x1 = V[(int64_t)i + ldv * q1], x2 = V[(int64_t)i + ldv * q2];
+    V[(int64_t)i + ldv * q1] = Q.x * x1 - Q.y * x2;
+    V[(int64_t)i + ldv * q2] = Q.y * x1 + Q.x * x2;
+  }
+}
+
+// out[0] = sum_{i != j} A_ij^2, out[1] = sum_i A_ii^2 (fixed-order reduction, one block)
+__global__ void __launch_bounds__(256) offdiag_kernel(const double* A, int64_t lda, int n, double* out) {
+  __shared__ double so[256], sd[256];
+  double o = 0.0, d = 0.0;
+  for (int64_t idx = threadIdx.x; idx < (int64_t)n * n; idx += blockDim.x) {
+    const int64_t i = idx % n, j = idx / n;
+    const double v = A[i + lda * j];
+    if (i == j) d += v * v;
+    else o += v * v;
+  }
+  so[threadIdx.x] = o;
+  sd[threadIdx.x] = d;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      so[threadIdx.x] += so[threadIdx.x + s];
+      sd[threadIdx.x] += sd[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = so[0];
+    out[1] = sd[0];
+  }
+}
+
+__global__ void set_identity_kernel(double* V, int64_t ldv, int n) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)n * n) return;
+  const int64_t i = idx % n, j = idx / n;
+  V[i + ldv * j] = (i == j) ? 1.0 : 0.0;
+}
+
+// ----------------------------------------------------------------- vectors
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ull;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+  return x ^ (x >> 31);
+}
+
+// uniform [-1/2, 1/2) guess vectors (the reference: random_number - 1/2)
+__global__ void fill_uniform_kernel(double* X, int64_t rows, int64_t cols, int64_t ldx, uint64_t seed) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= rows * cols) return;
+  const int64_t i = idx % rows, j = idx / rows;
+  const uint64_t h = splitmix64(seed ^ splitmix64((uint64_t)idx));
+  X[i + ldx * j] = (double)(h >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+}
+
+// column norms^2 (one block per column, fixed-order reduction)
+__global__ void __launch_bounds__(256) col_sqnorm_kernel(const double* X, int64_t rows, int64_t ldx, double* out) {
+  __shared__ double sh[256];
+  const int64_t j = blockIdx.x;
+  double s = 0.0;
+  for (int64_t i = threadIdx.x; i < rows; i += blockDim.x) {
+    const double v = X[i + ldx * j];
+    s += v * v;
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int k = 128; k > 0; k >>= 1) {
+    if (threadIdx.x < k) sh[threadIdx.x] += sh[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[j] = sh[0];
+}
+
+// X(:, j) *= colscale(j)  (colscale given as 1/sqrt(norm2) when inv_sqrt)
+__global__ void scale_cols_kernel(double* X, int64_t rows, int64_t cols, int64_t ldx, const double* s, int inv_sqrt) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= rows * cols) return;
+  const int64_t i = idx % rows, j = idx / rows;
+  const double f = inv_sqrt ? 1.0 / sqrt(s[j]) : s[j];
+  X[i + ldx * j] *= f;
+}
+
+// Y(k*NQ + q, ai) = R(q, ai) * f_k(ai), f_k = -alpha D/(D^2+u_k^2) * sqrt(w_k)
+__global__ void chi_scale_kernel(const double* R, int64_t ldR, int NQ, int64_t nov, const double* D, ChiGroup cg,
+                                 double* Y, int64_t ldy) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t total = (int64_t)NQ * nov;
+  if (idx >= total) return;
+  const int64_t q = idx % NQ, a = idx / NQ;
+  const double d = D[a];
+  const double r = R[q + ldR * a];
+  for (int k = 0; k < cg.n; ++k) {
+    const double f = -cg.alpha * d / (d * d + cg.u2[k]) * cg.sqrtw[k];
+    Y[(int64_t)k * NQ + q + ldy * a] = r * f;
+  }
+}
+
+// dst(:, j) = src(:, perm[j])
+__global__ void gather_cols_kernel(const double* src, int64_t lds, double* dst, int64_t ldd, int64_t rows,
+                                   int64_t cols, const int* perm, const double* colscale) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= rows * cols) return;
+  const int64_t i = idx % rows, j = idx / rows;
+  const double f = colscale ? colscale[j] : 1.0;
+  dst[i + ldd * j] = src[i + lds * perm[j]] * f;
+}
+
+// A <- (A + A^T)/2
+__global__ void symmetrize_avg_kernel(double* A, int64_t lda, int n) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)n * n) return;
+  const int64_t i = idx % n, j = idx / n;
+  if (i <= j) return;
+  const double v = 0.5 * (A[i + lda * j] + A[j + lda * i]);
+  A[i + lda * j] = v;
+  A[j + lda * i] = v;
+}
+
+inline unsigned blocks_for(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+cudaError_t launch_trsm_lower_left(const double* L, int64_t ldl, int64_t sL, double* X, int64_t ldx, int64_t sX,
+                                   int n, int ncols, int batch, cudaStream_t stream) {
+  cudaError_t e0 = cudaFuncSetAttribute(trsm_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem);
+  if (e0 != cudaSuccess) return e0;
+  for (int j0 = 0; j0 < n; j0 += TB) {
+    trsm_diag_kernel<<<dim3((ncols + TCOLS - 1) / TCOLS, batch), TCOLS, kTrsmSmem, stream>>>(L, ldl, sL, X, ldx, sX,
+                                                                                             n, ncols, j0);
+    ++g_launches;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    const int nb = min(TB, n - j0);
+    const int rest = n - j0 - nb;
+    if (rest <= 0) break;
+    GemmF64Args g{};
+    g.M = rest;
+    g.N = ncols;
+    g.K = nb;
+    g.A = L + (int64_t)(j0 + nb) + ldl * j0;
+    g.a_m = 1;
+    g.a_k = ldl;
+    g.sA = sL;
+    g.B = X + j0;
+    g.b_k = 1;
+    g.b_n = ldx;
+    g.sB = sX;
+    g.C = X + (j0 + nb);
+    g.ldc = ldx;
+    g.sC = sX;
+    g.alpha = -1.0;
+    g.beta = 1.0;
+    g.batch = batch;
+    e = launch_gemm_f64(g, stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_jacobi_sweep(double* A, int64_t lda, double* V, int64_t ldv, int n, double4* rot,
+                                cudaStream_t stream) {
+  const int m = n + (n & 1);
+  if (m < 2) return cudaSuccess;
+  const int half = m / 2;
+  for (int r = 0; r < m - 1; ++r) {
+    jacobi_params_kernel<<<blocks_for(half), 256, 0, stream>>>(A, lda, n, m, r, rot);
+    ++g_launches;
+    const int gx = (int)blocks_for(n > half ? n : half, 128);
+    jacobi_apply_kernel<<<dim3(gx, half, 2), 128, 0, stream>>>(A, lda, V, ldv, n, m, rot);
+    ++g_launches;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_offdiag(const double* A, int64_t lda, int n, double* out, cudaStream_t stream) {
+  offdiag_kernel<<<1, 256, 0, stream>>>(A, lda, n, out);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_set_identity(double* V, int64_t ldv, int n, cudaStream_t stream) {
+  set_identity_kernel<<<blocks_for((int64_t)n * n), 256, 0, stream>>>(V, ldv, n);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_uniform(double* X, int64_t rows, int64_t cols, int64_t ldx, uint64_t seed,
+                                cudaStream_t stream) {
+  if (rows * cols == 0) return cudaSuccess;
+  fill_uniform_kernel<<<blocks_for(rows * cols), 256, 0, stream>>>(X, rows, cols, ldx, seed);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_col_sqnorm(const double* X, int64_t rows, int64_t cols, int64_t ldx, double* out,
+                              cudaStream_t stream) {
+  if (cols == 0) return cudaSuccess;
+  col_sqnorm_kernel<<<(unsigned)cols, 256, 0, stream>>>(X, rows, ldx, out);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_scale_cols(double* X, int64_t rows, int64_t cols, int64_t ldx, const double* s, bool inv_sqrt,
+                              cudaStream_t stream) {
+  if (rows * cols == 0) return cudaSuccess;
+  scale_cols_kernel<<<blocks_for(rows * cols), 256, 0, stream>>>(X, rows, cols, ldx, s, inv_sqrt ? 1 : 0);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_chi_scale(const double* R, int64_t ldR, int NQ, int64_t nov, const double* D, const ChiGroup& cg,
+                             double* Y, int64_t ldy, cudaStream_t stream) {
+  chi_scale_kernel<<<blocks_for((int64_t)NQ * nov), 256, 0, stream>>>(R, ldR, NQ, nov, D, cg, Y, ldy);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_cols(const double* src, int64_t lds, double* dst, int64_t ldd, int64_t rows, int64_t cols,
+                               const int* perm, const double* colscale, cudaStream_t stream) {
+  if (rows * cols == 0) return cudaSuccess;
+  gather_cols_kernel<<<blocks_for(rows * cols), 256, 0, stream>>>(src, lds, dst, ldd, rows, cols, perm, colscale);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_symmetrize_avg(double* A, int64_t lda, int n, cudaStream_t stream) {
+  symmetrize_avg_kernel<<<blocks_for((int64_t)n * n), 256, 0, stream>>>(A, lda, n);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+}  // namespace rpa

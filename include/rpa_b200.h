@@ -124,6 +124,43 @@ int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* OrbEnergies, d
                        double* FreqWeights, int64_t* NFreqs);
 
 /*
+ * Direct-ring T2 amplitudes T2 = U diag(A) U^T (nov x nov) at coupling
+ * strength 1, by the randomised range finder of the reference: guess vectors
+ * Omega (nov x GuessNVecs; NULL -> uniform [-1/2,1/2) from `seed`), I*Omega,
+ * Gram eigen-decomposition with the linear-dependency cutoff
+ * SmallEigenvalsCutoff, Rayleigh-Ritz on T^T I T, A = a/(2(a+1)), and the
+ * eigenvalue cutoff of type CutoffType (0 EIG, 1 EIG_DIV_MAXEIG,
+ * 2 EIG_DIV_NELECTRON, 3 SUM_REJECTED) with threshold CutoffThresh; when
+ * *CommonThresh < 0 (supersystem) the threshold used is returned in it,
+ * otherwise *CommonThresh is used as the threshold (subsystems).
+ * Replaces rpa_CC_Diagonalize_PiU (src/rpa/rpa_CC.f90:1108-1129) and
+ * rpa_THC_CC_T2 / rpa_CC_T2_v5 / rpa_CC_IM_v5 / rpa_CC_MIM_v5 / rpa_T2_EigRPA
+ * (src/rpa/rpa_CC_Doubles.f90:369-1009).  (1 + Pi(u))^{-1} is applied through
+ * the Cholesky factors of the energy step instead of an eigen-decomposition of
+ * Pi(u).  Outputs: A (NVecsT2, ascending = largest |A| first), U (nov x
+ * NVecsT2, ldU >= nov; the Uaim layout), EigRPA(mu) = 2 A_mu |R U_mu|^2,
+ * Ec (may be NULL) the RPA energy of the same Pi(u).  MaxNVecsT2 bounds the
+ * capacity of A, U and EigRPA.
+ */
+int rpa_b200_dring_t2(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R, int64_t ldR,
+                      const double* OccEnergies, const double* VirtEnergies, int64_t NFreqs, const double* Freqs,
+                      const double* FreqWeights, double alpha, int64_t prec, int64_t GuessNVecs, const double* Omega,
+                      uint64_t seed, double SmallEigenvalsCutoff, double CutoffThresh, int64_t CutoffType,
+                      double* CommonThresh, int64_t MaxNVecsT2, double* A, double* U, int64_t ldU,
+                      int64_t* NVecsT2, double* EigRPA, double* Ec);
+
+/*
+ * Exchange (SOSEX) energy  Ex = -Alpha sum_{abij} (aj|bi) T_aibj with
+ * T = U diag(B) U^T, B = A (S2Operator = 0) or A/(1 - 4A^2) (S2Operator = 1).
+ * Replaces rpa_CC_Exchange_SOSEX + rpa_CC_EcExchange1
+ * (src/rpa/rpa_CC_Exchange.f90:36-116).  U is (nov x NVecsT2) column-major
+ * (ldU >= nov), i.e. the transpose of that routine's Vkai(NVecsT2, NVirt, NOcc).
+ */
+int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R,
+                            int64_t ldR, int64_t NVecsT2, const double* U, int64_t ldU, const double* A, double Alpha,
+                            int64_t S2Operator, double* Ex);
+
+/*
  * Allocation-free energy from given Pi(u) matrices.  No counterpart in the
  * reference: it exists for callers that cannot allocate GPU memory (a host
  * whose device memory belongs to a pool or arena it cannot grow, or code

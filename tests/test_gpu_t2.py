@@ -1,0 +1,102 @@
+"""GPU parity of the direct-ring T2 amplitudes and the SOSEX exchange energy
+against the FP64 oracle (rpa_THC_CC_T2 / rpa_T2_EigRPA / rpa_CC_Exchange_SOSEX
+restatements).  With the same guess vectors the GPU and the oracle follow the
+same algorithm, so amplitudes agree to rounding; with the library's own guess
+vectors parity is at the converged-subspace level (energies).
+
+Tolerances: A to 1e-8 relative; eigenvectors |<u_gpu, u_ref>| >= 1 - 1e-6;
+EigRPA sum and SOSEX energies to 1e-10 Eh (FP64); 1e-6 Eh with the split-BF16
+Pi or a different guess set.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import rpa_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def t2_case(seed, nq, no, nv, K, lam0=0.6):
+    s = O.make_system(nq, no, nv, seed, decay=nq / 5.0, lam0=lam0)
+    x, w = O.grid_for(s, K)
+    pi = O.pi_matrices(s.R, s.eps_o, s.eps_v, x)
+    vals, vecs = O.diagonalize_pi(pi)
+    nov = no * nv
+    G = min(int(math.ceil(3.0 * nq)), nov)
+    omega = np.random.default_rng(seed).uniform(size=(nov, G)) - 0.5
+    return s, x, w, pi, vals, vecs, omega
+
+
+@pytest.mark.parametrize("shape", [(60, 4, 20, 10), (150, 6, 50, 12)])
+def test_t2_matches_oracle_with_same_guess(handle, shape):
+    nq, no, nv, K = shape
+    s, x, w, pi, vals, vecs, omega = t2_case(11, nq, no, nv, K)
+    A_ref, U_ref, K_ref = O.t2_direct_ring(s.R, s.eps_o, s.eps_v, x, w, vals, vecs, omega, cutoff_thresh=1e-4)
+    res = handle.dring_t2(s.R, s.eps_o, s.eps_v, x, w, prec="fp64", guess=omega, cutoff_thresh=1e-4)
+    assert res["NT"] == len(A_ref)
+    assert np.allclose(res["A"], A_ref, rtol=1e-8, atol=1e-13)
+    dots = np.abs(np.sum(res["U"] * U_ref, axis=0))
+    assert np.all(dots > 1 - 1e-6)
+    eig_ref = O.t2_eig_rpa(U_ref, A_ref, s.R)
+    assert abs(res["EigRPA"].sum() - eig_ref.sum()) < 1e-10
+    assert res["common_thresh"] == pytest.approx(K_ref)
+    ec_ref, _ = O.ec_rpa_analytic(pi, w)
+    assert abs(res["Ec"] - ec_ref) < 1e-10
+
+
+def test_t2_energy_identity_with_device_guess(handle):
+    # identity (i): with every direction kept, sum_mu 2 A_mu |R U_mu|^2 == E_c
+    s, x, w, pi, vals, vecs, omega = t2_case(12, 60, 4, 20, 10)
+    res = handle.dring_t2(s.R, s.eps_o, s.eps_v, x, w, prec="fp64", seed=7, cutoff_thresh=1e-14)
+    ec_ref, _ = O.ec_rpa_analytic(pi, w)
+    assert abs(res["EigRPA"].sum() - ec_ref) < 1e-6 * abs(ec_ref)
+    # directions kept down to the 1e-10 Gram cutoff carry ~1e-16/1e-10 rounding: orthonormal to ~1e-6
+    assert np.allclose(res["U"].T @ res["U"], np.eye(res["NT"]), atol=1e-5)
+
+
+@pytest.mark.parametrize("ctype,thresh", [(0, 1e-4), (1, 1e-3), (2, 1e-3), (3, 1e-4)])
+def test_t2_cutoff_types(handle, ctype, thresh):
+    s, x, w, pi, vals, vecs, omega = t2_case(13, 60, 4, 20, 10)
+    A_ref, U_ref, K_ref = O.t2_direct_ring(s.R, s.eps_o, s.eps_v, x, w, vals, vecs, omega, cutoff_thresh=thresh,
+                                           cutoff_type=ctype, nocc=s.no)
+    res = handle.dring_t2(s.R, s.eps_o, s.eps_v, x, w, prec="fp64", guess=omega, cutoff_thresh=thresh,
+                          cutoff_type=ctype)
+    assert res["NT"] == len(A_ref)
+    assert res["common_thresh"] == pytest.approx(K_ref, rel=1e-8)
+
+
+def test_t2_subsystem_uses_common_threshold(handle):
+    s, x, w, pi, vals, vecs, omega = t2_case(14, 60, 4, 20, 10)
+    A_ref, _, _ = O.t2_direct_ring(s.R, s.eps_o, s.eps_v, x, w, vals, vecs, omega, common_thresh=3e-3)
+    res = handle.dring_t2(s.R, s.eps_o, s.eps_v, x, w, prec="fp64", guess=omega, common_thresh=3e-3)
+    assert res["NT"] == len(A_ref) and res["common_thresh"] == 3e-3
+
+
+def test_t2_split_precision_energy(handle):
+    s, x, w, pi, vals, vecs, omega = t2_case(15, 150, 6, 50, 12)
+    A_ref, U_ref, _ = O.t2_direct_ring(s.R, s.eps_o, s.eps_v, x, w, vals, vecs, omega, cutoff_thresh=1e-6)
+    res = handle.dring_t2(s.R, s.eps_o, s.eps_v, x, w, prec="split", guess=omega, cutoff_thresh=1e-6)
+    assert abs(res["EigRPA"].sum() - O.t2_eig_rpa(U_ref, A_ref, s.R).sum()) < 1e-6
+
+
+@pytest.mark.parametrize("s2", [False, True])
+def test_sosex_matches_oracle(handle, s2):
+    s, x, w, pi, vals, vecs, omega = t2_case(16, 150, 6, 50, 12)
+    A_ref, U_ref, _ = O.t2_direct_ring(s.R, s.eps_o, s.eps_v, x, w, vals, vecs, omega, cutoff_thresh=1e-4)
+    ref = O.exchange_sosex(np.ascontiguousarray(U_ref.T), A_ref, s.R, s.no, s.nv, alpha=1.0, s2_operator=s2)
+    got = handle.exchange_sosex(s.R, s.no, s.nv, U_ref, A_ref, alpha=1.0, s2_operator=s2)
+    assert abs(got - ref) < 1e-11 * max(1.0, abs(ref))
+
+
+def test_sosex_ragged_shapes(handle):
+    # NQ, nv and NT not multiples of the 64/16 tiles
+    rng = np.random.default_rng(3)
+    nq, no, nv, nt = 77, 5, 19, 45
+    R = rng.standard_normal((nq, no * nv)) * 0.1
+    U = rng.standard_normal((no * nv, nt)) * 0.2
+    A = -0.05 * rng.uniform(size=nt)
+    ref = O.exchange_sosex(np.ascontiguousarray(U.T), A, R, no, nv, alpha=2.0)
+    got = handle.exchange_sosex(R, no, nv, U, A, alpha=2.0)
+    assert abs(got - ref) < 1e-12 * max(1.0, abs(ref))
