@@ -46,6 +46,13 @@ _vp = ctypes.c_void_p
 _lib = None
 
 
+class _Instance(ctypes.Structure):
+    """struct rpa_instance of include/rpa_b200.h."""
+    _fields_ = [("NQ", _i64), ("NOcc", _i64), ("NVirt", _i64), ("R", _vp), ("ldR", _i64),
+                ("OccEnergies", _vp), ("VirtEnergies", _vp), ("NFreqs", _i64), ("Freqs", _vp),
+                ("FreqWeights", _vp), ("alpha", _dbl)]
+
+
 class RPAError(RuntimeError):
     def __init__(self, status: int, detail: str = ""):
         self.status = status
@@ -84,6 +91,7 @@ def load_library(path: str | os.PathLike | None = None):
     lib.rpa_b200_ec_from_pi_noalloc.argtypes = [_i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp, _vp]
     lib.rpa_b200_dring_t2.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _dbl, _i64, _i64,
                                       _vp, ctypes.c_uint64, _dbl, _dbl, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _vp]
+    lib.rpa_b200_ec_batched.argtypes = [_vp, _i64, _vp, _i64, _vp, _vp]
     lib.rpa_b200_exchange_sosex.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _dbl, _i64, _vp]
     if path is None:
         _lib = lib
@@ -229,6 +237,32 @@ class Handle:
         self._check(self.lib.rpa_b200_ec_from_pi(self._h, nq, K, p.ptr, nq, w.ptr, ctypes.byref(ec),
                                                  eu.ctypes.data))
         return ec.value, eu
+
+    def ec_batched(self, systems, prec="split"):
+        """Energies of many systems in one call (rpa_b200_ec_batched).
+
+        systems: sequence of (R, eps_o, eps_v, freqs, weights[, alpha]).  Returns (Ec array, list of E(u))."""
+        n = len(systems)
+        arr = (_Instance * n)()
+        keep = []
+        for i, sysx in enumerate(systems):
+            R, eo, ev, fr, w = sysx[:5]
+            alpha = sysx[5] if len(sysx) > 5 else 4.0
+            nq = int(R.shape[0])
+            r = _colmajor(R, nq)
+            a_eo, a_ev, a_fr, a_w = _vec(eo), _vec(ev), _vec(fr), _vec(w)
+            keep += [r, a_eo, a_ev, a_fr, a_w]
+            arr[i] = _Instance(nq, len(eo), len(ev), r.ptr, r.ld, a_eo.ptr, a_ev.ptr, len(fr), a_fr.ptr, a_w.ptr,
+                               float(alpha))
+        ec = np.zeros(n)
+        eu = np.zeros(sum(len(sysx[3]) for sysx in systems))
+        self._check(self.lib.rpa_b200_ec_batched(self._h, n, ctypes.cast(arr, _vp), _PREC[prec], ec.ctypes.data,
+                                                 eu.ctypes.data))
+        out, o = [], 0
+        for sysx in systems:
+            out.append(eu[o:o + len(sysx[3])].copy())
+            o += len(sysx[3])
+        return ec, out
 
     # ------------------------------------------------------------------ beyond RPA
     def dring_t2(self, R, eps_o, eps_v, freqs, weights, alpha=4.0, prec="fp64", guess=None, n_guess=None, seed=0,

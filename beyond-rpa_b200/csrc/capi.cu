@@ -37,6 +37,14 @@ struct rpa_b200_handle {
   DevBuf R, D, eps, Xhi, Xlo, diag_part, diag, Pi, Ldiag, ddbuf;
   // direct-ring T2 / exchange workspace
   DevBuf tZ, tOm, tIOm, tP, tS, tV, tT, tTIT, tVt, tW, tU, tRU, tSmall, tRot, tPerm;
+  // batched (many-instance) workspace: descriptors and per-batch results
+  DevBuf bDesc, bRes;
+  struct BatchGraph {
+    uint64_t key;
+    std::vector<cudaGraphExec_t> execs;
+    std::vector<int64_t> launches;
+  };
+  BatchGraph bgraph{0, {}, {}};
   int* err_dev = nullptr;    // device error word
   int* count_dev = nullptr;  // non-finite counter
   PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
@@ -662,8 +670,9 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
   if (h->own_stream) cudaStreamSynchronize(h->own_stream);
   for (DevBuf* b : {&h->R, &h->D, &h->eps, &h->Xhi, &h->Xlo, &h->diag_part, &h->diag, &h->Pi, &h->Ldiag, &h->ddbuf,
                     &h->tZ, &h->tOm, &h->tIOm, &h->tP, &h->tS, &h->tV, &h->tT, &h->tTIT, &h->tVt, &h->tW, &h->tU,
-                    &h->tRU, &h->tSmall, &h->tRot, &h->tPerm})
+                    &h->tRU, &h->tSmall, &h->tRot, &h->tPerm, &h->bDesc, &h->bRes})
     release(*b);
+  for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
   if (h->err_dev) cudaFree(h->err_dev);
   if (h->count_dev) cudaFree(h->count_dev);
   for (auto& e : h->ev)
@@ -1023,6 +1032,337 @@ int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
   dd acc{0.0, 0.0};
   for (double x : hp) acc = rpa::dd_add(acc, x);
   *Ex = -Alpha * (acc.hi + acc.lo);
+  finish_timings(h);
+  return RPA_OK;
+}
+
+int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* inst, int64_t prec, double* Ec,
+                        double* Eu) {
+  int s = begin_call(h);
+  if (s != RPA_OK) return s;
+  if (ninst < 1 || !inst || !Ec) return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_ec_batched");
+  if (prec != RPA_PREC_FP64 && prec != RPA_PREC_SPLIT_BF16)
+    return fail(h, RPA_ERR_INVALID_ARG, "unknown precision mode %lld", (long long)prec);
+  const int n = (int)ninst;
+  std::vector<Validated> v(n);
+  std::vector<int64_t> eu_off(n + 1, 0);
+  size_t host_R = 0, total_nov = 0;
+  for (int i = 0; i < n; ++i) {
+    const rpa_instance& I = inst[i];
+    if ((s = validate_common(h, I.NQ, I.NOcc, I.NVirt, I.R, I.ldR, I.OccEnergies, I.VirtEnergies, I.NFreqs, I.Freqs,
+                             I.alpha, prec, v[i])))
+      return fail(h, s, "instance %d: %s", i, h->last_error.c_str());
+    if (I.NFreqs > rpa::kMaxKgLaunch)
+      return fail(h, RPA_ERR_INVALID_ARG, "instance %d: NFreqs > %d in a batched call", i, rpa::kMaxKgLaunch);
+    if (!I.FreqWeights) return fail(h, RPA_ERR_INVALID_ARG, "instance %d: FreqWeights is NULL", i);
+    if ((s = fetch_small(h, I.FreqWeights, I.NFreqs, v[i].weights))) return s;
+    eu_off[i + 1] = eu_off[i] + I.NFreqs;
+    if (!is_device_ptr(I.R)) host_R += (size_t)I.NQ * v[i].nov;
+    total_nov += (size_t)v[i].nov;
+  }
+  // stage host R into one packed buffer (ld = NQ); D(ai) of every instance in one buffer
+  std::vector<const double*> Rd(n);
+  std::vector<int64_t> ldR(n), Doff(n);
+  RPA_CUDA(h, ensure(h->R, host_R * 8));
+  RPA_CUDA(h, ensure(h->D, total_nov * 8));
+  {
+    size_t off = 0, doff = 0;
+    std::vector<double> Dh(total_nov);
+    for (int i = 0; i < n; ++i) {
+      const rpa_instance& I = inst[i];
+      if (is_device_ptr(I.R)) {
+        Rd[i] = I.R;
+        ldR[i] = I.ldR;
+      } else {
+        double* dst = static_cast<double*>(h->R.p) + off;
+        RPA_CUDA(h, cudaMemcpy2DAsync(dst, (size_t)I.NQ * 8, I.R, (size_t)I.ldR * 8, (size_t)I.NQ * 8,
+                                      (size_t)v[i].nov, cudaMemcpyHostToDevice, h->stream));
+        Rd[i] = dst;
+        ldR[i] = I.NQ;
+        off += (size_t)I.NQ * v[i].nov;
+      }
+      Doff[i] = (int64_t)doff;
+      for (int64_t ii = 0; ii < v[i].no; ++ii)
+        for (int64_t a = 0; a < v[i].nv; ++a) Dh[doff + a + v[i].nv * ii] = v[i].ev[a] - v[i].eo[ii];
+      doff += (size_t)v[i].nov;
+    }
+    RPA_CUDA(h, cudaMemcpyAsync(h->D.p, Dh.data(), total_nov * 8, cudaMemcpyHostToDevice, h->stream));
+    RPA_CUDA(h, cudaMemsetAsync(h->count_dev, 0, sizeof(int), h->stream));
+    for (int i = 0; i < n; ++i)
+      RPA_CUDA(h, rpa::launch_count_nonfinite(Rd[i], ldR[i] * (v[i].nov - 1) + v[i].NQ, h->count_dev, h->stream));
+    int cnt = 0;
+    RPA_CUDA(h, cudaMemcpyAsync(&cnt, h->count_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    RPA_CUDA(h, cudaStreamSynchronize(h->stream));  // Dh must outlive its copy
+    if (cnt) return fail(h, RPA_ERR_NONFINITE, "%d non-finite entries in the Cholesky vectors", cnt);
+  }
+  RPA_CUDA(h, cudaEventRecord(h->ev[1], h->stream));
+  const double* D = static_cast<const double*>(h->D.p);
+
+  // ---- batch plan: greedy packing in instance order under a memory budget
+  struct Per {
+    int64_t pitch;
+    rpa::SplitPlan plan;
+    size_t xb, pib, smallb;
+  };
+  std::vector<Per> per(n);
+  for (int i = 0; i < n; ++i) {
+    const int64_t nov = v[i].nov;
+    per[i].pitch = (nov + 7) / 8 * 8;
+    per[i].plan = rpa::plan_scale_split(v[i].NQ, nov, h->num_sms);
+    per[i].xb = prec == RPA_PREC_SPLIT_BF16 ? (size_t)v[i].K * v[i].NQ * per[i].pitch * 2 : 0;  // each of hi, lo
+    per[i].pib = (size_t)v[i].K * v[i].NQ * v[i].NQ * 8;
+    per[i].smallb = (size_t)v[i].K * v[i].NQ * 8 * (2 + per[i].plan.nsplit) + 64 * (size_t)v[i].K;
+  }
+  size_t freeB = 0, totalB = 0;
+  RPA_CUDA(h, cudaMemGetInfo(&freeB, &totalB));
+  const size_t have = h->Xhi.bytes + h->Xlo.bytes + h->Pi.bytes + h->Ldiag.bytes;
+  const size_t budget = (size_t)(0.6 * (double)(freeB + have));
+  std::vector<std::pair<int, int>> batches;  // [b0, b1)
+  {
+    size_t acc = 0;
+    int b0 = 0;
+    for (int i = 0; i < n; ++i) {
+      const size_t need = 2 * per[i].xb + per[i].pib + per[i].smallb;
+      if (i > b0 && acc + need > budget) {
+        batches.push_back({b0, i});
+        b0 = i;
+        acc = 0;
+      }
+      acc += need;
+    }
+    batches.push_back({b0, n});
+  }
+  size_t maxX = 0, maxPi = 0, maxSmall = 0, maxDesc = 0;
+  std::vector<size_t> desc_off(batches.size() + 1, 0), res_off(batches.size() + 1, 0);
+  for (size_t b = 0; b < batches.size(); ++b) {
+    size_t x = 0, pi = 0, sm = 0, units = 0, work = 0, mats = 0;
+    for (int i = batches[b].first; i < batches[b].second; ++i) {
+      x += per[i].xb;
+      pi += per[i].pib;
+      sm += per[i].smallb;
+      units += (size_t)v[i].K * rpa::syrk_tc_blocks(v[i].NQ);
+      work += (size_t)per[i].plan.qtiles * per[i].plan.nsplit;
+      mats += (size_t)v[i].K;
+    }
+    const int ni = batches[b].second - batches[b].first;
+    const size_t desc = ((sizeof(rpa::SyrkInst) * ni + 255) / 256 + (sizeof(rpa::SplitJob) * ni + 255) / 256 +
+                         (sizeof(int64_t) * (ni + 1) + 255) / 256 + (sizeof(uint4) * units + 255) / 256 +
+                         (sizeof(int4) * work + 255) / 256 + (sizeof(rpa::MatDesc) * mats + 255) / 256) *
+                        256;
+    desc_off[b + 1] = desc_off[b] + desc;
+    res_off[b + 1] = res_off[b] + mats * 4;  // tr_dd, ld_dd per matrix
+    maxX = std::max(maxX, x);
+    maxPi = std::max(maxPi, pi);
+    maxSmall = std::max(maxSmall, sm);
+  }
+  (void)maxDesc;
+  if (prec == RPA_PREC_SPLIT_BF16) {
+    RPA_CUDA(h, ensure(h->Xhi, maxX + 256));
+    RPA_CUDA(h, ensure(h->Xlo, maxX + 256));
+  }
+  RPA_CUDA(h, ensure(h->Pi, maxPi + 256));
+  RPA_CUDA(h, ensure(h->Ldiag, maxSmall + 256));
+  RPA_CUDA(h, ensure(h->bDesc, desc_off.back() + 256));
+  RPA_CUDA(h, ensure(h->bRes, res_off.back() * 8 + 256));
+
+  // graph cache key: shapes, pointers and workspace addresses of this call
+  uint64_t key = 1469598103934665603ull;
+  auto mix = [&](uint64_t x) { key = (key ^ x) * 1099511628211ull; };
+  mix((uint64_t)prec);
+  mix((uint64_t)h->seg_chunks);
+  for (void* p : {h->Xhi.p, h->Xlo.p, h->Pi.p, h->Ldiag.p, h->bDesc.p, h->bRes.p, h->D.p, (void*)h->stream})
+    mix((uint64_t)(uintptr_t)p);
+  for (int i = 0; i < n; ++i) {
+    mix((uint64_t)(uintptr_t)Rd[i]);
+    mix((uint64_t)ldR[i]);
+    mix((uint64_t)v[i].NQ);
+    mix((uint64_t)v[i].nov);
+    for (int k = 0; k < v[i].K; ++k) {
+      uint64_t bits;
+      std::memcpy(&bits, &v[i].freqs[k], 8);
+      mix(bits);
+    }
+    uint64_t ab;
+    std::memcpy(&ab, &inst[i].alpha, 8);
+    mix(ab);
+  }
+  const bool cached = (h->bgraph.key == key && h->bgraph.execs.size() == batches.size());
+  if (!cached) {
+    for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
+    h->bgraph.execs.clear();
+    h->bgraph.launches.clear();
+    h->bgraph.key = 0;
+  }
+  uint8_t* descBase = static_cast<uint8_t*>(h->bDesc.p);
+  double* resBase = static_cast<double*>(h->bRes.p);
+  for (size_t b = 0; b < batches.size(); ++b) {
+    if (cached) {
+      RPA_CUDA(h, cudaGraphLaunch(h->bgraph.execs[b], h->stream));
+      rpa::g_launches += h->bgraph.launches[b];
+      continue;
+    }
+    const int i0 = batches[b].first, i1 = batches[b].second, ni = i1 - i0;
+    std::vector<rpa::SyrkInst> sinst(ni);
+    std::vector<rpa::SplitJob> jobs(ni);
+    std::vector<int64_t> offs(ni + 1, 0);
+    std::vector<uint4> units;
+    std::vector<int4> work;
+    std::vector<rpa::MatDesc> mats;
+    std::vector<uint2> coords;
+    size_t xo = 0, po = 0, so = 0;
+    double* res = resBase + res_off[b];
+    int nmax = 0;
+    for (int t = 0; t < ni; ++t) {
+      const int i = i0 + t;
+      const int NQ = v[i].NQ, K = v[i].K;
+      const int64_t nov = v[i].nov;
+      __nv_bfloat16* xh = reinterpret_cast<__nv_bfloat16*>(static_cast<uint8_t*>(h->Xhi.p) + xo);
+      __nv_bfloat16* xl = reinterpret_cast<__nv_bfloat16*>(static_cast<uint8_t*>(h->Xlo.p) + xo);
+      double* Pi = reinterpret_cast<double*>(static_cast<uint8_t*>(h->Pi.p) + po);
+      double* smallp = reinterpret_cast<double*>(static_cast<uint8_t*>(h->Ldiag.p) + so);
+      double* diag = smallp;                          // K*NQ
+      double* Ldiag = diag + (size_t)K * NQ;          // K*NQ
+      double* dpart = Ldiag + (size_t)K * NQ;         // nsplit*K*NQ
+      xo += (per[i].xb + 255) / 256 * 256;
+      po += (per[i].pib + 255) / 256 * 256;
+      so += (per[i].smallb + 255) / 256 * 256;
+      nmax = std::max(nmax, NQ);
+      if (prec == RPA_PREC_SPLIT_BF16) {
+        rpa::SplitJob& j = jobs[t];
+        j.R = Rd[i];
+        j.ldR = ldR[i];
+        j.NQ = NQ;
+        j.nov = nov;
+        j.D = D + Doff[i];
+        j.fg.n = K;
+        for (int k = 0; k < K; ++k) j.fg.u2[k] = v[i].freqs[k] * v[i].freqs[k];
+        j.alpha = inst[i].alpha;
+        j.Xhi = xh;
+        j.Xlo = xl;
+        j.pitch = per[i].pitch;
+        j.kstride = (int64_t)NQ * per[i].pitch;
+        j.diag_part = dpart;
+        j.ai_per_split = per[i].plan.ai_per_split;
+        j.nsplit = per[i].plan.nsplit;
+        j.diag = diag;
+        offs[t + 1] = offs[t] + (int64_t)K * NQ;
+        for (int q = 0; q < per[i].plan.qtiles; ++q)
+          for (int sp = 0; sp < per[i].plan.nsplit; ++sp) work.push_back(make_int4(t, q, sp, 0));
+        rpa::SyrkInst& si = sinst[t];
+        if ((s = encode_map(h, &si.tmAh, xh, nov, NQ, K, per[i].pitch, rpa::kSyrkTcTM))) return s;
+        if ((s = encode_map(h, &si.tmAl, xl, nov, NQ, K, per[i].pitch, rpa::kSyrkTcTM))) return s;
+        if ((s = encode_map(h, &si.tmBh, xh, nov, NQ, K, per[i].pitch, rpa::kSyrkTcTN))) return s;
+        if ((s = encode_map(h, &si.tmBl, xl, nov, NQ, K, per[i].pitch, rpa::kSyrkTcTN))) return s;
+        si.Pi = Pi;
+        si.ldPi = NQ;
+        si.piStride = (int64_t)NQ * NQ;
+        si.diag = diag;
+        si.NQ = NQ;
+        si.nchunks = (int)((nov + rpa::kSyrkTcTK - 1) / rpa::kSyrkTcTK);
+        rpa::syrk_tc_block_coords(NQ, coords);
+        for (int k = 0; k < K; ++k)
+          for (const uint2& c : coords) units.push_back(make_uint4((unsigned)t, (unsigned)k, c.x, c.y));
+      }
+      for (int k = 0; k < K; ++k) {
+        rpa::MatDesc md;
+        md.A = Pi + (size_t)k * NQ * NQ;
+        md.ld = NQ;
+        md.n = NQ;
+        md.Ldiag = Ldiag + (size_t)k * NQ;
+        md.tr_dd = res + 4 * mats.size();
+        md.ld_dd = md.tr_dd + 2;
+        mats.push_back(md);
+      }
+    }
+    // descriptors -> device (laid out as in desc_off)
+    uint8_t* d = descBase + desc_off[b];
+    auto put = [&](const void* src, size_t bytes) {
+      uint8_t* at = d;
+      if (bytes) cudaMemcpyAsync(at, src, bytes, cudaMemcpyHostToDevice, h->stream);
+      d += (bytes + 255) / 256 * 256;
+      return at;
+    };
+    auto* dSinst = reinterpret_cast<rpa::SyrkInst*>(put(sinst.data(), sizeof(rpa::SyrkInst) * sinst.size()));
+    auto* dJobs = reinterpret_cast<rpa::SplitJob*>(put(jobs.data(), sizeof(rpa::SplitJob) * jobs.size()));
+    auto* dOffs = reinterpret_cast<int64_t*>(put(offs.data(), sizeof(int64_t) * offs.size()));
+    auto* dUnits = reinterpret_cast<uint4*>(put(units.data(), sizeof(uint4) * units.size()));
+    auto* dWork = reinterpret_cast<int4*>(put(work.data(), sizeof(int4) * work.size()));
+    auto* dMats = reinterpret_cast<rpa::MatDesc*>(put(mats.data(), sizeof(rpa::MatDesc) * mats.size()));
+    RPA_CUDA(h, cudaGetLastError());
+    RPA_CUDA(h, cudaStreamSynchronize(h->stream));  // host vectors must outlive their copies
+    // capture the batch's launch sequence
+    const int64_t before = rpa::g_launches;
+    cudaGraph_t graph = nullptr;
+    RPA_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    if (prec == RPA_PREC_SPLIT_BF16) {
+      e = rpa::launch_scale_split_multi(dJobs, dWork, (int)work.size(), dOffs, ni, offs.back(), h->stream);
+      if (e == cudaSuccess)
+        e = rpa::launch_syrk_split_bf16_multi(dSinst, dUnits, (int)units.size(),
+                                              h->seg_chunks > 0 ? h->seg_chunks : 1 << 30, h->err_dev, h->num_sms,
+                                              h->stream);
+    } else {
+      for (int t = 0; t < ni && e == cudaSuccess; ++t) {
+        const int i = i0 + t;
+        rpa::DsyrkArgs a{};
+        a.A = Rd[i];
+        a.lda = ldR[i];
+        a.strideA = 0;
+        size_t mi = 0;  // first matrix of instance t in this batch
+        for (int u = 0; u < t; ++u) mi += (size_t)v[i0 + u].K;
+        a.C = mats[mi].A;
+        a.ldc = v[i].NQ;
+        a.strideC = (int64_t)v[i].NQ * v[i].NQ;
+        a.n = v[i].NQ;
+        a.kdim = v[i].nov;
+        a.batch = v[i].K;
+        a.D = D + Doff[i];
+        a.alpha = inst[i].alpha;
+        for (int k = 0; k < v[i].K; ++k) a.u2[k] = v[i].freqs[k] * v[i].freqs[k];
+        e = rpa::launch_dsyrk_lower(a, h->stream);
+      }
+    }
+    if (e == cudaSuccess) e = rpa::launch_logdet_varlen(dMats, (int)mats.size(), nmax, h->err_dev, h->stream);
+    cudaError_t e2 = cudaStreamEndCapture(h->stream, &graph);
+    const int64_t count = rpa::g_launches - before;
+    rpa::g_launches = before;
+    if (e != cudaSuccess || e2 != cudaSuccess || !graph) {
+      if (graph) cudaGraphDestroy(graph);
+      return fail(h, RPA_ERR_CUDA, "capture of batch %zu failed: %s", b, cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) return fail(h, RPA_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ei));
+    h->bgraph.execs.push_back(exec);
+    h->bgraph.launches.push_back(count);
+    RPA_CUDA(h, cudaGraphLaunch(exec, h->stream));
+    rpa::g_launches += count;
+  }
+  if (!cached) h->bgraph.key = key;
+  RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
+  std::vector<double> res(res_off.back());
+  RPA_CUDA(h, cudaMemcpyAsync(res.data(), resBase, res.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  if ((s = check_device_error(h))) return s;
+  // energies: results are laid out per batch in instance order, 4 doubles per (instance, frequency)
+  size_t m = 0;
+  for (int i = 0; i < n; ++i) {
+    dd ec{0.0, 0.0};
+    for (int k = 0; k < v[i].K; ++k, ++m) {
+      const dd trk{res[4 * m], res[4 * m + 1]};
+      const dd ldk{res[4 * m + 2], res[4 * m + 3]};
+      const dd eu = rpa::dd_add_dd(ldk, {-trk.hi, -trk.lo});
+      if (!std::isfinite(eu.hi)) return fail(h, RPA_ERR_NONFINITE, "non-finite E(u) in instance %d", i);
+      if (Eu) Eu[eu_off[i] + k] = eu.hi + eu.lo;
+      const double f = v[i].weights[k] / (2.0 * kPi);
+      const double p = eu.hi * f;
+      ec = rpa::dd_add_dd(ec, {p, std::fma(eu.hi, f, -p) + eu.lo * f});
+    }
+    Ec[i] = ec.hi + ec.lo;
+  }
   finish_timings(h);
   return RPA_OK;
 }

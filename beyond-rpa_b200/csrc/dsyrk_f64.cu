@@ -40,18 +40,14 @@ __device__ __forceinline__ void trap_decode(int b, int T, int Tc, int& tm, int& 
   tm = tn + (b - (tn * T - tn * (tn - 1) / 2));
 }
 
+// One 64 x 64 tile (tm, tn) of C(lower trapezoid, ncols columns) for matrix z.
 template <bool kScaled>
-__global__ void __launch_bounds__(kThreads) dsyrk_lower_kernel(const DsyrkArgs a, const int T, const int Tc) {
+__device__ __forceinline__ void dsyrk_tile(const DsyrkArgs& a, const double* A, double* C, int ncols, int tm, int tn,
+                                           int z) {
   __shared__ double As[2][BK][LDS];
   __shared__ double Bs[2][BK][LDS];
   __shared__ double sS[2][BK];
 
-  int tm, tn;
-  trap_decode(blockIdx.x, T, Tc, tm, tn);
-  const int ncols = a.ncols > 0 ? a.ncols : a.n;
-  const int z = blockIdx.y;
-  const double* A = a.A + (int64_t)z * a.strideA;
-  double* C = a.C + (int64_t)z * a.strideC;
   const int m0 = tm * BM, n0 = tn * BM;
   const int t = threadIdx.x;
   const int lane = t & 31, warp = t >> 5;
@@ -137,7 +133,58 @@ __global__ void __launch_bounds__(kThreads) dsyrk_lower_kernel(const DsyrkArgs a
     }
   }
 }
+
+template <bool kScaled>
+__global__ void __launch_bounds__(kThreads) dsyrk_lower_kernel(const DsyrkArgs a, const int T, const int Tc) {
+  int tm, tn;
+  trap_decode(blockIdx.x, T, Tc, tm, tn);
+  const int ncols = a.ncols > 0 ? a.ncols : a.n;
+  const int z = blockIdx.y;
+  dsyrk_tile<kScaled>(a, a.A + (int64_t)z * a.strideA, a.C + (int64_t)z * a.strideC, ncols, tm, tn, z);
+}
+
+// Variable-size batch: step of the two-level blocked Cholesky.
+//   mode 0 (panel update): C = A[j0+64:, j0+64:], n = N - j0 - 64, ncols = min(N, J0+256) - (j0+64), K = 64
+//   mode 1 (trailing):     C = A[J1:, J1:],       n = N - J1, J1 = min(N, J0+256), K = J1 - J0
+__global__ void __launch_bounds__(kThreads) dsyrk_varlen_kernel(const MatDesc* mats, int mode, int J0, int j0) {
+  const MatDesc md = mats[blockIdx.y];
+  const int N = md.n;
+  const int J1 = min(N, J0 + 256);
+  DsyrkArgs a{};
+  int ncols;
+  if (mode == 0) {
+    a.n = N - j0 - BM;
+    ncols = J1 - (j0 + BM);
+    a.kdim = BM;
+    a.A = md.A + (int64_t)(j0 + BM) + md.ld * (int64_t)j0;
+    a.C = md.A + (int64_t)(j0 + BM) + md.ld * (int64_t)(j0 + BM);
+  } else {
+    a.n = N - J1;
+    ncols = a.n;
+    a.kdim = J1 - J0;
+    a.A = md.A + (int64_t)J1 + md.ld * (int64_t)J0;
+    a.C = md.A + (int64_t)J1 + md.ld * (int64_t)J1;
+  }
+  if (a.n <= 0 || ncols <= 0 || a.kdim <= 0) return;
+  a.lda = md.ld;
+  a.ldc = md.ld;
+  const int T = (a.n + BM - 1) / BM;
+  const int Tc = (min(ncols, a.n) + BM - 1) / BM;
+  const int tiles = Tc * T - Tc * (Tc - 1) / 2;
+  if ((int)blockIdx.x >= tiles) return;
+  int tm, tn;
+  trap_decode(blockIdx.x, T, Tc, tm, tn);
+  dsyrk_tile<false>(a, a.A, a.C, min(ncols, a.n), tm, tn, 0);
+}
 }  // namespace
+
+cudaError_t launch_dsyrk_varlen(const MatDesc* mats, int nmat, int mode, int J0, int j0, int max_tiles,
+                                cudaStream_t stream) {
+  if (nmat <= 0 || max_tiles <= 0) return cudaSuccess;
+  dsyrk_varlen_kernel<<<dim3((unsigned)max_tiles, (unsigned)nmat), kThreads, 0, stream>>>(mats, mode, J0, j0);
+  ++g_launches;
+  return cudaGetLastError();
+}
 
 cudaError_t launch_dsyrk_lower(const DsyrkArgs& a, cudaStream_t stream) {
   if (a.n <= 0 || a.batch <= 0) return cudaSuccess;

@@ -2,6 +2,7 @@
 // sm_100a kernels.  Not installed; the public ABI is include/rpa_b200.h.
 #pragma once
 #include <cstdint>
+#include <vector>
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
@@ -29,6 +30,27 @@ struct SplitPlan {
 
 SplitPlan plan_scale_split(int NQ, int64_t nov, int num_sms);
 
+// One instance of a multi-instance scale/split launch.
+struct SplitJob {
+  const double* R;
+  int64_t ldR;
+  int NQ;
+  int64_t nov;
+  const double* D;
+  FreqGroup fg;
+  double alpha;
+  __nv_bfloat16* Xhi;
+  __nv_bfloat16* Xlo;
+  int64_t pitch, kstride;
+  double* diag_part;
+  int64_t ai_per_split;
+  int nsplit;
+  double* diag;  // [fg.n][NQ]
+};
+// work[b] = (job, q tile, ai split, 0); offsets[j] = sum_{i<j} fg.n * NQ of job i, total = sum.
+cudaError_t launch_scale_split_multi(const SplitJob* jobs, const int4* work, int nwork, const int64_t* offsets,
+                                     int njobs, int64_t total, cudaStream_t stream);
+
 // X_k = sqrt(alpha c_k) R split into bf16 hi/lo rows (Q-major rows, ai
 // contiguous, row pitch `pitch`, frequency stride `kstride` elements), plus
 // the exact FP64 diagonal diag[k*NQ + Q] = sum_ai X_k(Q,ai)^2.
@@ -54,6 +76,20 @@ struct SyrkTcArgs {
 cudaError_t launch_syrk_split_bf16(const CUtensorMap* tmA_hi, const CUtensorMap* tmA_lo, const CUtensorMap* tmB_hi,
                                    const CUtensorMap* tmB_lo, const SyrkTcArgs& a, int num_sms,
                                    cudaStream_t stream);
+// One instance (fragment) of a multi-instance SYRK launch.
+struct SyrkInst {
+  CUtensorMap tmAh, tmAl, tmBh, tmBl;  // 3-D views of this instance's X_hi / X_lo
+  double* Pi;
+  int64_t ldPi, piStride;
+  const double* diag;
+  int NQ;
+  int nchunks;  // ceil(nov / 32)
+};
+cudaError_t launch_syrk_split_bf16_multi(const SyrkInst* insts, const uint4* work, int nunits, int seg_chunks,
+                                         int* err, int num_sms, cudaStream_t stream);
+int syrk_tc_blocks(int NQ);
+// (tm, tn) of the lower-triangle 128 x 256 tiles in the kernel's unit order
+void syrk_tc_block_coords(int NQ, std::vector<uint2>& out);
 constexpr int kSyrkTcTM = 128;
 constexpr int kSyrkTcTN = 256;
 constexpr int kSyrkTcTK = 32;
@@ -155,5 +191,18 @@ cudaError_t launch_symmetrize_avg(double* A, int64_t lda, int n, cudaStream_t st
 cudaError_t launch_sosex(const double* R, int64_t ldR, int NQ, int no, int nv, const double* U, int64_t ldU, int NT,
                          const double* Bmu, double* partial, int64_t* npartial, cudaStream_t stream);
 int64_t sosex_partials(int NQ, int no, int NT);
+
+// ---------------------------------------------------------------- variable-size batches
+// One matrix of a batch of matrices of different orders (fragments).
+struct MatDesc {
+  double* A;       // column-major, lower triangle used
+  int64_t ld;
+  int n;
+  double* Ldiag;   // n pivots L_ii
+  double* tr_dd;   // 2 doubles: trace before the +1 shift (double-double)
+  double* ld_dd;   // 2 doubles: 2 sum log L_ii (double-double)
+};
+// trace_shift + blocked Cholesky + log sums for nmat matrices of orders <= nmax.
+cudaError_t launch_logdet_varlen(const MatDesc* mats, int nmat, int nmax, int* err, cudaStream_t stream);
 
 }  // namespace rpa

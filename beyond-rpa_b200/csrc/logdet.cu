@@ -8,22 +8,22 @@
 // (Pi = R diag(alpha c) R^T with c > 0), so ln det = 2 sum ln L_kk of its
 // Cholesky factor equals the QR value; the sums here are double-double.
 // A non-positive pivot is reported as an error, never as a NaN energy.
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace rpa {
 
 namespace {
 constexpr int NB = 64;  // Cholesky block size
+constexpr int NB2 = 256;  // outer block of the two-level schedule
 
 // Factor the NB x NB diagonal block of each matrix in shared memory.
 // Column j is used unscaled in step j (update of the columns right of it by
 // a_rj a_cj / d_j) and scaled by 1/sqrt(d_j) in step j+1, when nobody reads
 // it any more: one barrier per column.
-__global__ void __launch_bounds__(256) potrf_diag_kernel(double* A, int64_t ld, int64_t stride, int n, int j0,
-                                                         double* Ldiag, int* err) {
+__device__ __forceinline__ void potrf_diag_body(double* Az, int64_t ld, int n, int j0, double* Ldz, int* err) {
   __shared__ double L[NB][NB + 1];
-  const int z = blockIdx.x;
-  double* Az = A + (int64_t)z * stride;
   const int nbe = min(NB, n - j0);
   const int t = threadIdx.x;
   for (int idx = t; idx < NB * NB; idx += blockDim.x) {
@@ -71,15 +71,19 @@ __global__ void __launch_bounds__(256) potrf_diag_kernel(double* A, int64_t ld, 
     const int r = idx % NB, c = idx / NB;
     if (r >= c && r < nbe && c < nbe) Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] = L[r][c];
   }
-  for (int j = t; j < nbe; j += blockDim.x) Ldiag[(int64_t)z * n + j0 + j] = L[j][j];
+  for (int j = t; j < nbe; j += blockDim.x) Ldz[j0 + j] = L[j][j];
+}
+
+__global__ void __launch_bounds__(256) potrf_diag_kernel(double* A, int64_t ld, int64_t stride, int n, int j0,
+                                                         double* Ldiag, int* err) {
+  const int z = blockIdx.x;
+  potrf_diag_body(A + (int64_t)z * stride, ld, n, j0, Ldiag + (int64_t)z * n, err);
 }
 
 // Panel solve: rows below the diagonal block, X L_jj^T = A_panel.
-__global__ void __launch_bounds__(128) trsm_panel_kernel(double* A, int64_t ld, int64_t stride, int n, int j0) {
+__device__ __forceinline__ void trsm_panel_body(double* Az, int64_t ld, int n, int j0, int rblock) {
   __shared__ double Ls[NB][NB + 1];
   __shared__ double inv[NB];
-  const int z = blockIdx.y;
-  double* Az = A + (int64_t)z * stride;
   const int t = threadIdx.x;
   for (int idx = t; idx < NB * NB; idx += blockDim.x) {
     const int r = idx % NB, c = idx / NB;
@@ -88,7 +92,7 @@ __global__ void __launch_bounds__(128) trsm_panel_kernel(double* A, int64_t ld, 
   __syncthreads();
   if (t < NB) inv[t] = 1.0 / Ls[t][t];
   __syncthreads();
-  const int r = j0 + NB + blockIdx.x * blockDim.x + t;
+  const int r = j0 + NB + rblock * blockDim.x + t;
   if (r >= n) return;
   double x[NB];
 #pragma unroll
@@ -102,6 +106,23 @@ __global__ void __launch_bounds__(128) trsm_panel_kernel(double* A, int64_t ld, 
   }
 #pragma unroll
   for (int c = 0; c < NB; ++c) Az[(int64_t)r + ld * (int64_t)(j0 + c)] = x[c];
+}
+
+__global__ void __launch_bounds__(128) trsm_panel_kernel(double* A, int64_t ld, int64_t stride, int n, int j0) {
+  trsm_panel_body(A + (int64_t)blockIdx.y * stride, ld, n, j0, blockIdx.x);
+}
+
+// ----------------------------------------------------------------- variable-size batches
+__global__ void __launch_bounds__(256) potrf_varlen_kernel(const MatDesc* mats, int j0, int* err) {
+  const MatDesc md = mats[blockIdx.x];
+  if (j0 >= md.n) return;
+  potrf_diag_body(md.A, md.ld, md.n, j0, md.Ldiag, err);
+}
+
+__global__ void __launch_bounds__(128) trsm_varlen_kernel(const MatDesc* mats, int j0) {
+  const MatDesc md = mats[blockIdx.y];
+  if (md.n - j0 - NB <= 0 || (int)(blockIdx.x * blockDim.x) >= md.n - j0 - NB) return;
+  trsm_panel_body(md.A, md.ld, md.n, j0, blockIdx.x);
 }
 
 // Deterministic block reduction of double-double values (blockDim = 256).
@@ -150,6 +171,33 @@ __global__ void __launch_bounds__(256) logdet_sum_kernel(const double* Ldiag, in
   }
 }
 
+__global__ void __launch_bounds__(256) trace_shift_varlen_kernel(const MatDesc* mats) {
+  const MatDesc md = mats[blockIdx.x];
+  dd acc{0.0, 0.0};
+  for (int i = threadIdx.x; i < md.n; i += blockDim.x) {
+    double* p = md.A + (int64_t)i * (md.ld + 1);
+    const double v = *p;
+    acc = dd_add(acc, v);
+    *p = v + 1.0;
+  }
+  dd r = block_reduce_dd(acc);
+  if (threadIdx.x == 0) {
+    md.tr_dd[0] = r.hi;
+    md.tr_dd[1] = r.lo;
+  }
+}
+
+__global__ void __launch_bounds__(256) logdet_sum_varlen_kernel(const MatDesc* mats) {
+  const MatDesc md = mats[blockIdx.x];
+  dd acc{0.0, 0.0};
+  for (int i = threadIdx.x; i < md.n; i += blockDim.x) acc = dd_add(acc, 2.0 * log(md.Ldiag[i]));
+  dd r = block_reduce_dd(acc);
+  if (threadIdx.x == 0) {
+    md.ld_dd[0] = r.hi;
+    md.ld_dd[1] = r.lo;
+  }
+}
+
 __global__ void dai_kernel(const double* eps_o, const double* eps_v, int64_t no, int64_t nv, double* D) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= no * nv) return;
@@ -195,7 +243,6 @@ __global__ void copy_lower_kernel(const double* src, int64_t lds, int64_t stride
 // Two-level blocked right-looking Cholesky: 64-wide column panels (diagonal
 // factorization + panel solve + update of the rest of the 256-wide outer
 // block), then one rank-256 update of the trailing matrix per outer block.
-constexpr int NB2 = 256;
 
 cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag, int* err,
                                   cudaStream_t stream) {
@@ -247,6 +294,47 @@ cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, 
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+cudaError_t launch_dsyrk_varlen(const MatDesc* mats, int nmat, int mode, int J0, int j0, int max_tiles,
+                                cudaStream_t stream);
+
+// Same schedule as launch_cholesky_lower over matrices of different orders:
+// every step is launched for the largest order and matrices that are already
+// finished (or too small for the step) leave at once.
+cudaError_t launch_logdet_varlen(const MatDesc* mats, int nmat, int nmax, int* err, cudaStream_t stream) {
+  if (nmat <= 0) return cudaSuccess;
+  trace_shift_varlen_kernel<<<nmat, 256, 0, stream>>>(mats);
+  ++g_launches;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  auto tiles = [](int n, int ncols) {
+    if (n <= 0 || ncols <= 0) return 0;
+    const int T = (n + 63) / 64, Tc = (std::min(ncols, n) + 63) / 64;
+    return Tc * T - Tc * (Tc - 1) / 2;
+  };
+  for (int J0 = 0; J0 < nmax; J0 += NB2) {
+    const int J1 = std::min(nmax, J0 + NB2);
+    for (int j0 = J0; j0 < J1; j0 += NB) {
+      potrf_varlen_kernel<<<nmat, 256, 0, stream>>>(mats, j0, err);
+      ++g_launches;
+      const int below = nmax - j0 - NB;
+      if (below <= 0) break;
+      trsm_varlen_kernel<<<dim3((below + 127) / 128, nmat), 128, 0, stream>>>(mats, j0);
+      ++g_launches;
+      // the largest tile count of this step is reached by the largest matrix
+      const int ncols = std::min(nmax, J0 + NB2) - (j0 + NB);
+      e = launch_dsyrk_varlen(mats, nmat, 0, J0, j0, tiles(below, ncols), stream);
+      if (e != cudaSuccess) return e;
+    }
+    const int trail = nmax - J1;
+    if (trail <= 0) break;
+    e = launch_dsyrk_varlen(mats, nmat, 1, J0, 0, tiles(trail, trail), stream);
+    if (e != cudaSuccess) return e;
+  }
+  logdet_sum_varlen_kernel<<<nmat, 256, 0, stream>>>(mats);
+  ++g_launches;
+  return cudaGetLastError();
 }
 
 cudaError_t launch_trace_shift(double* A, int64_t ld, int64_t stride, int n, int nmat, const double* diag,

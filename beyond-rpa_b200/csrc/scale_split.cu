@@ -26,10 +26,10 @@ __device__ __forceinline__ uint32_t bf162_bits(__nv_bfloat162 v) {
   return *reinterpret_cast<uint32_t*>(&v);
 }
 
-__global__ void __launch_bounds__(kThreads, 3) scale_split_kernel(
+__device__ __forceinline__ void scale_split_body(
     const double* __restrict__ R, int64_t ldR, int NQ, int64_t nov, const double* __restrict__ D,
-    FreqGroup fg, double alpha, __nv_bfloat16* __restrict__ Xhi, __nv_bfloat16* __restrict__ Xlo, int64_t pitch,
-    int64_t kstride, double* __restrict__ diag_part, int64_t ai_per_split) {
+    const FreqGroup& fg, double alpha, __nv_bfloat16* __restrict__ Xhi, __nv_bfloat16* __restrict__ Xlo,
+    int64_t pitch, int64_t kstride, double* __restrict__ diag_part, int64_t ai_per_split, int qtile, int split) {
   extern __shared__ double dyn_smem[];
   auto sfac = reinterpret_cast<double(*)[kTA]>(dyn_smem);                          // [kMaxKgLaunch][kTA]
   auto sdiag = reinterpret_cast<double(*)[kMaxKgLaunch][kTQ]>(dyn_smem + kMaxKgLaunch * kTA);  // [8][k][q]
@@ -39,10 +39,10 @@ __global__ void __launch_bounds__(kThreads, 3) scale_split_kernel(
   const int t = threadIdx.x;
   const int qi = t & 31;
   const int wa = t >> 5;
-  const int q0 = blockIdx.x * kTQ;
+  const int q0 = qtile * kTQ;
   const int q = q0 + qi;
   const int kg = fg.n;
-  const int64_t a_begin = (int64_t)blockIdx.y * ai_per_split;
+  const int64_t a_begin = (int64_t)split * ai_per_split;
   const int64_t a_end = min(nov, a_begin + ai_per_split);
 
   for (int k = 0; k < kMaxKgLaunch; ++k) sdiag[wa][k][qi] = 0.0;
@@ -110,9 +110,45 @@ __global__ void __launch_bounds__(kThreads, 3) scale_split_kernel(
       double acc = 0.0;
 #pragma unroll
       for (int w = 0; w < 8; ++w) acc += sdiag[w][k][row];
-      diag_part[((int64_t)blockIdx.y * kg + k) * NQ + q0 + row] = acc;
+      diag_part[((int64_t)split * kg + k) * NQ + q0 + row] = acc;
     }
   }
+}
+
+__global__ void __launch_bounds__(kThreads, 3) scale_split_kernel(
+    const double* __restrict__ R, int64_t ldR, int NQ, int64_t nov, const double* __restrict__ D,
+    FreqGroup fg, double alpha, __nv_bfloat16* __restrict__ Xhi, __nv_bfloat16* __restrict__ Xlo, int64_t pitch,
+    int64_t kstride, double* __restrict__ diag_part, int64_t ai_per_split) {
+  scale_split_body(R, ldR, NQ, nov, D, fg, alpha, Xhi, Xlo, pitch, kstride, diag_part, ai_per_split, blockIdx.x,
+                   blockIdx.y);
+}
+
+// Many instances in one launch: CTA b handles (instance, q tile, ai split) = work[b].
+__global__ void __launch_bounds__(kThreads, 3) scale_split_multi_kernel(const SplitJob* __restrict__ jobs,
+                                                                        const int4* __restrict__ work) {
+  const int4 w = work[blockIdx.x];
+  const SplitJob& j = jobs[w.x];
+  scale_split_body(j.R, j.ldR, j.NQ, j.nov, j.D, j.fg, j.alpha, j.Xhi, j.Xlo, j.pitch, j.kstride, j.diag_part,
+                   j.ai_per_split, w.y, w.z);
+}
+
+// diag[k*NQ+q] = sum over splits, for every instance (one thread per (instance, k, q))
+__global__ void diag_reduce_multi_kernel(const SplitJob* __restrict__ jobs, const int64_t* __restrict__ offsets,
+                                         int njobs, int64_t total) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= total) return;
+  int lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (offsets[mid] <= idx) lo = mid;
+    else hi = mid - 1;
+  }
+  const SplitJob& j = jobs[lo];
+  const int64_t e = idx - offsets[lo];
+  const int64_t per = (int64_t)j.fg.n * j.NQ;
+  double s = 0.0;
+  for (int sp = 0; sp < j.nsplit; ++sp) s += j.diag_part[(int64_t)sp * per + e];
+  j.diag[e] = s;
 }
 
 __global__ void diag_reduce_kernel(const double* __restrict__ diag_part, int nsplit, int kg, int NQ,
@@ -143,6 +179,22 @@ SplitPlan plan_scale_split(int NQ, int64_t nov, int num_sms) {
 
 constexpr size_t kSplitSmem =
     sizeof(double) * (kMaxKgLaunch * kTA + 8 * kMaxKgLaunch * kTQ) + sizeof(uint32_t) * 2 * kTQ * kWordPitch;
+
+cudaError_t launch_scale_split_multi(const SplitJob* jobs, const int4* work, int nwork, const int64_t* offsets,
+                                     int njobs, int64_t total, cudaStream_t stream) {
+  cudaError_t e0 =
+      cudaFuncSetAttribute(scale_split_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmem);
+  if (e0 != cudaSuccess) return e0;
+  if (nwork > 0) {
+    scale_split_multi_kernel<<<nwork, kThreads, kSplitSmem, stream>>>(jobs, work);
+    ++g_launches;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || total == 0) return e;
+  diag_reduce_multi_kernel<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(jobs, offsets, njobs, total);
+  ++g_launches;
+  return cudaGetLastError();
+}
 
 cudaError_t launch_scale_split(const double* R, int64_t ldR, int NQ, int64_t nov, const double* D,
                                const FreqGroup& fg, double alpha, __nv_bfloat16* Xhi, __nv_bfloat16* Xlo,

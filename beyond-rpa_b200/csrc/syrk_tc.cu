@@ -24,6 +24,8 @@
 // nov = 65536 an unsegmented accumulator biases E_c by ~1e-5 Eh).
 // Smem pipeline: 4 stages of {A_hi, A_lo (128x32), B_hi, B_lo (256x32)}
 // bf16, 64-byte swizzle.
+#include <vector>
+
 #include "kernels.h"
 
 namespace rpa {
@@ -73,11 +75,63 @@ __device__ __forceinline__ UnitCoord decode_unit(int u, int nblocks, int ntm) {
   return c;
 }
 
-__global__ void __launch_bounds__(kThreads, 1)
-    syrk_split_bf16_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
-                           const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
-                           const SyrkTcArgs args, const int nblocks, const int ntm, const int nunits,
-                           const int nchunks, const int seg_chunks) {
+// What a CTA needs to know about one work unit.
+struct Unit {
+  int k, tm, tn, NQ, nchunks;
+  double* Pk;          // Pi of this frequency
+  int64_t ldPi;
+  const double* dk;    // exact diagonal of this frequency
+  const CUtensorMap* map[4];  // A_hi, A_lo, B_hi, B_lo
+};
+
+// Single instance: tensor maps are kernel parameters, units are decoded.
+struct SingleSource {
+  const CUtensorMap* maps[4];
+  SyrkTcArgs a;
+  int nblocks, ntm, nchunks, nunits;
+  __device__ __forceinline__ Unit get(int u) const {
+    const UnitCoord c = decode_unit(u, nblocks, ntm);
+    Unit x;
+    x.k = c.k;
+    x.tm = c.tm;
+    x.tn = c.tn;
+    x.NQ = a.NQ;
+    x.nchunks = nchunks;
+    x.Pk = a.Pi + (int64_t)c.k * a.piStride;
+    x.ldPi = a.ldPi;
+    x.dk = a.diag + (int64_t)c.k * a.NQ;
+    for (int i = 0; i < 4; ++i) x.map[i] = maps[i];
+    return x;
+  }
+};
+
+// Many instances: per-instance descriptors (tensor maps in global memory) and a work list.
+struct MultiSource {
+  const SyrkInst* insts;
+  const uint4* work;  // (instance, k, tm, tn)
+  int nunits;
+  __device__ __forceinline__ Unit get(int u) const {
+    const uint4 w = work[u];
+    const SyrkInst& in = insts[w.x];
+    Unit x;
+    x.k = (int)w.y;
+    x.tm = (int)w.z;
+    x.tn = (int)w.w;
+    x.NQ = in.NQ;
+    x.nchunks = in.nchunks;
+    x.Pk = in.Pi + (int64_t)x.k * in.piStride;
+    x.ldPi = in.ldPi;
+    x.dk = in.diag + (int64_t)x.k * in.NQ;
+    x.map[0] = &in.tmAh;
+    x.map[1] = &in.tmAl;
+    x.map[2] = &in.tmBh;
+    x.map[3] = &in.tmBl;
+    return x;
+  }
+};
+
+template <class Source>
+__device__ __forceinline__ void syrk_body(const Source& src, int* err, const int seg_chunks) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
@@ -89,7 +143,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  int* err = args.err;
+  const int nunits = src.nunits;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
@@ -102,12 +156,6 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     mbar_init(drain, 1);
     fence_mbar_init();
-  }
-  if (warp == 0 && lane == 0) {
-    tma_prefetch_desc(&tmA_hi);
-    tma_prefetch_desc(&tmA_lo);
-    tma_prefetch_desc(&tmB_hi);
-    tma_prefetch_desc(&tmB_lo);
   }
   if (warp == 1) tmem_alloc(tmem_slot, kTmemCols);
   tc_fence_before();
@@ -127,19 +175,24 @@ __global__ void __launch_bounds__(kThreads, 1)
       uint32_t phase = 0;
       uint32_t issued = 0, issued_par = 0;  // per-stage bit masks: issued, parity of the last issue
       bool ok = true;
+      const CUtensorMap* last = nullptr;
       for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
-        const UnitCoord c = decode_unit(u, nblocks, ntm);
-        for (int ch = 0; ch < nchunks; ++ch) {
+        const Unit x = src.get(u);
+        if (x.map[0] != last) {
+          for (int i = 0; i < 4; ++i) tma_prefetch_desc(x.map[i]);
+          last = x.map[0];
+        }
+        for (int ch = 0; ch < x.nchunks; ++ch) {
           if (!mbar_wait(&empty[stage], phase ^ 1u, err, kDevTimeoutTmaEmpty)) {
             ok = false;
             break;
           }
           mbar_arrive_expect_tx(&full[stage], kStageBytes);
-          const int x = ch * TK;
-          tma_load_3d(a_hi(stage), &tmA_hi, &full[stage], x, c.tm * TM, c.k);
-          tma_load_3d(a_lo(stage), &tmA_lo, &full[stage], x, c.tm * TM, c.k);
-          tma_load_3d(b_hi(stage), &tmB_hi, &full[stage], x, c.tn * TN, c.k);
-          tma_load_3d(b_lo(stage), &tmB_lo, &full[stage], x, c.tn * TN, c.k);
+          const int c0 = ch * TK;
+          tma_load_3d(a_hi(stage), x.map[0], &full[stage], c0, x.tm * TM, x.k);
+          tma_load_3d(a_lo(stage), x.map[1], &full[stage], c0, x.tm * TM, x.k);
+          tma_load_3d(b_hi(stage), x.map[2], &full[stage], c0, x.tn * TN, x.k);
+          tma_load_3d(b_lo(stage), x.map[3], &full[stage], c0, x.tn * TN, x.k);
           issued |= 1u << stage;
           issued_par = (issued_par & ~(1u << stage)) | (phase << stage);
           if (++stage == kStages) {
@@ -160,6 +213,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       int it = 0;  // segment counter (selects the TMEM accumulator)
       bool ok = true;
       for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+        const int nchunks = src.get(u).nchunks;
         for (int c0 = 0; c0 < nchunks && ok; c0 += seg_chunks, ++it) {
           const int b = it & 1;
           const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
@@ -209,11 +263,11 @@ __global__ void __launch_bounds__(kThreads, 1)
     bool ok = true;
     float run[kEpiCols];
     for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
-      const UnitCoord c = decode_unit(u, nblocks, ntm);
-      const int m = c.tm * TM + quarter * 32 + lane;
-      const int warp_max_m = c.tm * TM + quarter * 32 + 31;
-      const int nbase = c.tn * TN + colq * kEpiCols;
-      for (int c0 = 0; c0 < nchunks; c0 += seg_chunks, ++it) {
+      const Unit x = src.get(u);
+      const int m = x.tm * TM + quarter * 32 + lane;
+      const int warp_max_m = x.tm * TM + quarter * 32 + 31;
+      const int nbase = x.tn * TN + colq * kEpiCols;
+      for (int c0 = 0; c0 < x.nchunks; c0 += seg_chunks, ++it) {
         const int b = it & 1;
         const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
         if (!mbar_wait(&acc_full[b], acc_phase, err, kDevTimeoutAccFull)) {
@@ -224,7 +278,7 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
         for (int cc = 0; cc < kEpiCols / 8; ++cc) {
           const int n0 = nbase + cc * 8;
-          if (n0 <= warp_max_m && n0 < args.NQ)  // warp-uniform: skip columns above the diagonal
+          if (n0 <= warp_max_m && n0 < x.NQ)  // warp-uniform: skip columns above the diagonal
             tmem_ld_add_x8(tmem_base + (uint32_t)(b * TN + colq * kEpiCols + cc * 8) + ((uint32_t)(quarter * 32) << 16),
                            &run[cc * 8], c0 == 0);
         }
@@ -233,16 +287,15 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (lane == 0) mbar_arrive(&acc_empty[b]);
       }
       if (!ok) break;
-      if (m < args.NQ && nbase <= m) {
-        double* p = args.Pi + (int64_t)c.k * args.piStride + (int64_t)m + (int64_t)nbase * args.ldPi;
+      if (m < x.NQ && nbase <= m) {
+        double* p = x.Pk + (int64_t)m + (int64_t)nbase * x.ldPi;
         const int jd = m - nbase;  // column index of the diagonal element (may be >= kEpiCols)
 #pragma unroll
         for (int j = 0; j < kEpiCols; ++j) {
           if (j < jd) *p = (double)run[j];
-          p += args.ldPi;
+          p += x.ldPi;
         }
-        if (jd < kEpiCols) args.Pi[(int64_t)c.k * args.piStride + (int64_t)m * (args.ldPi + 1)] =
-            args.diag[(int64_t)c.k * args.NQ + m];
+        if (jd < kEpiCols) x.Pk[(int64_t)m * (x.ldPi + 1)] = x.dk[m];
       }
     }
   }
@@ -252,6 +305,35 @@ __global__ void __launch_bounds__(kThreads, 1)
     tc_fence_after();
     tmem_dealloc(tmem_base, kTmemCols);
   }
+}
+
+__global__ void __launch_bounds__(kThreads, 1)
+    syrk_split_bf16_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
+                           const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
+                           const SyrkTcArgs args, const int nblocks, const int ntm, const int nunits,
+                           const int nchunks, const int seg_chunks) {
+  SingleSource src;
+  src.maps[0] = &tmA_hi;
+  src.maps[1] = &tmA_lo;
+  src.maps[2] = &tmB_hi;
+  src.maps[3] = &tmB_lo;
+  src.a = args;
+  src.nblocks = nblocks;
+  src.ntm = ntm;
+  src.nchunks = nchunks;
+  src.nunits = nunits;
+  syrk_body(src, args.err, seg_chunks);
+}
+
+// Many instances (fragments) in one persistent launch.
+__global__ void __launch_bounds__(kThreads, 1)
+    syrk_split_bf16_multi_kernel(const SyrkInst* __restrict__ insts, const uint4* __restrict__ work, const int nunits,
+                                 int* err, const int seg_chunks) {
+  MultiSource src;
+  src.insts = insts;
+  src.work = work;
+  src.nunits = nunits;
+  syrk_body(src, err, seg_chunks);
 }
 }  // namespace
 
@@ -269,9 +351,37 @@ cudaError_t launch_syrk_split_bf16(const CUtensorMap* tmA_hi, const CUtensorMap*
       cudaFuncSetAttribute(syrk_split_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
   if (e != cudaSuccess) return e;
   const int grid = nunits < num_sms ? nunits : num_sms;
-  int seg_chunks = a.seg_chunks > 0 ? a.seg_chunks : nchunks;
+  const int seg_chunks = a.seg_chunks > 0 ? a.seg_chunks : nchunks;
   syrk_split_bf16_kernel<<<grid, kThreads, kSmemBytes, stream>>>(*tmA_hi, *tmA_lo, *tmB_hi, *tmB_lo, a, nblocks,
                                                                   ntm, nunits, nchunks, seg_chunks);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+int syrk_tc_blocks(int NQ) {
+  const int ntm = (NQ + TM - 1) / TM;
+  const int ntn = (NQ + TN - 1) / TN;
+  int nblocks = 0;
+  for (int tn = 0; tn < ntn; ++tn) nblocks += (ntm - 2 * tn > 0) ? (ntm - 2 * tn) : 0;
+  return nblocks;
+}
+
+void syrk_tc_block_coords(int NQ, std::vector<uint2>& out) {
+  const int ntm = (NQ + TM - 1) / TM;
+  const int ntn = (NQ + TN - 1) / TN;
+  out.clear();
+  for (int tn = 0; tn < ntn; ++tn)
+    for (int tm = 2 * tn; tm < ntm; ++tm) out.push_back(make_uint2((unsigned)tm, (unsigned)tn));
+}
+
+cudaError_t launch_syrk_split_bf16_multi(const SyrkInst* insts, const uint4* work, int nunits, int seg_chunks,
+                                         int* err, int num_sms, cudaStream_t stream) {
+  if (nunits == 0) return cudaSuccess;
+  cudaError_t e =
+      cudaFuncSetAttribute(syrk_split_bf16_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+  if (e != cudaSuccess) return e;
+  const int grid = nunits < num_sms ? nunits : num_sms;
+  syrk_split_bf16_multi_kernel<<<grid, kThreads, kSmemBytes, stream>>>(insts, work, nunits, err, seg_chunks);
   ++g_launches;
   return cudaGetLastError();
 }

@@ -123,6 +123,31 @@ int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* OrbEnergies, d
                        double TargetError, double TargetRelError, int64_t NFixed, double* Freqs,
                        double* FreqWeights, int64_t* NFreqs);
 
+/* One system (a many-body-expansion fragment) of a batched call. */
+typedef struct rpa_instance {
+  int64_t NQ, NOcc, NVirt;
+  const double* R; /* NQ x NOcc*NVirt, column-major, leading dimension ldR */
+  int64_t ldR;
+  const double* OccEnergies;
+  const double* VirtEnergies;
+  int64_t NFreqs; /* <= 16 */
+  const double* Freqs;
+  const double* FreqWeights;
+  double alpha;
+} rpa_instance;
+
+/*
+ * RPA correlation energies of many independent systems of uneven size in one
+ * call (the subsystem loop of rpa_PostSCF, src/rpa/rpa_driver.f90:175-240,
+ * which the reference runs sequentially).  Instances are packed into
+ * memory-bounded batches; per batch one multi-instance scale/split launch, one
+ * persistent multi-instance tensor-core SYRK launch and one variable-order
+ * batched Cholesky run as a single CUDA graph.  Ec[i] receives the energy of
+ * instance i; Eu (may be NULL) the E(u) of all instances concatenated.
+ */
+int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* inst, int64_t prec, double* Ec,
+                        double* Eu);
+
 /*
  * Direct-ring T2 amplitudes T2 = U diag(A) U^T (nov x nov) at coupling
  * strength 1, by the randomised range finder of the reference: guess vectors

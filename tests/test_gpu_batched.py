@@ -1,0 +1,65 @@
+"""GPU tests of the batched many-instance energy (rpa_b200_ec_batched):
+every instance must match the single-system entry point and the FP64
+oracle, and a dimer of non-interacting monomers must give a vanishing
+interaction energy (size consistency, rpa_Eint2Body src/rpa/rpa_driver.f90:381-386).
+
+Tolerances: FP64 1e-10 Eh per instance; split-BF16 1e-6 Eh per instance and
+1e-7 Eh on the interaction energy.
+"""
+import numpy as np
+import pytest
+
+from oracle import rpa_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def systems(seed=100, n=7):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        no = int(rng.integers(3, 9))
+        nv = int(round(rng.uniform(8, 12) * no))
+        nq = 4 * (no + nv)
+        K = int(rng.choice([8, 12, 16]))
+        s = O.make_system(nq, no, nv, seed + i, decay=nq / 6.0, lam0=0.8)
+        x, w = O.casimir_polder(K, 0.5 + 0.1 * i)
+        out.append((s.R, s.eps_o, s.eps_v, x, w))
+    return out
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("split", 1e-6)])
+def test_batched_matches_single_and_oracle(handle, prec, tol):
+    sys_ = systems()
+    ec, eus = handle.ec_batched(sys_, prec=prec)
+    for (R, eo, ev, x, w), e, eu in zip(sys_, ec, eus):
+        single, single_eu = handle.ec_rpa(R, eo, ev, x, w, prec=prec)
+        assert abs(e - single) < 1e-12
+        ref, _ = O.ec_rpa(R, eo, ev, x, w)
+        assert abs(e - ref) < tol
+        assert np.max(np.abs(eu - single_eu)) < 1e-11
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-11), ("split", 1e-7)])
+def test_batched_dimer_size_consistency(handle, prec, tol):
+    a = O.make_system(120, 4, 26, 201, decay=30.0, lam0=0.6)
+    b = O.make_system(96, 3, 29, 202, decay=25.0, lam0=0.6)
+    eo = np.concatenate([a.eps_o, b.eps_o])
+    ev = np.concatenate([a.eps_v, b.eps_v])
+    no, nv = len(eo), len(ev)
+    R = np.zeros((a.nq + b.nq, no * nv))
+    for (s, q0, i0, a0) in ((a, 0, 0, 0), (b, a.nq, a.no, a.nv)):
+        Rr = s.R.reshape(s.nq, s.nv, s.no, order="F")
+        for i in range(s.no):
+            R[q0:q0 + s.nq, a0 + nv * (i0 + i): a0 + nv * (i0 + i) + s.nv] = Rr[:, :, i]
+    x, w = O.casimir_polder(12, 0.6)
+    ec, _ = handle.ec_batched([(R, eo, ev, x, w), (a.R, a.eps_o, a.eps_v, x, w), (b.R, b.eps_o, b.eps_v, x, w)],
+                              prec=prec)
+    assert abs(O.eint_2body(ec[0], ec[1], ec[2])) < tol
+
+
+def test_batched_repeated_call_uses_cached_graph(handle):
+    sys_ = systems(seed=300, n=5)
+    a, _ = handle.ec_batched(sys_, prec="split")
+    b, _ = handle.ec_batched(sys_, prec="split")
+    assert np.array_equal(a, b)
