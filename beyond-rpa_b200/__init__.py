@@ -92,6 +92,8 @@ def load_library(path: str | os.PathLike | None = None):
     lib.rpa_b200_dring_t2.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _dbl, _i64, _i64,
                                       _vp, ctypes.c_uint64, _dbl, _dbl, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _vp]
     lib.rpa_b200_ec_batched.argtypes = [_vp, _i64, _vp, _i64, _vp, _vp]
+    lib.rpa_b200_ec_grad.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _dbl, _i64, _vp,
+                                     _vp, _i64, _vp, _vp]
     lib.rpa_b200_exchange_sosex.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _dbl, _i64, _vp]
     if path is None:
         _lib = lib
@@ -237,6 +239,29 @@ class Handle:
         self._check(self.lib.rpa_b200_ec_from_pi(self._h, nq, K, p.ptr, nq, w.ptr, ctypes.byref(ec),
                                                  eu.ctypes.data))
         return ec.value, eu
+
+    def ec_grad(self, R, eps_o, eps_v, freqs, weights, alpha=4.0, prec="split", out=None):
+        """E_c and its adjoint (rpa_b200_ec_grad): returns (Ec, dR, dOcc, dVirt).
+
+        dR has R's (NQ, nov) column-major layout; with torch inputs pass `out` = (dR, dOcc, dVirt) tensors."""
+        nq = int(R.shape[0])
+        no, nv, K = len(eps_o), len(eps_v), len(freqs)
+        r = _colmajor(R, nq)
+        eo, ev, fr, w = _vec(eps_o), _vec(eps_v), _vec(freqs), _vec(weights)
+        if out is None:
+            dR = np.zeros((nq, no * nv), order="F")
+            dO = np.zeros(no)
+            dV = np.zeros(nv)
+            p_dR, ld_dR, p_dO, p_dV = dR.ctypes.data, nq, dO.ctypes.data, dV.ctypes.data
+        else:
+            dR, dO, dV = out
+            a = _colmajor(dR, nq)
+            p_dR, ld_dR = a.ptr, a.ld
+            p_dO, p_dV = _vec(dO).ptr, _vec(dV).ptr
+        ec = ctypes.c_double()
+        self._check(self.lib.rpa_b200_ec_grad(self._h, nq, no, nv, r.ptr, r.ld, eo.ptr, ev.ptr, K, fr.ptr, w.ptr,
+                                              float(alpha), _PREC[prec], ctypes.byref(ec), p_dR, ld_dR, p_dO, p_dV))
+        return ec.value, dR, dO, dV
 
     def ec_batched(self, systems, prec="split"):
         """Energies of many systems in one call (rpa_b200_ec_batched).

@@ -39,6 +39,7 @@ struct rpa_b200_handle {
   DevBuf tZ, tOm, tIOm, tP, tS, tV, tT, tTIT, tVt, tW, tU, tRU, tSmall, tRot, tPerm;
   // batched (many-instance) workspace: descriptors and per-batch results
   DevBuf bDesc, bRes;
+  DevBuf gY, gD;  // adjoint workspace
   struct BatchGraph {
     uint64_t key;
     std::vector<cudaGraphExec_t> execs;
@@ -670,7 +671,7 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
   if (h->own_stream) cudaStreamSynchronize(h->own_stream);
   for (DevBuf* b : {&h->R, &h->D, &h->eps, &h->Xhi, &h->Xlo, &h->diag_part, &h->diag, &h->Pi, &h->Ldiag, &h->ddbuf,
                     &h->tZ, &h->tOm, &h->tIOm, &h->tP, &h->tS, &h->tV, &h->tT, &h->tTIT, &h->tVt, &h->tW, &h->tU,
-                    &h->tRU, &h->tSmall, &h->tRot, &h->tPerm, &h->bDesc, &h->bRes})
+                    &h->tRU, &h->tSmall, &h->tRot, &h->tPerm, &h->bDesc, &h->bRes, &h->gY, &h->gD})
     release(*b);
   for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
   if (h->err_dev) cudaFree(h->err_dev);
@@ -1362,6 +1363,96 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
       ec = rpa::dd_add_dd(ec, {p, std::fma(eu.hi, f, -p) + eu.lo * f});
     }
     Ec[i] = ec.hi + ec.lo;
+  }
+  finish_timings(h);
+  return RPA_OK;
+}
+
+int rpa_b200_ec_grad(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R, int64_t ldR,
+                     const double* OccEnergies, const double* VirtEnergies, int64_t NFreqs, const double* Freqs,
+                     const double* FreqWeights, double alpha, int64_t prec, double* Ec, double* dR, int64_t lddR,
+                     double* dOcc, double* dVirt) {
+  int s = begin_call(h);
+  if (s != RPA_OK) return s;
+  Validated v;
+  if ((s = validate_common(h, NQ, NOcc, NVirt, R, ldR, OccEnergies, VirtEnergies, NFreqs, Freqs, alpha, prec, v)))
+    return s;
+  if (!FreqWeights || !dR || lddR < NQ) return fail(h, RPA_ERR_INVALID_ARG, "invalid gradient arguments");
+  if ((s = fetch_small(h, FreqWeights, NFreqs, v.weights))) return s;
+  const double* Rd;
+  int64_t ldd;
+  if ((s = stage_R(h, v, R, ldR, &Rd, &ldd))) return s;
+  RPA_CUDA(h, cudaEventRecord(h->ev[1], h->stream));
+  // recompute Pi(u) for every frequency and factor 1 + Pi(u) (the energy comes out on the way)
+  if ((s = build_pi(h, v, Rd, ldd, alpha, prec))) return s;
+  double ec = 0.0;
+  if ((s = energy_from_workspace(h, v.NQ, v.K, v.weights, &ec, nullptr))) return s;
+  if (Ec) *Ec = ec;
+  const int n = v.NQ;
+  const int64_t nov = v.nov;
+  // Y_k = (1 + Pi_k)^{-1} R for groups of frequencies sized to the free memory
+  size_t freeB = 0, totalB = 0;
+  RPA_CUDA(h, cudaMemGetInfo(&freeB, &totalB));
+  const size_t perK = (size_t)n * nov * 8;
+  int grp = (int)std::max<size_t>(1, std::min<size_t>(16, (size_t)(0.5 * (double)(freeB + h->gY.bytes)) / perK));
+  grp = std::min(grp, v.K);
+  RPA_CUDA(h, ensure(h->gY, perK * grp));
+  RPA_CUDA(h, ensure(h->gD, (size_t)nov * 8));
+  const bool dev_out = is_device_ptr(dR);
+  double* dRd = dR;
+  int64_t lddr = lddR;
+  if (!dev_out) {
+    RPA_CUDA(h, ensure(h->tU, (size_t)n * nov * 8));  // device staging of dR
+    dRd = static_cast<double*>(h->tU.p);
+    lddr = n;
+  }
+  double* Y = static_cast<double*>(h->gY.p);
+  double* dD = static_cast<double*>(h->gD.p);
+  const double* L = static_cast<const double*>(h->Pi.p);
+  for (int g0 = 0; g0 < v.K; g0 += grp) {
+    const int nb = std::min(grp, v.K - g0);
+    RPA_CUDA(h, rpa::launch_replicate(Rd, ldd, n, nov, Y, n, (int64_t)n * nov, nb, h->stream));
+    const double* Lg = L + (int64_t)g0 * n * n;
+    RPA_CUDA(h, rpa::launch_trsm_lower_left(Lg, n, (int64_t)n * n, Y, n, (int64_t)n * nov, n, (int)nov, nb,
+                                            h->stream));
+    RPA_CUDA(h, rpa::launch_trsm_lower_trans_left(Lg, n, (int64_t)n * n, Y, n, (int64_t)n * nov, n, (int)nov, nb,
+                                                  h->stream));
+    rpa::GradGroup gg{};
+    gg.n = nb;
+    gg.alpha = alpha;
+    for (int k = 0; k < nb; ++k) {
+      gg.u2[k] = v.freqs[g0 + k] * v.freqs[g0 + k];
+      gg.f[k] = v.weights[g0 + k] / (2.0 * kPi);
+    }
+    RPA_CUDA(h, rpa::launch_grad_accum(Rd, ldd, Y, n, (int64_t)n * nov, n, nov, static_cast<const double*>(h->D.p),
+                                       gg, dRd, lddr, dD, g0 == 0, h->stream));
+  }
+  if (!dev_out)
+    RPA_CUDA(h, cudaMemcpy2DAsync(dR, (size_t)lddR * 8, dRd, (size_t)n * 8, (size_t)n * 8, (size_t)nov,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  std::vector<double> dDh((size_t)nov);
+  RPA_CUDA(h, cudaMemcpyAsync(dDh.data(), dD, (size_t)nov * 8, cudaMemcpyDeviceToHost, h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  if ((s = check_device_error(h))) return s;
+  // dE/de_a = sum_i dE/dD(ai), dE/de_i = -sum_a dE/dD(ai)
+  if (dOcc || dVirt) {
+    std::vector<double> go((size_t)v.no, 0.0), gv((size_t)v.nv, 0.0);
+    for (int64_t i = 0; i < v.no; ++i)
+      for (int64_t a = 0; a < v.nv; ++a) {
+        const double x = dDh[(size_t)(a + v.nv * i)];
+        go[i] -= x;
+        gv[a] += x;
+      }
+    std::vector<double>* outs[2] = {&go, &gv};
+    double* dst[2] = {dOcc, dVirt};
+    for (int t = 0; t < 2; ++t) {
+      if (!dst[t]) continue;
+      if (is_device_ptr(dst[t]))
+        RPA_CUDA(h, cudaMemcpy(dst[t], outs[t]->data(), outs[t]->size() * 8, cudaMemcpyHostToDevice));
+      else
+        std::memcpy(dst[t], outs[t]->data(), outs[t]->size() * 8);
+    }
   }
   finish_timings(h);
   return RPA_OK;

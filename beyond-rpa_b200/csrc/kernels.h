@@ -163,6 +163,21 @@ cudaError_t launch_gemm_f64(const GemmF64Args& g, cudaStream_t stream);
 // Batched forward substitution L_b X_b = B_b in place (L lower, column-major).
 cudaError_t launch_trsm_lower_left(const double* L, int64_t ldl, int64_t sL, double* X, int64_t ldx, int64_t sX,
                                    int n, int ncols, int batch, cudaStream_t stream);
+// Batched backward substitution L_b^T X_b = B_b in place (L lower, column-major).
+cudaError_t launch_trsm_lower_trans_left(const double* L, int64_t ldl, int64_t sL, double* X, int64_t ldx,
+                                         int64_t sX, int n, int ncols, int batch, cudaStream_t stream);
+// Adjoint of E_c for a group of <= 16 frequencies (f_k = w_k / 2pi).
+struct GradGroup {
+  int n;
+  double alpha;
+  double u2[16];
+  double f[16];
+};
+cudaError_t launch_grad_accum(const double* R, int64_t ldR, const double* Y, int64_t ldy, int64_t sY, int NQ,
+                              int64_t nov, const double* D, const GradGroup& gg, double* dR, int64_t lddR, double* dD,
+                              bool first, cudaStream_t stream);
+cudaError_t launch_replicate(const double* R, int64_t ldR, int NQ, int64_t nov, double* Y, int64_t ldy, int64_t sY,
+                             int nb, cudaStream_t stream);
 // One sweep (m-1 rounds) of the parallel two-sided Jacobi method: A <- J^T A J, V <- V J.
 cudaError_t launch_jacobi_sweep(double* A, int64_t lda, double* V, int64_t ldv, int n, double4* rot,
                                 cudaStream_t stream);

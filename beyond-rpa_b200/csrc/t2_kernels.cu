@@ -53,6 +53,91 @@ __global__ void __launch_bounds__(TCOLS) trsm_diag_kernel(const double* L, int64
   }
 }
 
+// X_b(j0:j0+nb, cols) <- L_b(j0:j0+nb, j0:j0+nb)^{-T} X_b(j0:j0+nb, cols)  (backward substitution)
+__global__ void __launch_bounds__(TCOLS) trsm_diag_trans_kernel(const double* L, int64_t ldl, int64_t sL, double* X,
+                                                                int64_t ldx, int64_t sX, int n, int ncols, int j0) {
+  extern __shared__ double trsm_smem[];
+  auto Ls = reinterpret_cast<double(*)[TB + 1]>(trsm_smem);
+  auto Xs = reinterpret_cast<double(*)[TCOLS + 1]>(trsm_smem + TB * (TB + 1));
+  const int b = blockIdx.y;
+  const double* Lb = L + (int64_t)b * sL;
+  double* Xb = X + (int64_t)b * sX;
+  const int nb = min(TB, n - j0);
+  const int c0 = blockIdx.x * TCOLS;
+  const int t = threadIdx.x;
+  for (int idx = t; idx < TB * TB; idx += blockDim.x) {
+    const int r = idx % TB, c = idx / TB;
+    Ls[r][c] = (r < nb && c <= r) ? Lb[(int64_t)(j0 + r) + ldl * (j0 + c)] : 0.0;
+  }
+  for (int idx = t; idx < TB * TCOLS; idx += blockDim.x) {
+    const int r = idx % TB, c = idx / TB;
+    Xs[r][c] = (r < nb && c0 + c < ncols) ? Xb[(int64_t)(j0 + r) + ldx * (c0 + c)] : 0.0;
+  }
+  __syncthreads();
+  for (int r = nb - 1; r >= 0; --r) {
+    double s = Xs[r][t];
+    for (int m = r + 1; m < nb; ++m) s -= Ls[m][r] * Xs[m][t];
+    Xs[r][t] = s / Ls[r][r];
+  }
+  __syncthreads();
+  for (int idx = t; idx < TB * TCOLS; idx += blockDim.x) {
+    const int r = idx % TB, c = idx / TB;
+    if (r < nb && c0 + c < ncols) Xb[(int64_t)(j0 + r) + ldx * (c0 + c)] = Xs[r][c];
+  }
+}
+
+// Adjoint accumulation for a group of frequencies, one warp per column ai:
+//   dR(:,ai) (+)= sum_k 2 alpha f_k c_k(ai) (Y_k - R)(:,ai)
+//   dD(ai)   (+)= sum_k alpha f_k dc_k/dD(ai) R(:,ai)^T (Y_k - R)(:,ai)
+// f_k = w_k/(2 pi), c = D/(D^2+u^2), dc/dD = (u^2-D^2)/(D^2+u^2)^2.
+__global__ void __launch_bounds__(256) grad_accum_kernel(const double* R, int64_t ldR, const double* Y, int64_t ldy,
+                                                         int64_t sY, int NQ, int64_t nov, const double* D,
+                                                         GradGroup gg, double* dR, int64_t lddR, double* dD,
+                                                         int first) {
+  const int64_t a = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (a >= nov) return;
+  const double d = D[a];
+  double cfac[16], dfac[16];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    if (k < gg.n) {
+      const double den = d * d + gg.u2[k];
+      cfac[k] = 2.0 * gg.alpha * gg.f[k] * d / den;
+      dfac[k] = gg.alpha * gg.f[k] * (gg.u2[k] - d * d) / (den * den);
+    } else {
+      cfac[k] = dfac[k] = 0.0;
+    }
+  }
+  double dot = 0.0;
+  for (int q = lane; q < NQ; q += 32) {
+    const double r = R[(int64_t)q + ldR * a];
+    double g = first ? 0.0 : dR[(int64_t)q + lddR * a];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      if (k < gg.n) {
+        const double m = Y[(int64_t)k * sY + (int64_t)q + ldy * a] - r;
+        g += cfac[k] * m;
+        dot += dfac[k] * r * m;
+      }
+    }
+    dR[(int64_t)q + lddR * a] = g;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) dot += __shfl_down_sync(0xffffffffu, dot, off);
+  if (lane == 0) dD[a] = (first ? 0.0 : dD[a]) + dot;
+}
+
+// Y_b = R for every b (strided copy of a column-major matrix)
+__global__ void replicate_kernel(const double* R, int64_t ldR, int NQ, int64_t nov, double* Y, int64_t ldy,
+                                 int64_t sY, int nb) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)NQ * nov) return;
+  const int64_t q = idx % NQ, a = idx / NQ;
+  const double r = R[q + ldR * a];
+  for (int b = 0; b < nb; ++b) Y[(int64_t)b * sY + q + ldy * a] = r;
+}
+
 // ----------------------------------------------------------------- Jacobi
 __device__ __forceinline__ int rr_index(int j, int r, int m) { return j == 0 ? 0 : 1 + (j - 1 + r) % (m - 1); }
 
@@ -281,6 +366,62 @@ cudaError_t launch_trsm_lower_left(const double* L, int64_t ldl, int64_t sL, dou
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+cudaError_t launch_trsm_lower_trans_left(const double* L, int64_t ldl, int64_t sL, double* X, int64_t ldx,
+                                         int64_t sX, int n, int ncols, int batch, cudaStream_t stream) {
+  cudaError_t e0 =
+      cudaFuncSetAttribute(trsm_diag_trans_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem);
+  if (e0 != cudaSuccess) return e0;
+  const int nblk = (n + TB - 1) / TB;
+  for (int bi = nblk - 1; bi >= 0; --bi) {
+    const int j0 = bi * TB;
+    trsm_diag_trans_kernel<<<dim3((ncols + TCOLS - 1) / TCOLS, batch), TCOLS, kTrsmSmem, stream>>>(
+        L, ldl, sL, X, ldx, sX, n, ncols, j0);
+    ++g_launches;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (j0 == 0) break;
+    const int nb = min(TB, n - j0);
+    // X(0:j0, :) -= L(j0:j0+nb, 0:j0)^T X(j0:j0+nb, :)
+    GemmF64Args g{};
+    g.M = j0;
+    g.N = ncols;
+    g.K = nb;
+    g.A = L + j0;  // A(m, k) = L(j0 + k, m)
+    g.a_m = ldl;
+    g.a_k = 1;
+    g.sA = sL;
+    g.B = X + j0;
+    g.b_k = 1;
+    g.b_n = ldx;
+    g.sB = sX;
+    g.C = X;
+    g.ldc = ldx;
+    g.sC = sX;
+    g.alpha = -1.0;
+    g.beta = 1.0;
+    g.batch = batch;
+    e = launch_gemm_f64(g, stream);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_grad_accum(const double* R, int64_t ldR, const double* Y, int64_t ldy, int64_t sY, int NQ,
+                              int64_t nov, const double* D, const GradGroup& gg, double* dR, int64_t lddR, double* dD,
+                              bool first, cudaStream_t stream) {
+  grad_accum_kernel<<<(unsigned)((nov + 7) / 8), 256, 0, stream>>>(R, ldR, Y, ldy, sY, NQ, nov, D, gg, dR, lddR, dD,
+                                                                   first ? 1 : 0);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_replicate(const double* R, int64_t ldR, int NQ, int64_t nov, double* Y, int64_t ldy, int64_t sY,
+                             int nb, cudaStream_t stream) {
+  replicate_kernel<<<blocks_for((int64_t)NQ * nov), 256, 0, stream>>>(R, ldR, NQ, nov, Y, ldy, sY, nb);
+  ++g_launches;
+  return cudaGetLastError();
 }
 
 cudaError_t launch_jacobi_sweep(double* A, int64_t lda, double* V, int64_t ldv, int n, double4* rot,

@@ -83,3 +83,32 @@ def make_single_system(name="single_4096", seed=0, device="cuda", K=None):
     Rt *= math.sqrt(kw["lam0"] / lam)
     x, w = freq_grid(np.concatenate([eo, ev]), no, nv, nfixed=K)
     return SyntheticSystem(R=R, eps_o=eo, eps_v=ev, freqs=x, weights=w)
+
+
+def make_mbe_batch(n_inst=512, seed=0, device="cuda", dimer_frac=0.6):
+    """Many-body-expansion fragment batch: n_inst instances (dimer_frac dimers, the
+    rest trimers) with NOcc ~ U{16..48}, NVirt = round(U[8,12] NOcc),
+    NQ = 4 (NOcc + NVirt), K in {8, 12, 16}; each drawn like the water-dimer
+    twin (occ U[-1.3,-0.4], virt log-U[0.03,4], R ~ N(0,1) exp(-Q/(NQ/8)),
+    lambda_max(Pi(0)) = 0.8) from seed + instance id.  Returns a list of
+    (R, eps_o, eps_v, freqs, weights) and the dimer/trimer labels."""
+    import torch
+    from . import freq_grid
+    rng = np.random.default_rng(seed)
+    out, kinds = [], []
+    for i in range(n_inst):
+        no = int(rng.integers(16, 49))
+        nv = int(round(rng.uniform(8.0, 12.0) * no))
+        nq = 4 * (no + nv)
+        K = int(rng.choice([8, 12, 16]))
+        eo, ev = orbital_energies(no, nv, seed + 7919 * (i + 1), (-1.3, -0.4), (0.03, 4.0))
+        g = torch.Generator(device=device).manual_seed(seed + i + 1)
+        Rt = torch.randn((no * nv, nq), generator=g, device=device, dtype=torch.float64)
+        Rt *= torch.exp(-torch.arange(nq, device=device, dtype=torch.float64) / (nq / 8.0))[None, :]
+        d = torch.from_numpy((ev[:, None] - eo[None, :]).reshape(-1, order="F")).to(device)
+        lam = lambda_max_pi0(Rt.T, d, iters=25)
+        Rt *= math.sqrt(0.8 / lam)
+        x, w = freq_grid(np.concatenate([eo, ev]), no, nv, nfixed=K)
+        out.append((Rt.T, eo, ev, x, w))
+        kinds.append("dimer" if i < int(round(dimer_frac * n_inst)) else "trimer")
+    return out, kinds

@@ -123,6 +123,21 @@ int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* OrbEnergies, d
                        double TargetError, double TargetRelError, int64_t NFixed, double* Freqs,
                        double* FreqWeights, int64_t* NFreqs);
 
+/*
+ * Adjoint of the RPA energy: dE_c/dR (NQ x nov, leading dimension lddR),
+ * dE_c/dOccEnergies (NOcc) and dE_c/dVirtEnergies (NVirt); Ec (may be NULL)
+ * the energy itself.  No counterpart in the reference (it has no gradients):
+ *   dE/dR(:,ai) = sum_u w_u/(2 pi) 2 alpha c_u(ai) ((1+Pi_u)^{-1} - 1) R(:,ai),
+ *   dE/dD(ai)   = sum_u w_u/(2 pi) alpha R(:,ai)^T ((1+Pi_u)^{-1} - 1) R(:,ai) dc_u/dD,
+ * c_u = D/(D^2+u^2).  Pi(u) is recomputed (prec as in rpa_b200_ec) and
+ * factorised; (1+Pi_u)^{-1} R comes from two batched triangular solves in FP64.
+ * dR/dOcc/dVirt may be host or device pointers (dOcc/dVirt may be NULL).
+ */
+int rpa_b200_ec_grad(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R, int64_t ldR,
+                     const double* OccEnergies, const double* VirtEnergies, int64_t NFreqs, const double* Freqs,
+                     const double* FreqWeights, double alpha, int64_t prec, double* Ec, double* dR, int64_t lddR,
+                     double* dOcc, double* dVirt);
+
 /* One system (a many-body-expansion fragment) of a batched call. */
 typedef struct rpa_instance {
   int64_t NQ, NOcc, NVirt;
