@@ -1114,8 +1114,14 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
     per[i].pib = (size_t)v[i].K * v[i].NQ * v[i].NQ * 8;
     per[i].smallb = (size_t)v[i].K * v[i].NQ * 8 * (2 + per[i].plan.nsplit) + 64 * (size_t)v[i].K;
   }
+  if (prec == RPA_PREC_FP64) {  // the bf16 operands are not used: give their memory to Pi
+    RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+    release(h->Xhi);
+    release(h->Xlo);
+  }
   size_t freeB = 0, totalB = 0;
   RPA_CUDA(h, cudaMemGetInfo(&freeB, &totalB));
+  // buffers that ensure() below may free and reallocate count as available
   const size_t have = h->Xhi.bytes + h->Xlo.bytes + h->Pi.bytes + h->Ldiag.bytes;
   const size_t budget = (size_t)(0.6 * (double)(freeB + have));
   std::vector<std::pair<int, int>> batches;  // [b0, b1)

@@ -3,7 +3,8 @@ torch.autograd.Function): against the FP64 oracle gradient and central finite
 differences (step 1e-5) on 64 random entries.
 
 Tolerances: FP64 path relative error <= 1e-10 against the oracle gradient and
-<= 1e-6 against finite differences; split-BF16 Pi relative error <= 3e-4 (the
+<= 1e-6 (plus 1e-7 of the largest gradient entry, the O(h^2) truncation of
+central differences) against finite differences; split-BF16 Pi relative error <= 3e-4 (the
 Pi contraction carries ~1e-5 relative rounding into (1+Pi)^{-1}).
 """
 import numpy as np
@@ -47,14 +48,16 @@ def test_grad_central_finite_differences(handle):
         Rm[q, ai] -= h
         fd = (handle.ec_rpa(Rp, s.eps_o, s.eps_v, x, w, prec="fp64")[0] -
               handle.ec_rpa(Rm, s.eps_o, s.eps_v, x, w, prec="fp64")[0]) / (2 * h)
-        assert abs(fd - dR[q, ai]) <= 1e-6 * max(abs(fd), 1e-3 * np.max(np.abs(dR)))
+        # central differences carry an O(h^2) truncation error (~1e-10 here): relative 1e-6 on the
+        # entry plus 1e-7 of the gradient's largest entry
+        assert abs(fd - dR[q, ai]) <= 1e-6 * abs(fd) + 1e-7 * np.max(np.abs(dR))
     for i in range(s.no):
         ep, em = s.eps_o.copy(), s.eps_o.copy()
         ep[i] += h
         em[i] -= h
         fd = (handle.ec_rpa(s.R, ep, s.eps_v, x, w, prec="fp64")[0] -
               handle.ec_rpa(s.R, em, s.eps_v, x, w, prec="fp64")[0]) / (2 * h)
-        assert abs(fd - do[i]) <= 1e-6 * max(abs(fd), 1e-9)
+        assert abs(fd - do[i]) <= 1e-6 * abs(fd) + 1e-7 * np.max(np.abs(do))
 
 
 def test_autograd_function_matches_entry_point(handle, pkg):
