@@ -360,6 +360,70 @@ def run_mbe(args):
     h.close()
 
 
+def run_adjoint(args):
+    """Adjoint workload (adjoint_2560: NQ=2560, NOcc=48, NVirt=640, K=16): time of E_c + dE/dR, dE/de,
+    split vs FP64, and a central finite-difference check (step 1e-5, FP64) on 64 random entries of R."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    pkg = load_package()
+    from beyond_rpa_b200.workloads import make_single_system, SINGLE_SYSTEM
+    nq, no, nv, K, _ = SINGLE_SYSTEM[args.workload]
+    h = pkg.Handle(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    h.set_stream(stream.cuda_stream)
+    s = make_single_system(args.workload, seed=77)
+    nov = no * nv
+    dR = torch.empty((nov, nq), dtype=torch.float64, device="cuda").T
+    dO = torch.empty(no, dtype=torch.float64, device="cuda")
+    dV = torch.empty(nv, dtype=torch.float64, device="cuda")
+    eo = torch.from_numpy(s.eps_o).cuda()
+    ev = torch.from_numpy(s.eps_v).cuda()
+    out = {}
+    grads = {}
+    for prec in ("split", "fp64"):
+        for _ in range(args.warmup):
+            h.ec_grad(s.R, eo, ev, s.freqs, s.weights, prec=prec, out=(dR, dO, dV))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            ec, *_ = h.ec_grad(s.R, eo, ev, s.freqs, s.weights, prec=prec, out=(dR, dO, dV))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[prec] = {"ms_per_gradient": e0.elapsed_time(e1) / args.steps, "Ec": ec}
+        grads[prec] = (dR.clone(), dO.clone(), dV.clone())
+    g64 = grads["fp64"][0]
+    out["split_vs_fp64_rel_err_dR"] = float((grads["split"][0] - g64).abs().max() / g64.abs().max())
+    out["split_vs_fp64_rel_err_deps"] = float(
+        max((grads["split"][1] - grads["fp64"][1]).abs().max() / grads["fp64"][1].abs().max(),
+            (grads["split"][2] - grads["fp64"][2]).abs().max() / grads["fp64"][2].abs().max()))
+    # central finite differences on 64 random entries (FP64 energies)
+    rng = np.random.default_rng(9)
+    hstep = 1e-5
+    worst = 0.0
+    worst_abs = 0.0
+    gmax = float(g64.abs().max())
+    for _ in range(64):
+        q, ai = int(rng.integers(nq)), int(rng.integers(nov))
+        old = float(s.R[q, ai])
+        s.R[q, ai] = old + hstep
+        ep, _ = h.ec_rpa(s.R, eo, ev, s.freqs, s.weights, prec="fp64")
+        s.R[q, ai] = old - hstep
+        em, _ = h.ec_rpa(s.R, eo, ev, s.freqs, s.weights, prec="fp64")
+        s.R[q, ai] = old
+        fd = (ep - em) / (2 * hstep)
+        worst = max(worst, abs(fd - float(g64[q, ai])) / max(abs(fd), 1e-3 * gmax))
+        worst_abs = max(worst_abs, abs(fd - float(g64[q, ai])))
+    out["fd_max_rel_err_64_entries"] = worst
+    out["fd_max_abs_err_over_max_grad"] = worst_abs / gmax
+    print(json.dumps({"metric": "RPA E_c adjoint (dE/dR, dE/de)", "workload": f"{args.workload}: NQ={nq} "
+                      f"NOcc={no} NVirt={nv} K={K}", "value": 1e3 / out["split"]["ms_per_gradient"],
+                      "unit": "gradients/s", **out}), flush=True)
+    h.close()
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -405,6 +469,8 @@ def main():
         run_reference(args)
     elif args.workload.startswith("mbe"):
         run_mbe(args)
+    elif args.workload.startswith("adjoint"):
+        run_adjoint(args)
     else:
         run_ours(args)
 
