@@ -207,6 +207,7 @@ def run_ours(args):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     contraction, split, logdet, launches, ecs = [], [], [], 0, []
+    pi_ms, staging, other = [], [], []
     e0.record(stream)
     for _ in range(args.steps):
         ec, eu = h.ec_rpa(s.R, s.eps_o, s.eps_v, s.freqs, s.weights, prec="split")
@@ -214,6 +215,9 @@ def run_ours(args):
         contraction.append(tm["contraction_ms"])
         split.append(tm["split_ms"])
         logdet.append(tm["logdet_ms"])
+        pi_ms.append(tm["pi_ms"])
+        staging.append(tm["staging_ms"])
+        other.append(tm["other_ms"])
         launches += h.launches()
         ecs.append(ec)
     e1.record(stream)
@@ -295,7 +299,8 @@ def run_ours(args):
                      "note": f"peak = bf16_tflops_sustained ({src}); achieved = 3 bf16 SYRK products "
                              f"3*NQ^2*nov*K / contraction time"},
         "phase_ms": {"contraction": tc_ms, "scale_split": statistics.mean(split),
-                     "logdet": statistics.mean(logdet)},
+                     "logdet": statistics.mean(logdet), "pi_build_total": statistics.mean(pi_ms),
+                     "staging": statistics.mean(staging), "result_copies": statistics.mean(other)},
         "pi_build_tflops_fp64_equiv": pi_flops / ((tc_ms + statistics.mean(split)) / 1e3) / 1e12,
         "fp64_form": {"ms_per_step": t64_ms, "contraction_ms": t64["contraction_ms"],
                       "logdet_ms": t64["logdet_ms"], "speedup_split_vs_fp64": t64_ms / (t_ms / args.steps)},

@@ -9,7 +9,7 @@
 // A is column-major (rows contiguous), exactly the Cholesky-vector layout
 // R(Q, ai) and the panel layout of a column-major lower Cholesky factor.
 // CTA tile 64 x 64, 4 warps in 2 x 2, warp tile 32 x 32 (4 x 4 DMMA tiles),
-// 16-deep K chunks double-buffered through shared memory.
+// 16-deep K chunks streamed through a 3-stage cp.async pipeline.
 #include "kernels.h"
 
 namespace rpa {
@@ -41,12 +41,28 @@ __device__ __forceinline__ void trap_decode(int b, int T, int Tc, int& tm, int& 
 }
 
 // One 64 x 64 tile (tm, tn) of C(lower trapezoid, ncols columns) for matrix z.
+constexpr int kStages = 3;  // cp.async pipeline depth
+constexpr size_t kTileSmem = sizeof(double) * (size_t)kStages * (2 * BK * LDS + BK);
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem), "r"(valid ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// One 64 x 64 tile (tm, tn) of C(lower trapezoid, ncols columns) for matrix z.
+// Operands stream global -> shared through a kStages-deep cp.async pipeline
+// (out-of-range elements zero-filled); one barrier per 16-deep K chunk.
 template <bool kScaled>
 __device__ __forceinline__ void dsyrk_tile(const DsyrkArgs& a, const double* A, double* C, int ncols, int tm, int tn,
                                            int z) {
-  __shared__ double As[2][BK][LDS];
-  __shared__ double Bs[2][BK][LDS];
-  __shared__ double sS[2][BK];
+  extern __shared__ double tile_smem[];
+  auto As = reinterpret_cast<double(*)[BK][LDS]>(tile_smem);                        // [kStages]
+  auto Bs = reinterpret_cast<double(*)[BK][LDS]>(tile_smem + kStages * BK * LDS);   // [kStages]
+  auto sS = reinterpret_cast<double(*)[BK]>(tile_smem + 2 * kStages * BK * LDS);    // [kStages]
 
   const int m0 = tm * BM, n0 = tn * BM;
   const int t = threadIdx.x;
@@ -60,61 +76,57 @@ __device__ __forceinline__ void dsyrk_tile(const DsyrkArgs& a, const double* A, 
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-  double ra[8], rb[8];
-  auto gload = [&](int64_t k0) {
+  auto load_stage = [&](int st, int64_t k0) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       const int idx = t + kThreads * i;
       const int col = idx / BM, row = idx % BM;
       const int64_t k = k0 + col;
       const bool kin = k < a.kdim;
-      ra[i] = (kin && m0 + row < a.n) ? A[(int64_t)(m0 + row) + a.lda * k] : 0.0;
-      rb[i] = (kin && n0 + row < a.n) ? A[(int64_t)(n0 + row) + a.lda * k] : 0.0;
+      const bool va = kin && m0 + row < a.n, vb = kin && n0 + row < a.n;
+      cp_async8(&As[st][col][row], va ? A + (int64_t)(m0 + row) + a.lda * k : A, va);
+      cp_async8(&Bs[st][col][row], vb ? A + (int64_t)(n0 + row) + a.lda * k : A, vb);
     }
-  };
-  auto sstore = [&](int buf, int64_t k0) {
     if (kScaled && t < BK) {
       const int64_t k = k0 + t;
-      double s = 0.0;
+      double sc = 0.0;
       if (k < a.kdim) {
         const double d = a.D[k];
-        s = a.alpha * d / (d * d + u2);
+        sc = a.alpha * d / (d * d + u2);
       }
-      sS[buf][t] = s;
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int idx = t + kThreads * i;
-      const int col = idx / BM, row = idx % BM;
-      As[buf][col][row] = ra[i];
-      Bs[buf][col][row] = rb[i];
+      sS[st][t] = sc;
     }
   };
 
   const int64_t nch = (a.kdim + BK - 1) / BK;
-  gload(0);
-  sstore(0, 0);
-  __syncthreads();
+#pragma unroll
+  for (int st = 0; st < kStages - 1; ++st) {
+    if (st < nch) load_stage(st, (int64_t)st * BK);
+    cp_async_commit();
+  }
   for (int64_t c = 0; c < nch; ++c) {
-    const int buf = (int)(c & 1);
-    if (c + 1 < nch) gload((c + 1) * BK);
+    cp_async_wait<kStages - 2>();
+    __syncthreads();
+    const int64_t cn = c + kStages - 1;
+    if (cn < nch) load_stage((int)(cn % kStages), cn * BK);
+    cp_async_commit();
+    const int buf = (int)(c % kStages);
 #pragma unroll
     for (int kk = 0; kk < BK; kk += 4) {
       const int kr = kk + (lane & 3);
       double af[4], bf[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) af[i] = As[buf][kr][wm * 32 + i * 8 + (lane >> 2)];
-      const double s = kScaled ? sS[buf][kr] : 1.0;
+      const double sc = kScaled ? sS[buf][kr] : 1.0;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bf[j] = Bs[buf][kr][wn * 32 + j * 8 + (lane >> 2)] * s;
+      for (int j = 0; j < 4; ++j) bf[j] = Bs[buf][kr][wn * 32 + j * 8 + (lane >> 2)] * sc;
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
     }
-    if (c + 1 < nch) sstore(buf ^ 1, (c + 1) * BK);
-    __syncthreads();
   }
+  cp_async_wait<0>();
 
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
@@ -135,7 +147,7 @@ __device__ __forceinline__ void dsyrk_tile(const DsyrkArgs& a, const double* A, 
 }
 
 template <bool kScaled>
-__global__ void __launch_bounds__(kThreads) dsyrk_lower_kernel(const DsyrkArgs a, const int T, const int Tc) {
+__global__ void __launch_bounds__(kThreads, 4) dsyrk_lower_kernel(const DsyrkArgs a, const int T, const int Tc) {
   int tm, tn;
   trap_decode(blockIdx.x, T, Tc, tm, tn);
   const int ncols = a.ncols > 0 ? a.ncols : a.n;
@@ -146,7 +158,7 @@ __global__ void __launch_bounds__(kThreads) dsyrk_lower_kernel(const DsyrkArgs a
 // Variable-size batch: step of the two-level blocked Cholesky.
 //   mode 0 (panel update): C = A[j0+64:, j0+64:], n = N - j0 - 64, ncols = min(N, J0+256) - (j0+64), K = 64
 //   mode 1 (trailing):     C = A[J1:, J1:],       n = N - J1, J1 = min(N, J0+256), K = J1 - J0
-__global__ void __launch_bounds__(kThreads) dsyrk_varlen_kernel(const MatDesc* mats, int mode, int J0, int j0) {
+__global__ void __launch_bounds__(kThreads, 4) dsyrk_varlen_kernel(const MatDesc* mats, int mode, int J0, int j0) {
   const MatDesc md = mats[blockIdx.y];
   const int N = md.n;
   const int J1 = min(N, J0 + 256);
@@ -181,7 +193,9 @@ __global__ void __launch_bounds__(kThreads) dsyrk_varlen_kernel(const MatDesc* m
 cudaError_t launch_dsyrk_varlen(const MatDesc* mats, int nmat, int mode, int J0, int j0, int max_tiles,
                                 cudaStream_t stream) {
   if (nmat <= 0 || max_tiles <= 0) return cudaSuccess;
-  dsyrk_varlen_kernel<<<dim3((unsigned)max_tiles, (unsigned)nmat), kThreads, 0, stream>>>(mats, mode, J0, j0);
+  cudaError_t e0 = cudaFuncSetAttribute(dsyrk_varlen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem);
+  if (e0 != cudaSuccess) return e0;
+  dsyrk_varlen_kernel<<<dim3((unsigned)max_tiles, (unsigned)nmat), kThreads, kTileSmem, stream>>>(mats, mode, J0, j0);
   ++g_launches;
   return cudaGetLastError();
 }
@@ -193,8 +207,13 @@ cudaError_t launch_dsyrk_lower(const DsyrkArgs& a, cudaStream_t stream) {
   const int Tc = (nc + BM - 1) / BM;
   const int64_t tiles = (int64_t)Tc * T - (int64_t)Tc * (Tc - 1) / 2;
   dim3 grid((unsigned)tiles, (unsigned)a.batch);
-  if (a.D) dsyrk_lower_kernel<true><<<grid, kThreads, 0, stream>>>(a, T, Tc);
-  else dsyrk_lower_kernel<false><<<grid, kThreads, 0, stream>>>(a, T, Tc);
+  cudaError_t e0 = a.D ? cudaFuncSetAttribute(dsyrk_lower_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)kTileSmem)
+                       : cudaFuncSetAttribute(dsyrk_lower_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)kTileSmem);
+  if (e0 != cudaSuccess) return e0;
+  if (a.D) dsyrk_lower_kernel<true><<<grid, kThreads, kTileSmem, stream>>>(a, T, Tc);
+  else dsyrk_lower_kernel<false><<<grid, kThreads, kTileSmem, stream>>>(a, T, Tc);
   ++g_launches;
   return cudaGetLastError();
 }
