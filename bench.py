@@ -317,24 +317,40 @@ def run_ours(args):
 
 
 def run_mbe(args):
-    """Batched many-fragment workload: instances/s of rpa_b200_ec_batched, split vs FP64."""
+    """Batched many-fragment workload: instances/s of rpa_b200_ec_batched, split vs FP64.
+    N > 1: fragments dealt out to ranks by cost (strong scaling, no data-path collective)."""
     import torch
+    import torch.distributed as dist
+    from datetime import timedelta
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     pkg = load_package()
-    from beyond_rpa_b200.workloads import make_mbe_batch
+    from beyond_rpa_b200.workloads import make_mbe_batch, mbe_specs
+    from beyond_rpa_b200 import distributed as D
     n_inst = int(args.workload.split("_")[1]) if "_" in args.workload else 512
+    specs = mbe_specs(n_inst, seed=4000)
+    mine = D.shard([D.instance_cost(nq, no * nv, K) for no, nv, nq, K in specs], rank, world)
     h = pkg.Handle(local)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     h.set_stream(stream.cuda_stream)
-    systems, kinds = make_mbe_batch(n_inst, seed=4000 + rank)
+    systems, kinds = make_mbe_batch(n_inst, seed=4000, only=mine)
     torch.cuda.synchronize()
     flops = sum(float(R.shape[0]) ** 2 * len(eo) * len(ev) * len(x) for R, eo, ev, x, w in systems)
     ld_flops = sum(float(R.shape[0]) ** 3 / 3 * len(x) for R, eo, ev, x, w in systems)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
     for _ in range(args.warmup):
         h.ec_batched(systems, prec="split")
+    barrier()
+    torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -342,27 +358,35 @@ def run_mbe(args):
         ec, _ = h.ec_batched(systems, prec="split")
     e1.record(stream)
     torch.cuda.synchronize()
-    t_ms = e0.elapsed_time(e1) / args.steps
+    barrier()
+    t_ms = D.max_over_ranks(e0.elapsed_time(e1) / args.steps, device="cuda")
     launches = h.launches()
     h.ec_batched(systems, prec="fp64")
+    barrier()
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
     e2.record(stream)
     ec64, _ = h.ec_batched(systems, prec="fp64")
     e3.record(stream)
     torch.cuda.synchronize()
-    t64 = e2.elapsed_time(e3)
+    barrier()
+    t64 = D.max_over_ranks(e2.elapsed_time(e3), device="cuda")
+    all_ec = D.gather_energies(mine, ec, n_inst, device="cuda")
+    all_ec64 = D.gather_energies(mine, ec64, n_inst, device="cuda")
     if rank == 0:
         print(json.dumps({
             "metric": "RPA E_c of a batched many-body-expansion workload", "workload": args.workload,
             "value": n_inst / (t_ms / 1e3), "unit": "instances/s", "ms_per_step": t_ms, "steps": args.steps,
-            "instances": n_inst, "dimers": kinds.count("dimer"), "trimers": kinds.count("trimer"),
-            "pi_fp64_equiv_tflops": flops / (t_ms / 1e3) / 1e12, "pi_flops": flops, "logdet_flops": ld_flops,
-            "gpu_launches_per_step": launches,
+            "n_gpus": world, "scaling": "strong", "instances": n_inst, "dimers": kinds.count("dimer"),
+            "trimers": kinds.count("trimer"),
+            "pi_fp64_equiv_tflops_rank0": flops / (t_ms / 1e3) / 1e12, "pi_flops_rank0": flops,
+            "logdet_flops_rank0": ld_flops, "gpu_launches_per_step_rank0": launches,
             "fp64_form": {"ms_per_step": t64, "speedup_split_vs_fp64": t64 / t_ms},
-            "max_abs_dEc_split_vs_fp64": float(np.max(np.abs(np.asarray(ec) - np.asarray(ec64)))),
+            "max_abs_dEc_split_vs_fp64": float(np.max(np.abs(all_ec - all_ec64))),
         }), flush=True)
     h.close()
+    if world > 1:
+        dist.destroy_process_group()
 
 
 def run_adjoint(args):

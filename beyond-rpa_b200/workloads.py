@@ -85,22 +85,32 @@ def make_single_system(name="single_4096", seed=0, device="cuda", K=None):
     return SyntheticSystem(R=R, eps_o=eo, eps_v=ev, freqs=x, weights=w)
 
 
-def make_mbe_batch(n_inst=512, seed=0, device="cuda", dimer_frac=0.6):
+def mbe_specs(n_inst=512, seed=0):
+    """(NOcc, NVirt, NQ, K) of every fragment of the many-body-expansion batch."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(n_inst):
+        no = int(rng.integers(16, 49))
+        nv = int(round(rng.uniform(8.0, 12.0) * no))
+        specs.append((no, nv, 4 * (no + nv), int(rng.choice([8, 12, 16]))))
+    return specs
+
+
+def make_mbe_batch(n_inst=512, seed=0, device="cuda", dimer_frac=0.6, only=None):
     """Many-body-expansion fragment batch: n_inst instances (dimer_frac dimers, the
     rest trimers) with NOcc ~ U{16..48}, NVirt = round(U[8,12] NOcc),
     NQ = 4 (NOcc + NVirt), K in {8, 12, 16}; each drawn like the water-dimer
     twin (occ U[-1.3,-0.4], virt log-U[0.03,4], R ~ N(0,1) exp(-Q/(NQ/8)),
-    lambda_max(Pi(0)) = 0.8) from seed + instance id.  Returns a list of
-    (R, eps_o, eps_v, freqs, weights) and the dimer/trimer labels."""
+    lambda_max(Pi(0)) = 0.8) from seed + instance id.  `only` restricts the
+    materialised instances to a subset of ids (a rank's share).  Returns a
+    list of (R, eps_o, eps_v, freqs, weights) and the dimer/trimer labels."""
     import torch
     from . import freq_grid
-    rng = np.random.default_rng(seed)
+    specs = mbe_specs(n_inst, seed)
+    ids = range(n_inst) if only is None else only
     out, kinds = [], []
-    for i in range(n_inst):
-        no = int(rng.integers(16, 49))
-        nv = int(round(rng.uniform(8.0, 12.0) * no))
-        nq = 4 * (no + nv)
-        K = int(rng.choice([8, 12, 16]))
+    for i in ids:
+        no, nv, nq, K = specs[i]
         eo, ev = orbital_energies(no, nv, seed + 7919 * (i + 1), (-1.3, -0.4), (0.03, 4.0))
         g = torch.Generator(device=device).manual_seed(seed + i + 1)
         Rt = torch.randn((no * nv, nq), generator=g, device=device, dtype=torch.float64)

@@ -1,0 +1,74 @@
+"""World-size-2 gloo tests (CPU) of the multi-rank host logic of the batched
+path: cost-balanced sharding, max-over-ranks timing and the energy gather."""
+import os
+import socket
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, q):
+    import torch.distributed as dist
+    sys.path.insert(0, str(ROOT / "tests"))
+    import conftest
+    pkg = conftest.load_package()
+    import importlib
+    D = importlib.import_module("beyond_rpa_b200.distributed")
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    rng = np.random.default_rng(0)
+    costs = [D.instance_cost(int(rng.integers(700, 2300)), int(rng.integers(2000, 25000)), int(rng.choice([8, 12, 16])))
+             for _ in range(40)]
+    mine = D.shard(costs, rank, world)
+    t = D.max_over_ranks(1.0 + rank)
+    ec = D.gather_energies(mine, [-(i + 1) * 0.001 for i in mine], len(costs))
+    q.put((rank, mine, t, ec.tolist(), sum(costs[i] for i in mine)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_rank_shard_timing_and_gather():
+    world = 2
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    res.sort()
+    owned = sorted(res[0][1] + res[1][1])
+    assert owned == list(range(40))                       # every instance exactly once
+    assert set(res[0][1]).isdisjoint(res[1][1])
+    loads = [r[4] for r in res]
+    assert max(loads) / min(loads) < 1.1                   # cost-balanced
+    assert res[0][2] == res[1][2] == 2.0                   # max over ranks
+    expect = [-(i + 1) * 0.001 for i in range(40)]
+    assert np.allclose(res[0][3], expect) and np.allclose(res[1][3], expect)
+
+
+def test_single_process_fallbacks():
+    sys.path.insert(0, str(ROOT / "tests"))
+    import conftest
+    conftest.load_package()
+    import importlib
+    D = importlib.import_module("beyond_rpa_b200.distributed")
+    assert D.shard([3.0, 1.0, 2.0], 0, 1) == [0, 1, 2]
+    assert D.max_over_ranks(4.5) == 4.5
+    assert np.allclose(D.gather_energies([0, 2], [1.0, 3.0], 3), [1.0, 0.0, 3.0])
