@@ -95,6 +95,8 @@ def load_library(path: str | os.PathLike | None = None):
     lib.rpa_b200_ec_grad.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _dbl, _i64, _vp,
                                      _vp, _i64, _vp, _vp]
     lib.rpa_b200_exchange_sosex.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _dbl, _i64, _vp]
+    lib.rpa_b200_exchange_mbpt3.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _i64, _vp, _vp,
+                                            _vp, _i64]
     if path is None:
         _lib = lib
     return lib
@@ -336,6 +338,23 @@ class Handle:
                                                      u.ld, a.ptr, float(alpha), int(bool(s2_operator)),
                                                      ctypes.byref(ex)))
         return ex.value
+
+    def exchange_mbpt3(self, R, eps_o, eps_v, U, A, return_x=False):
+        """MBPT3 exchange energy -Tr(X K) (rpa_b200_exchange_mbpt3); with return_x also the
+        Lyapunov solution X."""
+        nq = int(R.shape[0])
+        no, nv = len(eps_o), len(eps_v)
+        nov = no * nv
+        nt = int(U.shape[1])
+        r = _colmajor(R, nq)
+        u = _colmajor(U, nov)
+        a, eo, ev = _vec(A), _vec(eps_o), _vec(eps_v)
+        ex = ctypes.c_double()
+        X = np.zeros((nt, nt), order="F") if return_x else None
+        self._check(self.lib.rpa_b200_exchange_mbpt3(self._h, nq, no, nv, r.ptr, r.ld, eo.ptr, ev.ptr, nt, u.ptr, u.ld,
+                                                     a.ptr, ctypes.byref(ex),
+                                                     X.ctypes.data if return_x else None, nt))
+        return (ex.value, X) if return_x else ex.value
 
     def ec_rpa(self, R, eps_o, eps_v, freqs, weights, alpha=4.0, prec="split"):
         """Fused Pi build + energy: returns (E_c, E(u))."""

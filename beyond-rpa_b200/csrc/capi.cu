@@ -40,6 +40,7 @@ struct rpa_b200_handle {
   // batched (many-instance) workspace: descriptors and per-batch results
   DevBuf bDesc, bRes;
   DevBuf gY, gD;  // adjoint workspace
+  DevBuf xM;      // MBPT3 exchange: NT x NT matrices, R U and U X
   struct BatchGraph {
     uint64_t key;
     std::vector<cudaGraphExec_t> execs;
@@ -671,7 +672,8 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
   if (h->own_stream) cudaStreamSynchronize(h->own_stream);
   for (DevBuf* b : {&h->R, &h->D, &h->eps, &h->Xhi, &h->Xlo, &h->diag_part, &h->diag, &h->Pi, &h->Ldiag, &h->ddbuf,
                     &h->tZ, &h->tOm, &h->tIOm, &h->tP, &h->tS, &h->tV, &h->tT, &h->tTIT, &h->tVt, &h->tW, &h->tU,
-                    &h->tRU, &h->tSmall, &h->tRot, &h->tPerm, &h->bDesc, &h->bRes, &h->gY, &h->gD})
+                    &h->tRU, &h->tSmall, &h->tRot, &h->tPerm, &h->bDesc, &h->bRes, &h->gY, &h->gD,
+                    &h->xM})
     release(*b);
   for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
   if (h->err_dev) cudaFree(h->err_dev);
@@ -1023,7 +1025,8 @@ int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
   RPA_CUDA(h, cudaMemcpyAsync(Bd, B.data(), (size_t)NT * 8, cudaMemcpyHostToDevice, h->stream));
   RPA_CUDA(h, cudaEventRecord(h->ev[1], h->stream));
   int64_t npart = 0;
-  RPA_CUDA(h, rpa::launch_sosex(Rd, ldr, (int)NQ, (int)NOcc, (int)NVirt, Ud, ldu, NT, Bd, part, &npart, h->stream));
+  RPA_CUDA(h, rpa::launch_sosex(Rd, ldr, (int)NQ, (int)NOcc, (int)NVirt, Ud, ldu, nullptr, 0, NT, Bd, part, &npart,
+                                h->stream));
   RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
   RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
   std::vector<double> hp((size_t)npart);
@@ -1033,6 +1036,190 @@ int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
   dd acc{0.0, 0.0};
   for (double x : hp) acc = rpa::dd_add(acc, x);
   *Ex = -Alpha * (acc.hi + acc.lo);
+  finish_timings(h);
+  return RPA_OK;
+}
+
+// MBPT3 exchange (rpa_CC_Exchange_MBPT3_1, src/rpa/rpa_CC_Exchange.f90:232-272, with rpa_CC_Ukl :177,
+// rpa_CC_Dkl and rpa_CC_TrXK :275).  The reference solves B^T X + X B = A by a real Schur form and
+// DTRSYL (real_Lyapunov, src/linear-algebra/real_linalg.f90:125-171).  Here the operator is split
+// into its symmetric part S = (B + B^T)/2, inverted exactly through S = Q diag(mu) Q^T
+// ((S Y + Y S)_mn = mu_m + mu_n in the eigenbasis), and the antisymmetric part 2 U_mn (A_n - A_m),
+// which is small because |A| << 1; the residual-correction iteration
+//   X <- X + Q [(Q^T (A - B^T X - X B) Q)_mn / (mu_m + mu_n)] Q^T
+// contracts by about three orders of magnitude per step.  All matrix products are FP64 DMMA GEMMs.
+int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R,
+                            int64_t ldR, const double* OccEnergies, const double* VirtEnergies, int64_t NVecsT2,
+                            const double* U, int64_t ldU, const double* A, double* Ex, double* X, int64_t ldX) {
+  int s = begin_call(h);
+  if (s != RPA_OK) return s;
+  const int64_t nov = NOcc * NVirt;
+  if (NQ < 1 || NOcc < 1 || NVirt < 1 || NVecsT2 < 1 || ldR < NQ || ldU < nov || !R || !U || !A || !Ex ||
+      !OccEnergies || !VirtEnergies || (X && ldX < NVecsT2))
+    return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_exchange_mbpt3");
+  if (NQ > INT32_MAX || nov > INT32_MAX || NVecsT2 > 65535)
+    return fail(h, RPA_ERR_TOO_LARGE, "rpa_b200_exchange_mbpt3: dimensions too large");
+  const int NT = (int)NVecsT2;
+  std::vector<double> Ah, eo, ev;
+  if ((s = fetch_small(h, A, NT, Ah)) || (s = fetch_small(h, OccEnergies, NOcc, eo)) ||
+      (s = fetch_small(h, VirtEnergies, NVirt, ev)))
+    return s;
+  std::vector<double> Dh((size_t)nov);
+  for (int64_t i = 0; i < NOcc; ++i)
+    for (int64_t a = 0; a < NVirt; ++a) Dh[(size_t)(a + NVirt * i)] = ev[a] - eo[i];
+  for (double x : Ah)
+    if (!std::isfinite(x)) return fail(h, RPA_ERR_NONFINITE, "non-finite T2 eigenvalue");
+  for (double x : Dh)
+    if (!std::isfinite(x)) return fail(h, RPA_ERR_NONFINITE, "non-finite orbital energy");
+
+  const double* Rd = R;
+  int64_t ldr = ldR;
+  if (!is_device_ptr(R)) {
+    RPA_CUDA(h, ensure(h->R, (size_t)NQ * nov * 8));
+    RPA_CUDA(h, cudaMemcpy2DAsync(h->R.p, (size_t)NQ * 8, R, (size_t)ldR * 8, (size_t)NQ * 8, (size_t)nov,
+                                  cudaMemcpyHostToDevice, h->stream));
+    Rd = static_cast<const double*>(h->R.p);
+    ldr = NQ;
+  }
+  const double* Ud = U;
+  int64_t ldu = ldU;
+  if (!is_device_ptr(U)) {
+    RPA_CUDA(h, ensure(h->tU, (size_t)nov * NT * 8));
+    RPA_CUDA(h, cudaMemcpy2DAsync(h->tU.p, (size_t)nov * 8, U, (size_t)ldU * 8, (size_t)nov * 8, (size_t)NT,
+                                  cudaMemcpyHostToDevice, h->stream));
+    Ud = static_cast<const double*>(h->tU.p);
+    ldu = nov;
+  }
+  // workspace: 8 NT x NT matrices, R U (NQ x NT), U X (nov x NT), D, A, mu, partials
+  const size_t nn = (size_t)NT * NT;
+  const int64_t np = rpa::sosex_partials((int)NQ, (int)NOcc, NT);
+  const size_t words = 8 * nn + (size_t)NQ * NT + (size_t)nov * NT + (size_t)nov + 3 * (size_t)NT + (size_t)np + 8;
+  RPA_CUDA(h, ensure(h->xM, words * 8));
+  RPA_CUDA(h, ensure(h->tSmall, (size_t)std::max<int64_t>(NT, 64) * 8 + 64));
+  RPA_CUDA(h, ensure(h->tRot, (size_t)(NT / 2 + 2) * sizeof(double4)));
+  RPA_CUDA(h, ensure(h->tPerm, (size_t)NT * sizeof(int)));
+  double* w = static_cast<double*>(h->xM.p);
+  double* Ukl = w;
+  double* Dkl = Ukl + nn;
+  double* Am = Dkl + nn;
+  double* Bm = Am + nn;
+  double* Sm = Bm + nn;  // symmetric part; diagonalised in place
+  double* Q = Sm + nn;
+  double* Xd = Q + nn;
+  double* Res = Xd + nn;
+  double* RU = Res + nn;
+  double* UX = RU + (size_t)NQ * NT;
+  double* Dd = UX + (size_t)nov * NT;
+  double* Ad = Dd + nov;
+  double* mud = Ad + NT;
+  double* ones = mud + NT;
+  double* part = ones + NT;
+  int* bad = h->count_dev;
+  RPA_CUDA(h, cudaMemcpyAsync(Dd, Dh.data(), (size_t)nov * 8, cudaMemcpyHostToDevice, h->stream));
+  RPA_CUDA(h, cudaMemcpyAsync(Ad, Ah.data(), (size_t)NT * 8, cudaMemcpyHostToDevice, h->stream));
+  {
+    std::vector<double> one((size_t)NT, 1.0);
+    RPA_CUDA(h, cudaMemcpyAsync(ones, one.data(), (size_t)NT * 8, cudaMemcpyHostToDevice, h->stream));
+    RPA_CUDA(h, cudaStreamSynchronize(h->stream));  // host vectors must outlive their copies
+  }
+  RPA_CUDA(h, cudaEventRecord(h->ev[1], h->stream));
+
+  // Ukl = (R U)^T (R U), Dkl = U^T diag(D) U, then the A, B and S matrices
+  RPA_CUDA(h, rpa::launch_gemm_f64(gemm_nn((int)NQ, NT, nov, Rd, ldr, Ud, ldu, RU, NQ), h->stream));
+  RPA_CUDA(h, rpa::launch_gemm_f64(gemm_tn(NT, NT, NQ, RU, NQ, RU, NQ, Ukl, NT), h->stream));
+  {
+    rpa::GemmF64Args g = gemm_tn(NT, NT, nov, Ud, ldu, Ud, ldu, Dkl, NT);
+    g.kscale = Dd;
+    RPA_CUDA(h, rpa::launch_gemm_f64(g, h->stream));
+  }
+  RPA_CUDA(h, rpa::launch_mbpt3_build(Ukl, Dkl, Ad, NT, Am, Bm, Sm, h->stream));
+  std::vector<double> mu;
+  std::vector<int> order;
+  if ((s = jacobi_eig(h, Sm, Q, NT, mu, order))) return s;
+  RPA_CUDA(h, cudaMemcpyAsync(mud, mu.data(), (size_t)NT * 8, cudaMemcpyHostToDevice, h->stream));
+  RPA_CUDA(h, cudaMemsetAsync(bad, 0, sizeof(int), h->stream));
+
+  // residual-correction iteration, X_0 = 0
+  double* red = static_cast<double*>(h->tSmall.p);
+  RPA_CUDA(h, cudaMemsetAsync(Xd, 0, nn * 8, h->stream));
+  auto sqnorm = [&](const double* M, double& out) -> int {
+    double od[2];
+    RPA_CUDA(h, rpa::launch_offdiag(M, NT, NT, red, h->stream));
+    RPA_CUDA(h, cudaMemcpyAsync(od, red, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+    out = od[0] + od[1];
+    return RPA_OK;
+  };
+  double a2 = 0.0;
+  if ((s = sqnorm(Am, a2))) return s;
+  bool converged = (a2 == 0.0);
+  double r2 = a2;
+  for (int it = 0; it < 60 && !converged; ++it) {
+    // Res = A - B^T X - X B
+    RPA_CUDA(h, cudaMemcpyAsync(Res, Am, nn * 8, cudaMemcpyDeviceToDevice, h->stream));
+    if (it > 0) {
+      rpa::GemmF64Args g1 = gemm_tn(NT, NT, NT, Bm, NT, Xd, NT, Res, NT);
+      g1.alpha = -1.0;
+      g1.beta = 1.0;
+      RPA_CUDA(h, rpa::launch_gemm_f64(g1, h->stream));
+      rpa::GemmF64Args g2 = gemm_nn(NT, NT, NT, Xd, NT, Bm, NT, Res, NT);
+      g2.alpha = -1.0;
+      g2.beta = 1.0;
+      RPA_CUDA(h, rpa::launch_gemm_f64(g2, h->stream));
+      if ((s = sqnorm(Res, r2))) return s;
+      if (!std::isfinite(r2) || r2 > 1e4 * a2)
+        return fail(h, RPA_ERR_NOT_CONVERGED, "MBPT3 Lyapunov iteration diverged (|res|/|A| = %.3e)",
+                    std::sqrt(r2 / a2));
+      if (r2 <= 1e-26 * a2) {
+        converged = true;
+        break;
+      }
+    }
+    // Y = Q^T Res Q / (mu_m + mu_n);  X += Q Y Q^T   (Sm and Ukl serve as scratch)
+    RPA_CUDA(h, rpa::launch_gemm_f64(gemm_tn(NT, NT, NT, Q, NT, Res, NT, Sm, NT), h->stream));
+    RPA_CUDA(h, rpa::launch_gemm_f64(gemm_nn(NT, NT, NT, Sm, NT, Q, NT, Ukl, NT), h->stream));
+    RPA_CUDA(h, rpa::launch_lyap_scale(Ukl, mud, NT, bad, h->stream));
+    RPA_CUDA(h, rpa::launch_gemm_f64(gemm_nn(NT, NT, NT, Q, NT, Ukl, NT, Sm, NT), h->stream));
+    rpa::GemmF64Args g3 = gemm_nn(NT, NT, NT, Sm, NT, Q, NT, Xd, NT);
+    g3.b_k = NT;  // Q^T
+    g3.b_n = 1;
+    g3.beta = 1.0;
+    RPA_CUDA(h, rpa::launch_gemm_f64(g3, h->stream));
+    if (it == 0) {
+      int nbad = 0;
+      RPA_CUDA(h, cudaMemcpyAsync(&nbad, bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+      RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+      if (nbad)
+        return fail(h, RPA_ERR_NOT_CONVERGED,
+                    "MBPT3 Lyapunov solve: symmetric part of B is not positive definite (%d pairs)", nbad);
+    }
+  }
+  if (!converged)
+    return fail(h, RPA_ERR_NOT_CONVERGED, "MBPT3 Lyapunov iteration did not converge (|res|/|A| = %.3e)",
+                std::sqrt(r2 / a2));
+
+  // Tr(XK): W_ij from U, W_ji from U X
+  RPA_CUDA(h, rpa::launch_gemm_f64(gemm_nn((int)nov, NT, NT, Ud, ldu, Xd, NT, UX, nov), h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
+  int64_t npart = 0;
+  RPA_CUDA(h, rpa::launch_sosex(Rd, ldr, (int)NQ, (int)NOcc, (int)NVirt, Ud, ldu, UX, nov, NT, ones, part, &npart,
+                                h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
+  std::vector<double> hp((size_t)npart);
+  RPA_CUDA(h, cudaMemcpyAsync(hp.data(), part, (size_t)npart * 8, cudaMemcpyDeviceToHost, h->stream));
+  if (X) {
+    if (is_device_ptr(X))
+      RPA_CUDA(h, cudaMemcpy2DAsync(X, (size_t)ldX * 8, Xd, (size_t)NT * 8, (size_t)NT * 8, (size_t)NT,
+                                    cudaMemcpyDeviceToDevice, h->stream));
+    else
+      RPA_CUDA(h, cudaMemcpy2DAsync(X, (size_t)ldX * 8, Xd, (size_t)NT * 8, (size_t)NT * 8, (size_t)NT,
+                                    cudaMemcpyDeviceToHost, h->stream));
+  }
+  RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  dd acc{0.0, 0.0};
+  for (double x : hp) acc = rpa::dd_add(acc, x);
+  *Ex = -(acc.hi + acc.lo);
   finish_timings(h);
   return RPA_OK;
 }

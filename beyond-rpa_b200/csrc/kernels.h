@@ -203,8 +203,15 @@ cudaError_t launch_symmetrize_avg(double* A, int64_t lda, int n, cudaStream_t st
 
 // SOSEX pair contraction: partial[tile] of -sum_{i>=j} (2 - delta_ij) sum_{Q,mu} B_mu W_ij W_ji,
 // W_ij = R(:, :, i) U(:, :, j)^T; partials reduced on the host in fixed order.
-cudaError_t launch_sosex(const double* R, int64_t ldR, int NQ, int no, int nv, const double* U, int64_t ldU, int NT,
-                         const double* Bmu, double* partial, int64_t* npartial, cudaStream_t stream);
+// U2 (nullptr: U) forms W_ji.
+cudaError_t launch_sosex(const double* R, int64_t ldR, int NQ, int no, int nv, const double* U, int64_t ldU,
+                         const double* U2, int64_t ldU2, int NT, const double* Bmu, double* partial, int64_t* npartial,
+                         cudaStream_t stream);
+// MBPT3 exchange: A_mn = A_m D_mn + D_mn A_n, B_mn = D_mn + 2 U_mn + 4 U_mn A_n, Bs = (B + B^T)/2.
+cudaError_t launch_mbpt3_build(const double* Ukl, const double* Dkl, const double* Avec, int n, double* Amat,
+                               double* Bmat, double* Bsym, cudaStream_t stream);
+// Y_mn /= (mu_m + mu_n); counts pairs with mu_m + mu_n <= 0 into *bad.
+cudaError_t launch_lyap_scale(double* Y, const double* mu, int n, int* bad, cudaStream_t stream);
 int64_t sosex_partials(int NQ, int no, int NT);
 
 // ---------------------------------------------------------------- variable-size batches

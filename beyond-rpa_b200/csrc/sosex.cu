@@ -38,14 +38,18 @@ __device__ __forceinline__ void pair_decode(int p, int& i, int& j) {
   j = p - t * (t + 1) / 2;
 }
 
+// W_ij is formed from U1 and W_ji from U2 (U2 == U1 for SOSEX; U1 = U X for
+// the Tr(XK) contraction of the MBPT3 exchange).
 __global__ void __launch_bounds__(kThreads) sosex_kernel(const double* __restrict__ R, int64_t ldR, int NQ, int nv,
-                                                         const double* __restrict__ U, int64_t ldU, int NT,
+                                                         const double* __restrict__ U, int64_t ldU,
+                                                         const double* __restrict__ U2, int64_t ldU2, int NT,
                                                          const double* __restrict__ Bmu, double* partial) {
   __shared__ double Ri[BK][LDS], Rj[BK][LDS], Uj[BK][LDS], Ui[BK][LDS];
   __shared__ double red[kThreads / 32];
   int i, j;
   pair_decode(blockIdx.x, i, j);
-  const bool diag = (i == j);
+  const bool same = (U2 == U);
+  const bool diag = (i == j) && same;  // W_ii W_ii: one accumulator suffices
   const int q0 = blockIdx.y * BM, m0 = blockIdx.z * BM;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int wm = warp >> 1, wn = warp & 1;
@@ -75,7 +79,7 @@ __global__ void __launch_bounds__(kThreads) sosex_kernel(const double* __restric
       const int mu = m0 + r, a = a0 + c;
       const bool ok = (mu < NT && a < nv);
       Uj[c][r] = ok ? U[((int64_t)a + (int64_t)nv * j) + ldU * mu] : 0.0;
-      Ui[c][r] = (ok && !diag) ? U[((int64_t)a + (int64_t)nv * i) + ldU * mu] : 0.0;
+      Ui[c][r] = (ok && !diag) ? U2[((int64_t)a + (int64_t)nv * i) + ldU2 * mu] : 0.0;
     }
     __syncthreads();
 #pragma unroll
@@ -123,7 +127,7 @@ __global__ void __launch_bounds__(kThreads) sosex_kernel(const double* __restric
     double tot = 0.0;
     for (int w = 0; w < kThreads / 32; ++w) tot += red[w];
     const int64_t idx = ((int64_t)blockIdx.x * gridDim.y + blockIdx.y) * gridDim.z + blockIdx.z;
-    partial[idx] = (diag ? 1.0 : 2.0) * tot;
+    partial[idx] = (i == j ? 1.0 : 2.0) * tot;
   }
 }
 }  // namespace
@@ -132,13 +136,15 @@ int64_t sosex_partials(int NQ, int no, int NT) {
   return (int64_t)no * (no + 1) / 2 * ((NQ + BM - 1) / BM) * ((NT + BM - 1) / BM);
 }
 
-cudaError_t launch_sosex(const double* R, int64_t ldR, int NQ, int no, int nv, const double* U, int64_t ldU, int NT,
-                         const double* Bmu, double* partial, int64_t* npartial, cudaStream_t stream) {
+cudaError_t launch_sosex(const double* R, int64_t ldR, int NQ, int no, int nv, const double* U, int64_t ldU,
+                         const double* U2, int64_t ldU2, int NT, const double* Bmu, double* partial, int64_t* npartial,
+                         cudaStream_t stream) {
   const int npairs = no * (no + 1) / 2;
   dim3 grid((unsigned)npairs, (unsigned)((NQ + BM - 1) / BM), (unsigned)((NT + BM - 1) / BM));
   *npartial = sosex_partials(NQ, no, NT);
   if (npairs == 0 || NT == 0) return cudaSuccess;
-  sosex_kernel<<<grid, kThreads, 0, stream>>>(R, ldR, NQ, nv, U, ldU, NT, Bmu, partial);
+  sosex_kernel<<<grid, kThreads, 0, stream>>>(R, ldR, NQ, nv, U, ldU, U2 ? U2 : U, U2 ? ldU2 : ldU, NT, Bmu,
+                                               partial);
   ++g_launches;
   return cudaGetLastError();
 }

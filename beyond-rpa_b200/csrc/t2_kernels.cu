@@ -327,6 +327,31 @@ __global__ void symmetrize_avg_kernel(double* A, int64_t lda, int n) {
   A[j + lda * i] = v;
 }
 
+__global__ void mbpt3_build_kernel(const double* Ukl, const double* Dkl, const double* Av, int n, double* Amat,
+                                   double* Bmat, double* Bsym) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)n * n) return;
+  const int64_t m = idx % n, k = idx / n;  // element (m, k)
+  const double d = Dkl[idx], u = Ukl[idx];
+  Amat[idx] = Av[m] * d + d * Av[k];
+  Bmat[idx] = d + 2.0 * u + 4.0 * u * Av[k];
+  // symmetric part: (B_mk + B_km)/2, with D and U symmetric
+  Bsym[idx] = d + 2.0 * u + 2.0 * u * (Av[k] + Av[m]);
+}
+
+__global__ void lyap_scale_kernel(double* Y, const double* mu, int n, int* bad) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)n * n) return;
+  const int64_t m = idx % n, k = idx / n;
+  const double den = mu[m] + mu[k];
+  if (!(den > 0.0)) {
+    atomicAdd(bad, 1);
+    Y[idx] = 0.0;
+    return;
+  }
+  Y[idx] /= den;
+}
+
 inline unsigned blocks_for(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
@@ -420,6 +445,19 @@ cudaError_t launch_grad_accum(const double* R, int64_t ldR, const double* Y, int
 cudaError_t launch_replicate(const double* R, int64_t ldR, int NQ, int64_t nov, double* Y, int64_t ldy, int64_t sY,
                              int nb, cudaStream_t stream) {
   replicate_kernel<<<blocks_for((int64_t)NQ * nov), 256, 0, stream>>>(R, ldR, NQ, nov, Y, ldy, sY, nb);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mbpt3_build(const double* Ukl, const double* Dkl, const double* Avec, int n, double* Amat,
+                               double* Bmat, double* Bsym, cudaStream_t stream) {
+  mbpt3_build_kernel<<<blocks_for((int64_t)n * n), 256, 0, stream>>>(Ukl, Dkl, Avec, n, Amat, Bmat, Bsym);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_lyap_scale(double* Y, const double* mu, int n, int* bad, cudaStream_t stream) {
+  lyap_scale_kernel<<<blocks_for((int64_t)n * n), 256, 0, stream>>>(Y, mu, n, bad);
   ++g_launches;
   return cudaGetLastError();
 }

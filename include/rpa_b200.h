@@ -201,6 +201,21 @@ int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
                             int64_t S2Operator, double* Ex);
 
 /*
+ * MBPT3 exchange energy  Ex = -Tr(X K) = -sum_{abij} (aj|bi) (U X U^T)_aibj,
+ * where X (NVecsT2 x NVecsT2) solves B^T X + X B = A with
+ * A_mn = A_m D_mn + D_mn A_n, B_mn = D_mn + 2 U_mn + 4 U_mn A_n,
+ * Ukl = (R U)^T (R U), Dkl = U^T diag(e_a - e_i) U.  Replaces
+ * rpa_CC_Exchange_MBPT3_1 + rpa_CC_Ukl + rpa_CC_Dkl + rpa_CC_TrXK
+ * (src/rpa/rpa_CC_Exchange.f90:177-336; the Lyapunov solve replaces
+ * real_Lyapunov, src/linear-algebra/real_linalg.f90:125-171).  U and A are
+ * the outputs of rpa_b200_dring_t2.  X (may be NULL, ldX >= NVecsT2) receives
+ * the Lyapunov solution.  RPA_ERR_NOT_CONVERGED if the solve fails.
+ */
+int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R,
+                            int64_t ldR, const double* OccEnergies, const double* VirtEnergies, int64_t NVecsT2,
+                            const double* U, int64_t ldU, const double* A, double* Ex, double* X, int64_t ldX);
+
+/*
  * Allocation-free energy from given Pi(u) matrices.  No counterpart in the
  * reference: it exists for callers that cannot allocate GPU memory (a host
  * whose device memory belongs to a pool or arena it cannot grow, or code

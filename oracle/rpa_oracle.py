@@ -578,3 +578,37 @@ def to_bf16(x):
     b = f.view(np.uint32).astype(np.uint64)
     b = (b + 0x7FFF + ((b >> 16) & 1)) & 0xFFFF0000
     return b.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def exchange_mbpt3_1(U, A, R, eps_o, eps_v):
+    """MBPT3 exchange: E_x = -Tr(X K), the default exchange of the CC path.
+
+    rpa_CC_Exchange_MBPT3_1 + rpa_CC_Ukl + rpa_CC_Dkl + rpa_CC_TrXK,
+    src/rpa/rpa_CC_Exchange.f90:177-336, with real_Lyapunov
+    (src/linear-algebra/real_linalg.f90:125-171: Schur form + DTRSYL; here
+    scipy.linalg.solve_sylvester, the same Bartels-Stewart method):
+      Ukl = (R U)^T (R U),  Dkl = U^T diag(D) U,
+      A_mn = A_m D_mn + D_mn A_n,  B_mn = D_mn + 2 U_mn + 4 U_mn A_n,
+      solve B^T X + X B = A,
+      TrXK = sum_{i>=j} (2 - delta_ij) sum_mn X_mn (W_ji^T W_ij)_mn,  W_ij = R_i U_j^T.
+    U is (nov, NT) (the Uaim layout; the routine's Vkai is its transpose)."""
+    no, nv = len(eps_o), len(eps_v)
+    nq = R.shape[0]
+    nt = U.shape[1]
+    d = dai(eps_o, eps_v)
+    RU = R @ U
+    Ukl = RU.T @ RU
+    Dkl = U.T @ (d[:, None] * U)
+    Am = A[:, None] * Dkl + Dkl * A[None, :]
+    Bm = Dkl + 2.0 * Ukl + 4.0 * Ukl * A[None, :]
+    X = scipy.linalg.solve_sylvester(Bm.T, Bm, Am)
+    Rr = R.reshape(nq, nv, no, order="F")
+    Vr = U.T.reshape(nt, nv, no, order="F")
+    acc = []
+    for j in range(no):
+        for i in range(j, no):
+            Wij = Rr[:, :, i] @ Vr[:, :, j].T
+            Wji = Rr[:, :, j] @ Vr[:, :, i].T if i != j else Wij
+            W = Wji.T @ Wij
+            acc.append((2.0 if i != j else 1.0) * float(np.sum(X * W)))
+    return -math.fsum(acc), X

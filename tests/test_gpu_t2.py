@@ -100,3 +100,51 @@ def test_sosex_ragged_shapes(handle):
     ref = O.exchange_sosex(np.ascontiguousarray(U.T), A, R, no, nv, alpha=2.0)
     got = handle.exchange_sosex(R, no, nv, U, A, alpha=2.0)
     assert abs(got - ref) < 1e-12 * max(1.0, abs(ref))
+
+
+# ----------------------------------------------------------------------------- MBPT3 exchange
+# Tolerances: E_x to 1e-11 relative (FP64 throughout; the GPU Lyapunov solve
+# stops at |res| <= 1e-13 |A|); X to 1e-10 relative to max|X|.
+
+def test_mbpt3_matches_oracle(handle):
+    s, x, w, pi, vals, vecs, omega = t2_case(17, 150, 6, 50, 12)
+    A_ref, U_ref, _ = O.t2_direct_ring(s.R, s.eps_o, s.eps_v, x, w, vals, vecs, omega, cutoff_thresh=1e-4)
+    ref, X_ref = O.exchange_mbpt3_1(U_ref, A_ref, s.R, s.eps_o, s.eps_v)
+    got, X = handle.exchange_mbpt3(s.R, s.eps_o, s.eps_v, U_ref, A_ref, return_x=True)
+    assert abs(got - ref) < 1e-11 * max(1.0, abs(ref))
+    assert np.max(np.abs(X - X_ref)) < 1e-10 * np.max(np.abs(X_ref))
+
+
+def test_mbpt3_ragged_shapes(handle):
+    # NQ, nv and an odd NT not multiples of any tile; orthonormal U, small negative A
+    rng = np.random.default_rng(5)
+    s = O.make_system(77, 5, 19, 21, decay=12.0, lam0=0.6)
+    nt = 45
+    U, _ = np.linalg.qr(rng.standard_normal((s.no * s.nv, nt)))
+    A = -0.08 * rng.uniform(size=nt)
+    ref, X_ref = O.exchange_mbpt3_1(U, A, s.R, s.eps_o, s.eps_v)
+    got, X = handle.exchange_mbpt3(s.R, s.eps_o, s.eps_v, U, A, return_x=True)
+    assert abs(got - ref) < 1e-11 * max(1.0, abs(ref))
+    assert np.max(np.abs(X - X_ref)) < 1e-10 * np.max(np.abs(X_ref))
+
+
+def test_mbpt3_after_gpu_t2(handle):
+    # the CC-path chain: T2 amplitudes from the GPU, then the MBPT3 exchange from them
+    s, x, w, pi, vals, vecs, omega = t2_case(18, 120, 5, 40, 10)
+    res = handle.dring_t2(s.R, s.eps_o, s.eps_v, x, w, prec="fp64", guess=omega, cutoff_thresh=1e-4)
+    ref, _ = O.exchange_mbpt3_1(res["U"], res["A"], s.R, s.eps_o, s.eps_v)
+    got = handle.exchange_mbpt3(s.R, s.eps_o, s.eps_v, res["U"], res["A"])
+    assert abs(got - ref) < 1e-11 * max(1.0, abs(ref))
+
+
+def test_mbpt3_indefinite_operator_is_reported(handle, pkg):
+    # occupied energies above the virtual ones make D, hence the symmetric part of B, negative
+    rng = np.random.default_rng(6)
+    s = O.make_system(40, 3, 10, 22, decay=10.0, lam0=0.5)
+    U, _ = np.linalg.qr(rng.standard_normal((30, 12)))
+    A = -0.05 * rng.uniform(size=12)
+    with pytest.raises(pkg.RPAError) as e:
+        handle.exchange_mbpt3(s.R, s.eps_v[:3] + 10.0, s.eps_v, U, A)
+    assert e.value.status == pkg.RPA_ERR_NOT_CONVERGED
+    got = handle.exchange_mbpt3(s.R, s.eps_o, s.eps_v, U, A)  # the handle stays usable
+    assert np.isfinite(got)

@@ -169,3 +169,24 @@ def test_golden_fixtures(name):
     ec, eu = O.ec_rpa_analytic(pi, w)
     assert ec == pytest.approx(g["Ec"], abs=1e-12)
     assert np.allclose(eu, g["Eu"], rtol=1e-11, atol=1e-13)
+
+
+def test_mbpt3_lyapunov_solution_and_pair_sum():
+    s, x, w = small_system(seed=9, nq=40, no=3, nv=12, lam0=0.6)
+    pi = O.pi_matrices(s.R, s.eps_o, s.eps_v, x)
+    vals, vecs = O.diagonalize_pi(pi)
+    omega = np.random.default_rng(3).uniform(size=(s.no * s.nv, s.no * s.nv)) - 0.5
+    A, U, K = O.t2_direct_ring(s.R, s.eps_o, s.eps_v, x, w, vals, vecs, omega, cutoff_thresh=1e-4)
+    ex, X = O.exchange_mbpt3_1(U, A, s.R, s.eps_o, s.eps_v)
+    d = O.dai(s.eps_o, s.eps_v)
+    RU = s.R @ U
+    Ukl, Dkl = RU.T @ RU, U.T @ (d[:, None] * U)
+    Bm = Dkl + 2 * Ukl + 4 * Ukl * A[None, :]
+    Am = A[:, None] * Dkl + Dkl * A[None, :]
+    assert np.allclose(Bm.T @ X + X @ Bm, Am, atol=1e-12 * np.abs(Am).max())
+    assert np.allclose(X, X.T, atol=1e-10 * np.abs(X).max())
+    # dense form: -sum_{abij} (aj|bi) (dT)_aibj with dT = U X U^T
+    dT = U @ X @ U.T
+    Rr = s.R.reshape(s.nq, s.nv, s.no, order="F")
+    Kx = np.einsum("qaj,qbi->aibj", Rr, Rr)
+    assert ex == pytest.approx(-np.sum(Kx * dT.reshape(s.nv, s.no, s.nv, s.no, order="F")), rel=1e-10)
