@@ -453,6 +453,60 @@ def run_adjoint(args):
     h.close()
 
 
+def run_cc(args):
+    """CC-path workload (cc_1024: NQ=1024, NOcc=32, NVirt=256, K=12; cc_2048): one direct-ring T2
+    (split Pi, G = 3 NQ guess vectors, cutoff 1e-4) followed by the SOSEX and MBPT3 exchange energies
+    from the same amplitudes.  Reports the time of each stage and its FP64 DMMA rate."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    pkg = load_package()
+    from beyond_rpa_b200.workloads import make_single_system, SINGLE_SYSTEM
+    nq, no, nv, K, _ = SINGLE_SYSTEM[args.workload]
+    nov = no * nv
+    G = min(3 * nq, nov)
+    h = pkg.Handle(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    h.set_stream(stream.cuda_stream)
+    s = make_single_system(args.workload, seed=91)
+    eo = torch.from_numpy(s.eps_o).cuda()
+    ev = torch.from_numpy(s.eps_v).cuda()
+    u_out = torch.empty((G, nov), dtype=torch.float64, device="cuda").T
+    ev_ = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    times = {"t2": [], "sosex": [], "mbpt3": []}
+    res = ex_s = ex_m = None
+    for it in range(args.warmup + args.steps):
+        ev_[0].record(stream)
+        res = h.dring_t2(s.R, eo, ev, s.freqs, s.weights, prec="split", n_guess=G, seed=5, cutoff_thresh=1e-4,
+                         u_out=u_out)
+        ev_[1].record(stream)
+        ex_s = h.exchange_sosex(s.R, no, nv, res["U"], res["A"], alpha=1.0)
+        ev_[2].record(stream)
+        ex_m = h.exchange_mbpt3(s.R, eo, ev, res["U"], res["A"])
+        ev_[3].record(stream)
+        torch.cuda.synchronize()
+        if it >= args.warmup:
+            times["t2"].append(ev_[0].elapsed_time(ev_[1]))
+            times["sosex"].append(ev_[1].elapsed_time(ev_[2]))
+            times["mbpt3"].append(ev_[2].elapsed_time(ev_[3]))
+    NT = res["NT"]
+    ms = {k: statistics.mean(v) for k, v in times.items()}
+    flops = {"t2": K * (4.0 * nq * nov * G + 2.0 * nq * nq * nov),
+             "sosex": 2.0 * no * no * nq * nv * NT,
+             "mbpt3": 2.0 * nq * nov * NT + 2.0 * NT * NT * (nq + nov) + 2.0 * nov * NT * NT
+             + 2.0 * no * no * nq * nv * NT}
+    total = sum(ms.values())
+    print(json.dumps({"metric": "CC-path energies (direct-ring T2 + SOSEX + MBPT3 exchange)",
+                      "workload": f"{args.workload}: NQ={nq} NOcc={no} NVirt={nv} nov={nov} K={K} G={G}",
+                      "value": 1e3 / total, "unit": "CC-path evaluations/s", "steps": args.steps,
+                      "warmup": args.warmup, "ms": ms, "NT": NT,
+                      "algorithmic_tflops": {k: flops[k] / (ms[k] * 1e-3) / 1e12 for k in ms},
+                      "Ec_logdet": res["Ec"], "Ec_T2_eig": float(np.sum(res["EigRPA"])),
+                      "Ex_sosex": ex_s, "Ex_mbpt3": ex_m}), flush=True)
+    h.close()
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -500,6 +554,8 @@ def main():
         run_mbe(args)
     elif args.workload.startswith("adjoint"):
         run_adjoint(args)
+    elif args.workload.startswith("cc"):
+        run_cc(args)
     else:
         run_ours(args)
 

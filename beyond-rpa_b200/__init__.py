@@ -95,6 +95,7 @@ def load_library(path: str | os.PathLike | None = None):
     lib.rpa_b200_ec_grad.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _dbl, _i64, _vp,
                                      _vp, _i64, _vp, _vp]
     lib.rpa_b200_exchange_sosex.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _dbl, _i64, _vp]
+    lib.rpa_b200_syevd.argtypes = [_vp, _i64, _vp, _i64, _vp]
     lib.rpa_b200_exchange_mbpt3.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _i64, _vp, _vp,
                                             _vp, _i64]
     if path is None:
@@ -293,8 +294,10 @@ class Handle:
 
     # ------------------------------------------------------------------ beyond RPA
     def dring_t2(self, R, eps_o, eps_v, freqs, weights, alpha=4.0, prec="fp64", guess=None, n_guess=None, seed=0,
-                 small_cutoff=1e-10, cutoff_thresh=1e-4, cutoff_type=0, common_thresh=-1.0, max_vecs=None):
+                 small_cutoff=1e-10, cutoff_thresh=1e-4, cutoff_type=0, common_thresh=-1.0, max_vecs=None,
+                 u_out=None):
         """Direct-ring T2 = U diag(A) U^T (rpa_b200_dring_t2).  guess: (nov, G) guess vectors or None.
+        u_out: optional column-major (nov, cap) device tensor that receives U (then returned as a view).
 
         Returns dict(A, U (nov x NT), EigRPA, NT, common_thresh, Ec)."""
         nq = int(R.shape[0])
@@ -310,20 +313,27 @@ class Handle:
             gm = None
             G = int(n_guess if n_guess is not None else min(int(np.ceil(3.0 * nq)), nov))
             gptr = None
-        cap = int(max_vecs or G)
+        if u_out is not None:
+            uo = _colmajor(u_out, nov)
+            cap = int(u_out.shape[1])
+            U, uptr, ldu = u_out, uo.ptr, uo.ld
+        else:
+            cap = int(max_vecs or G)
+            U = np.zeros((nov, cap), order="F")
+            uptr, ldu = U.ctypes.data, nov
         A = np.zeros(cap)
         eig = np.zeros(cap)
-        U = np.zeros((nov, cap), order="F")
         nt = ctypes.c_int64()
         ct = ctypes.c_double(common_thresh)
         ec = ctypes.c_double()
         self._check(self.lib.rpa_b200_dring_t2(self._h, nq, no, nv, r.ptr, r.ld, eo.ptr, ev.ptr, K, fr.ptr, w.ptr,
                                                float(alpha), _PREC[prec], G, gptr, int(seed), float(small_cutoff),
                                                float(cutoff_thresh), int(cutoff_type), ctypes.byref(ct), cap,
-                                               A.ctypes.data, U.ctypes.data, nov, ctypes.byref(nt),
+                                               A.ctypes.data, uptr, ldu, ctypes.byref(nt),
                                                eig.ctypes.data, ctypes.byref(ec)))
         n = nt.value
-        return {"A": A[:n].copy(), "U": np.asfortranarray(U[:, :n]), "EigRPA": eig[:n].copy(), "NT": n,
+        Uo = U[:, :n] if u_out is not None else np.asfortranarray(U[:, :n])
+        return {"A": A[:n].copy(), "U": Uo, "EigRPA": eig[:n].copy(), "NT": n,
                 "common_thresh": ct.value, "Ec": ec.value}
 
     def exchange_sosex(self, R, nocc, nvirt, U, A, alpha=1.0, s2_operator=False):
@@ -338,6 +348,14 @@ class Handle:
                                                      u.ld, a.ptr, float(alpha), int(bool(s2_operator)),
                                                      ctypes.byref(ex)))
         return ex.value
+
+    def syevd(self, A):
+        """Eigenvalues (ascending) and eigenvectors of the symmetric matrix A (rpa_b200_syevd)."""
+        n = int(A.shape[0])
+        Z = np.array(A, dtype=np.float64, order="F", copy=True)
+        w = np.zeros(n)
+        self._check(self.lib.rpa_b200_syevd(self._h, n, Z.ctypes.data, n, w.ctypes.data))
+        return w, Z
 
     def exchange_mbpt3(self, R, eps_o, eps_v, U, A, return_x=False):
         """MBPT3 exchange energy -Tr(X K) (rpa_b200_exchange_mbpt3); with return_x also the

@@ -18,7 +18,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 INCLUDE = HERE.parent / "include"
 LIB = HERE / "librpa_b200.so"
-SOURCES = ["capi.cu", "scale_split.cu", "syrk_tc.cu", "dsyrk_f64.cu", "logdet.cu", "freq_grid.cu", "noalloc.cu", "gemm_f64.cu", "t2_kernels.cu", "sosex.cu"]
+SOURCES = ["capi.cu", "scale_split.cu", "syrk_tc.cu", "dsyrk_f64.cu", "logdet.cu", "freq_grid.cu", "noalloc.cu", "gemm_f64.cu", "t2_kernels.cu", "sosex.cu", "syevd.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -38,6 +38,7 @@ def needs_build() -> bool:
         return True
     t = LIB.stat().st_mtime
     deps = sources() + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    deps.append(Path(__file__))
     return any(p.stat().st_mtime > t for p in deps)
 
 
@@ -68,7 +69,7 @@ def build(force: bool = False, verbose_ptxas: bool = False, jobs: int | None = N
     if failed:
         raise RuntimeError("nvcc compilation failed")
     tmp = LIB.with_suffix(".so.tmp")
-    link = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs)]
+    link = [nvcc(), *ARCH, "-shared", "-Xlinker", "--no-undefined", "-o", str(tmp), *map(str, objs)]
     subprocess.run(link, check=True)
     tmp.replace(LIB)
     return LIB

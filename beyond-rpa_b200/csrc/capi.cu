@@ -36,11 +36,12 @@ struct rpa_b200_handle {
   std::string last_error;
   DevBuf R, D, eps, Xhi, Xlo, diag_part, diag, Pi, Ldiag, ddbuf;
   // direct-ring T2 / exchange workspace
-  DevBuf tZ, tOm, tIOm, tP, tS, tV, tT, tTIT, tVt, tW, tU, tRU, tSmall, tRot, tPerm;
+  DevBuf tZ, tOm, tIOm, tP, tS, tV, tT, tTIT, tVt, tW, tU, tRU, tSmall, tPerm;
   // batched (many-instance) workspace: descriptors and per-batch results
   DevBuf bDesc, bRes;
   DevBuf gY, gD;  // adjoint workspace
   DevBuf xM;      // MBPT3 exchange: NT x NT matrices, R U and U X
+  DevBuf eW, eA, eZ;  // symmetric eigensolver workspace, input and eigenvector buffers
   struct BatchGraph {
     uint64_t key;
     std::vector<cudaGraphExec_t> execs;
@@ -492,54 +493,16 @@ int normalize_columns(rpa_b200_handle* h, double* X, int64_t rows, int cols) {
   return RPA_OK;
 }
 
-// Symmetric eigen-decomposition of A (n x n, ld n) by parallel Jacobi sweeps:
-// on return V holds the eigenvectors (unsorted), evals the eigenvalues and
-// order the permutation that sorts them ascending.
-int jacobi_eig(rpa_b200_handle* h, double* A, double* V, int n, std::vector<double>& evals, std::vector<int>& order) {
-  RPA_CUDA(h, rpa::launch_set_identity(V, n, n, h->stream));
-  double4* rot = static_cast<double4*>(h->tRot.p);
-  double* red = static_cast<double*>(h->tSmall.p);
-  // one sweep = (m-1) rounds x 2 kernels: captured once, replayed per sweep
-  cudaGraphExec_t exec = nullptr;
-  const int64_t before = rpa::g_launches;
-  int64_t per_sweep = 0;
-  {
-    cudaGraph_t graph = nullptr;
-    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-      cudaError_t e = rpa::launch_jacobi_sweep(A, n, V, n, n, rot, h->stream);
-      cudaError_t e2 = cudaStreamEndCapture(h->stream, &graph);
-      per_sweep = rpa::g_launches - before;
-      rpa::g_launches = before;
-      if (e != cudaSuccess || e2 != cudaSuccess || !graph || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
-        exec = nullptr;
-      if (graph) cudaGraphDestroy(graph);
-    }
-    cudaGetLastError();
-  }
+// Symmetric eigen-decomposition of A (n x n, ld n; destroyed) on the GPU (Householder
+// tridiagonalisation + divide and conquer, syevd.cu): V receives the eigenvectors, evals their
+// eigenvalues (in V's column order) and order the permutation that sorts them ascending.
+int sym_eig(rpa_b200_handle* h, double* A, double* V, int n, std::vector<double>& evals, std::vector<int>& order) {
+  RPA_CUDA(h, ensure(h->eW, rpa::syevd_workspace_bytes(n)));
   bool converged = false;
-  for (int sweep = 0; sweep < 60; ++sweep) {
-    double od[2];
-    RPA_CUDA(h, rpa::launch_offdiag(A, n, n, red, h->stream));
-    RPA_CUDA(h, cudaMemcpyAsync(od, red, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-    RPA_CUDA(h, cudaStreamSynchronize(h->stream));
-    if (!(std::isfinite(od[0]) && std::isfinite(od[1]))) break;
-    if (std::sqrt(od[0]) <= 1e-14 * std::sqrt(od[0] + od[1]) || od[0] == 0.0) {
-      converged = true;
-      break;
-    }
-    if (exec) {
-      RPA_CUDA(h, cudaGraphLaunch(exec, h->stream));
-      rpa::g_launches += per_sweep;
-    } else {
-      RPA_CUDA(h, rpa::launch_jacobi_sweep(A, n, V, n, n, rot, h->stream));
-    }
-  }
-  if (exec) cudaGraphExecDestroy(exec);
-  if (!converged) return fail(h, RPA_ERR_NOT_CONVERGED, "Jacobi eigensolver did not converge (n=%d)", n);
-  evals.resize(n);
-  RPA_CUDA(h, cudaMemcpy2DAsync(evals.data(), sizeof(double), A, (size_t)(n + 1) * sizeof(double), sizeof(double),
-                                (size_t)n, cudaMemcpyDeviceToHost, h->stream));
-  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  RPA_CUDA(h, rpa::syevd(A, n, V, h->eW.p, h->eW.bytes, evals, converged, h->stream));
+  if (!converged) return fail(h, RPA_ERR_NOT_CONVERGED, "symmetric eigensolver: a leaf did not converge (n=%d)", n);
+  for (double x : evals)
+    if (!std::isfinite(x)) return fail(h, RPA_ERR_NONFINITE, "symmetric eigensolver: non-finite eigenvalue (n=%d)", n);
   order.resize(n);
   for (int i = 0; i < n; ++i) order[i] = i;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return evals[a] < evals[b]; });
@@ -672,8 +635,8 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
   if (h->own_stream) cudaStreamSynchronize(h->own_stream);
   for (DevBuf* b : {&h->R, &h->D, &h->eps, &h->Xhi, &h->Xlo, &h->diag_part, &h->diag, &h->Pi, &h->Ldiag, &h->ddbuf,
                     &h->tZ, &h->tOm, &h->tIOm, &h->tP, &h->tS, &h->tV, &h->tT, &h->tTIT, &h->tVt, &h->tW, &h->tU,
-                    &h->tRU, &h->tSmall, &h->tRot, &h->tPerm, &h->bDesc, &h->bRes, &h->gY, &h->gD,
-                    &h->xM})
+                    &h->tRU, &h->tSmall, &h->tPerm, &h->bDesc, &h->bRes, &h->gY, &h->gD,
+                    &h->xM, &h->eW, &h->eA, &h->eZ})
     release(*b);
   for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
   if (h->err_dev) cudaFree(h->err_dev);
@@ -859,7 +822,6 @@ int rpa_b200_dring_t2(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVir
   RPA_CUDA(h, ensure(h->tS, (size_t)G * G * 8));
   RPA_CUDA(h, ensure(h->tV, (size_t)G * G * 8));
   RPA_CUDA(h, ensure(h->tSmall, (size_t)std::max<int64_t>(G, 64) * 8 + 64));
-  RPA_CUDA(h, ensure(h->tRot, (size_t)(G / 2 + 2) * sizeof(double4)));
   RPA_CUDA(h, ensure(h->tPerm, (size_t)G * sizeof(int)));
   if (c.z_resident)
     for (int g0 = 0; g0 < v.K; g0 += c.zk)
@@ -883,7 +845,7 @@ int rpa_b200_dring_t2(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVir
   RPA_CUDA(h, rpa::launch_symmetrize_avg(S, G, G, h->stream));
   std::vector<double> sval;
   std::vector<int> sord;
-  if ((s = jacobi_eig(h, S, Vs, G, sval, sord))) return s;
+  if ((s = sym_eig(h, S, Vs, G, sval, sord))) return s;
   int NT = 0;
   for (int i = G - 1; i >= 0; --i) {
     if (sval[sord[i]] > SmallEigenvalsCutoff) ++NT;
@@ -913,7 +875,7 @@ int rpa_b200_dring_t2(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVir
   RPA_CUDA(h, rpa::launch_symmetrize_avg(TIT, NT, NT, h->stream));
   std::vector<double> aval;
   std::vector<int> aord;
-  if ((s = jacobi_eig(h, TIT, Vt, NT, aval, aord))) return s;
+  if ((s = sym_eig(h, TIT, Vt, NT, aval, aord))) return s;
   std::vector<double> Aall(NT);
   for (int i = 0; i < NT; ++i) {
     const double a = aval[aord[i]];
@@ -1096,7 +1058,6 @@ int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
   const size_t words = 8 * nn + (size_t)NQ * NT + (size_t)nov * NT + (size_t)nov + 3 * (size_t)NT + (size_t)np + 8;
   RPA_CUDA(h, ensure(h->xM, words * 8));
   RPA_CUDA(h, ensure(h->tSmall, (size_t)std::max<int64_t>(NT, 64) * 8 + 64));
-  RPA_CUDA(h, ensure(h->tRot, (size_t)(NT / 2 + 2) * sizeof(double4)));
   RPA_CUDA(h, ensure(h->tPerm, (size_t)NT * sizeof(int)));
   double* w = static_cast<double*>(h->xM.p);
   double* Ukl = w;
@@ -1135,7 +1096,7 @@ int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
   RPA_CUDA(h, rpa::launch_mbpt3_build(Ukl, Dkl, Ad, NT, Am, Bm, Sm, h->stream));
   std::vector<double> mu;
   std::vector<int> order;
-  if ((s = jacobi_eig(h, Sm, Q, NT, mu, order))) return s;
+  if ((s = sym_eig(h, Sm, Q, NT, mu, order))) return s;
   RPA_CUDA(h, cudaMemcpyAsync(mud, mu.data(), (size_t)NT * 8, cudaMemcpyHostToDevice, h->stream));
   RPA_CUDA(h, cudaMemsetAsync(bad, 0, sizeof(int), h->stream));
 
@@ -1220,6 +1181,48 @@ int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
   dd acc{0.0, 0.0};
   for (double x : hp) acc = rpa::dd_add(acc, x);
   *Ex = -(acc.hi + acc.lo);
+  finish_timings(h);
+  return RPA_OK;
+}
+
+// Replaces real_EVD (src/linear-algebra/real_linalg.f90:1501-1559, LAPACK dsyevd) with
+// ComputeEigenvecs = .true.: eigenvalues ascending, A overwritten by the eigenvectors.
+int rpa_b200_syevd(rpa_b200_handle* h, int64_t N, double* A, int64_t ldA, double* Eigenvals) {
+  int s = begin_call(h);
+  if (s != RPA_OK) return s;
+  if (N < 1 || ldA < N || !A || !Eigenvals) return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_syevd");
+  if (N > 46340) return fail(h, RPA_ERR_TOO_LARGE, "rpa_b200_syevd: N too large");
+  const int n = (int)N;
+  const size_t nn = (size_t)n * n;
+  RPA_CUDA(h, ensure(h->eA, nn * 8));
+  RPA_CUDA(h, ensure(h->eZ, nn * 8));
+  double* Ad = static_cast<double*>(h->eA.p);
+  double* Zd = static_cast<double*>(h->eZ.p);
+  const bool dev = is_device_ptr(A);
+  RPA_CUDA(h, cudaMemcpy2DAsync(Ad, (size_t)n * 8, A, (size_t)ldA * 8, (size_t)n * 8, (size_t)n,
+                                dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, h->stream));
+  RPA_CUDA(h, cudaMemsetAsync(h->count_dev, 0, sizeof(int), h->stream));
+  RPA_CUDA(h, rpa::launch_count_nonfinite(Ad, (int64_t)nn, h->count_dev, h->stream));
+  int cnt = 0;
+  RPA_CUDA(h, cudaMemcpyAsync(&cnt, h->count_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (cnt) return fail(h, RPA_ERR_NONFINITE, "%d non-finite entries in A", cnt);
+  RPA_CUDA(h, cudaEventRecord(h->ev[1], h->stream));
+  std::vector<double> ev;
+  std::vector<int> order;
+  if ((s = sym_eig(h, Ad, Zd, n, ev, order))) return s;
+  RPA_CUDA(h, ensure(h->tPerm, (size_t)n * sizeof(int)));
+  if ((s = gather(h, Zd, n, Ad, order, nullptr))) return s;  // columns in ascending order
+  RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
+  RPA_CUDA(h, cudaMemcpy2DAsync(A, (size_t)ldA * 8, Ad, (size_t)n * 8, (size_t)n * 8, (size_t)n,
+                                dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream));
+  std::vector<double> sorted(n);
+  for (int i = 0; i < n; ++i) sorted[i] = ev[order[i]];
+  RPA_CUDA(h, cudaMemcpyAsync(Eigenvals, sorted.data(), (size_t)n * 8,
+                              is_device_ptr(Eigenvals) ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost, h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
   finish_timings(h);
   return RPA_OK;
 }

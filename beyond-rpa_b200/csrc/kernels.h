@@ -178,11 +178,7 @@ cudaError_t launch_grad_accum(const double* R, int64_t ldR, const double* Y, int
                               bool first, cudaStream_t stream);
 cudaError_t launch_replicate(const double* R, int64_t ldR, int NQ, int64_t nov, double* Y, int64_t ldy, int64_t sY,
                              int nb, cudaStream_t stream);
-// One sweep (m-1 rounds) of the parallel two-sided Jacobi method: A <- J^T A J, V <- V J.
-cudaError_t launch_jacobi_sweep(double* A, int64_t lda, double* V, int64_t ldv, int n, double4* rot,
-                                cudaStream_t stream);
 cudaError_t launch_offdiag(const double* A, int64_t lda, int n, double* out, cudaStream_t stream);
-cudaError_t launch_set_identity(double* V, int64_t ldv, int n, cudaStream_t stream);
 cudaError_t launch_fill_uniform(double* X, int64_t rows, int64_t cols, int64_t ldx, uint64_t seed,
                                 cudaStream_t stream);
 cudaError_t launch_col_sqnorm(const double* X, int64_t rows, int64_t cols, int64_t ldx, double* out,
@@ -226,5 +222,14 @@ struct MatDesc {
 };
 // trace_shift + blocked Cholesky + log sums for nmat matrices of orders <= nmax.
 cudaError_t launch_logdet_varlen(const MatDesc* mats, int nmat, int nmax, int* err, cudaStream_t stream);
+
+// ---------------------------------------------------------------- symmetric eigensolver
+// Householder tridiagonalisation + divide and conquer + WY back-transformation (syevd.cu).
+size_t syevd_workspace_bytes(int n);
+// A (n x n, ld n) is destroyed; Z (n x n, ld n) receives the eigenvectors and evals (host) the
+// eigenvalues in the order of Z's columns; converged is false if a leaf solve failed.
+// Synchronises the stream.
+cudaError_t syevd(double* A, int n, double* Z, void* work, size_t work_bytes, std::vector<double>& evals,
+                  bool& converged, cudaStream_t stream);
 
 }  // namespace rpa

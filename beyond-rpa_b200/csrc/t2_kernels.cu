@@ -138,83 +138,7 @@ __global__ void replicate_kernel(const double* R, int64_t ldR, int NQ, int64_t n
   for (int b = 0; b < nb; ++b) Y[(int64_t)b * sY + q + ldy * a] = r;
 }
 
-// ----------------------------------------------------------------- Jacobi
-__device__ __forceinline__ int rr_index(int j, int r, int m) { return j == 0 ? 0 : 1 + (j - 1 + r) % (m - 1); }
-
-// Rotation (c, s) of every pair of round r, from the current matrix.
-__global__ void jacobi_params_kernel(const double* A, int64_t lda, int n, int m, int r, double4* rot) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= m / 2) return;
-  int p = rr_index(k, r, m), q = rr_index(m - 1 - k, r, m);
-  if (p > q) {
-    const int x = p;
-    p = q;
-    q = x;
-  }
-  double c = 1.0, s = 0.0;
-  if (q < n) {
-    const double app = A[(int64_t)p * (lda + 1)], aqq = A[(int64_t)q * (lda + 1)];
-    const double apq = A[(int64_t)p + lda * q];
-    if (fabs(apq) > 1e-300 && fabs(apq) > 1e-18 * sqrt(fabs(app * aqq))) {
-      const double tau = (aqq - app) / (2.0 * apq);
-      const double tt = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-      c = 1.0 / sqrt(1.0 + tt * tt);
-      s = tt * c;
-    }
-  }
-  rot[k] = make_double4(c, s, (double)p, (double)q);
-}
-
-// A <- J^T A J for the 2x2 blocks (pair P, pair Q); V <- V J.
-// blockIdx.y < m/2: A block rows; blockIdx.y == m/2: V (all n rows, pair Q).
-__global__ void jacobi_apply_kernel(double* A, int64_t lda, double* V, int64_t ldv, int n, int m,
-                                    const double4* rot) {
-  const int half = m / 2;
-  const int Pk = blockIdx.x * blockDim.x + threadIdx.x;
-  const int Qk = blockIdx.y;
-  if (blockIdx.z == 0) {
-    if (Pk >= half) return;
-    const double4 P = rot[Pk], Q = rot[Qk];
-    const int p1 = (int)P.z, p2 = (int)P.w, q1 = (int)Q.z, q2 = (int)Q.w;
-    if (p2 >= n || q2 >= n) {
-      // a dummy index (odd n): rotate only the real one
-      if (p2 >= n && q2 >= n) return;
-      if (p2 >= n) {  // rows: only p1 exists; columns rotate
-        const double x1 = A[(int64_t)p1 + lda * q1], x2 = A[(int64_t)p1 + lda * q2];
-        A[(int64_t)p1 + lda * q1] = Q.x * x1 - Q.y * x2;
-        A[(int64_t)p1 + lda * q2] = Q.y * x1 + Q.x * x2;
-      } else {  // columns: only q1 exists; rows rotate
-        const double x1 = A[(int64_t)p1 + lda * q1], x2 = A[(int64_t)p2 + lda * q1];
-        A[(int64_t)p1 + lda * q1] = P.x * x1 - P.y * x2;
-        A[(int64_t)p2 + lda * q1] = P.y * x1 + P.x * x2;
-      }
-      return;
-    }
-    // X = [[a11, a12], [a21, a22]] over rows (p1, p2), columns (q1, q2)
-    const double a11 = A[(int64_t)p1 + lda * q1], a12 = A[(int64_t)p1 + lda * q2];
-    const double a21 = A[(int64_t)p2 + lda * q1], a22 = A[(int64_t)p2 + lda * q2];
-    // X J_Q : col q1' = c x_q1 - s x_q2 ; col q2' = s x_q1 + c x_q2
-    const double b11 = Q.x * a11 - Q.y * a12, b12 = Q.y * a11 + Q.x * a12;
-    const double b21 = Q.x * a21 - Q.y * a22, b22 = Q.y * a21 + Q.x * a22;
-    // J_P^T (X J_Q) : row p1' = c r_p1 - s r_p2 ; row p2' = s r_p1 + c r_p2
-    A[(int64_t)p1 + lda * q1] = P.x * b11 - P.y * b21;
-    A[(int64_t)p1 + lda * q2] = P.x * b12 - P.y * b22;
-    A[(int64_t)p2 + lda * q1] = P.y * b11 + P.x * b21;
-    A[(int64_t)p2 + lda * q2] = P.y * b12 + P.x * b22;
-  } else {
-    // V J_Q over all rows i = Pk (grid covers n rows)
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const double4 Q = rot[Qk];
-    const int q1 = (int)Q.z, q2 = (int)Q.w;
-    if (q2 >= n) return;
-    const double x1 = V[(int64_t)i + ldv * q1], x2 = V[(int64_t)i + ldv * q2];
-    V[(int64_t)i + ldv * q1] = Q.x * x1 - Q.y * x2;
-    V[(int64_t)i + ldv * q2] = Q.y * x1 + Q.x * x2;
-  }
-}
-
-// out[0] = sum_{i != j} A_ij^2, out[1] = sum_i A_ii^2 (fixed-order reduction, one block)
+// Sums of squares of the off-diagonal (out[0]) and diagonal (out[1]) entries (one CTA).
 __global__ void __launch_bounds__(256) offdiag_kernel(const double* A, int64_t lda, int n, double* out) {
   __shared__ double so[256], sd[256];
   double o = 0.0, d = 0.0;
@@ -238,13 +162,6 @@ __global__ void __launch_bounds__(256) offdiag_kernel(const double* A, int64_t l
     out[0] = so[0];
     out[1] = sd[0];
   }
-}
-
-__global__ void set_identity_kernel(double* V, int64_t ldv, int n) {
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (int64_t)n * n) return;
-  const int64_t i = idx % n, j = idx / n;
-  V[i + ldv * j] = (i == j) ? 1.0 : 0.0;
 }
 
 // ----------------------------------------------------------------- vectors
@@ -462,29 +379,8 @@ cudaError_t launch_lyap_scale(double* Y, const double* mu, int n, int* bad, cuda
   return cudaGetLastError();
 }
 
-cudaError_t launch_jacobi_sweep(double* A, int64_t lda, double* V, int64_t ldv, int n, double4* rot,
-                                cudaStream_t stream) {
-  const int m = n + (n & 1);
-  if (m < 2) return cudaSuccess;
-  const int half = m / 2;
-  for (int r = 0; r < m - 1; ++r) {
-    jacobi_params_kernel<<<blocks_for(half), 256, 0, stream>>>(A, lda, n, m, r, rot);
-    ++g_launches;
-    const int gx = (int)blocks_for(n > half ? n : half, 128);
-    jacobi_apply_kernel<<<dim3(gx, half, 2), 128, 0, stream>>>(A, lda, V, ldv, n, m, rot);
-    ++g_launches;
-  }
-  return cudaGetLastError();
-}
-
 cudaError_t launch_offdiag(const double* A, int64_t lda, int n, double* out, cudaStream_t stream) {
   offdiag_kernel<<<1, 256, 0, stream>>>(A, lda, n, out);
-  ++g_launches;
-  return cudaGetLastError();
-}
-
-cudaError_t launch_set_identity(double* V, int64_t ldv, int n, cudaStream_t stream) {
-  set_identity_kernel<<<blocks_for((int64_t)n * n), 256, 0, stream>>>(V, ldv, n);
   ++g_launches;
   return cudaGetLastError();
 }

@@ -27,6 +27,11 @@ SINGLE_SYSTEM = {
     # adjoint workload shapes
     "adjoint_2560": (2560, 48, 640, 16, dict(occ_range=(-1.3, -0.4), virt_range=(0.03, 4.0), decay=320.0,
                                              scale=1.0, lam0=0.8)),
+    # CC path (direct-ring T2 + SOSEX + MBPT3 exchange) shapes, one scaled-down large case each
+    "cc_1024": (1024, 32, 256, 12, dict(occ_range=(-1.3, -0.4), virt_range=(0.03, 4.0), decay=128.0,
+                                        scale=1.0, lam0=0.8)),
+    "cc_2048": (2048, 48, 512, 12, dict(occ_range=(-1.3, -0.4), virt_range=(0.03, 4.0), decay=256.0,
+                                        scale=1.0, lam0=0.8)),
     # beyond-RPA large case shapes
     "large_8192": (8192, 128, 2048, 20, dict(occ_range=(-1.3, -0.4), virt_range=(0.03, 4.0), decay=1024.0,
                                              scale=1.0, lam0=0.8)),

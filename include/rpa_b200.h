@@ -201,6 +201,17 @@ int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
                             int64_t S2Operator, double* Ex);
 
 /*
+ * Symmetric eigen-decomposition A = Z diag(Eigenvals) Z^T, Eigenvals ascending,
+ * A (N x N, column-major, ldA >= N; lower and upper triangles both read)
+ * overwritten by the eigenvectors Z.  Replaces real_EVD with
+ * ComputeEigenvecs = .true. (src/linear-algebra/real_linalg.f90:1501-1559,
+ * LAPACK dsyevd): Householder tridiagonalisation, divide and conquer and
+ * back-transformation, all on the GPU.  Used inside rpa_b200_dring_t2 and
+ * rpa_b200_exchange_mbpt3.
+ */
+int rpa_b200_syevd(rpa_b200_handle* h, int64_t N, double* A, int64_t ldA, double* Eigenvals);
+
+/*
  * MBPT3 exchange energy  Ex = -Tr(X K) = -sum_{abij} (aj|bi) (U X U^T)_aibj,
  * where X (NVecsT2 x NVecsT2) solves B^T X + X B = A with
  * A_mn = A_m D_mn + D_mn A_n, B_mn = D_mn + 2 U_mn + 4 U_mn A_n,
