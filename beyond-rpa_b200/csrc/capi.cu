@@ -1057,7 +1057,7 @@ int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
   const int64_t np = rpa::sosex_partials((int)NQ, (int)NOcc, NT);
   const size_t words = 8 * nn + (size_t)NQ * NT + (size_t)nov * NT + (size_t)nov + 3 * (size_t)NT + (size_t)np + 8;
   RPA_CUDA(h, ensure(h->xM, words * 8));
-  RPA_CUDA(h, ensure(h->tSmall, (size_t)std::max<int64_t>(NT, 64) * 8 + 64));
+  RPA_CUDA(h, ensure(h->tSmall, (size_t)std::max<int64_t>(NT, 256) * 8 + 64));
   RPA_CUDA(h, ensure(h->tPerm, (size_t)NT * sizeof(int)));
   double* w = static_cast<double*>(h->xM.p);
   double* Ukl = w;

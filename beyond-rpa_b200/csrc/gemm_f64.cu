@@ -8,8 +8,11 @@
 // C column-major (ld), optional per-k scale ks (ks_stride per batch) and
 // per-row scale rs.  Either stride of each operand may be 1; the loader maps
 // consecutive threads along the unit-stride index.
-// CTA tile 64 x 64, 4 warps (2 x 2) of 32 x 32, K chunks of 16 double-buffered
-// through shared memory.
+// CTA tile 64 x 64, 4 warps (2 x 2) of 32 x 32 (4 x 4 DMMA tiles each), K chunks
+// of 16 streamed through a 3-stage cp.async pipeline, 4 CTAs per SM.  Each
+// operand's shared-memory tile follows its unit-stride index: [k][m] with row
+// pitch 72 when m (or n) is contiguous, [m][k] with pitch 18 when k is; both
+// pitches make the m8n8k4 fragment loads hit every bank pair exactly twice.
 #include "kernels.h"
 
 namespace rpa {
@@ -17,28 +20,58 @@ namespace rpa {
 namespace {
 constexpr int BM = 64;
 constexpr int BK = 16;
-constexpr int LDS = BM + 8;
+constexpr int LDM = BM + 8;   // [k][m] pitch
+constexpr int LDK = BK + 2;   // [m][k] pitch
+constexpr int kTileWords = BK * LDM;  // == BM * LDK = 1152
+static_assert(BK * LDM == BM * LDK, "both tile layouts take the same space");
 constexpr int kThreads = 128;
+constexpr int kStages = 3;
+constexpr size_t kSmem = sizeof(double) * (size_t)kStages * (2 * kTileWords + BK);
 
 __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                : "+d"(c0), "+d"(c1)
                : "d"(a), "d"(b));
 }
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem), "r"(valid ? 8 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-__global__ void __launch_bounds__(kThreads) gemm_f64_kernel(const GemmF64Args g) {
-  __shared__ double As[2][BK][LDS];
-  __shared__ double Bs[2][BK][LDS];
+// kMC: the operand's row index (m for A, n for B) is the contiguous one -> [k][r] tile;
+// otherwise k is contiguous -> [r][k] tile.
+template <bool kMC>
+__device__ __forceinline__ int tile_off(int r, int k) {
+  return kMC ? k * LDM + r : r * LDK + k;
+}
+
+template <bool kAM, bool kBN>
+__global__ void __launch_bounds__(kThreads, 4) gemm_f64_kernel(const GemmF64Args g) {
+  extern __shared__ double smem[];
+  double* As = smem;                              // [kStages][kTileWords]
+  double* Bs = smem + kStages * kTileWords;       // [kStages][kTileWords]
+  double* Ss = smem + 2 * kStages * kTileWords;   // [kStages][BK]
   const int b = blockIdx.z;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BM;
-  const double* A = g.A + (int64_t)b * g.sA;
-  const double* B = g.B + (int64_t)b * g.sB;
-  double* C = g.C + (int64_t)b * g.sC;
-  const double* ks = g.kscale ? g.kscale + (int64_t)b * g.ks_stride : nullptr;
+  const bool split = g.splitk > 1;
+  // split-K: blockIdx.z selects the K range [kbeg, kend) and its partial-product buffer
+  int64_t kbeg = 0, kend = g.K;
+  if (split) {
+    const int64_t kc = ((g.K + g.splitk - 1) / g.splitk + BK - 1) / BK * BK;
+    kbeg = (int64_t)b * kc;
+    kend = min(g.K, kbeg + kc);
+  }
+  const double* A = g.A + (split ? 0 : (int64_t)b * g.sA);
+  const double* B = g.B + (split ? 0 : (int64_t)b * g.sB);
+  double* C = split ? g.work + (int64_t)b * g.M * g.N : g.C + (int64_t)b * g.sC;
+  const int64_t ldc = split ? g.M : g.ldc;
+  const double* ks = g.kscale ? g.kscale + (split ? 0 : (int64_t)b * g.ks_stride) : nullptr;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int wm = warp >> 1, wn = warp & 1;
-  const bool a_mcontig = (g.a_m == 1);
-  const bool b_ncontig = (g.b_n == 1);
 
   double acc[4][4][2];
 #pragma unroll
@@ -46,68 +79,59 @@ __global__ void __launch_bounds__(kThreads) gemm_f64_kernel(const GemmF64Args g)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-  double ra[8], rb[8];
-  auto idx_of = [&](int i, bool contig_first, int& r, int& c) {
-    // 1024 elements of a 64 x 16 tile: r in [0,64) (m or n), c in [0,16) (k)
-    const int idx = t + kThreads * i;
-    if (contig_first) {
-      r = idx % BM;
-      c = idx / BM;
-    } else {
-      r = idx / BK;
-      c = idx % BK;
-    }
-  };
-  auto gload = [&](int64_t k0) {
+  auto load_stage = [&](int st, int64_t k0) {
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      int r, c;
-      idx_of(i, a_mcontig, r, c);
-      const int64_t k = k0 + c;
-      const int m = m0 + r;
-      ra[i] = (m < g.M && k < g.K) ? A[(int64_t)m * g.a_m + k * g.a_k] : 0.0;
-      idx_of(i, b_ncontig, r, c);
-      const int64_t k2 = k0 + c;
-      const int n = n0 + r;
-      double v = (n < g.N && k2 < g.K) ? B[k2 * g.b_k + (int64_t)n * g.b_n] : 0.0;
-      if (ks && k2 < g.K) v *= ks[k2];
-      rb[i] = v;
+      const int idx = t + kThreads * i;
+      // consecutive threads walk the operand's unit-stride index
+      const int ra = kAM ? idx % BM : idx / BK, ca = kAM ? idx / BM : idx % BK;
+      const int64_t ka = k0 + ca;
+      const bool va = (m0 + ra < g.M) && (ka < kend);
+      cp_async8(As + st * kTileWords + tile_off<kAM>(ra, ca),
+                va ? A + (int64_t)(m0 + ra) * g.a_m + ka * g.a_k : A, va);
+      const int rb = kBN ? idx % BM : idx / BK, cb = kBN ? idx / BM : idx % BK;
+      const int64_t kb = k0 + cb;
+      const bool vb = (n0 + rb < g.N) && (kb < kend);
+      cp_async8(Bs + st * kTileWords + tile_off<kBN>(rb, cb),
+                vb ? B + kb * g.b_k + (int64_t)(n0 + rb) * g.b_n : B, vb);
     }
-  };
-  auto sstore = [&](int buf) {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      int r, c;
-      idx_of(i, a_mcontig, r, c);
-      As[buf][c][r] = ra[i];
-      idx_of(i, b_ncontig, r, c);
-      Bs[buf][c][r] = rb[i];
+    if (ks && t < BK) {
+      const int64_t k = k0 + t;
+      Ss[st * BK + t] = k < kend ? ks[k] : 0.0;
     }
   };
 
-  const int64_t nch = (g.K + BK - 1) / BK;
-  gload(0);
-  sstore(0);
-  __syncthreads();
+  const int64_t nch = kend > kbeg ? (kend - kbeg + BK - 1) / BK : 0;
+#pragma unroll
+  for (int st = 0; st < kStages - 1; ++st) {
+    if (st < nch) load_stage(st, kbeg + (int64_t)st * BK);
+    cp_async_commit();
+  }
   for (int64_t c = 0; c < nch; ++c) {
-    const int buf = (int)(c & 1);
-    if (c + 1 < nch) gload((c + 1) * BK);
+    cp_async_wait<kStages - 2>();
+    __syncthreads();
+    const int64_t cn = c + kStages - 1;
+    if (cn < nch) load_stage((int)(cn % kStages), kbeg + cn * BK);
+    cp_async_commit();
+    const int st = (int)(c % kStages);
+    const double* at = As + st * kTileWords;
+    const double* bt = Bs + st * kTileWords;
 #pragma unroll
     for (int kk = 0; kk < BK; kk += 4) {
       const int kr = kk + (lane & 3);
       double af[4], bf[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) af[i] = As[buf][kr][wm * 32 + i * 8 + (lane >> 2)];
+      for (int i = 0; i < 4; ++i) af[i] = at[tile_off<kAM>(wm * 32 + i * 8 + (lane >> 2), kr)];
+      const double sc = ks ? Ss[st * BK + kr] : 1.0;
 #pragma unroll
-      for (int j = 0; j < 4; ++j) bf[j] = Bs[buf][kr][wn * 32 + j * 8 + (lane >> 2)];
+      for (int j = 0; j < 4; ++j) bf[j] = bt[tile_off<kBN>(wn * 32 + j * 8 + (lane >> 2), kr)] * sc;
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
     }
-    if (c + 1 < nch) sstore(buf ^ 1);
-    __syncthreads();
   }
+  cp_async_wait<0>();
 
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
@@ -120,21 +144,63 @@ __global__ void __launch_bounds__(kThreads) gemm_f64_kernel(const GemmF64Args g)
       for (int v = 0; v < 2; ++v) {
         const int n = n0 + wn * 32 + j * 8 + 2 * (lane & 3) + v;
         if (n >= g.N) continue;
-        double* p = C + (int64_t)m + g.ldc * (int64_t)n;
-        const double val = g.alpha * rsm * acc[i][j][v];
-        *p = (g.beta == 0.0) ? val : val + g.beta * *p;
+        double* p = C + (int64_t)m + ldc * (int64_t)n;
+        if (split) {
+          *p = acc[i][j][v];
+        } else {
+          const double val = g.alpha * rsm * acc[i][j][v];
+          *p = (g.beta == 0.0) ? val : val + g.beta * *p;
+        }
       }
     }
   }
+}
+
+// C = alpha rs(m) sum_s P_s + beta C, partials summed in a fixed order.
+__global__ void splitk_reduce_kernel(const GemmF64Args g) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t mn = (int64_t)g.M * g.N;
+  if (idx >= mn) return;
+  const int64_t m = idx % g.M, n = idx / g.M;
+  double s = 0.0;
+  for (int z = 0; z < g.splitk; ++z) s += g.work[z * mn + idx];
+  double* p = g.C + m + g.ldc * n;
+  const double val = g.alpha * (g.rowscale ? g.rowscale[m] : 1.0) * s;
+  *p = (g.beta == 0.0) ? val : val + g.beta * *p;
+}
+
+template <bool kAM, bool kBN>
+cudaError_t launch_variant(const GemmF64Args& g, cudaStream_t stream) {
+  static uint64_t attr_set = 0;  // per-variant bit per device: dynamic shared memory opted in
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev >= 64 || !(attr_set >> dev & 1)) {
+    e = cudaFuncSetAttribute(gemm_f64_kernel<kAM, kBN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+    if (e != cudaSuccess) return e;
+    if (dev < 64) attr_set |= 1ull << dev;
+  }
+  const bool split = g.splitk > 1;
+  dim3 grid((unsigned)((g.N + BM - 1) / BM), (unsigned)((g.M + BM - 1) / BM),
+            (unsigned)(split ? g.splitk : g.batch));
+  gemm_f64_kernel<kAM, kBN><<<grid, kThreads, kSmem, stream>>>(g);
+  if (split) {
+    const int64_t mn = (int64_t)g.M * g.N;
+    splitk_reduce_kernel<<<(unsigned)((mn + 255) / 256), 256, 0, stream>>>(g);
+  }
+  return cudaGetLastError();
 }
 }  // namespace
 
 cudaError_t launch_gemm_f64(const GemmF64Args& g, cudaStream_t stream) {
   if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return cudaSuccess;
-  dim3 grid((unsigned)((g.N + BM - 1) / BM), (unsigned)((g.M + BM - 1) / BM), (unsigned)g.batch);
-  gemm_f64_kernel<<<grid, kThreads, 0, stream>>>(g);
-  ++g_launches;
-  return cudaGetLastError();
+  if (g.splitk > 1 && (g.batch != 1 || !g.work)) return cudaErrorInvalidValue;
+  const bool am = (g.a_m == 1), bn = (g.b_n == 1);
+  cudaError_t e;
+  if (am) e = bn ? launch_variant<true, true>(g, stream) : launch_variant<true, false>(g, stream);
+  else e = bn ? launch_variant<false, true>(g, stream) : launch_variant<false, false>(g, stream);
+  g_launches += g.splitk > 1 ? 2 : 1;
+  return e;
 }
 
 }  // namespace rpa

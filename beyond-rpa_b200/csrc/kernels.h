@@ -156,6 +156,10 @@ struct GemmF64Args {
   int64_t ks_stride;
   const double* rowscale;  // optional, per m
   int batch;
+  // split-K (batch must be 1): splitk partial products over K ranges go to work
+  // (splitk * M * N doubles) and are summed in a fixed order by a second kernel
+  int splitk;
+  double* work;
 };
 cudaError_t launch_gemm_f64(const GemmF64Args& g, cudaStream_t stream);
 
@@ -178,6 +182,7 @@ cudaError_t launch_grad_accum(const double* R, int64_t ldR, const double* Y, int
                               bool first, cudaStream_t stream);
 cudaError_t launch_replicate(const double* R, int64_t ldR, int NQ, int64_t nov, double* Y, int64_t ldy, int64_t sY,
                              int nb, cudaStream_t stream);
+// out: 2 + 240 doubles (sums in out[0], out[1]; per-CTA partials after them)
 cudaError_t launch_offdiag(const double* A, int64_t lda, int n, double* out, cudaStream_t stream);
 cudaError_t launch_fill_uniform(double* X, int64_t rows, int64_t cols, int64_t ldx, uint64_t seed,
                                 cudaStream_t stream);

@@ -152,16 +152,24 @@ __global__ void __launch_bounds__(kHouseThreads) house_kernel(double* A, int n, 
   }
 }
 
-// y(c) = sum_{r > j} A(r, c) v(r) for c > j: one warp per column.
+// y(c) = sum_{r > j} A(r, c) v(r) for c > j: one warp per column, four independent
+// accumulators per lane so that four loads of each lane are in flight.
 __global__ void __launch_bounds__(256) trailing_gemv_kernel(const double* A, int n, const double* v, int j,
                                                             double* y) {
   const int c = j + 1 + (int)blockIdx.x * 8 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (c >= n) return;
   const double* col = A + (int64_t)n * c;
-  double acc = 0.0;
-  for (int r = j + 1 + lane; r < n; r += 32) acc += col[r] * v[r];
-  acc = warp_sum(acc);
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int r = j + 1 + lane;
+  for (; r + 96 < n; r += 128) {
+    a0 += col[r] * v[r];
+    a1 += col[r + 32] * v[r + 32];
+    a2 += col[r + 64] * v[r + 64];
+    a3 += col[r + 96] * v[r + 96];
+  }
+  for (; r < n; r += 32) a0 += col[r] * v[r];
+  const double acc = warp_sum((a0 + a1) + (a2 + a3));
   if (lane == 0) y[c] = acc;
 }
 
@@ -170,19 +178,27 @@ __global__ void __launch_bounds__(256) trailing_gemv_kernel(const double* A, int
 // T (upper triangular, nb x nb, ld kNB) of the block reflector H_p ... H_{p+nb-1} = I - V T V^T,
 // from G = V^T V (ld kNB): T(i,i) = tau_i, T(0:i, i) = -tau_i T(0:i, 0:i) G(0:i, i).
 __global__ void build_t_kernel(const double* G, const double* tau, int nb, double* T) {
+  __shared__ double Gs[kNB][kNB + 1], Ts[kNB][kNB + 1], ts[kNB];
   const int r = threadIdx.x;  // row of T
+  for (int c = 0; c < kNB; ++c) {
+    Gs[r][c] = (r < nb && c < nb) ? G[r + kNB * c] : 0.0;
+    Ts[r][c] = 0.0;
+  }
+  ts[r] = r < nb ? tau[r] : 0.0;
+  __syncwarp();
   for (int i = 0; i < nb; ++i) {
     double val = 0.0;
     if (r < i) {
-      for (int c = r; c < i; ++c) val += T[r + kNB * c] * G[c + kNB * i];
-      val *= -tau[i];
+      for (int c = r; c < i; ++c) val += Ts[r][c] * Gs[c][i];
+      val *= -ts[i];
     } else if (r == i) {
-      val = tau[i];
+      val = ts[i];
     }
     __syncwarp();
-    if (r < kNB) T[r + kNB * i] = val;
+    Ts[r][i] = val;
     __syncwarp();
   }
+  for (int c = 0; c < kNB; ++c) T[r + kNB * c] = Ts[r][c];
 }
 
 // ---------------------------------------------------------------- stage 2: divide and conquer
@@ -584,6 +600,7 @@ size_t syevd_workspace_bytes(int n) {
   b += align256((size_t)n * kNB * 8);  // Wp
   b += 2 * align256((size_t)kNB * n * 8);  // Y, Y2
   b += 2 * align256((size_t)kNB * kNB * 8);  // G, T
+  b += align256(std::max((size_t)16 * kNB * n, (size_t)64 * kNB * kNB) * 8);  // split-K partials
   b += 6 * align256((size_t)n * 8);  // y, tau, d, e, zhat, D
   b += align256((size_t)2 * n * 8) + align256((size_t)2 * n * 4);  // sort keys
   b += 9 * align256((size_t)n * 8);  // ds zs dk zk ddef rc rs tau rho
@@ -615,6 +632,7 @@ cudaError_t syevd(double* A, int n, double* Z, void* work, size_t work_bytes, st
   double* Y2 = (double*)take((size_t)kNB * n * 8);
   double* Gm = (double*)take((size_t)kNB * kNB * 8);
   double* Tb = (double*)take((size_t)kNB * kNB * 8);
+  double* Pk = (double*)take(std::max((size_t)16 * kNB * n, (size_t)64 * kNB * kNB) * 8);
   double* y = (double*)take((size_t)n * 8);
   double* tau = (double*)take((size_t)n * 8);
   double* d = (double*)take((size_t)n * 8);
@@ -750,10 +768,18 @@ cudaError_t syevd(double* A, int n, double* Z, void* work, size_t work_bytes, st
     const int nb = std::min(kNB, n - 1 - p);
     const int mr = n - 1 - p;  // rows p+1 .. n-1
     const double* Vb = V + (p + 1) + ld * p;
-    SY_CHECK(launch_gemm_f64(gemm_args(nb, nb, mr, Vb, ld, 1, Vb, 1, ld, Gm, kNB, 1.0, 0.0), stream));
+    // G = V_b^T V_b and Y = V_b^T Z have few output tiles and K = mr: split K
+    GemmF64Args gg = gemm_args(nb, nb, mr, Vb, ld, 1, Vb, 1, ld, Gm, kNB, 1.0, 0.0);
+    gg.splitk = std::max(1, std::min(64, mr / 256));
+    gg.work = Pk;
+    SY_CHECK(launch_gemm_f64(gg, stream));
     build_t_kernel<<<1, 32, 0, stream>>>(Gm, tau + p, nb, Tb);
     ++g_launches;
-    SY_CHECK(launch_gemm_f64(gemm_args(nb, n, mr, Vb, ld, 1, Z + (p + 1), 1, ld, Y, kNB, 1.0, 0.0), stream));
+    GemmF64Args gy = gemm_args(nb, n, mr, Vb, ld, 1, Z + (p + 1), 1, ld, Y, kNB, 1.0, 0.0);
+    const int ytiles = (n + 63) / 64;  // about 600 CTA slots (148 SMs x 4), K chunks >= 256
+    gy.splitk = std::max(1, std::min(16, std::min(mr / 256, 600 / ytiles)));
+    gy.work = Pk;
+    SY_CHECK(launch_gemm_f64(gy, stream));
     SY_CHECK(launch_gemm_f64(gemm_args(nb, n, nb, Tb, 1, kNB, Y, 1, kNB, Y2, kNB, 1.0, 0.0), stream));
     SY_CHECK(launch_gemm_f64(gemm_args(mr, n, nb, Vb, 1, ld, Y2, 1, kNB, Z + (p + 1), ld, -1.0, 1.0), stream));
   }

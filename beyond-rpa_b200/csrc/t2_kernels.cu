@@ -138,11 +138,15 @@ __global__ void replicate_kernel(const double* R, int64_t ldR, int NQ, int64_t n
   for (int b = 0; b < nb; ++b) Y[(int64_t)b * sY + q + ldy * a] = r;
 }
 
-// Sums of squares of the off-diagonal (out[0]) and diagonal (out[1]) entries (one CTA).
+// Sums of squares of the off-diagonal (out[0]) and diagonal (out[1]) entries: kOffBlocks
+// CTAs write partial sums to out[2 ...], the last kernel adds them in a fixed order.
+constexpr int kOffBlocks = 120;
 __global__ void __launch_bounds__(256) offdiag_kernel(const double* A, int64_t lda, int n, double* out) {
   __shared__ double so[256], sd[256];
   double o = 0.0, d = 0.0;
-  for (int64_t idx = threadIdx.x; idx < (int64_t)n * n; idx += blockDim.x) {
+  const int64_t total = (int64_t)n * n;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = idx % n, j = idx / n;
     const double v = A[i + lda * j];
     if (i == j) d += v * v;
@@ -159,9 +163,20 @@ __global__ void __launch_bounds__(256) offdiag_kernel(const double* A, int64_t l
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    out[0] = so[0];
-    out[1] = sd[0];
+    out[2 + 2 * blockIdx.x] = so[0];
+    out[3 + 2 * blockIdx.x] = sd[0];
   }
+}
+
+__global__ void offdiag_final_kernel(double* out) {
+  if (threadIdx.x != 0) return;
+  double o = 0.0, d = 0.0;
+  for (int b = 0; b < kOffBlocks; ++b) {
+    o += out[2 + 2 * b];
+    d += out[3 + 2 * b];
+  }
+  out[0] = o;
+  out[1] = d;
 }
 
 // ----------------------------------------------------------------- vectors
@@ -380,8 +395,9 @@ cudaError_t launch_lyap_scale(double* Y, const double* mu, int n, int* bad, cuda
 }
 
 cudaError_t launch_offdiag(const double* A, int64_t lda, int n, double* out, cudaStream_t stream) {
-  offdiag_kernel<<<1, 256, 0, stream>>>(A, lda, n, out);
-  ++g_launches;
+  offdiag_kernel<<<kOffBlocks, 256, 0, stream>>>(A, lda, n, out);
+  offdiag_final_kernel<<<1, 32, 0, stream>>>(out);
+  g_launches += 2;
   return cudaGetLastError();
 }
 
