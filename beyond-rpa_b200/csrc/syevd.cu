@@ -19,6 +19,8 @@
 //     run in the same launches.
 //  3. Back-transformation V = Q_H Z with compact-WY block reflectors
 //     (I - V_b T_b V_b^T), three GEMMs per panel.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -31,7 +33,6 @@ namespace {
 
 constexpr int kNB = 32;    // panel width of the reduction and of the back-transformation
 constexpr int kLeaf = 32;  // largest leaf of the divide-and-conquer tree
-constexpr int kHouseThreads = 1024;
 constexpr double kEps = 1.1102230246251565e-16;  // unit roundoff 2^-53
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -75,62 +76,103 @@ __device__ double block_max(double v, double* red) {
 
 // ---------------------------------------------------------------- stage 1: reduction
 
-// One single-CTA step of the panel reduction (panel starts at column p; Wp is n x kNB, ld n).
+namespace cg = cooperative_groups;
+constexpr int kCS = 8;    // CTAs per cluster of the per-column reduction step
+constexpr int kCT = 512;  // threads per CTA
+
+// Cluster-wide sum of cnt per-CTA partials (part[buf][0..cnt), written by the caller and
+// followed by __syncthreads): after the cluster barrier every CTA adds the kCS partials in
+// rank order through distributed shared memory, so all CTAs get identical totals in out.
+// part is double-buffered: a CTA rewrites part[buf] only after the next barrier, which no CTA
+// passes before every CTA has finished reading the previous buffer.
+__device__ __forceinline__ void cluster_sum(cg::cluster_group& cl, double (*part)[2 * kNB], int& buf, int cnt,
+                                            double* out) {
+  cl.sync();
+  if ((int)threadIdx.x < cnt) {
+    double acc = 0.0;
+    for (int k = 0; k < kCS; ++k) acc += cl.map_shared_rank(&part[buf][0], k)[threadIdx.x];
+    out[threadIdx.x] = acc;
+  }
+  __syncthreads();
+  buf ^= 1;
+}
+
+// One step of the panel reduction (panel starts at column p; Wp is n x kNB, ld n), run by one
+// cluster of kCS CTAs; CTA `rank` owns rows [j+1 + rank*chunk, ...) of the active column.
 //  fin >= 0: finish w of panel column fin from y = A_trailing v (the deferred update of the
 //            trailing matrix by panel columns < fin is applied here), store W(:, fin).
 //  nxt >= 0: bring column p+nxt up to date, generate its reflector (tau, d, e, V(:, p+nxt)).
-__global__ void __launch_bounds__(kHouseThreads) house_kernel(double* A, int n, double* V, double* Wp, int p, int fin,
-                                                              int nxt, const double* y, double* tau, double* d,
-                                                              double* e) {
+__global__ void __cluster_dims__(kCS, 1, 1) __launch_bounds__(kCT)
+    house_kernel(double* A, int n, double* V, double* Wp, int p, int fin, int nxt, const double* y, double* tau,
+                 double* d, double* e) {
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  __shared__ double part[2][2 * kNB];
+  __shared__ double tot[2 * kNB];
+  __shared__ double wj[kNB], vj[kNB];
   __shared__ double red[33];
-  __shared__ double s1[kNB], s2[kNB];
+  int buf = 0;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int64_t ld = n;
+  const int gt = rank * kCT + t;  // thread index within the cluster
   if (fin >= 0) {
     const int j = p + fin;
     const double* v = V + ld * j;
-    // s1_c = V_c^T v, s2_c = W_c^T v over rows > j (warp per dot product)
-    for (int q = warp; q < 2 * fin; q += kHouseThreads / 32) {
+    const int m = n - 1 - j, chunk = (m + kCS - 1) / kCS;
+    const int r0 = j + 1 + rank * chunk, r1 = min(n, r0 + chunk);
+    // s1_c = V_c^T v (q = 2c), s2_c = W_c^T v (q = 2c + 1): warp per product over this CTA's rows
+    for (int q = warp; q < 2 * fin; q += kCT / 32) {
       const int c = q >> 1;
       const double* col = (q & 1) ? (Wp + ld * c) : (V + ld * (p + c));
       double acc = 0.0;
-      for (int r = j + 1 + lane; r < n; r += 32) acc += col[r] * v[r];
+      for (int r = r0 + lane; r < r1; r += 32) acc += col[r] * v[r];
       acc = warp_sum(acc);
-      if (lane == 0) {
-        if (q & 1) s2[c] = acc;
-        else s1[c] = acc;
-      }
+      if (lane == 0) part[buf][q] = acc;
     }
     __syncthreads();
+    cluster_sum(cl, part, buf, 2 * fin, tot);
     const double tj = tau[j];
     double* w = Wp + ld * fin;
-    double part = 0.0;
-    for (int r = t; r < n; r += kHouseThreads) {
-      double val = 0.0;
-      if (r > j) {
-        val = y[r];
-        for (int c = 0; c < fin; ++c) val -= V[r + ld * (p + c)] * s2[c] + Wp[r + ld * c] * s1[c];
-        val *= tj;
-        part += val * v[r];
-      }
+    double pv = 0.0;
+    for (int r = r0 + t; r < r1; r += kCT) {
+      double val = y[r];
+      for (int c = 0; c < fin; ++c) val -= V[r + ld * (p + c)] * tot[2 * c + 1] + Wp[r + ld * c] * tot[2 * c];
+      val *= tj;
       w[r] = val;
+      pv += val * v[r];
     }
-    const double alpha = -0.5 * tj * block_sum(part, red);
-    for (int r = j + 1 + t; r < n; r += kHouseThreads) w[r] += alpha * v[r];
+    for (int r = gt; r <= j; r += kCS * kCT) w[r] = 0.0;
+    pv = block_sum(pv, red);
+    if (t == 0) part[buf][0] = pv;
     __syncthreads();
+    cluster_sum(cl, part, buf, 1, tot);
+    const double alpha = -0.5 * tj * tot[0];
+    for (int r = r0 + t; r < r1; r += kCT) w[r] += alpha * v[r];
+    cl.sync();  // W(:, fin) complete and visible to the whole cluster
   }
   if (nxt >= 0) {
     const int j = p + nxt;
     double* a = A + ld * j;
-    // deferred update of column j (rows >= j) from panel columns < nxt
-    double part = 0.0;
-    for (int r = j + t; r < n; r += kHouseThreads) {
-      double val = a[r];
-      for (int c = 0; c < nxt; ++c) val -= V[r + ld * (p + c)] * Wp[j + ld * c] + Wp[r + ld * c] * V[j + ld * (p + c)];
-      a[r] = val;
-      if (r >= j + 2) part += val * val;
+    const int m = n - j, chunk = (m + kCS - 1) / kCS;
+    const int r0 = j + rank * chunk, r1 = min(n, r0 + chunk);
+    if (t < nxt) {
+      wj[t] = Wp[j + ld * t];
+      vj[t] = V[j + ld * (p + t)];
     }
-    const double sigma2 = block_sum(part, red);  // also orders the column writes above
+    __syncthreads();
+    // deferred update of column j (rows >= j) from panel columns < nxt
+    double ps = 0.0;
+    for (int r = r0 + t; r < r1; r += kCT) {
+      double val = a[r];
+      for (int c = 0; c < nxt; ++c) val -= V[r + ld * (p + c)] * wj[c] + Wp[r + ld * c] * vj[c];
+      a[r] = val;
+      if (r >= j + 2) ps += val * val;
+    }
+    ps = block_sum(ps, red);
+    if (t == 0) part[buf][0] = ps;
+    __syncthreads();
+    cluster_sum(cl, part, buf, 1, tot);  // its barrier also publishes the updated column
+    const double sigma2 = tot[0];
     const double alpha = a[j + 1];
     double beta, tj, scale;
     if (sigma2 == 0.0) {
@@ -143,13 +185,16 @@ __global__ void __launch_bounds__(kHouseThreads) house_kernel(double* A, int n, 
       scale = 1.0 / (alpha - beta);
     }
     double* v = V + ld * j;
-    for (int r = t; r < n; r += kHouseThreads) v[r] = (r <= j) ? 0.0 : (r == j + 1 ? 1.0 : a[r] * scale);
-    if (t == 0) {
+    for (int r = r0 + t; r < r1; r += kCT)
+      if (r > j) v[r] = (r == j + 1) ? 1.0 : a[r] * scale;
+    for (int r = gt; r <= j; r += kCS * kCT) v[r] = 0.0;
+    if (rank == 0 && t == 0) {
       tau[j] = tj;
       d[j] = a[j];
       e[j] = beta;
     }
   }
+  cl.sync();  // no CTA leaves while another may still read its shared memory
 }
 
 // y(c) = sum_{r > j} A(r, c) v(r) for c > j: one warp per column, four independent
@@ -671,14 +716,14 @@ cudaError_t syevd(double* A, int n, double* Z, void* work, size_t work_bytes, st
   // ---- stage 1: tridiagonal reduction
   for (int p = 0; p <= n - 2; p += kNB) {
     const int nb = std::min(kNB, n - 1 - p);
-    house_kernel<<<1, kHouseThreads, 0, stream>>>(A, n, V, Wp, p, -1, 0, y, tau, d, e);
+    house_kernel<<<kCS, kCT, 0, stream>>>(A, n, V, Wp, p, -1, 0, y, tau, d, e);
     ++g_launches;
     for (int i = 0; i < nb; ++i) {
       const int j = p + i;
       const int m = n - 1 - j;
       trailing_gemv_kernel<<<(m + 7) / 8, 256, 0, stream>>>(A, n, V + ld * j, j, y);
       ++g_launches;
-      house_kernel<<<1, kHouseThreads, 0, stream>>>(A, n, V, Wp, p, i, i + 1 < nb ? i + 1 : -1, y, tau, d, e);
+      house_kernel<<<kCS, kCT, 0, stream>>>(A, n, V, Wp, p, i, i + 1 < nb ? i + 1 : -1, y, tau, d, e);
       ++g_launches;
     }
     SY_CHECK(cudaGetLastError());
