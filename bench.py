@@ -507,6 +507,71 @@ def run_cc(args):
     h.close()
 
 
+def run_split(args):
+    """One system split over the N GPUs (ai columns per rank, reduce-scatter of Pi over the
+    frequency index, distributed log-dets): E_c/s of the whole job, strong scaling.
+    --workload split_<system> (e.g. split_single_4096)."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    group = None
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    pkg = load_package()
+    from beyond_rpa_b200.workloads import make_single_system, SINGLE_SYSTEM
+    from beyond_rpa_b200 import distributed as D
+    system = args.workload[len("split_"):]
+    nq, no, nv, K, _ = SINGLE_SYSTEM[system]
+    h = pkg.Handle(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    h.set_stream(stream.cuda_stream)
+    s = make_single_system(system, seed=1000)  # the same system on every rank
+    torch.cuda.synchronize()
+
+    def pi_fn(Rc, eo, ev, fr, out):
+        h.pi_u(Rc, eo, ev, fr, prec="split", out=out)
+
+    def ec_fn(pi, wk):
+        return h.ec_from_pi(pi, wk)
+
+    def step():
+        return D.ec_rpa_ai_split(pi_fn, ec_fn, s.R, s.eps_o, s.eps_v, s.freqs, s.weights, group=group)
+
+    for _ in range(args.warmup):
+        step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        ec, eu = step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t_ms = float(t.item())
+    if rank == 0:
+        print(json.dumps({"metric": "RPA E_c of one system split over the GPUs (ai columns)", "workload":
+                          f"{args.workload}: NQ={nq} NOcc={no} NVirt={nv} K={K}", "value": args.steps / (t_ms / 1e3),
+                          "unit": "E_c/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": t_ms / args.steps, "scaling": "strong", "Ec": ec,
+                          "collectives": "reduce_scatter (K*NQ^2 FP64) + all_reduce (K+1)"}), flush=True)
+    h.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -556,6 +621,8 @@ def main():
         run_adjoint(args)
     elif args.workload.startswith("cc"):
         run_cc(args)
+    elif args.workload.startswith("split_"):
+        run_split(args)
     else:
         run_ours(args)
 

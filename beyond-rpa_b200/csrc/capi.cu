@@ -277,11 +277,17 @@ int build_pi(rpa_b200_handle* h, const Validated& v, const double* Rd, int64_t l
   // split-BF16: groups of frequencies sized to the free device memory
   const int64_t pitch = (nov + 7) / 8 * 8;
   const size_t perFreq = (size_t)NQ * pitch * 2 * 2;  // hi + lo
-  size_t freeB = 0, totalB = 0;
-  RPA_CUDA(h, cudaMemGetInfo(&freeB, &totalB));
-  const size_t have = h->Xhi.bytes + h->Xlo.bytes;
-  size_t budget = (size_t)((double)(freeB + have) * 0.7);
-  int kg = (int)std::min<size_t>((size_t)std::min(v.K, rpa::kMaxKgLaunch), std::max<size_t>(1, budget / perFreq));
+  // The free-memory query can stall the host for tens of ms while the GPU idles: ask only when
+  // the buffers from an earlier call cannot already hold the largest group.
+  const int kmax = std::min(v.K, rpa::kMaxKgLaunch);
+  int kg = kmax;
+  if (h->Xhi.bytes < (size_t)kmax * NQ * pitch * 2 || h->Xlo.bytes < (size_t)kmax * NQ * pitch * 2) {
+    size_t freeB = 0, totalB = 0;
+    RPA_CUDA(h, cudaMemGetInfo(&freeB, &totalB));
+    const size_t have = h->Xhi.bytes + h->Xlo.bytes;
+    const size_t budget = (size_t)((double)(freeB + have) * 0.7);
+    kg = (int)std::min<size_t>((size_t)kmax, std::max<size_t>(1, budget / perFreq));
+  }
   RPA_CUDA(h, ensure(h->Xhi, (size_t)kg * NQ * pitch * 2));
   RPA_CUDA(h, ensure(h->Xlo, (size_t)kg * NQ * pitch * 2));
   const rpa::SplitPlan plan = rpa::plan_scale_split(NQ, nov, h->num_sms);
