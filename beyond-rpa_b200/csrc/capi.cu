@@ -33,6 +33,7 @@ struct rpa_b200_handle {
   int num_sms = 0;
   cudaStream_t stream = nullptr;      // stream the calls run on
   cudaStream_t own_stream = nullptr;  // the handle's own stream
+  cudaStream_t copy_stream = nullptr;  // host-to-device staging overlapped with compute
   std::string last_error;
   DevBuf R, D, eps, Xhi, Xlo, diag_part, diag, Pi, Ldiag, ddbuf;
   // direct-ring T2 / exchange workspace
@@ -201,6 +202,17 @@ int validate_common(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt,
 }
 
 // Stage R (NQ x nov, ldR) on the device; returns a device pointer and its ld.
+// Orbital energies -> D(ai) on the device (no synchronisation).
+int stage_eps(rpa_b200_handle* h, const Validated& v) {
+  RPA_CUDA(h, ensure(h->eps, (size_t)(v.no + v.nv) * 8));
+  double* ed = static_cast<double*>(h->eps.p);
+  RPA_CUDA(h, cudaMemcpyAsync(ed, v.eo.data(), (size_t)v.no * 8, cudaMemcpyHostToDevice, h->stream));
+  RPA_CUDA(h, cudaMemcpyAsync(ed + v.no, v.ev.data(), (size_t)v.nv * 8, cudaMemcpyHostToDevice, h->stream));
+  RPA_CUDA(h, ensure(h->D, (size_t)v.nov * 8));
+  RPA_CUDA(h, rpa::launch_dai(ed, ed + v.no, v.no, v.nv, static_cast<double*>(h->D.p), h->stream));
+  return RPA_OK;
+}
+
 int stage_R(rpa_b200_handle* h, const Validated& v, const double* R, int64_t ldR, const double** Rd, int64_t* ldd) {
   if (is_device_ptr(R)) {
     *Rd = R;
@@ -218,13 +230,8 @@ int stage_R(rpa_b200_handle* h, const Validated& v, const double* R, int64_t ldR
   // NaN/Inf screen of the Cholesky vectors (ld may exceed NQ: screen the span)
   RPA_CUDA(h, cudaMemsetAsync(h->count_dev, 0, sizeof(int), h->stream));
   RPA_CUDA(h, rpa::launch_count_nonfinite(*Rd, (*ldd) * (v.nov - 1) + v.NQ, h->count_dev, h->stream));
-  // orbital energies -> D(ai)
-  RPA_CUDA(h, ensure(h->eps, (size_t)(v.no + v.nv) * 8));
-  double* ed = static_cast<double*>(h->eps.p);
-  RPA_CUDA(h, cudaMemcpyAsync(ed, v.eo.data(), (size_t)v.no * 8, cudaMemcpyHostToDevice, h->stream));
-  RPA_CUDA(h, cudaMemcpyAsync(ed + v.no, v.ev.data(), (size_t)v.nv * 8, cudaMemcpyHostToDevice, h->stream));
-  RPA_CUDA(h, ensure(h->D, (size_t)v.nov * 8));
-  RPA_CUDA(h, rpa::launch_dai(ed, ed + v.no, v.no, v.nv, static_cast<double*>(h->D.p), h->stream));
+  int s = stage_eps(h, v);
+  if (s != RPA_OK) return s;
   int cnt = 0;
   RPA_CUDA(h, cudaMemcpyAsync(&cnt, h->count_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   RPA_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -245,6 +252,24 @@ int encode_map(rpa_b200_handle* h, CUtensorMap* m, void* base, int64_t nov, int 
 }
 
 // Build the lower triangles of Pi_k (k = 0..K-1) into h->Pi (ld = NQ).
+// Frequencies per split-BF16 group (all of them unless the device is short of memory).  The
+// free-memory query can stall the host for tens of ms while the GPU idles: ask only when the
+// buffers from an earlier call cannot already hold the largest group.  Returns -status on error.
+int choose_kg(rpa_b200_handle* h, const Validated& v, int64_t pitch) {
+  const size_t perFreq = (size_t)v.NQ * pitch * 2 * 2;  // hi + lo
+  const int kmax = std::min(v.K, rpa::kMaxKgLaunch);
+  if (h->Xhi.bytes >= (size_t)kmax * v.NQ * pitch * 2 && h->Xlo.bytes >= (size_t)kmax * v.NQ * pitch * 2) return kmax;
+  size_t freeB = 0, totalB = 0;
+  cudaError_t e = cudaMemGetInfo(&freeB, &totalB);
+  if (e != cudaSuccess) {
+    fail(h, RPA_ERR_CUDA, "CUDA error %s", cudaGetErrorString(e));
+    return -RPA_ERR_CUDA;
+  }
+  const size_t have = h->Xhi.bytes + h->Xlo.bytes;
+  const size_t budget = (size_t)((double)(freeB + have) * 0.7);
+  return (int)std::min<size_t>((size_t)kmax, std::max<size_t>(1, budget / perFreq));
+}
+
 int build_pi(rpa_b200_handle* h, const Validated& v, const double* Rd, int64_t ldR, double alpha, int64_t prec) {
   const int NQ = v.NQ;
   const int64_t nov = v.nov;
@@ -276,18 +301,8 @@ int build_pi(rpa_b200_handle* h, const Validated& v, const double* Rd, int64_t l
   }
   // split-BF16: groups of frequencies sized to the free device memory
   const int64_t pitch = (nov + 7) / 8 * 8;
-  const size_t perFreq = (size_t)NQ * pitch * 2 * 2;  // hi + lo
-  // The free-memory query can stall the host for tens of ms while the GPU idles: ask only when
-  // the buffers from an earlier call cannot already hold the largest group.
-  const int kmax = std::min(v.K, rpa::kMaxKgLaunch);
-  int kg = kmax;
-  if (h->Xhi.bytes < (size_t)kmax * NQ * pitch * 2 || h->Xlo.bytes < (size_t)kmax * NQ * pitch * 2) {
-    size_t freeB = 0, totalB = 0;
-    RPA_CUDA(h, cudaMemGetInfo(&freeB, &totalB));
-    const size_t have = h->Xhi.bytes + h->Xlo.bytes;
-    const size_t budget = (size_t)((double)(freeB + have) * 0.7);
-    kg = (int)std::min<size_t>((size_t)kmax, std::max<size_t>(1, budget / perFreq));
-  }
+  int kg = 0;
+  if ((kg = choose_kg(h, v, pitch)) <= 0) return -kg;
   RPA_CUDA(h, ensure(h->Xhi, (size_t)kg * NQ * pitch * 2));
   RPA_CUDA(h, ensure(h->Xlo, (size_t)kg * NQ * pitch * 2));
   const rpa::SplitPlan plan = rpa::plan_scale_split(NQ, nov, h->num_sms);
@@ -321,6 +336,86 @@ int build_pi(rpa_b200_handle* h, const Validated& v, const double* Rd, int64_t l
     a.diag = diag;
     a.err = h->err_dev;
     a.seg_chunks = h->seg_chunks;
+    RPA_CUDA(h, rpa::launch_syrk_split_bf16(&mAh, &mAl, &mBh, &mBl, a, h->num_sms, h->stream));
+    RPA_CUDA(h, cudaEventRecord(e2, h->stream));
+    h->tc_ev.push_back({e1, e2});
+  }
+  return RPA_OK;
+}
+
+// Split-BF16 Pi build from Cholesky vectors in host memory, all frequencies in one group: the ai
+// columns are staged in kPipe pieces on the copy stream while the compute stream screens, scales,
+// splits and contracts the pieces that have arrived (the tensor-core SYRK of piece c > 0 adds
+// into Pi in FP64; the last piece writes the exact diagonal).  The diagonal partials are indexed
+// by the global split, so the result equals the one-shot build.  count_dev collects the number of
+// non-finite entries of R; the caller reads it after the stream has been synchronised.
+// Returns 1 (nothing done) when the frequencies do not fit in one group.
+int build_pi_pipelined(rpa_b200_handle* h, const Validated& v, const double* Rh, int64_t ldR, double alpha) {
+  constexpr int kPipe = 4;
+  const int NQ = v.NQ;
+  const int64_t nov = v.nov;
+  const int64_t pitch = (nov + 7) / 8 * 8;
+  int kg = 0;
+  if ((kg = choose_kg(h, v, pitch)) <= 0) return -kg;
+  const rpa::SplitPlan plan = rpa::plan_scale_split(NQ, nov, h->num_sms);
+  if (kg < v.K || plan.nsplit < kPipe || plan.ai_per_split % 32 != 0) return 1;
+  RPA_CUDA(h, ensure(h->R, (size_t)NQ * nov * 8));
+  RPA_CUDA(h, ensure(h->Pi, (size_t)v.K * NQ * NQ * 8));
+  RPA_CUDA(h, ensure(h->diag, (size_t)v.K * NQ * 8));
+  RPA_CUDA(h, ensure(h->Xhi, (size_t)kg * NQ * pitch * 2));
+  RPA_CUDA(h, ensure(h->Xlo, (size_t)kg * NQ * pitch * 2));
+  RPA_CUDA(h, ensure(h->diag_part, (size_t)plan.nsplit * kg * NQ * 8));
+  double* Rd = static_cast<double*>(h->R.p);
+  double* Pi = static_cast<double*>(h->Pi.p);
+  double* diag = static_cast<double*>(h->diag.p);
+  const double* D = static_cast<const double*>(h->D.p);
+  rpa::FreqGroup fg{};
+  fg.n = v.K;
+  for (int k = 0; k < v.K; ++k) fg.u2[k] = v.freqs[k] * v.freqs[k];
+  CUtensorMap mAh, mAl, mBh, mBl;
+  int s;
+  if ((s = encode_map(h, &mAh, h->Xhi.p, nov, NQ, v.K, pitch, rpa::kSyrkTcTM)) != RPA_OK) return s;
+  if ((s = encode_map(h, &mAl, h->Xlo.p, nov, NQ, v.K, pitch, rpa::kSyrkTcTM)) != RPA_OK) return s;
+  if ((s = encode_map(h, &mBh, h->Xhi.p, nov, NQ, v.K, pitch, rpa::kSyrkTcTN)) != RPA_OK) return s;
+  if ((s = encode_map(h, &mBl, h->Xlo.p, nov, NQ, v.K, pitch, rpa::kSyrkTcTN)) != RPA_OK) return s;
+  RPA_CUDA(h, cudaMemsetAsync(h->count_dev, 0, sizeof(int), h->stream));
+  // the copy stream starts after earlier work of this stream (R may still be read by it)
+  cudaEvent_t start = pool_event(h);
+  RPA_CUDA(h, cudaEventRecord(start, h->stream));
+  RPA_CUDA(h, cudaStreamWaitEvent(h->copy_stream, start, 0));
+  for (int c = 0; c < kPipe; ++c) {
+    const int s0 = (int)((int64_t)plan.nsplit * c / kPipe), s1 = (int)((int64_t)plan.nsplit * (c + 1) / kPipe);
+    const int64_t a0 = (int64_t)s0 * plan.ai_per_split, a1 = std::min(nov, (int64_t)s1 * plan.ai_per_split);
+    if (a1 <= a0) continue;
+    cudaEvent_t arrived = pool_event(h);
+    RPA_CUDA(h, cudaMemcpy2DAsync(Rd + a0 * NQ, (size_t)NQ * 8, Rh + a0 * ldR, (size_t)ldR * 8, (size_t)NQ * 8,
+                                  (size_t)(a1 - a0), cudaMemcpyHostToDevice, h->copy_stream));
+    RPA_CUDA(h, cudaEventRecord(arrived, h->copy_stream));
+    RPA_CUDA(h, cudaStreamWaitEvent(h->stream, arrived, 0));
+    RPA_CUDA(h, rpa::launch_count_nonfinite(Rd + a0 * NQ, (a1 - a0) * NQ, h->count_dev, h->stream));
+    cudaEvent_t e0 = pool_event(h), e1 = pool_event(h), e2 = pool_event(h);
+    RPA_CUDA(h, cudaEventRecord(e0, h->stream));
+    RPA_CUDA(h, rpa::launch_scale_split_part(Rd, NQ, NQ, nov, D, fg, alpha, static_cast<__nv_bfloat16*>(h->Xhi.p),
+                                             static_cast<__nv_bfloat16*>(h->Xlo.p), pitch, (int64_t)NQ * pitch,
+                                             static_cast<double*>(h->diag_part.p), plan, s0, s1, h->stream));
+    const bool last = (s1 == plan.nsplit);
+    if (last)
+      RPA_CUDA(h, rpa::launch_diag_reduce(static_cast<double*>(h->diag_part.p), plan, v.K, NQ, diag, h->stream));
+    RPA_CUDA(h, cudaEventRecord(e1, h->stream));
+    h->split_ev.push_back({e0, e1});
+    rpa::SyrkTcArgs a{};
+    a.NQ = NQ;
+    a.nov = nov;
+    a.kg = v.K;
+    a.Pi = Pi;
+    a.ldPi = NQ;
+    a.piStride = (int64_t)NQ * NQ;
+    a.diag = last ? diag : nullptr;
+    a.err = h->err_dev;
+    a.seg_chunks = h->seg_chunks;
+    a.chunk0 = (int)(a0 / 32);
+    a.nov_part = a1 - a0;
+    a.accumulate = (c > 0) ? 1 : 0;
     RPA_CUDA(h, rpa::launch_syrk_split_bf16(&mAh, &mAl, &mBh, &mBl, a, h->num_sms, h->stream));
     RPA_CUDA(h, cudaEventRecord(e2, h->stream));
     h->tc_ev.push_back({e1, e2});
@@ -615,6 +710,7 @@ int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) {
   h->num_sms = prop.multiProcessorCount;
   if (cudaSetDevice(h->device) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&h->err_dev, sizeof(int)) != cudaSuccess || cudaMalloc(&h->count_dev, sizeof(int)) != cudaSuccess) {
     delete h;
     return RPA_ERR_CUDA;
@@ -639,6 +735,7 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->own_stream) cudaStreamSynchronize(h->own_stream);
+  if (h->copy_stream) cudaStreamSynchronize(h->copy_stream);
   for (DevBuf* b : {&h->R, &h->D, &h->eps, &h->Xhi, &h->Xlo, &h->diag_part, &h->diag, &h->Pi, &h->Ldiag, &h->ddbuf,
                     &h->tZ, &h->tOm, &h->tIOm, &h->tP, &h->tS, &h->tV, &h->tT, &h->tTIT, &h->tVt, &h->tW, &h->tU,
                     &h->tRU, &h->tSmall, &h->tPerm, &h->bDesc, &h->bRes, &h->gY, &h->gD,
@@ -652,6 +749,7 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
   for (auto& e : h->pool) cudaEventDestroy(e);
   for (auto& g : h->chol_graphs) cudaGraphExecDestroy(g.exec);
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   delete h;
   return RPA_OK;
 }
@@ -764,6 +862,24 @@ int rpa_b200_ec(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, con
     return s;
   if (!FreqWeights || !Ec) return fail(h, RPA_ERR_INVALID_ARG, "FreqWeights or Ec is NULL");
   if ((s = fetch_small(h, FreqWeights, NFreqs, v.weights))) return s;
+  if (prec == RPA_PREC_SPLIT_BF16 && !is_device_ptr(R)) {
+    // host R: staging overlapped with the Pi build, piece by piece
+    if ((s = stage_eps(h, v))) return s;
+    RPA_CUDA(h, cudaEventRecord(h->ev[1], h->stream));
+    s = build_pi_pipelined(h, v, R, ldR, alpha);
+    if (s == RPA_OK) {
+      int cnt = 0;
+      RPA_CUDA(h, cudaMemcpyAsync(&cnt, h->count_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+      const int se = energy_from_workspace(h, v.NQ, v.K, v.weights, Ec, Eu);
+      RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+      if (cnt) return fail(h, RPA_ERR_NONFINITE, "%d non-finite entries in the Cholesky vectors", cnt);
+      if (se) return se;
+      RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+      finish_timings(h);
+      return RPA_OK;
+    }
+    if (s != 1) return s;  // 1: frequencies need several groups, stage R whole instead
+  }
   const double* Rd;
   int64_t ldd;
   if ((s = stage_R(h, v, R, ldR, &Rd, &ldd))) return s;

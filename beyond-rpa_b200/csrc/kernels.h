@@ -58,6 +58,14 @@ cudaError_t launch_scale_split(const double* R, int64_t ldR, int NQ, int64_t nov
                                const FreqGroup& fg, double alpha, __nv_bfloat16* Xhi, __nv_bfloat16* Xlo,
                                int64_t pitch, int64_t kstride, double* diag_part, double* diag,
                                const SplitPlan& plan, cudaStream_t stream);
+// The splits split0 .. split1-1 of the same pass (ai columns split*ai_per_split ..), without the
+// diagonal reduction; launch_diag_reduce completes the diagonal once every split has run.
+cudaError_t launch_scale_split_part(const double* R, int64_t ldR, int NQ, int64_t nov, const double* D,
+                                    const FreqGroup& fg, double alpha, __nv_bfloat16* Xhi, __nv_bfloat16* Xlo,
+                                    int64_t pitch, int64_t kstride, double* diag_part, const SplitPlan& plan,
+                                    int split0, int split1, cudaStream_t stream);
+cudaError_t launch_diag_reduce(const double* diag_part, const SplitPlan& plan, int kg, int NQ, double* diag,
+                               cudaStream_t stream);
 
 // ---------------------------------------------------------------- tcgen05 SYRK
 struct SyrkTcArgs {
@@ -67,9 +75,13 @@ struct SyrkTcArgs {
   double* Pi;        // output, lower triangle of Pi_k written (incl. diagonal)
   int64_t ldPi;
   int64_t piStride;  // elements between consecutive Pi_k
-  const double* diag;  // exact diagonal [kg][NQ]
+  const double* diag;  // exact diagonal [kg][NQ]; nullptr: the diagonal is left untouched
   int* err;
   int seg_chunks;    // 32-column chunks per accumulation segment (<= 0: no segmentation)
+  // ai sub-range: 32-column chunks chunk0 .. chunk0 + ceil(nov_part / 32) - 1 of X (0, nov: all)
+  int chunk0;
+  int64_t nov_part;
+  int accumulate;    // 1: Pi_k += the sub-range's contribution (FP64), 0: Pi_k = it
 };
 // Tensor maps: 3-D (ai, Q, k) bf16 views of X_hi / X_lo; A maps use a
 // 128-row box, B maps a 256-row box, 32 ai per box, 64-byte swizzle.

@@ -118,9 +118,9 @@ __device__ __forceinline__ void scale_split_body(
 __global__ void __launch_bounds__(kThreads, 3) scale_split_kernel(
     const double* __restrict__ R, int64_t ldR, int NQ, int64_t nov, const double* __restrict__ D,
     FreqGroup fg, double alpha, __nv_bfloat16* __restrict__ Xhi, __nv_bfloat16* __restrict__ Xlo, int64_t pitch,
-    int64_t kstride, double* __restrict__ diag_part, int64_t ai_per_split) {
+    int64_t kstride, double* __restrict__ diag_part, int64_t ai_per_split, int split0) {
   scale_split_body(R, ldR, NQ, nov, D, fg, alpha, Xhi, Xlo, pitch, kstride, diag_part, ai_per_split, blockIdx.x,
-                   blockIdx.y);
+                   split0 + (int)blockIdx.y);
 }
 
 // Many instances in one launch: CTA b handles (instance, q tile, ai split) = work[b].
@@ -204,12 +204,31 @@ cudaError_t launch_scale_split(const double* R, int64_t ldR, int NQ, int64_t nov
   cudaError_t e0 = cudaFuncSetAttribute(scale_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmem);
   if (e0 != cudaSuccess) return e0;
   scale_split_kernel<<<grid, kThreads, kSplitSmem, stream>>>(R, ldR, NQ, nov, D, fg, alpha, Xhi, Xlo, pitch, kstride,
-                                                     diag_part, plan.ai_per_split);
+                                                     diag_part, plan.ai_per_split, 0);
   ++g_launches;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  const int64_t n = (int64_t)fg.n * NQ;
-  diag_reduce_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(diag_part, plan.nsplit, fg.n, NQ, diag);
+  return launch_diag_reduce(diag_part, plan, fg.n, NQ, diag, stream);
+}
+
+cudaError_t launch_scale_split_part(const double* R, int64_t ldR, int NQ, int64_t nov, const double* D,
+                                    const FreqGroup& fg, double alpha, __nv_bfloat16* Xhi, __nv_bfloat16* Xlo,
+                                    int64_t pitch, int64_t kstride, double* diag_part, const SplitPlan& plan,
+                                    int split0, int split1, cudaStream_t stream) {
+  if (split0 < 0 || split1 > plan.nsplit || split1 <= split0) return cudaErrorInvalidValue;
+  cudaError_t e0 = cudaFuncSetAttribute(scale_split_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSplitSmem);
+  if (e0 != cudaSuccess) return e0;
+  dim3 grid(plan.qtiles, split1 - split0);
+  scale_split_kernel<<<grid, kThreads, kSplitSmem, stream>>>(R, ldR, NQ, nov, D, fg, alpha, Xhi, Xlo, pitch, kstride,
+                                                     diag_part, plan.ai_per_split, split0);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_diag_reduce(const double* diag_part, const SplitPlan& plan, int kg, int NQ, double* diag,
+                               cudaStream_t stream) {
+  const int64_t n = (int64_t)kg * NQ;
+  diag_reduce_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(diag_part, plan.nsplit, kg, NQ, diag);
   ++g_launches;
   return cudaGetLastError();
 }

@@ -78,6 +78,8 @@ __device__ __forceinline__ UnitCoord decode_unit(int u, int nblocks, int ntm) {
 // What a CTA needs to know about one work unit.
 struct Unit {
   int k, tm, tn, NQ, nchunks;
+  int chunk0;          // first 32-column chunk of X
+  bool accumulate;     // Pi += contribution instead of Pi = contribution
   double* Pk;          // Pi of this frequency
   int64_t ldPi;
   const double* dk;    // exact diagonal of this frequency
@@ -97,9 +99,11 @@ struct SingleSource {
     x.tn = c.tn;
     x.NQ = a.NQ;
     x.nchunks = nchunks;
+    x.chunk0 = a.chunk0;
+    x.accumulate = a.accumulate != 0;
     x.Pk = a.Pi + (int64_t)c.k * a.piStride;
     x.ldPi = a.ldPi;
-    x.dk = a.diag + (int64_t)c.k * a.NQ;
+    x.dk = a.diag ? a.diag + (int64_t)c.k * a.NQ : nullptr;
     for (int i = 0; i < 4; ++i) x.map[i] = maps[i];
     return x;
   }
@@ -119,6 +123,8 @@ struct MultiSource {
     x.tn = (int)w.w;
     x.NQ = in.NQ;
     x.nchunks = in.nchunks;
+    x.chunk0 = 0;
+    x.accumulate = false;
     x.Pk = in.Pi + (int64_t)x.k * in.piStride;
     x.ldPi = in.ldPi;
     x.dk = in.diag + (int64_t)x.k * in.NQ;
@@ -188,7 +194,7 @@ __device__ __forceinline__ void syrk_body(const Source& src, int* err, const int
             break;
           }
           mbar_arrive_expect_tx(&full[stage], kStageBytes);
-          const int c0 = ch * TK;
+          const int c0 = (x.chunk0 + ch) * TK;
           tma_load_3d(a_hi(stage), x.map[0], &full[stage], c0, x.tm * TM, x.k);
           tma_load_3d(a_lo(stage), x.map[1], &full[stage], c0, x.tm * TM, x.k);
           tma_load_3d(b_hi(stage), x.map[2], &full[stage], c0, x.tn * TN, x.k);
@@ -290,12 +296,20 @@ __device__ __forceinline__ void syrk_body(const Source& src, int* err, const int
       if (m < x.NQ && nbase <= m) {
         double* p = x.Pk + (int64_t)m + (int64_t)nbase * x.ldPi;
         const int jd = m - nbase;  // column index of the diagonal element (may be >= kEpiCols)
+        if (x.accumulate) {
 #pragma unroll
-        for (int j = 0; j < kEpiCols; ++j) {
-          if (j < jd) *p = (double)run[j];
-          p += x.ldPi;
+          for (int j = 0; j < kEpiCols; ++j) {
+            if (j < jd) *p += (double)run[j];
+            p += x.ldPi;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < kEpiCols; ++j) {
+            if (j < jd) *p = (double)run[j];
+            p += x.ldPi;
+          }
         }
-        if (jd < kEpiCols) x.Pk[(int64_t)m * (x.ldPi + 1)] = x.dk[m];
+        if (jd < kEpiCols && x.dk) x.Pk[(int64_t)m * (x.ldPi + 1)] = x.dk[m];
       }
     }
   }
@@ -345,7 +359,9 @@ cudaError_t launch_syrk_split_bf16(const CUtensorMap* tmA_hi, const CUtensorMap*
   int nblocks = 0;
   for (int tn = 0; tn < ntn; ++tn) nblocks += (ntm - 2 * tn > 0) ? (ntm - 2 * tn) : 0;
   const int nunits = nblocks * a.kg;
-  const int nchunks = (int)((a.nov + TK - 1) / TK);
+  const int64_t span = a.nov_part > 0 ? a.nov_part : a.nov;
+  const int nchunks = (int)((span + TK - 1) / TK);
+  if (a.chunk0 < 0 || (int64_t)a.chunk0 * TK + span > ((a.nov + TK - 1) / TK) * TK) return cudaErrorInvalidValue;
   if (nunits == 0 || nchunks == 0) return cudaSuccess;
   cudaError_t e =
       cudaFuncSetAttribute(syrk_split_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);

@@ -32,8 +32,12 @@ def systems(seed=100, n=7):
 def test_batched_matches_single_and_oracle(handle, prec, tol):
     sys_ = systems()
     ec, eus = handle.ec_batched(sys_, prec=prec)
+    import torch
     for (R, eo, ev, x, w), e, eu in zip(sys_, ec, eus):
-        single, single_eu = handle.ec_rpa(R, eo, ev, x, w, prec=prec)
+        # device R: the single call runs the same one-shot arithmetic as the batched launch
+        # (host R is staged in pieces whose contributions are summed in FP64 instead)
+        Rd = torch.from_numpy(np.ascontiguousarray(R.T)).cuda().T
+        single, single_eu = handle.ec_rpa(Rd, eo, ev, x, w, prec=prec)
         assert abs(e - single) < 1e-12
         ref, _ = O.ec_rpa(R, eo, ev, x, w)
         assert abs(e - ref) < tol

@@ -148,3 +148,30 @@ def test_bad_dimensions_are_rejected(handle, pkg):
     with pytest.raises(pkg.RPAError) as e:
         handle.ec_rpa(s.R, s.eps_o, s.eps_v, np.zeros(65), np.zeros(65))
     assert e.value.status == pkg.RPA_ERR_INVALID_ARG
+
+
+def test_host_r_pipelined_staging_matches_device_r(handle):
+    # host R with several ai pieces: staging overlapped with the split and the SYRK of earlier
+    # pieces (FP64 accumulation across pieces), against the one-shot build from device R
+    import torch
+    s = O.make_system(700, 12, 180, 41, decay=90.0, lam0=0.8)
+    x, w = O.casimir_polder(14, 0.8)
+    host = handle.ec_rpa(s.R, s.eps_o, s.eps_v, x, w, prec="split")
+    Rt = torch.from_numpy(np.ascontiguousarray(s.R.T)).cuda()
+    dev = handle.ec_rpa(Rt.T, s.eps_o, s.eps_v, x, w, prec="split")
+    assert abs(host[0] - dev[0]) < 1e-9
+    assert np.max(np.abs(host[1] - dev[1])) < 1e-9
+    ref, _ = O.ec_rpa(s.R, s.eps_o, s.eps_v, x, w)
+    assert abs(host[0] - ref) < 1e-6
+
+
+def test_host_r_pipelined_nonfinite_is_reported(handle, pkg):
+    s = O.make_system(700, 12, 180, 41, decay=90.0, lam0=0.8)
+    x, w = O.casimir_polder(14, 0.8)
+    R = s.R.copy()
+    R[5, R.shape[1] - 3] = np.inf  # in the last staged piece
+    with pytest.raises(pkg.RPAError) as e:
+        handle.ec_rpa(R, s.eps_o, s.eps_v, x, w, prec="split")
+    assert e.value.status == pkg.RPA_ERR_NONFINITE
+    ec, _ = handle.ec_rpa(s.R, s.eps_o, s.eps_v, x, w, prec="split")  # the handle stays usable
+    assert np.isfinite(ec)
