@@ -15,6 +15,7 @@ Python names follow the reference routines they stand in for:
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 from pathlib import Path
 
@@ -96,6 +97,9 @@ def load_library(path: str | os.PathLike | None = None):
                                      _vp, _i64, _vp, _vp]
     lib.rpa_b200_exchange_sosex.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _dbl, _i64, _vp]
     lib.rpa_b200_syevd.argtypes = [_vp, _i64, _vp, _i64, _vp]
+    lib.rpa_b200_piu_basis.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _dbl, _dbl, _i64, _i64, _dbl,
+                                       _vp, _i64, ctypes.c_uint64, _vp, _i64, _vp, _vp, _vp]
+    lib.rpa_b200_project_basis.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64]
     lib.rpa_b200_exchange_mbpt3.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _i64, _vp, _vp,
                                             _vp, _i64]
     if path is None:
@@ -356,6 +360,37 @@ class Handle:
         w = np.zeros(n)
         self._check(self.lib.rpa_b200_syevd(self._h, n, Z.ctypes.data, n, w.ctypes.data))
         return w, Z
+
+    def piu_basis(self, R, eps_o, eps_v, lowest_freq, target_error=math.sqrt(1e-5), basis="eigen", prec="fp64",
+                  guess=None, seed=0, alpha=4.0):
+        """Compressed Pi basis (rpa_b200_piu_basis): returns (G (NQ x NVecs), trace_error, exact_trace)."""
+        nq = int(R.shape[0])
+        no, nv = len(eps_o), len(eps_v)
+        r = _colmajor(R, nq)
+        eo, ev = _vec(eps_o), _vec(eps_v)
+        bt = {"random": 1, "eigen": 2, "full": 3}[basis]
+        G = np.zeros((nq, nq), order="F")
+        gm = _colmajor(guess, nq) if guess is not None else None
+        nvec = ctypes.c_int64()
+        terr = ctypes.c_double()
+        tex = ctypes.c_double()
+        self._check(self.lib.rpa_b200_piu_basis(self._h, nq, no, nv, r.ptr, r.ld, eo.ptr, ev.ptr, float(lowest_freq),
+                                                float(alpha), _PREC[prec], bt, float(target_error),
+                                                gm.ptr if gm else None, gm.ld if gm else nq, int(seed),
+                                                G.ctypes.data, nq, ctypes.byref(nvec), ctypes.byref(terr),
+                                                ctypes.byref(tex)))
+        return np.asfortranarray(G[:, :nvec.value]), terr.value, tex.value
+
+    def project_basis(self, G, R):
+        """R' = G^T R (rpa_b200_project_basis), numpy in, numpy out."""
+        nq, nvec = int(G.shape[0]), int(G.shape[1])
+        nov = int(R.shape[1])
+        g = _colmajor(G, nq)
+        r = _colmajor(R, nq)
+        out = np.zeros((nvec, nov), order="F")
+        self._check(self.lib.rpa_b200_project_basis(self._h, nq, nvec, nov, g.ptr, g.ld, r.ptr, r.ld,
+                                                    out.ctypes.data, nvec))
+        return out
 
     def exchange_mbpt3(self, R, eps_o, eps_v, U, A, return_x=False):
         """MBPT3 exchange energy -Tr(X K) (rpa_b200_exchange_mbpt3); with return_x also the

@@ -1349,6 +1349,197 @@ int rpa_b200_syevd(rpa_b200_handle* h, int64_t N, double* A, int64_t ldA, double
   return RPA_OK;
 }
 
+// Basis of the effective dielectric matrix from Pi at the lowest frequency: rpa_G
+// (src/rpa/rpa.f90:31-173).  EIGEN: eigenvectors of Pi by descending eigenvalue; RANDOM: two
+// subspace iterations G <- qr(Pi G), the QR by CholeskyQR2 (the same Gram-Schmidt Q as Householder
+// QR up to column signs), trace weights diag(G^T Pi G); FULL: G = I.  NVecs is chosen by the
+// reference's tail scan of the trace weights against TargetError.
+int rpa_b200_piu_basis(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R, int64_t ldR,
+                       const double* OccEnergies, const double* VirtEnergies, double LowestFreq, double alpha,
+                       int64_t prec, int64_t BasisType, double TargetError, const double* Guess, int64_t ldGuess,
+                       uint64_t seed, double* G, int64_t ldG, int64_t* NVecs, double* TraceError,
+                       double* ExactTrace) {
+  int s = begin_call(h);
+  if (s != RPA_OK) return s;
+  if (BasisType < 1 || BasisType > 3) return fail(h, RPA_ERR_INVALID_ARG, "invalid basis type %lld", (long long)BasisType);
+  if (!G || ldG < NQ || !NVecs || !(TargetError >= 0.0) || (Guess && ldGuess < NQ))
+    return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_piu_basis");
+  if (NQ > 46340) return fail(h, RPA_ERR_TOO_LARGE, "rpa_b200_piu_basis: NQ too large");
+  Validated v;
+  if ((s = validate_common(h, NQ, NOcc, NVirt, R, ldR, OccEnergies, VirtEnergies, 1, &LowestFreq, alpha, prec, v)))
+    return s;
+  const int n = (int)NQ;
+  const size_t nn = (size_t)n * n;
+  const double* Rd;
+  int64_t ldd;
+  if ((s = stage_R(h, v, R, ldR, &Rd, &ldd))) return s;
+  RPA_CUDA(h, cudaEventRecord(h->ev[1], h->stream));
+  if ((s = build_pi(h, v, Rd, ldd, alpha, prec))) return s;
+  double* Pi = static_cast<double*>(h->Pi.p);
+  RPA_CUDA(h, rpa::launch_symmetrize(Pi, n, (int64_t)nn, n, 1, h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
+  std::vector<double> dg(n);
+  RPA_CUDA(h, cudaMemcpy2DAsync(dg.data(), 8, Pi, (size_t)(n + 1) * 8, 8, (size_t)n, cudaMemcpyDeviceToHost,
+                                h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  if ((s = check_device_error(h))) return s;
+  dd exact{0.0, 0.0};
+  for (double x : dg) exact = rpa::dd_add(exact, x);
+  if (ExactTrace) *ExactTrace = exact.hi + exact.lo;
+  RPA_CUDA(h, ensure(h->eA, nn * 8));
+  RPA_CUDA(h, ensure(h->eZ, nn * 8));
+  double* Gd = static_cast<double*>(h->eA.p);  // the full basis, column-major n x n
+  std::vector<double> rwr(n);
+  if (BasisType == 3) {  // full Cholesky space
+    std::vector<double> eye(nn, 0.0);
+    for (int i = 0; i < n; ++i) eye[(size_t)i * (n + 1)] = 1.0;
+    RPA_CUDA(h, cudaMemcpyAsync(Gd, eye.data(), nn * 8, cudaMemcpyHostToDevice, h->stream));
+    RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+    *NVecs = n;
+    if (TraceError) *TraceError = 0.0;
+  } else {
+    if (BasisType == 2) {  // eigenvectors, descending eigenvalues
+      double* Zd = static_cast<double*>(h->eZ.p);
+      RPA_CUDA(h, cudaMemcpyAsync(Zd, Pi, nn * 8, cudaMemcpyDeviceToDevice, h->stream));
+      std::vector<double> ev;
+      std::vector<int> order;
+      RPA_CUDA(h, ensure(h->tPerm, (size_t)n * sizeof(int)));
+      RPA_CUDA(h, ensure(h->tSmall, (size_t)std::max(n, 64) * 8 + 64));
+      // sym_eig destroys its input: diagonalise the copy in Zd, eigenvectors into Gd, then reorder
+      if ((s = sym_eig(h, Zd, Gd, n, ev, order))) return s;
+      std::vector<int> desc(order.rbegin(), order.rend());
+      if ((s = gather(h, Gd, n, Zd, desc, nullptr))) return s;
+      RPA_CUDA(h, cudaMemcpyAsync(Gd, Zd, nn * 8, cudaMemcpyDeviceToDevice, h->stream));
+      for (int i = 0; i < n; ++i) rwr[i] = ev[desc[i]];
+    } else {  // random subspace
+      double* Yt = static_cast<double*>(h->eZ.p);  // holds Q^T
+      RPA_CUDA(h, ensure(h->tS, nn * 8));
+      RPA_CUDA(h, ensure(h->Ldiag, (size_t)n * 8));
+      RPA_CUDA(h, ensure(h->tSmall, (size_t)std::max(n, 256) * 8 + 64));
+      double* S = static_cast<double*>(h->tS.p);
+      double* Q0 = Gd;
+      if (Guess) {
+        RPA_CUDA(h, cudaMemcpy2DAsync(Q0, (size_t)n * 8, Guess, (size_t)ldGuess * 8, (size_t)n * 8, (size_t)n,
+                                      is_device_ptr(Guess) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                      h->stream));
+      } else {
+        RPA_CUDA(h, rpa::launch_fill_uniform(Q0, n, n, n, seed, h->stream));
+      }
+      // Yt = (Pi G0)^T = G0^T Pi
+      RPA_CUDA(h, rpa::launch_gemm_f64(gemm_tn(n, n, n, Q0, n, Pi, n, Yt, n), h->stream));
+      for (int it = 0; it < 2; ++it) {
+        if (it > 0)  // Yt <- Q^T Pi  (Y = Pi Q)
+          RPA_CUDA(h, rpa::launch_gemm_f64(gemm_nn(n, n, n, Gd, n, Pi, n, Yt, n), h->stream));
+        // shifted CholeskyQR3 on the columns of Y = Yt^T (Fukaya, Kannan, Nakatsukasa, Zhang,
+        // Yamamoto, SIAM J. Sci. Comput. 42 (2020) A477): the first pass factors Y^T Y +
+        // 11 (n^2 + n(n+1)) u ||Y||_F^2 I, which succeeds for numerically rank-deficient Y; two
+        // plain passes then make Q orthonormal.  The composite R is upper triangular, so Q is the
+        // Gram-Schmidt Q of Householder QR up to column signs.
+        for (int pass = 0; pass < 3; ++pass) {
+          rpa::GemmF64Args g = gemm_nn(n, n, n, Yt, n, Yt, n, S, n);  // S = Yt Yt^T
+          g.b_k = n;
+          g.b_n = 1;
+          RPA_CUDA(h, rpa::launch_gemm_f64(g, h->stream));
+          if (pass == 0) {
+            double* red = static_cast<double*>(h->tSmall.p);
+            RPA_CUDA(h, rpa::launch_offdiag(Yt, n, n, red, h->stream));  // red[0] + red[1] = ||Y||_F^2
+            const double shift = 11.0 * (2.0 * (double)n * n + (double)n) * 1.1102230246251565e-16;
+            RPA_CUDA(h, rpa::launch_add_diag_scaled(S, n, n, shift, red, h->stream));
+            RPA_CUDA(h, rpa::launch_add_diag_scaled(S, n, n, shift, red + 1, h->stream));
+          }
+          if ((s = cholesky(h, S, n, (int64_t)nn, n, 1, static_cast<double*>(h->Ldiag.p)))) return s;
+          RPA_CUDA(h, rpa::launch_trsm_lower_left(S, n, (int64_t)nn, Yt, n, (int64_t)nn, n, n, 1, h->stream));
+        }
+        RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+        if (check_device_error(h) != RPA_OK)
+          return fail(h, RPA_ERR_NOT_SPD, "random Pi basis: Pi G is numerically rank deficient (CholeskyQR)");
+        RPA_CUDA(h, cudaMemcpyAsync(Gd, Yt, nn * 8, cudaMemcpyDeviceToDevice, h->stream));  // Gd <- Q^T
+      }
+      // trace weights diag(Q^T Pi Q): T = Q^T Pi, rwr_p = sum_k T(p,k) Q^T(p,k)
+      RPA_CUDA(h, rpa::launch_gemm_f64(gemm_nn(n, n, n, Yt, n, Pi, n, S, n), h->stream));
+      std::vector<double> Th(nn), Qh(nn);
+      RPA_CUDA(h, cudaMemcpyAsync(Th.data(), S, nn * 8, cudaMemcpyDeviceToHost, h->stream));
+      RPA_CUDA(h, cudaMemcpyAsync(Qh.data(), Yt, nn * 8, cudaMemcpyDeviceToHost, h->stream));
+      RPA_CUDA(h, rpa::launch_transpose(Yt, n, n, n, Gd, n, h->stream));  // G = Q
+      RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+      for (int p = 0; p < n; ++p) {
+        dd acc{0.0, 0.0};
+        for (int k = 0; k < n; ++k) acc = rpa::dd_add(acc, Th[(size_t)p + (size_t)n * k] * Qh[(size_t)p + (size_t)n * k]);
+        rwr[p] = acc.hi + acc.lo;
+      }
+    }
+    // the reference's tail scan: drop RWR(p,p) from the end while the sum stays below the target
+    int nv = n;
+    dd abs_err{0.0, 0.0};
+    for (int p = n - 1; p >= 0; --p) {
+      const dd next = rpa::dd_add(abs_err, rwr[p]);
+      if (next.hi + next.lo < TargetError) {
+        abs_err = next;
+        nv = p + 1;
+      } else {
+        break;
+      }
+    }
+    *NVecs = nv;
+    if (TraceError) *TraceError = abs_err.hi + abs_err.lo;
+  }
+  RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
+  RPA_CUDA(h, cudaMemcpy2DAsync(G, (size_t)ldG * 8, Gd, (size_t)n * 8, (size_t)n * 8, (size_t)*NVecs,
+                                is_device_ptr(G) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  finish_timings(h);
+  return RPA_OK;
+}
+
+// R' = G^T R (NVecs x nov): the Cholesky vectors in the compressed Pi basis (the Cholesky-path
+// counterpart of THC_ZgkPiU = Zgk G(:, 1:NVecsPiU), src/rpa/rpa.f90:2318-2320).
+int rpa_b200_project_basis(rpa_b200_handle* h, int64_t NQ, int64_t NVecs, int64_t nov, const double* G, int64_t ldG,
+                           const double* R, int64_t ldR, double* Rp, int64_t ldRp) {
+  int s = begin_call(h);
+  if (s != RPA_OK) return s;
+  if (NQ < 1 || NVecs < 1 || NVecs > NQ || nov < 1 || !G || !R || !Rp || ldG < NQ || ldR < NQ || ldRp < NVecs)
+    return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_project_basis");
+  if (NQ > INT32_MAX || nov > INT32_MAX) return fail(h, RPA_ERR_TOO_LARGE, "rpa_b200_project_basis: too large");
+  const double* Gd = G;
+  int64_t ldg = ldG;
+  if (!is_device_ptr(G)) {
+    RPA_CUDA(h, ensure(h->eA, (size_t)NQ * NVecs * 8));
+    RPA_CUDA(h, cudaMemcpy2DAsync(h->eA.p, (size_t)NQ * 8, G, (size_t)ldG * 8, (size_t)NQ * 8, (size_t)NVecs,
+                                  cudaMemcpyHostToDevice, h->stream));
+    Gd = static_cast<const double*>(h->eA.p);
+    ldg = NQ;
+  }
+  const double* Rd = R;
+  int64_t ldr = ldR;
+  if (!is_device_ptr(R)) {
+    RPA_CUDA(h, ensure(h->R, (size_t)NQ * nov * 8));
+    RPA_CUDA(h, cudaMemcpy2DAsync(h->R.p, (size_t)NQ * 8, R, (size_t)ldR * 8, (size_t)NQ * 8, (size_t)nov,
+                                  cudaMemcpyHostToDevice, h->stream));
+    Rd = static_cast<const double*>(h->R.p);
+    ldr = NQ;
+  }
+  const bool dev_out = is_device_ptr(Rp);
+  double* out = Rp;
+  int64_t ldo = ldRp;
+  if (!dev_out) {
+    RPA_CUDA(h, ensure(h->eZ, (size_t)NVecs * nov * 8));
+    out = static_cast<double*>(h->eZ.p);
+    ldo = NVecs;
+  }
+  RPA_CUDA(h, cudaEventRecord(h->ev[1], h->stream));
+  RPA_CUDA(h, rpa::launch_gemm_f64(gemm_tn((int)NVecs, (int)nov, NQ, Gd, ldg, Rd, ldr, out, ldo), h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
+  if (!dev_out)
+    RPA_CUDA(h, cudaMemcpy2DAsync(Rp, (size_t)ldRp * 8, out, (size_t)NVecs * 8, (size_t)NVecs * 8, (size_t)nov,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  finish_timings(h);
+  return RPA_OK;
+}
+
 int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* inst, int64_t prec, double* Ec,
                         double* Eu) {
   int s = begin_call(h);

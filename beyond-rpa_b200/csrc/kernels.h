@@ -220,6 +220,12 @@ cudaError_t launch_symmetrize_avg(double* A, int64_t lda, int n, cudaStream_t st
 cudaError_t launch_sosex(const double* R, int64_t ldR, int NQ, int no, int nv, const double* U, int64_t ldU,
                          const double* U2, int64_t ldU2, int NT, const double* Bmu, double* partial, int64_t* npartial,
                          cudaStream_t stream);
+// A(i, i) += s * fro2[0]  (shift of a Gram matrix by a multiple of a device-side norm).
+cudaError_t launch_add_diag_scaled(double* A, int64_t lda, int n, double s, const double* fro2,
+                                  cudaStream_t stream);
+// B = A^T (A: rows x cols, column-major).
+cudaError_t launch_transpose(const double* A, int64_t lda, int rows, int cols, double* B, int64_t ldb,
+                             cudaStream_t stream);
 // MBPT3 exchange: A_mn = A_m D_mn + D_mn A_n, B_mn = D_mn + 2 U_mn + 4 U_mn A_n, Bs = (B + B^T)/2.
 cudaError_t launch_mbpt3_build(const double* Ukl, const double* Dkl, const double* Avec, int n, double* Amat,
                                double* Bmat, double* Bsym, cudaStream_t stream);

@@ -2,9 +2,6 @@
 // src/rpa/rpa_CC_Doubles.f90:491-984):
 //   * batched blocked forward substitution L X = B (the (1 + Pi_u)^{-1}
 //     factors of rpa_CC_IM_v5 come from the Cholesky factors of the energy);
-//   * a parallel two-sided Jacobi eigensolver (FP64) for the Gram matrix of
-//     the guess vectors and the Rayleigh-Ritz matrix T^T I T
-//     (symmetric_eigenproblem calls at rpa_CC_Doubles.f90:771, 805);
 //   * guess-vector generation, column normalisation (rpa_CC_NormalizeColumns,
 //     rpa_CC_Doubles.f90:80-91), scalings, gathers and column norms.
 #include "kernels.h"
@@ -284,6 +281,27 @@ __global__ void lyap_scale_kernel(double* Y, const double* mu, int n, int* bad) 
   Y[idx] /= den;
 }
 
+// A(i, i) += s * (*fro2) for i < n  (fro2: a device scalar, e.g. ||Y||_F^2)
+__global__ void add_diag_scaled_kernel(double* A, int64_t lda, int n, double s, const double* fro2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) A[(int64_t)i * (lda + 1)] += s * fro2[0];
+}
+
+// B = A^T (A rows x cols, column-major), 32 x 32 tiles through shared memory.
+__global__ void transpose_kernel(const double* A, int64_t lda, int rows, int cols, double* B, int64_t ldb) {
+  __shared__ double tile[32][33];
+  const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int r = r0 + threadIdx.x, c = c0 + i;
+    tile[i][threadIdx.x] = (r < rows && c < cols) ? A[r + lda * c] : 0.0;
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    const int c = c0 + threadIdx.x, r = r0 + i;  // B(c, r) = A(r, c)
+    if (c < cols && r < rows) B[c + ldb * r] = tile[threadIdx.x][i];
+  }
+}
+
 inline unsigned blocks_for(int64_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
@@ -377,6 +395,21 @@ cudaError_t launch_grad_accum(const double* R, int64_t ldR, const double* Y, int
 cudaError_t launch_replicate(const double* R, int64_t ldR, int NQ, int64_t nov, double* Y, int64_t ldy, int64_t sY,
                              int nb, cudaStream_t stream) {
   replicate_kernel<<<blocks_for((int64_t)NQ * nov), 256, 0, stream>>>(R, ldR, NQ, nov, Y, ldy, sY, nb);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_add_diag_scaled(double* A, int64_t lda, int n, double s, const double* fro2,
+                                  cudaStream_t stream) {
+  add_diag_scaled_kernel<<<blocks_for(n), 256, 0, stream>>>(A, lda, n, s, fro2);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_transpose(const double* A, int64_t lda, int rows, int cols, double* B, int64_t ldb,
+                             cudaStream_t stream) {
+  dim3 grid((unsigned)((cols + 31) / 32), (unsigned)((rows + 31) / 32));
+  transpose_kernel<<<grid, dim3(32, 8), 0, stream>>>(A, lda, rows, cols, B, ldb);
   ++g_launches;
   return cudaGetLastError();
 }

@@ -200,6 +200,38 @@ int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
                             int64_t ldR, int64_t NVecsT2, const double* U, int64_t ldU, const double* A, double Alpha,
                             int64_t S2Operator, double* Ex);
 
+/* Basis types of the effective dielectric matrix (src/rpa/rpa_definitions.f90:92-104). */
+#define RPA_BASIS_RANDOM 1
+#define RPA_BASIS_EIGEN 2
+#define RPA_BASIS_FULL_CHOLESKY 3
+
+/*
+ * Basis G of the effective dielectric matrix from Pi(LowestFreq) (one frequency of
+ * rpa_b200_pi).  Replaces rpa_G (src/rpa/rpa.f90:31-173): BasisType
+ * RPA_BASIS_EIGEN = eigenvectors of Pi by descending eigenvalue, RPA_BASIS_RANDOM
+ * = two subspace iterations G <- qr(Pi G) from Guess (NQ x NQ, ldGuess; NULL:
+ * uniform numbers from `seed`), RPA_BASIS_FULL_CHOLESKY = identity.  NVecs is
+ * the smallest p with sum_{q>=p} RWR(q,q) < TargetError (RWR = diag of G^T Pi G),
+ * scanning from the last column as the reference does; TraceError receives
+ * that sum and ExactTrace Tr Pi (both may be NULL).  G (NQ x NVecs used, ldG >= NQ)
+ * must hold NQ columns.  The random basis orthonormalises by shifted CholeskyQR3
+ * and returns RPA_ERR_NOT_SPD when Pi G is numerically rank deficient (use the
+ * eigenvector basis, the reference's default, for such Pi).
+ */
+int rpa_b200_piu_basis(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R, int64_t ldR,
+                       const double* OccEnergies, const double* VirtEnergies, double LowestFreq, double alpha,
+                       int64_t prec, int64_t BasisType, double TargetError, const double* Guess, int64_t ldGuess,
+                       uint64_t seed, double* G, int64_t ldG, int64_t* NVecs, double* TraceError,
+                       double* ExactTrace);
+
+/*
+ * Rp = G^T R (NVecs x nov, ldRp >= NVecs): Cholesky vectors in the compressed basis,
+ * the Cholesky-path counterpart of THC_ZgkPiU = Zgk G(:, 1:NVecsPiU)
+ * (src/rpa/rpa.f90:2318-2320).  Energies and T2 then run with NQ = NVecs.
+ */
+int rpa_b200_project_basis(rpa_b200_handle* h, int64_t NQ, int64_t NVecs, int64_t nov, const double* G, int64_t ldG,
+                           const double* R, int64_t ldR, double* Rp, int64_t ldRp);
+
 /*
  * Symmetric eigen-decomposition A = Z diag(Eigenvals) Z^T, Eigenvals ascending,
  * A (N x N, column-major, ldA >= N; lower and upper triangles both read)

@@ -612,3 +612,49 @@ def exchange_mbpt3_1(U, A, R, eps_o, eps_v):
             W = Wji.T @ Wij
             acc.append((2.0 if i != j else 1.0) * float(np.sum(X * W)))
     return -math.fsum(acc), X
+
+
+# Pi(u) basis types (src/rpa/rpa_definitions.f90:92-104) and the default trace target
+# (TargetErrorRandom = sqrt(1e-5), src/rpa/rpa_definitions.f90:279).
+RPA_BASIS_RANDOM = 1
+RPA_BASIS_EIGEN = 2
+RPA_BASIS_FULL_CHOLESKY = 3
+TARGET_ERROR_RANDOM = math.sqrt(1.0e-5)
+
+
+def piu_basis(pi1, target_error=TARGET_ERROR_RANDOM, basis_type=RPA_BASIS_EIGEN, guess=None):
+    """Basis G of the effective dielectric matrix from Pi at the lowest frequency.
+
+    rpa_G, src/rpa/rpa.f90:31-173:
+      EIGEN:  columns of G = eigenvectors of Pi, eigenvalues descending; RWR -> diag(lambda)
+      RANDOM: G = guess; two subspace iterations G <- qr(Pi G); RWR -> G^T Pi G
+      FULL:   G = I
+    NVecs = the smallest p (1-based) with sum_{q=p}^{N} RWR(q,q) < target_error, scanning q from
+    N down and stopping at the first failure (NVecs = N when RWR(N,N) >= target_error), exactly as
+    the reference's loop; the reported trace error is that sum.  The reference draws the random
+    guess with its own generator, so `guess` (N x N) is an input here.
+    Returns (G, nvecs, abs_error, exact_trace)."""
+    n = pi1.shape[0]
+    exact = math.fsum(np.diag(pi1).tolist())
+    if basis_type == RPA_BASIS_FULL_CHOLESKY:
+        return np.eye(n), n, 0.0, exact
+    if basis_type == RPA_BASIS_EIGEN:
+        w, V = np.linalg.eigh(-pi1)
+        G = V
+        rwr = -w
+    elif basis_type == RPA_BASIS_RANDOM:
+        G = np.array(guess, dtype=np.float64)
+        for _ in range(2):
+            G, _ = np.linalg.qr(pi1 @ G)
+        rwr = np.diag(G.T @ pi1 @ G).copy()
+    else:
+        raise ValueError("invalid basis type")
+    nvecs, acc = n, []
+    for p in range(n - 1, -1, -1):
+        nxt = math.fsum(acc + [rwr[p]])
+        if nxt < target_error:
+            acc.append(rwr[p])
+            nvecs = p + 1
+        else:
+            break
+    return G, nvecs, math.fsum(acc), exact

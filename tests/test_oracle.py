@@ -190,3 +190,27 @@ def test_mbpt3_lyapunov_solution_and_pair_sum():
     Rr = s.R.reshape(s.nq, s.nv, s.no, order="F")
     Kx = np.einsum("qaj,qbi->aibj", Rr, Rr)
     assert ex == pytest.approx(-np.sum(Kx * dT.reshape(s.nv, s.no, s.nv, s.no, order="F")), rel=1e-10)
+
+
+def test_piu_basis_eigen_trace_error_and_energy():
+    s, x, w = small_system(seed=12, nq=60, no=4, nv=20)
+    pi1 = O.pi_matrices(s.R, s.eps_o, s.eps_v, x[:1])[0]
+    G, nv_, err, exact = O.piu_basis(pi1, 1e-3)
+    lam = np.linalg.eigvalsh(pi1)[::-1]
+    assert exact == pytest.approx(np.trace(pi1), rel=1e-14)
+    assert 1 <= nv_ <= s.nq
+    # the dropped tail (indices nvecs-1 .. N-1, the reference's accounting) is below the target
+    assert err == pytest.approx(lam[nv_ - 1:].sum(), rel=1e-10, abs=1e-16) and err < 1e-3
+    if nv_ > 1:
+        assert lam[nv_ - 2:].sum() >= 1e-3
+    # projected R' = G^T R reproduces E_c up to the dropped part of the spectrum
+    Rp = G[:, :nv_].T @ s.R
+    e_full, _ = O.ec_rpa(s.R, s.eps_o, s.eps_v, x, w)
+    e_proj, _ = O.ec_rpa(Rp, s.eps_o, s.eps_v, x, w)
+    assert abs(e_proj - e_full) < 1e-2 * abs(e_full)
+    # full basis: identity, no truncation; random basis spans the dominant subspace
+    Gf, nf, ef, _ = O.piu_basis(pi1, 1e-3, O.RPA_BASIS_FULL_CHOLESKY)
+    assert nf == s.nq and ef == 0.0 and np.array_equal(Gf, np.eye(s.nq))
+    g0 = np.random.default_rng(0).standard_normal((s.nq, s.nq))
+    Gr, nr, er, _ = O.piu_basis(pi1, 1e-3, O.RPA_BASIS_RANDOM, guess=g0)
+    assert np.allclose(Gr.T @ Gr, np.eye(s.nq), atol=1e-10) and er < 1e-3
