@@ -572,6 +572,53 @@ def run_split(args):
         dist.destroy_process_group()
 
 
+def run_thc(args):
+    """THC workload (thc_4096: NGrid = 8192, NQ = 4096, NOcc = 64, NVirt = 1024, K = 16): R formed from
+    THC factors on the GPU (FP64 tensor-core GEMM) + the split-BF16 energy, per step."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    pkg = load_package()
+    from beyond_rpa_b200.workloads import SINGLE_SYSTEM, orbital_energies
+    from beyond_rpa_b200 import freq_grid
+    system = "single_" + args.workload.split("_")[1]
+    nq, no, nv, K, kw = SINGLE_SYSTEM[system]
+    ng = 2 * nq
+    h = pkg.Handle(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    h.set_stream(stream.cuda_stream)
+    g = torch.Generator(device="cuda").manual_seed(7)
+    Z = torch.randn((nq, ng), generator=g, device="cuda", dtype=torch.float64).T  # column-major NGrid x NQ
+    Z *= (0.05 * torch.exp(-torch.arange(nq, device="cuda", dtype=torch.float64) / kw["decay"]))[None, :]
+    Xa = torch.randn((nv, ng), generator=g, device="cuda", dtype=torch.float64).T / ng ** 0.5
+    Xi = torch.randn((no, ng), generator=g, device="cuda", dtype=torch.float64).T / ng ** 0.5
+    eo, ev = orbital_energies(no, nv, 7, kw["occ_range"], kw["virt_range"])
+    x, w = freq_grid(np.concatenate([eo, ev]), no, nv)
+    x, w = x[:K], w[:K]
+    Rbuf = torch.empty((no * nv, nq), dtype=torch.float64, device="cuda").T
+    for _ in range(args.warmup):
+        h.ec_thc(Z, Xa, Xi, eo, ev, x, w)
+    torch.cuda.synchronize()
+    e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    e[0].record(stream)
+    for _ in range(args.steps):
+        ec, _ = h.ec_thc(Z, Xa, Xi, eo, ev, x, w)
+    e[1].record(stream)
+    for _ in range(args.steps):
+        h.thc_r(Z, Xa, Xi, out=Rbuf)
+    e[2].record(stream)
+    torch.cuda.synchronize()
+    ms = e[0].elapsed_time(e[1]) / args.steps
+    ms_r = e[1].elapsed_time(e[2]) / args.steps
+    flops_r = 2.0 * nq * ng * no * nv
+    print(json.dumps({"metric": "RPA E_c from THC factors", "workload": f"{args.workload}: NGrid={ng} NQ={nq} "
+                      f"NOcc={no} NVirt={nv} K={len(x)}", "value": 1e3 / ms, "unit": "E_c/s", "steps": args.steps,
+                      "ms_per_step": ms, "r_formation_ms": ms_r, "r_formation_tflops_fp64": flops_r / ms_r / 1e9,
+                      "Ec": ec}), flush=True)
+    h.close()
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -623,6 +670,8 @@ def main():
         run_cc(args)
     elif args.workload.startswith("split_"):
         run_split(args)
+    elif args.workload.startswith("thc_"):
+        run_thc(args)
     else:
         run_ours(args)
 

@@ -97,6 +97,9 @@ def load_library(path: str | os.PathLike | None = None):
                                      _vp, _i64, _vp, _vp]
     lib.rpa_b200_exchange_sosex.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _dbl, _i64, _vp]
     lib.rpa_b200_syevd.argtypes = [_vp, _i64, _vp, _i64, _vp]
+    lib.rpa_b200_thc_r.argtypes = [_vp, _i64, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64]
+    lib.rpa_b200_ec_thc.argtypes = [_vp, _i64, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _i64,
+                                    _vp, _vp, _dbl, _i64, _vp, _vp]
     lib.rpa_b200_piu_basis.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _dbl, _dbl, _i64, _i64, _dbl,
                                        _vp, _i64, ctypes.c_uint64, _vp, _i64, _vp, _vp, _vp]
     lib.rpa_b200_project_basis.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64]
@@ -391,6 +394,36 @@ class Handle:
         self._check(self.lib.rpa_b200_project_basis(self._h, nq, nvec, nov, g.ptr, g.ld, r.ptr, r.ld,
                                                     out.ctypes.data, nvec))
         return out
+
+    def thc_r(self, Zgk, Xga, Xgi, out=None):
+        """Cholesky vectors from THC factors (rpa_b200_thc_r): R (NQ x NOcc*NVirt); numpy, or `out`
+        (a column-major device tensor) when given."""
+        ng = int(Zgk.shape[0])
+        nq, nv, no = int(Zgk.shape[1]), int(Xga.shape[1]), int(Xgi.shape[1])
+        z, xa, xi = _colmajor(Zgk, ng), _colmajor(Xga, ng), _colmajor(Xgi, ng)
+        if out is not None:
+            o = _colmajor(out, nq)
+            R, rptr, ldr = out, o.ptr, o.ld
+        else:
+            R = np.zeros((nq, no * nv), order="F")
+            rptr, ldr = R.ctypes.data, nq
+        self._check(self.lib.rpa_b200_thc_r(self._h, ng, nq, no, nv, z.ptr, z.ld, xa.ptr, xa.ld, xi.ptr, xi.ld,
+                                            rptr, ldr))
+        return R
+
+    def ec_thc(self, Zgk, Xga, Xgi, eps_o, eps_v, freqs, weights, alpha=4.0, prec="split"):
+        """RPA energy from THC factors (rpa_b200_ec_thc): (E_c, E(u))."""
+        ng = int(Zgk.shape[0])
+        nq, nv, no = int(Zgk.shape[1]), int(Xga.shape[1]), int(Xgi.shape[1])
+        z, xa, xi = _colmajor(Zgk, ng), _colmajor(Xga, ng), _colmajor(Xgi, ng)
+        eo, ev, fr, w = _vec(eps_o), _vec(eps_v), _vec(freqs), _vec(weights)
+        K = len(freqs)
+        ec = ctypes.c_double()
+        eu = np.zeros(K)
+        self._check(self.lib.rpa_b200_ec_thc(self._h, ng, nq, no, nv, z.ptr, z.ld, xa.ptr, xa.ld, xi.ptr, xi.ld,
+                                             eo.ptr, ev.ptr, K, fr.ptr, w.ptr, float(alpha), _PREC[prec],
+                                             ctypes.byref(ec), eu.ctypes.data))
+        return ec.value, eu
 
     def exchange_mbpt3(self, R, eps_o, eps_v, U, A, return_x=False):
         """MBPT3 exchange energy -Tr(X K) (rpa_b200_exchange_mbpt3); with return_x also the

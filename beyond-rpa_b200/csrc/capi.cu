@@ -43,6 +43,7 @@ struct rpa_b200_handle {
   DevBuf gY, gD;  // adjoint workspace
   DevBuf xM;      // MBPT3 exchange: NT x NT matrices, R U and U X
   DevBuf eW, eA, eZ;  // symmetric eigensolver workspace, input and eigenvector buffers
+  DevBuf thZ, thXa, thXi, thYX, thR;  // THC factors, Khatri-Rao block, Cholesky vectors formed from them
   struct BatchGraph {
     uint64_t key;
     std::vector<cudaGraphExec_t> execs;
@@ -739,7 +740,7 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
   for (DevBuf* b : {&h->R, &h->D, &h->eps, &h->Xhi, &h->Xlo, &h->diag_part, &h->diag, &h->Pi, &h->Ldiag, &h->ddbuf,
                     &h->tZ, &h->tOm, &h->tIOm, &h->tP, &h->tS, &h->tV, &h->tT, &h->tTIT, &h->tVt, &h->tW, &h->tU,
                     &h->tRU, &h->tSmall, &h->tPerm, &h->bDesc, &h->bRes, &h->gY, &h->gD,
-                    &h->xM, &h->eW, &h->eA, &h->eZ})
+                    &h->xM, &h->eW, &h->eA, &h->eZ, &h->thZ, &h->thXa, &h->thXi, &h->thYX, &h->thR})
     release(*b);
   for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
   if (h->err_dev) cudaFree(h->err_dev);
@@ -1538,6 +1539,109 @@ int rpa_b200_project_basis(rpa_b200_handle* h, int64_t NQ, int64_t NVecs, int64_
   RPA_CUDA(h, cudaStreamSynchronize(h->stream));
   finish_timings(h);
   return RPA_OK;
+}
+
+// Device copy of a column-major (rows x cols) input, or the input itself when it is already on
+// the device; ld receives the leading dimension of the returned pointer.
+int stage_matrix(rpa_b200_handle* h, DevBuf& buf, const double* A, int64_t lda, int64_t rows, int64_t cols,
+                 const double** out, int64_t* ld) {
+  if (is_device_ptr(A)) {
+    *out = A;
+    *ld = lda;
+    return RPA_OK;
+  }
+  RPA_CUDA(h, ensure(buf, (size_t)rows * cols * 8));
+  RPA_CUDA(h, cudaMemcpy2DAsync(buf.p, (size_t)rows * 8, A, (size_t)lda * 8, (size_t)rows * 8, (size_t)cols,
+                                cudaMemcpyHostToDevice, h->stream));
+  *out = static_cast<const double*>(buf.p);
+  *ld = rows;
+  return RPA_OK;
+}
+
+// R = Z^T (Xa * Xi) into Rout (device, NQ x nov, ld ldR): Khatri-Rao blocks of whole occupied
+// orbitals (<= ~1 GB each) and one FP64 DMMA GEMM per block.
+int form_thc_r(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zd, int64_t ldz,
+               const double* Xad, int64_t ldxa, const double* Xid, int64_t ldxi, double* Rout, int64_t ldR) {
+  const int64_t per_occ = NGrid * NVirt;
+  int64_t ib = std::max<int64_t>(1, std::min<int64_t>(NOcc, (int64_t)(1ll << 27) / std::max<int64_t>(per_occ, 1)));
+  RPA_CUDA(h, ensure(h->thYX, (size_t)per_occ * ib * 8));
+  double* YX = static_cast<double*>(h->thYX.p);
+  for (int64_t i0 = 0; i0 < NOcc; i0 += ib) {
+    const int64_t ni = std::min(ib, NOcc - i0);
+    RPA_CUDA(h, rpa::launch_khatri_rao(Xad, ldxa, Xid, ldxi, (int)NGrid, (int)NVirt, (int)i0, (int)ni, YX, h->stream));
+    RPA_CUDA(h, rpa::launch_gemm_f64(gemm_tn((int)NQ, (int)(NVirt * ni), NGrid, Zd, ldz, YX, NGrid,
+                                             Rout + ldR * (i0 * NVirt), ldR),
+                                     h->stream));
+  }
+  return RPA_OK;
+}
+
+int check_thc_args(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zgk,
+                   int64_t ldZ, const double* Xga, int64_t ldXa, const double* Xgi, int64_t ldXi) {
+  if (NGrid < 1 || NQ < 1 || NOcc < 1 || NVirt < 1 || !Zgk || !Xga || !Xgi || ldZ < NGrid || ldXa < NGrid ||
+      ldXi < NGrid)
+    return fail(h, RPA_ERR_INVALID_ARG, "invalid THC factor dimensions");
+  if (NGrid > INT32_MAX || NQ > INT32_MAX || NOcc * NVirt > INT32_MAX)
+    return fail(h, RPA_ERR_TOO_LARGE, "THC dimensions too large");
+  return RPA_OK;
+}
+
+// Cholesky vectors from THC factors, R(k, ai) = sum_g Z(g, k) Xa(g, a) Xi(g, i), ai = a + NVirt i:
+// rpa_THC_Rkab / rpa_THC_Rkai (src/rpa/rpa_THC.f90:374-426).
+int rpa_b200_thc_r(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zgk,
+                   int64_t ldZ, const double* Xga, int64_t ldXa, const double* Xgi, int64_t ldXi, double* R,
+                   int64_t ldR) {
+  int s = begin_call(h);
+  if (s != RPA_OK) return s;
+  if ((s = check_thc_args(h, NGrid, NQ, NOcc, NVirt, Zgk, ldZ, Xga, ldXa, Xgi, ldXi))) return s;
+  if (!R || ldR < NQ) return fail(h, RPA_ERR_INVALID_ARG, "R is NULL or ldR < NQ");
+  const int64_t nov = NOcc * NVirt;
+  const double *Zd, *Xad, *Xid;
+  int64_t ldz, ldxa, ldxi;
+  if ((s = stage_matrix(h, h->thZ, Zgk, ldZ, NGrid, NQ, &Zd, &ldz))) return s;
+  if ((s = stage_matrix(h, h->thXa, Xga, ldXa, NGrid, NVirt, &Xad, &ldxa))) return s;
+  if ((s = stage_matrix(h, h->thXi, Xgi, ldXi, NGrid, NOcc, &Xid, &ldxi))) return s;
+  const bool dev = is_device_ptr(R);
+  double* Rd = R;
+  int64_t ldr = ldR;
+  if (!dev) {
+    RPA_CUDA(h, ensure(h->thR, (size_t)NQ * nov * 8));
+    Rd = static_cast<double*>(h->thR.p);
+    ldr = NQ;
+  }
+  RPA_CUDA(h, cudaEventRecord(h->ev[1], h->stream));
+  if ((s = form_thc_r(h, NGrid, NQ, NOcc, NVirt, Zd, ldz, Xad, ldxa, Xid, ldxi, Rd, ldr))) return s;
+  RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
+  if (!dev)
+    RPA_CUDA(h, cudaMemcpy2DAsync(R, (size_t)ldR * 8, Rd, (size_t)NQ * 8, (size_t)NQ * 8, (size_t)nov,
+                                  cudaMemcpyDeviceToHost, h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  finish_timings(h);
+  return RPA_OK;
+}
+
+// RPA energy from THC factors (the FullRkai branch of rpa_THC_PiU, src/rpa/rpa_THC.f90:215-329):
+// R is formed on the device and handed to the energy path; it never leaves the GPU.
+int rpa_b200_ec_thc(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zgk,
+                    int64_t ldZ, const double* Xga, int64_t ldXa, const double* Xgi, int64_t ldXi,
+                    const double* OccEnergies, const double* VirtEnergies, int64_t NFreqs, const double* Freqs,
+                    const double* FreqWeights, double alpha, int64_t prec, double* Ec, double* Eu) {
+  int s = begin_call(h);
+  if (s != RPA_OK) return s;
+  if ((s = check_thc_args(h, NGrid, NQ, NOcc, NVirt, Zgk, ldZ, Xga, ldXa, Xgi, ldXi))) return s;
+  const int64_t nov = NOcc * NVirt;
+  const double *Zd, *Xad, *Xid;
+  int64_t ldz, ldxa, ldxi;
+  if ((s = stage_matrix(h, h->thZ, Zgk, ldZ, NGrid, NQ, &Zd, &ldz))) return s;
+  if ((s = stage_matrix(h, h->thXa, Xga, ldXa, NGrid, NVirt, &Xad, &ldxa))) return s;
+  if ((s = stage_matrix(h, h->thXi, Xgi, ldXi, NGrid, NOcc, &Xid, &ldxi))) return s;
+  RPA_CUDA(h, ensure(h->thR, (size_t)NQ * nov * 8));
+  double* Rd = static_cast<double*>(h->thR.p);
+  if ((s = form_thc_r(h, NGrid, NQ, NOcc, NVirt, Zd, ldz, Xad, ldxa, Xid, ldxi, Rd, NQ))) return s;
+  return rpa_b200_ec(h, NQ, NOcc, NVirt, Rd, NQ, OccEnergies, VirtEnergies, NFreqs, Freqs, FreqWeights, alpha, prec,
+                     Ec, Eu);
 }
 
 int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* inst, int64_t prec, double* Ec,

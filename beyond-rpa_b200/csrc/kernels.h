@@ -220,6 +220,9 @@ cudaError_t launch_symmetrize_avg(double* A, int64_t lda, int n, cudaStream_t st
 cudaError_t launch_sosex(const double* R, int64_t ldR, int NQ, int no, int nv, const double* U, int64_t ldU,
                          const double* U2, int64_t ldU2, int NT, const double* Bmu, double* partial, int64_t* npartial,
                          cudaStream_t stream);
+// YX(g, a + nv*ii) = Xa(g, a) Xi(g, i0 + ii) for ii < ni (YX: ngrid x nv*ni, ld ngrid).
+cudaError_t launch_khatri_rao(const double* Xa, int64_t ldXa, const double* Xi, int64_t ldXi, int ngrid, int nv,
+                              int i0, int ni, double* YX, cudaStream_t stream);
 // A(i, i) += s * fro2[0]  (shift of a Gram matrix by a multiple of a device-side norm).
 cudaError_t launch_add_diag_scaled(double* A, int64_t lda, int n, double s, const double* fro2,
                                   cudaStream_t stream);

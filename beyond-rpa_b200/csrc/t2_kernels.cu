@@ -281,6 +281,18 @@ __global__ void lyap_scale_kernel(double* Y, const double* mu, int n, int* bad) 
   Y[idx] /= den;
 }
 
+// Khatri-Rao block of the THC factors: YX(g, a + nv*ii) = Xa(g, a) * Xi(g, i0 + ii), ii < ni
+// (rpa_THC_Rkab / rpa_THC_Rkai, src/rpa/rpa_THC.f90:374-426).
+__global__ void khatri_rao_kernel(const double* Xa, int64_t ldXa, const double* Xi, int64_t ldXi, int ngrid, int nv,
+                                  int i0, int ni, double* YX) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t total = (int64_t)ngrid * nv * ni;
+  if (idx >= total) return;
+  const int64_t g = idx % ngrid, col = idx / ngrid;
+  const int64_t a = col % nv, ii = col / nv;
+  YX[idx] = Xa[g + ldXa * a] * Xi[g + ldXi * (i0 + ii)];
+}
+
 // A(i, i) += s * (*fro2) for i < n  (fro2: a device scalar, e.g. ||Y||_F^2)
 __global__ void add_diag_scaled_kernel(double* A, int64_t lda, int n, double s, const double* fro2) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -395,6 +407,14 @@ cudaError_t launch_grad_accum(const double* R, int64_t ldR, const double* Y, int
 cudaError_t launch_replicate(const double* R, int64_t ldR, int NQ, int64_t nov, double* Y, int64_t ldy, int64_t sY,
                              int nb, cudaStream_t stream) {
   replicate_kernel<<<blocks_for((int64_t)NQ * nov), 256, 0, stream>>>(R, ldR, NQ, nov, Y, ldy, sY, nb);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_khatri_rao(const double* Xa, int64_t ldXa, const double* Xi, int64_t ldXi, int ngrid, int nv,
+                              int i0, int ni, double* YX, cudaStream_t stream) {
+  const int64_t total = (int64_t)ngrid * nv * ni;
+  khatri_rao_kernel<<<blocks_for(total), 256, 0, stream>>>(Xa, ldXa, Xi, ldXi, ngrid, nv, i0, ni, YX);
   ++g_launches;
   return cudaGetLastError();
 }

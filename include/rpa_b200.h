@@ -200,6 +200,25 @@ int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
                             int64_t ldR, int64_t NVecsT2, const double* U, int64_t ldU, const double* A, double Alpha,
                             int64_t S2Operator, double* Ex);
 
+/*
+ * Cholesky vectors from THC factors: R(k, ai) = sum_g Zgk(g, k) Xga(g, a) Xgi(g, i),
+ * ai = a + NVirt i, R (NQ x NOcc*NVirt, ldR >= NQ).  Zgk (NGrid x NQ), Xga (NGrid x
+ * NVirt), Xgi (NGrid x NOcc) column-major.  Replaces rpa_THC_Rkab / rpa_THC_Rkai
+ * (src/rpa/rpa_THC.f90:374-426): Khatri-Rao blocks and FP64 tensor-core GEMMs.
+ */
+int rpa_b200_thc_r(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zgk,
+                   int64_t ldZ, const double* Xga, int64_t ldXa, const double* Xgi, int64_t ldXi, double* R,
+                   int64_t ldR);
+
+/*
+ * RPA energy from THC factors (rpa_THC_PiU with FullRkai, src/rpa/rpa_THC.f90:215-329,
+ * followed by the energy of rpa_b200_ec): R is formed on the device and never leaves it.
+ */
+int rpa_b200_ec_thc(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zgk,
+                    int64_t ldZ, const double* Xga, int64_t ldXa, const double* Xgi, int64_t ldXi,
+                    const double* OccEnergies, const double* VirtEnergies, int64_t NFreqs, const double* Freqs,
+                    const double* FreqWeights, double alpha, int64_t prec, double* Ec, double* Eu);
+
 /* Basis types of the effective dielectric matrix (src/rpa/rpa_definitions.f90:92-104). */
 #define RPA_BASIS_RANDOM 1
 #define RPA_BASIS_EIGEN 2

@@ -658,3 +658,23 @@ def piu_basis(pi1, target_error=TARGET_ERROR_RANDOM, basis_type=RPA_BASIS_EIGEN,
         else:
             break
     return G, nvecs, math.fsum(acc), exact
+
+
+def thc_r(Zgk, Xga, Xgi):
+    """Cholesky vectors from THC factors, R(k, ai) = sum_g Z(g,k) X_a(g,a) X_i(g,i),
+    ai = a + NVirt*i.  rpa_THC_Rkab / rpa_THC_Rkai, src/rpa/rpa_THC.f90:374-426."""
+    ng, nv = Xga.shape
+    no = Xgi.shape[1]
+    kr = (Xga[:, :, None] * Xgi[:, None, :]).reshape(ng, nv * no, order="F")
+    return Zgk.T @ kr
+
+
+def make_thc_factors(ngrid, nq, no, nv, seed, scale=0.3):
+    """Seeded synthetic THC factors (Zgk, Xga, Xgi) and orbital energies."""
+    rng = np.random.default_rng(seed)
+    Z = rng.standard_normal((ngrid, nq)) * scale * np.exp(-np.arange(nq) / (nq / 3.0))[None, :]
+    Xa = rng.standard_normal((ngrid, nv)) / math.sqrt(ngrid)
+    Xi = rng.standard_normal((ngrid, no)) / math.sqrt(ngrid)
+    eo = np.sort(rng.uniform(-1.3, -0.4, no))
+    ev = np.sort(np.exp(rng.uniform(math.log(0.03), math.log(4.0), nv)))
+    return Z, Xa, Xi, eo, ev

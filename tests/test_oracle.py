@@ -214,3 +214,11 @@ def test_piu_basis_eigen_trace_error_and_energy():
     g0 = np.random.default_rng(0).standard_normal((s.nq, s.nq))
     Gr, nr, er, _ = O.piu_basis(pi1, 1e-3, O.RPA_BASIS_RANDOM, guess=g0)
     assert np.allclose(Gr.T @ Gr, np.eye(s.nq), atol=1e-10) and er < 1e-3
+
+
+def test_thc_r_matches_explicit_sum():
+    Z, Xa, Xi, eo, ev = O.make_thc_factors(40, 12, 3, 5, 7)
+    R = O.thc_r(Z, Xa, Xi)
+    for (k, a, i) in ((0, 0, 0), (5, 4, 2), (11, 2, 1)):
+        ref = math.fsum(Z[g, k] * Xa[g, a] * Xi[g, i] for g in range(40))
+        assert R[k, a + 5 * i] == pytest.approx(ref, rel=1e-12, abs=1e-15)
