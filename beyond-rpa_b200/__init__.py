@@ -97,6 +97,8 @@ def load_library(path: str | os.PathLike | None = None):
                                      _vp, _i64, _vp, _vp]
     lib.rpa_b200_exchange_sosex.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _dbl, _i64, _vp]
     lib.rpa_b200_syevd.argtypes = [_vp, _i64, _vp, _i64, _vp]
+    lib.rpa_b200_jctc2024.argtypes = [_vp, _i64, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _vp, _i64,
+                                      _vp, _vp, _i64, _dbl, _i64, _dbl, _vp, _vp]
     lib.rpa_b200_thc_r.argtypes = [_vp, _i64, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _i64]
     lib.rpa_b200_ec_thc.argtypes = [_vp, _i64, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _vp, _vp, _i64,
                                     _vp, _vp, _dbl, _i64, _vp, _vp]
@@ -424,6 +426,24 @@ class Handle:
                                              eo.ptr, ev.ptr, K, fr.ptr, w.ptr, float(alpha), _PREC[prec],
                                              ctypes.byref(ec), eu.ctypes.data))
         return ec.value, eu
+
+    def jctc2024(self, Zgk, Xgi, Yga, U, A, Lik=None, cutoff_pno=1e-5, boys_screening=False,
+                 cutoff_vabij=1e-6):
+        """Particle-hole corrections (rpa_b200_jctc2024): ((EcRPA_PNO, Ec1b, Ec2bcd, Ec2ghij),
+        (max NVirtPNO, sum NVirtPNO, pairs without PNOs))."""
+        ng = int(Zgk.shape[0])
+        nq, no, nv = int(Zgk.shape[1]), int(Xgi.shape[1]), int(Yga.shape[1])
+        z, xi, ya = _colmajor(Zgk, ng), _colmajor(Xgi, ng), _colmajor(Yga, ng)
+        u = _colmajor(U, no * nv)
+        a = _vec(A)
+        lk = _colmajor(Lik, no) if Lik is not None else None
+        en = np.zeros(4)
+        st = np.zeros(3, dtype=np.int64)
+        self._check(self.lib.rpa_b200_jctc2024(self._h, ng, nq, no, nv, z.ptr, z.ld, xi.ptr, xi.ld, ya.ptr, ya.ld,
+                                               int(U.shape[1]), u.ptr, u.ld, a.ptr, lk.ptr if lk else None,
+                                               lk.ld if lk else no, float(cutoff_pno), int(bool(boys_screening)),
+                                               float(cutoff_vabij), en.ctypes.data, st.ctypes.data))
+        return tuple(en), tuple(int(x) for x in st)
 
     def exchange_mbpt3(self, R, eps_o, eps_v, U, A, return_x=False):
         """MBPT3 exchange energy -Tr(X K) (rpa_b200_exchange_mbpt3); with return_x also the

@@ -44,6 +44,7 @@ struct rpa_b200_handle {
   DevBuf xM;      // MBPT3 exchange: NT x NT matrices, R U and U X
   DevBuf eW, eA, eZ;  // symmetric eigensolver workspace, input and eigenvector buffers
   DevBuf thZ, thXa, thXi, thYX, thR;  // THC factors, Khatri-Rao block, Cholesky vectors formed from them
+  DevBuf jU, jL, jX, jPno, jWork;      // particle-hole corrections: localised T2 vectors, PNOs, scratch
   struct BatchGraph {
     uint64_t key;
     std::vector<cudaGraphExec_t> execs;
@@ -740,7 +741,8 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
   for (DevBuf* b : {&h->R, &h->D, &h->eps, &h->Xhi, &h->Xlo, &h->diag_part, &h->diag, &h->Pi, &h->Ldiag, &h->ddbuf,
                     &h->tZ, &h->tOm, &h->tIOm, &h->tP, &h->tS, &h->tV, &h->tT, &h->tTIT, &h->tVt, &h->tW, &h->tU,
                     &h->tRU, &h->tSmall, &h->tPerm, &h->bDesc, &h->bRes, &h->gY, &h->gD,
-                    &h->xM, &h->eW, &h->eA, &h->eZ, &h->thZ, &h->thXa, &h->thXi, &h->thYX, &h->thR})
+                    &h->xM, &h->eW, &h->eA, &h->eZ, &h->thZ, &h->thXa, &h->thXi, &h->thYX, &h->thR,
+                    &h->jU, &h->jL, &h->jX, &h->jPno, &h->jWork})
     release(*b);
   for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
   if (h->err_dev) cudaFree(h->err_dev);
@@ -1642,6 +1644,305 @@ int rpa_b200_ec_thc(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc,
   if ((s = form_thc_r(h, NGrid, NQ, NOcc, NVirt, Zd, ldz, Xad, ldxa, Xid, ldxi, Rd, NQ))) return s;
   return rpa_b200_ec(h, NQ, NOcc, NVirt, Rd, NQ, OccEnergies, VirtEnergies, NFreqs, Freqs, FreqWeights, alpha, prec,
                      Ec, Eu);
+}
+
+// Device buffer grown to `bytes` keeping its first `used` bytes.
+int grow_keep(rpa_b200_handle* h, DevBuf& b, size_t bytes, size_t used) {
+  if (b.p && b.bytes >= bytes) return RPA_OK;
+  const size_t nb = std::max(bytes, b.bytes * 2);
+  void* p = nullptr;
+  RPA_CUDA(h, cudaMalloc(&p, nb));
+  if (b.p && used) RPA_CUDA(h, cudaMemcpyAsync(p, b.p, used, cudaMemcpyDeviceToDevice, h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (b.p) cudaFree(b.p);
+  b.p = p;
+  b.bytes = nb;
+  return RPA_OK;
+}
+
+// C = alpha A op(B) (+ beta C) with A (M x K) column-major and B given as (K x N) column-major
+// (bt = false) or as (N x K) column-major, i.e. B^T (bt = true).
+rpa::GemmF64Args gemm_g(int M, int N, int64_t K, const double* A, int64_t lda, bool at, const double* B,
+                        int64_t ldb, bool bt, double* C, int64_t ldc, double alpha = 1.0, double beta = 0.0) {
+  rpa::GemmF64Args g = gemm_nn(M, N, K, A, lda, B, ldb, C, ldc);
+  if (at) {
+    g.a_m = lda;
+    g.a_k = 1;
+  }
+  if (bt) {
+    g.b_k = ldb;
+    g.b_n = 1;
+  }
+  g.alpha = alpha;
+  g.beta = beta;
+  return g;
+}
+
+// Particle-hole corrections to direct RPA with pair-natural orbitals on THC factors:
+// rpa_JCTC2024_Corrections and its helpers (src/rpa/rpa_JCTC2024.f90:24-703).  PNOs of each pair
+// i >= j: T_ij = U_i diag(A) U_j^T, SVD through the eigen-decomposition of T T^T (U, s^2) and
+// s V = T^T U for the singular values above CutoffThreshPNO.  Every product is an FP64 tensor-core
+// GEMM (the Hadamard products with the THC orbital factors are folded into their k- and row-scales);
+// every trace is a deterministic partial-sum reduction collected once at the end.
+int rpa_b200_jctc2024(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zgk,
+                      int64_t ldZ, const double* Xgi, int64_t ldXi, const double* Yga, int64_t ldYa, int64_t NVecsT2,
+                      const double* U, int64_t ldU, const double* Am, const double* Lik, int64_t ldL,
+                      double CutoffThreshPNO, int64_t BoysScreening, double CutoffThreshVabij, double* Energies,
+                      int64_t* PNOStats) {
+  int s = begin_call(h);
+  if (s != RPA_OK) return s;
+  if (NGrid < 1 || NQ < 1 || NOcc < 1 || NVirt < 1 || NVecsT2 < 1 || !Zgk || !Xgi || !Yga || !U || !Am ||
+      !Energies || ldZ < NGrid || ldXi < NGrid || ldYa < NGrid || ldU < NOcc * NVirt || (Lik && ldL < NOcc) ||
+      !(CutoffThreshPNO >= 0.0))
+    return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_jctc2024");
+  if (NGrid > INT32_MAX || NQ > INT32_MAX || NOcc * NVirt > INT32_MAX || NVecsT2 > INT32_MAX || NVirt > 46340)
+    return fail(h, RPA_ERR_TOO_LARGE, "rpa_b200_jctc2024: dimensions too large");
+  const int ng = (int)NGrid, nq = (int)NQ, no = (int)NOcc, nv = (int)NVirt, nt = (int)NVecsT2;
+  const int64_t nov = NOcc * NVirt;
+  const double *Zd, *Yd, *Xd0, *Ud0, *Ld = nullptr;
+  int64_t ldz, ldy, ldx0, ldu0, ldl = 0;
+  if ((s = stage_matrix(h, h->thZ, Zgk, ldZ, NGrid, NQ, &Zd, &ldz))) return s;
+  if ((s = stage_matrix(h, h->thXa, Yga, ldYa, NGrid, NVirt, &Yd, &ldy))) return s;
+  if ((s = stage_matrix(h, h->thXi, Xgi, ldXi, NGrid, NOcc, &Xd0, &ldx0))) return s;
+  if ((s = stage_matrix(h, h->tU, U, ldU, nov, NVecsT2, &Ud0, &ldu0))) return s;
+  if (Lik && (s = stage_matrix(h, h->jL, Lik, ldL, NOcc, NOcc, &Ld, &ldl))) return s;
+  std::vector<double> Ah;
+  if ((s = fetch_small(h, Am, NVecsT2, Ah))) return s;
+  // scratch: A, localised X and U, T, M, eigenvectors, products, partial sums
+  const int64_t npairs = (int64_t)no * (no + 1) / 2;
+  const int64_t nslot = 5 * npairs;  // S1a, S1b, S2ghij, S2bcd, Vijij per pair
+  RPA_CUDA(h, ensure(h->jX, (size_t)ng * no * 8));
+  RPA_CUDA(h, ensure(h->jU, (size_t)nov * nt * 8));
+  const size_t nvv = (size_t)nv * nv;
+  const size_t wwords = (size_t)nt + 3 * nvv + (size_t)nq * nv + 2 * (size_t)ng * nv + (size_t)nq + (size_t)ng +
+                        2 * nvv + 4 * nvv + 2 * nvv + 2 * (size_t)ng * nv + (size_t)nslot * rpa::kDotPartials + 64;
+  RPA_CUDA(h, ensure(h->jWork, wwords * 8));
+  double* w = static_cast<double*>(h->jWork.p);
+  double* Ad = w;
+  double* Tm = Ad + nt;            // T_ij (nv x nv)
+  double* Mm = Tm + nvv;           // T T^T
+  double* Vm = Mm + nvv;           // its eigenvectors
+  double* ZYXk = Vm + nvv;         // NQ x nv
+  double* ZYXg = ZYXk + (size_t)nq * nv;  // NGrid x nv
+  double* Wg = ZYXg + (size_t)ng * nv;    // NGrid x nv
+  double* zk = Wg + (size_t)ng * nv;      // NQ
+  double* zg = zk + nq;                   // NGrid
+  double* Gg = zg + ng;                   // G for 2g..2j (nv x nv)
+  double* Gb = Gg + nvv;                  // G for 2b..2d
+  double* Sm = Gb + nvv;                  // 4 S blocks (<= nv x nv each)
+  double* QS = Sm + 4 * nvv;              // nv x 2 Nkj
+  double* Wx = QS + 2 * nvv;              // NGrid x N
+  double* Wy = Wx + (size_t)ng * nv;
+  double* part = Wy + (size_t)ng * nv;
+  RPA_CUDA(h, cudaMemcpyAsync(Ad, Ah.data(), (size_t)nt * 8, cudaMemcpyHostToDevice, h->stream));
+  RPA_CUDA(h, cudaMemsetAsync(part, 0, (size_t)nslot * rpa::kDotPartials * 8, h->stream));
+  double* Xd = static_cast<double*>(h->jX.p);
+  double* Ud = static_cast<double*>(h->jU.p);
+  const int64_t ldx = ng, ldu = nov;
+  RPA_CUDA(h, cudaEventRecord(h->ev[1], h->stream));
+  // occupied localisation: X <- X L, U(:, :, mu) <- U(:, :, mu) L
+  if (Ld) {
+    RPA_CUDA(h, rpa::launch_gemm_f64(gemm_g(ng, no, no, Xd0, ldx0, false, Ld, ldl, false, Xd, ldx), h->stream));
+    rpa::GemmF64Args g = gemm_g(nv, no, no, Ud0, nv, false, Ld, ldl, false, Ud, nv);
+    g.batch = nt;
+    g.sA = ldu0;
+    g.sB = 0;
+    g.sC = nov;
+    RPA_CUDA(h, rpa::launch_gemm_f64(g, h->stream));
+  } else {
+    RPA_CUDA(h, cudaMemcpy2DAsync(Xd, (size_t)ng * 8, Xd0, (size_t)ldx0 * 8, (size_t)ng * 8, (size_t)no,
+                                  cudaMemcpyDeviceToDevice, h->stream));
+    RPA_CUDA(h, cudaMemcpy2DAsync(Ud, (size_t)nov * 8, Ud0, (size_t)ldu0 * 8, (size_t)nov * 8, (size_t)nt,
+                                  cudaMemcpyDeviceToDevice, h->stream));
+  }
+  // max_a (aa|aa) for the Schwarz screening of the (ab|ij) blocks (Boys orbitals)
+  double maxvabab = 0.0;
+  if (BoysScreening) {
+    RPA_CUDA(h, rpa::launch_hadamard(Yd, ldy, Yd, ldy, ng, nv, Wg, ng, h->stream));
+    RPA_CUDA(h, rpa::launch_gemm_f64(gemm_g(nq, nv, ng, Zd, ldz, true, Wg, ng, false, ZYXk, nq), h->stream));
+    std::vector<double> zz((size_t)nq * nv);
+    RPA_CUDA(h, cudaMemcpyAsync(zz.data(), ZYXk, zz.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+    RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+    for (int a = 0; a < nv; ++a) {
+      dd acc{0.0, 0.0};
+      for (int k = 0; k < nq; ++k) {
+        const double v = zz[(size_t)k + (size_t)nq * a];
+        acc = rpa::dd_add(acc, v * v);
+      }
+      maxvabab = std::max(maxvabab, acc.hi + acc.lo);
+    }
+  }
+
+  // ---- pair-natural orbitals of every pair i >= j: packed [U | s V] (nv x 2n) per pair
+  std::vector<int64_t> poff((size_t)no * no, -1);
+  std::vector<int> pn((size_t)no * no, 0);
+  size_t pno_used = 0;
+  const double thr2 = CutoffThreshPNO * CutoffThreshPNO;
+  int64_t max_n = 0, sum_n = 0, zero_pairs = 0;
+  RPA_CUDA(h, ensure(h->tPerm, (size_t)nv * sizeof(int)));
+  RPA_CUDA(h, ensure(h->tSmall, (size_t)std::max(nv, 256) * 8 + 64));
+  for (int j = 0; j < no; ++j) {
+    for (int i = j; i < no; ++i) {
+      // T(a, b) = sum_mu U(a, i, mu) A_mu U(b, j, mu)
+      rpa::GemmF64Args gt = gemm_g(nv, nv, nt, Ud + (int64_t)nv * i, ldu, false, Ud + (int64_t)nv * j, ldu, true, Tm, nv);
+      gt.kscale = Ad;
+      RPA_CUDA(h, rpa::launch_gemm_f64(gt, h->stream));
+      RPA_CUDA(h, rpa::launch_gemm_f64(gemm_g(nv, nv, nv, Tm, nv, false, Tm, nv, true, Mm, nv), h->stream));
+      std::vector<double> ev;
+      std::vector<int> order;
+      if ((s = sym_eig(h, Mm, Vm, nv, ev, order))) return s;
+      std::vector<int> keep;
+      for (int q = nv - 1; q >= 0; --q)  // descending singular values
+        if (ev[order[q]] > thr2) keep.push_back(order[q]);
+        else break;
+      const int n = (int)keep.size();
+      max_n = std::max<int64_t>(max_n, n);
+      sum_n += n;
+      if (n == 0) {
+        ++zero_pairs;
+        continue;
+      }
+      const size_t bytes = (size_t)nv * 2 * n * 8;
+      if ((s = grow_keep(h, h->jPno, pno_used + bytes, pno_used))) return s;
+      double* dst = reinterpret_cast<double*>(static_cast<char*>(h->jPno.p) + pno_used);
+      if ((s = gather(h, Vm, nv, dst, keep, nullptr))) return s;  // U
+      RPA_CUDA(h, rpa::launch_gemm_f64(gemm_g(nv, n, nv, Tm, nv, true, dst, nv, false, dst + (size_t)nv * n, nv),
+                                       h->stream));  // s V = T^T U
+      poff[(size_t)i + (size_t)no * j] = poff[(size_t)j + (size_t)no * i] = (int64_t)(pno_used / 8);
+      pn[(size_t)i + (size_t)no * j] = pn[(size_t)j + (size_t)no * i] = n;
+      pno_used += bytes;
+    }
+  }
+  if (PNOStats) {
+    PNOStats[0] = max_n;
+    PNOStats[1] = sum_n;
+    PNOStats[2] = zero_pairs;
+  }
+  RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
+  const double* pno = static_cast<const double*>(h->jPno.p);
+
+  // ---- energy terms (rpa_JCTC2024_Gaibj_Gabij_v2)
+  const double c2b = -2.0, c2c = -2.0, c2d = 2.0, c2g = -4.0, c2h = -4.0, c2i = 2.0, c2j = 2.0;
+  auto slot = [&](int64_t pair, int term) { return part + (size_t)(5 * pair + term) * rpa::kDotPartials; };
+  auto G = [&](const rpa::GemmF64Args& g) { return rpa::launch_gemm_f64(g, h->stream); };
+  int64_t pair = 0;
+  std::vector<std::pair<int, int>> pair_ij;
+  for (int j = 0; j < no; ++j) {
+    const double* xj = Xd + (int64_t)ldx * j;
+    // ZYX(k, b) = sum_g Z(g, k) X(g, j) Y(g, b); ZYX(g, b) = Z ZYX(k, b)
+    rpa::GemmF64Args g1 = gemm_g(nq, nv, ng, Zd, ldz, true, Yd, ldy, false, ZYXk, nq);
+    g1.kscale = xj;
+    RPA_CUDA(h, G(g1));
+    RPA_CUDA(h, G(gemm_g(ng, nv, nq, Zd, ldz, false, ZYXk, nq, false, ZYXg, ng)));
+    for (int i = j; i < no; ++i, ++pair) {
+      pair_ij.push_back({i, j});
+      const double* xi = Xd + (int64_t)ldx * i;
+      // ZXX(k) = sum_g Z(g, k) X(g, i) X(g, j), its norm for the screening, ZXX(g) = Z ZXX(k)
+      rpa::GemmF64Args g2 = gemm_g(nq, 1, ng, Zd, ldz, true, xj, ng, false, zk, nq);
+      g2.kscale = xi;
+      RPA_CUDA(h, G(g2));
+      RPA_CUDA(h, rpa::launch_dot_partials(zk, nq, zk, nq, nq, 1, nullptr, slot(pair, 4), h->stream));
+      RPA_CUDA(h, G(gemm_g(ng, 1, nq, Zd, ldz, false, zk, nq, false, zg, ng)));
+      // S1a, S1b of the pair (i, j)
+      const int nij = pn[(size_t)i + (size_t)no * j];
+      if (nij > 0) {
+        const double* P = pno + poff[(size_t)i + (size_t)no * j];
+        const double* Q = P + (size_t)nv * nij;
+        for (int t = 0; t < 2; ++t) {  // t = 0: S1b (Y Q, ZYX P); t = 1: S1a (Y P, ZYX Q)
+          rpa::GemmF64Args gx = gemm_g(ng, nij, nv, Yd, ldy, false, t == 0 ? Q : P, nv, false, Wx, ng);
+          gx.rowscale = xi;
+          RPA_CUDA(h, G(gx));
+          RPA_CUDA(h, G(gemm_g(ng, nij, nv, ZYXg, ng, false, t == 0 ? P : Q, nv, false, Wy, ng)));
+          RPA_CUDA(h, rpa::launch_dot_partials(Wx, ng, Wy, ng, ng, nij, nullptr, slot(pair, t == 0 ? 1 : 0),
+                                               h->stream));
+        }
+      }
+      // G(ba; ji) for 2g..2j and G(bj; ai) for 2b..2d, accumulated over k
+      RPA_CUDA(h, cudaMemsetAsync(Gg, 0, nvv * 8, h->stream));
+      RPA_CUDA(h, cudaMemsetAsync(Gb, 0, nvv * 8, h->stream));
+      for (int k = 0; k < no; ++k) {
+        const int nkj = pn[(size_t)k + (size_t)no * j], nki = pn[(size_t)k + (size_t)no * i];
+        if (nkj == 0 || nki == 0) continue;
+        const double* kj[2] = {pno + poff[(size_t)k + (size_t)no * j], nullptr};
+        kj[1] = kj[0] + (size_t)nv * nkj;
+        const double* ki[2] = {pno + poff[(size_t)k + (size_t)no * i], nullptr};
+        ki[1] = ki[0] + (size_t)nv * nki;
+        int Pki, Qki, Pik, Qik, Pkj, Qkj, Pjk, Qjk;
+        if (k >= i) { Pki = 0; Qki = 1; Pik = 1; Qik = 0; } else { Pki = 1; Qki = 0; Pik = 0; Qik = 1; }
+        if (k >= j) { Pkj = 0; Qkj = 1; Pjk = 1; Qjk = 0; } else { Pkj = 1; Qkj = 0; Pjk = 0; Qjk = 1; }
+        double* S_jk_ki = Sm;
+        double* S_jk_ik = Sm + nvv;
+        double* S_kj_ki = Sm + 2 * nvv;
+        double* S_kj_ik = Sm + 3 * nvv;
+        RPA_CUDA(h, G(gemm_g(nkj, nki, nv, kj[Qjk], nv, true, ki[Pki], nv, false, S_jk_ki, nkj)));
+        RPA_CUDA(h, G(gemm_g(nkj, nki, nv, kj[Qjk], nv, true, ki[Pik], nv, false, S_jk_ik, nkj)));
+        RPA_CUDA(h, G(gemm_g(nkj, nki, nv, kj[Qkj], nv, true, ki[Pki], nv, false, S_kj_ki, nkj)));
+        RPA_CUDA(h, G(gemm_g(nkj, nki, nv, kj[Qkj], nv, true, ki[Pik], nv, false, S_kj_ik, nkj)));
+        double* qs[2] = {QS, QS + (size_t)nv * nkj};
+        // alpha ki[q] S^T (+ beta qs) into qs[x]:  (nv x nki)(nki x nkj)
+        auto qsum = [&](int x, int q, const double* S, double alpha, double beta) {
+          return G(gemm_g(nv, nkj, nki, ki[q], nv, false, S, nkj, true, qs[x], nv, alpha, beta));
+        };
+        // 2g..2j (always formed; the screening drops its trace at the end)
+        if (i != j) {
+          RPA_CUDA(h, qsum(Pjk, Qki, S_jk_ki, 2.0 * c2g, 0.0));
+          RPA_CUDA(h, qsum(Pjk, Qik, S_jk_ik, c2i + c2j, 1.0));
+          RPA_CUDA(h, qsum(Pkj, Qik, S_kj_ik, 2.0 * c2h, 0.0));
+          RPA_CUDA(h, qsum(Pkj, Qki, S_kj_ki, c2i + c2j, 1.0));
+        } else {
+          RPA_CUDA(h, qsum(Pjk, Qki, S_jk_ki, c2g, 0.0));
+          RPA_CUDA(h, qsum(Pjk, Qik, S_jk_ik, c2i + c2j, 1.0));
+          RPA_CUDA(h, qsum(Pkj, Qik, S_kj_ik, c2h, 0.0));
+        }
+        RPA_CUDA(h, G(gemm_g(nv, nv, 2 * nkj, kj[0], nv, false, QS, nv, true, Gg, nv, 1.0, 1.0)));
+        // 2b..2d
+        if (i != j) {
+          RPA_CUDA(h, qsum(Pkj, Qik, S_kj_ik, 2.0 * c2d, 0.0));
+          RPA_CUDA(h, qsum(Pkj, Qki, S_kj_ki, c2b + c2c, 1.0));
+          RPA_CUDA(h, qsum(Pjk, Qik, S_jk_ik, c2b + c2c, 0.0));
+          RPA_CUDA(h, G(gemm_g(nv, nv, 2 * nkj, kj[0], nv, false, QS, nv, true, Gb, nv, 1.0, 1.0)));
+        } else {
+          RPA_CUDA(h, qsum(Pkj, Qik, S_kj_ik, c2d, 0.0));
+          RPA_CUDA(h, qsum(Pkj, Qki, S_kj_ki, c2b + c2c, 1.0));
+          RPA_CUDA(h, G(gemm_g(nv, nv, nkj, kj[Pkj], nv, false, qs[Pkj], nv, true, Gb, nv, 1.0, 1.0)));
+        }
+      }
+      // Tr V G: sum_ga Y(g,a) ZXX(g) (Y G)(g,a)  and  sum_ga (ZYX G)(g,a) X(g,i) Y(g,a)
+      rpa::GemmF64Args gg = gemm_g(ng, nv, nv, Yd, ldy, false, Gg, nv, false, Wg, ng);
+      gg.rowscale = zg;
+      RPA_CUDA(h, G(gg));
+      RPA_CUDA(h, rpa::launch_dot_partials(Yd, ldy, Wg, ng, ng, nv, nullptr, slot(pair, 2), h->stream));
+      RPA_CUDA(h, G(gemm_g(ng, nv, nv, ZYXg, ng, false, Gb, nv, false, Wg, ng)));
+      RPA_CUDA(h, rpa::launch_dot_partials(Wg, ng, Yd, ldy, ng, nv, xi, slot(pair, 3), h->stream));
+    }
+  }
+  RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
+  std::vector<double> ph((size_t)nslot * rpa::kDotPartials);
+  RPA_CUDA(h, cudaMemcpyAsync(ph.data(), part, ph.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+  RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  auto total = [&](int64_t p, int term) {
+    dd acc{0.0, 0.0};
+    const double* q = ph.data() + (size_t)(5 * p + term) * rpa::kDotPartials;
+    for (int b = 0; b < rpa::kDotPartials; ++b) acc = rpa::dd_add(acc, q[b]);
+    return acc.hi + acc.lo;
+  };
+  dd erpa{0.0, 0.0}, e1b{0.0, 0.0}, e2bcd{0.0, 0.0}, e2ghij{0.0, 0.0};
+  for (int64_t p = 0; p < npairs; ++p) {
+    const double weight = (pair_ij[p].first != pair_ij[p].second) ? 2.0 : 1.0;
+    erpa = rpa::dd_add(erpa, 2.0 * weight * total(p, 0));
+    e1b = rpa::dd_add(e1b, -2.0 * weight * total(p, 1));
+    bool contrib = true;
+    if (BoysScreening) contrib = std::sqrt(std::fabs(maxvabab * total(p, 4))) > CutoffThreshVabij;
+    if (contrib) e2ghij = rpa::dd_add(e2ghij, total(p, 2));
+    e2bcd = rpa::dd_add(e2bcd, total(p, 3));
+  }
+  Energies[0] = erpa.hi + erpa.lo;
+  Energies[1] = e1b.hi + e1b.lo;
+  Energies[2] = e2bcd.hi + e2bcd.lo;
+  Energies[3] = e2ghij.hi + e2ghij.lo;
+  finish_timings(h);
+  return RPA_OK;
 }
 
 int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* inst, int64_t prec, double* Ec,

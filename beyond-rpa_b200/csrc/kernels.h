@@ -220,6 +220,13 @@ cudaError_t launch_symmetrize_avg(double* A, int64_t lda, int n, cudaStream_t st
 cudaError_t launch_sosex(const double* R, int64_t ldR, int NQ, int no, int nv, const double* U, int64_t ldU,
                          const double* U2, int64_t ldU2, int NT, const double* Bmu, double* partial, int64_t* npartial,
                          cudaStream_t stream);
+// C = A o B (element-wise).
+cudaError_t launch_hadamard(const double* A, int64_t lda, const double* B, int64_t ldb, int rows, int cols,
+                            double* C, int64_t ldc, cudaStream_t stream);
+// out[0 .. kDotPartials) = per-CTA partial sums of sum_{r,c} w(r) A(r,c) B(r,c) (w may be nullptr).
+constexpr int kDotPartials = 64;
+cudaError_t launch_dot_partials(const double* A, int64_t lda, const double* B, int64_t ldb, int rows, int cols,
+                                const double* w, double* out, cudaStream_t stream);
 // YX(g, a + nv*ii) = Xa(g, a) Xi(g, i0 + ii) for ii < ni (YX: ngrid x nv*ni, ld ngrid).
 cudaError_t launch_khatri_rao(const double* Xa, int64_t ldXa, const double* Xi, int64_t ldXi, int ngrid, int nv,
                               int i0, int ni, double* YX, cudaStream_t stream);

@@ -281,6 +281,38 @@ __global__ void lyap_scale_kernel(double* Y, const double* mu, int n, int* bad) 
   Y[idx] /= den;
 }
 
+// C = A o B (element-wise, rows x cols, column-major)
+__global__ void hadamard_kernel(const double* A, int64_t lda, const double* B, int64_t ldb, int rows, int cols,
+                                double* C, int64_t ldc) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)rows * cols) return;
+  const int64_t r = idx % rows, c = idx / rows;
+  C[r + ldc * c] = A[r + lda * c] * B[r + ldb * c];
+}
+
+// Partial sums of sum_{r,c} w(r) A(r,c) B(r,c) (w optional): kDotBlocks CTAs each write one
+// partial to out[blockIdx.x]; the caller adds them in a fixed order.
+constexpr int kDotBlocks = kDotPartials;
+__global__ void __launch_bounds__(256) dot_partials_kernel(const double* A, int64_t lda, const double* B, int64_t ldb,
+                                                           int rows, int cols, const double* w, double* out) {
+  __shared__ double red[256];
+  const int64_t total = (int64_t)rows * cols;
+  double acc = 0.0;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = idx % rows, c = idx / rows;
+    const double v = A[r + lda * c] * B[r + ldb * c];
+    acc += w ? w[r] * v : v;
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = red[0];
+}
+
 // Khatri-Rao block of the THC factors: YX(g, a + nv*ii) = Xa(g, a) * Xi(g, i0 + ii), ii < ni
 // (rpa_THC_Rkab / rpa_THC_Rkai, src/rpa/rpa_THC.f90:374-426).
 __global__ void khatri_rao_kernel(const double* Xa, int64_t ldXa, const double* Xi, int64_t ldXi, int ngrid, int nv,
@@ -407,6 +439,20 @@ cudaError_t launch_grad_accum(const double* R, int64_t ldR, const double* Y, int
 cudaError_t launch_replicate(const double* R, int64_t ldR, int NQ, int64_t nov, double* Y, int64_t ldy, int64_t sY,
                              int nb, cudaStream_t stream) {
   replicate_kernel<<<blocks_for((int64_t)NQ * nov), 256, 0, stream>>>(R, ldR, NQ, nov, Y, ldy, sY, nb);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_hadamard(const double* A, int64_t lda, const double* B, int64_t ldb, int rows, int cols,
+                            double* C, int64_t ldc, cudaStream_t stream) {
+  hadamard_kernel<<<blocks_for((int64_t)rows * cols), 256, 0, stream>>>(A, lda, B, ldb, rows, cols, C, ldc);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dot_partials(const double* A, int64_t lda, const double* B, int64_t ldb, int rows, int cols,
+                                const double* w, double* out, cudaStream_t stream) {
+  dot_partials_kernel<<<kDotBlocks, 256, 0, stream>>>(A, lda, B, ldb, rows, cols, w, out);
   ++g_launches;
   return cudaGetLastError();
 }

@@ -219,6 +219,24 @@ int rpa_b200_ec_thc(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc,
                     const double* OccEnergies, const double* VirtEnergies, int64_t NFreqs, const double* Freqs,
                     const double* FreqWeights, double alpha, int64_t prec, double* Ec, double* Eu);
 
+/*
+ * Particle-hole corrections to direct RPA on THC factors with pair-natural orbitals
+ * (rpa_JCTC2024_Corrections and helpers, src/rpa/rpa_JCTC2024.f90:24-703; Cieslinski,
+ * Tucholska, Modrzejewski, J. Chem. Theory Comput. 19, 6619 (2023)).  Zgk (NGrid x NQ),
+ * Xgi (NGrid x NOcc), Yga (NGrid x NVirt): THC factors; U (NOcc*NVirt x NVecsT2, the Uaim
+ * layout) and Am: the direct-ring T2 of rpa_b200_dring_t2; Lik (NOcc x NOcc, may be NULL):
+ * the occupied localisation.  PNOs of each pair: singular vectors of T(ab;ij) with singular
+ * values > CutoffThreshPNO.  BoysScreening = 1 skips the (ab|ij) contribution of pairs with
+ * sqrt(max_a (aa|aa) (ij|ij)) <= CutoffThreshVabij.  Energies[4] = { EcRPA(PNO), Ec1b,
+ * Ec2bcd, Ec2ghij }: E(SOSEX cumulant) = Ec1b / 2, E(PH3) = Ec2bcd + Ec2ghij.  PNOStats[3]
+ * (may be NULL) = { max NVirtPNO, sum NVirtPNO, pairs without PNOs }.
+ */
+int rpa_b200_jctc2024(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zgk,
+                      int64_t ldZ, const double* Xgi, int64_t ldXi, const double* Yga, int64_t ldYa, int64_t NVecsT2,
+                      const double* U, int64_t ldU, const double* Am, const double* Lik, int64_t ldL,
+                      double CutoffThreshPNO, int64_t BoysScreening, double CutoffThreshVabij, double* Energies,
+                      int64_t* PNOStats);
+
 /* Basis types of the effective dielectric matrix (src/rpa/rpa_definitions.f90:92-104). */
 #define RPA_BASIS_RANDOM 1
 #define RPA_BASIS_EIGEN 2

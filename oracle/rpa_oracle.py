@@ -678,3 +678,109 @@ def make_thc_factors(ngrid, nq, no, nv, seed, scale=0.3):
     eo = np.sort(rng.uniform(-1.3, -0.4, no))
     ev = np.sort(np.exp(rng.uniform(math.log(0.03), math.log(4.0), nv)))
     return Z, Xa, Xi, eo, ev
+
+
+def jctc2024_corrections(Zgk, Xgi, Yga, U, A, Lik=None, cutoff_pno=1.0e-5, boys_screening=False,
+                         cutoff_vabij=1.0e-6):
+    """Particle-hole corrections to direct RPA on THC factors with pair-natural orbitals.
+
+    rpa_JCTC2024_Corrections, src/rpa/rpa_JCTC2024.f90:24-257, with _Tabij (684-703),
+    _MaxVabab (260-278), _PackTransfMatrices (281-320), _Gaibj_Gabij_v2 (323-548), _S1ab
+    (551-572) and _phRPA_Gab_jik (575-681).  U is (nov x NT) (the Uaim layout), A (NT); Lik
+    (NOcc x NOcc) the occupied localisation (None: canonical orbitals).  The PNOs of each pair
+    i >= j come from the full SVD of T(ab;ij) = sum_mu U(a,i,mu) A_mu U(b,j,mu) with singular
+    values > cutoff_pno (RPA_SVD_FULL; the randomized SVD of the reference reduces to it when
+    NVirt fits its subspace).
+    Returns (EcRPA_PNO, Ec1b, Ec2bcd, Ec2ghij); E(SOSEX cumulant) = Ec1b / 2,
+    E(PH3) = Ec2bcd + Ec2ghij."""
+    ng, nq = Zgk.shape
+    no = Xgi.shape[1]
+    nv = Yga.shape[1]
+    nt = len(A)
+    Ur = np.asarray(U, dtype=np.float64).reshape(nv, no, nt, order="F")
+    if Lik is not None:
+        Xgi = Xgi @ Lik
+        Ur = np.einsum("aim,ik->akm", Ur, Lik)
+    maxvabab = 0.0
+    if boys_screening:
+        zxx = Zgk.T @ (Yga ** 2)
+        maxvabab = float(np.max(np.sum(zxx ** 2, axis=0)))
+    # pair-natural orbitals: T_ij = U s V^T, TaxPNO = [U | s V]
+    tax = {}
+    for j in range(no):
+        for i in range(j, no):
+            T = Ur[:, i, :] @ (Ur[:, j, :] * A[None, :]).T
+            u, s, vt = np.linalg.svd(T)
+            n = int(np.sum(s > cutoff_pno))
+            if n > 0:
+                tax[(i, j)] = np.concatenate([u[:, :n], vt[:n].T * s[None, :n]], axis=1)
+
+    def packed(k, i):  # TaxPNO of the pair {k, i} or None
+        return tax.get((max(k, i), min(k, i)))
+
+    ec_rpa = ec1b = ec2bcd = ec2ghij = 0.0
+    c2b = c2c = -4.0 * 0.5
+    c2d = 2.0
+    c2g = c2h = -4.0
+    c2i = c2j = 2.0
+    for j in range(no):
+        wga = Yga * Xgi[:, j][:, None]
+        zyx_gbj = Zgk @ (Zgk.T @ wga)
+        for i in range(j, no):
+            weight = 2.0 if i != j else 1.0
+            wg = Xgi[:, i] * Xgi[:, j]
+            zxx_kij = Zgk.T @ wg
+            if boys_screening:
+                vijij = float(zxx_kij @ zxx_kij)
+                contrib = math.sqrt(abs(maxvabab * vijij)) > cutoff_vabij
+            else:
+                contrib = True
+            zxx_gij = Zgk @ zxx_kij if contrib else None
+            yx_gai = Yga * Xgi[:, i][:, None]
+            pq_ij = packed(i, j)
+            if pq_ij is not None:
+                nij = pq_ij.shape[1] // 2
+                P, Q = pq_ij[:, :nij], pq_ij[:, nij:]
+                s1b = float(np.sum((yx_gai @ Q) * (zyx_gbj @ P)))
+                s1a = float(np.sum((yx_gai @ P) * (zyx_gbj @ Q)))
+                ec1b -= 2.0 * weight * s1b
+                ec_rpa += 2.0 * weight * s1a
+            g_bcd = np.zeros((nv, nv))
+            g_ghij = np.zeros((nv, nv))
+            for k in range(no):
+                pq_kj, pq_ki = packed(k, j), packed(k, i)
+                if pq_kj is None or pq_ki is None:
+                    continue
+                nkj, nki = pq_kj.shape[1] // 2, pq_ki.shape[1] // 2
+                kj = [pq_kj[:, :nkj], pq_kj[:, nkj:]]
+                ki = [pq_ki[:, :nki], pq_ki[:, nki:]]
+                Pki, Qki, Pik, Qik = (0, 1, 1, 0) if k >= i else (1, 0, 0, 1)
+                Pkj, Qkj, Pjk, Qjk = (0, 1, 1, 0) if k >= j else (1, 0, 0, 1)
+                S_jk_ki = kj[Qjk].T @ ki[Pki]
+                S_jk_ik = kj[Qjk].T @ ki[Pik]
+                S_kj_ki = kj[Qkj].T @ ki[Pki]
+                S_kj_ik = kj[Qkj].T @ ki[Pik]
+                QS_jk_ki = ki[Qki] @ S_jk_ki.T
+                QS_jk_ik = ki[Qik] @ S_jk_ik.T
+                QS_kj_ki = ki[Qki] @ S_kj_ki.T
+                QS_kj_ik = ki[Qik] @ S_kj_ik.T
+                QS = [None, None]
+                if contrib:
+                    if i != j:
+                        QS[Pjk] = (2.0 * c2g) * QS_jk_ki + (c2i + c2j) * QS_jk_ik
+                        QS[Pkj] = (2.0 * c2h) * QS_kj_ik + (c2i + c2j) * QS_kj_ki
+                    else:
+                        QS[Pjk] = c2g * QS_jk_ki + (c2i + c2j) * QS_jk_ik
+                        QS[Pkj] = c2h * QS_kj_ik
+                    g_ghij += kj[0] @ QS[0].T + kj[1] @ QS[1].T
+                if i != j:
+                    QS[Pkj] = (2.0 * c2d) * QS_kj_ik + (c2b + c2c) * QS_kj_ki
+                    QS[Pjk] = (c2b + c2c) * QS_jk_ik
+                    g_bcd += kj[0] @ QS[0].T + kj[1] @ QS[1].T
+                else:
+                    QS[Pkj] = c2d * QS_kj_ik + (c2b + c2c) * QS_kj_ki
+                    g_bcd += kj[Pkj] @ QS[Pkj].T
+            if contrib:
+                ec2ghij += float(np.sum(Yga * ((Yga @ g_ghij) * zxx_gij[:, None])))
+            ec2bcd += float(np.sum((zyx_gbj @ g_bcd) * yx_gai))
+    return ec_rpa, ec1b, ec2bcd, ec2ghij

@@ -222,3 +222,23 @@ def test_thc_r_matches_explicit_sum():
     for (k, a, i) in ((0, 0, 0), (5, 4, 2), (11, 2, 1)):
         ref = math.fsum(Z[g, k] * Xa[g, a] * Xi[g, i] for g in range(40))
         assert R[k, a + 5 * i] == pytest.approx(ref, rel=1e-12, abs=1e-15)
+
+
+def test_jctc2024_pno_rpa_energy_and_sosex_limit():
+    # with every PNO kept (cutoff 0) the PNO direct-ring term equals the T2 eigenvalue energy
+    # sum_mu 2 A_mu |R U_mu|^2 = 2 sum (ai|bj) T_aibj, and Ec1b equals -2x the exchange sum
+    Z, Xa, Xi, eo, ev = O.make_thc_factors(60, 20, 3, 7, 21)
+    R = O.thc_r(Z, Xa, Xi)
+    rng = np.random.default_rng(2)
+    nt = 9
+    U, _ = np.linalg.qr(rng.standard_normal((R.shape[1], nt)))
+    A = -0.1 * rng.uniform(size=nt)
+    ec_rpa, ec1b, e2bcd, e2ghij = O.jctc2024_corrections(Z, Xi, Xa, U, A, cutoff_pno=0.0)
+    eig = O.t2_eig_rpa(U, A, R)
+    assert ec_rpa == pytest.approx(eig.sum(), rel=1e-10)
+    ex = O.exchange_sosex(np.ascontiguousarray(U.T), A, R, 3, 7, alpha=1.0)
+    assert 0.5 * ec1b == pytest.approx(ex, rel=1e-10)
+    # localisation by an orthogonal Lik leaves every term unchanged
+    L, _ = np.linalg.qr(rng.standard_normal((3, 3)))
+    loc = O.jctc2024_corrections(Z, Xi, Xa, U, A, Lik=L, cutoff_pno=0.0)
+    assert np.allclose(loc, (ec_rpa, ec1b, e2bcd, e2ghij), rtol=1e-9, atol=1e-14)
