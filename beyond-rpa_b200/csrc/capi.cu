@@ -45,6 +45,7 @@ struct rpa_b200_handle {
   DevBuf eW, eA, eZ;  // symmetric eigensolver workspace, input and eigenvector buffers
   DevBuf thZ, thXa, thXi, thYX, thR;  // THC factors, Khatri-Rao block, Cholesky vectors formed from them
   DevBuf jU, jL, jX, jPno, jWork;      // particle-hole corrections: localised T2 vectors, PNOs, scratch
+  DevBuf jPack, jQS, jS, jD;           // per-orbital PNO packs, QS slots, S blocks, grouped-GEMM descriptors
   struct BatchGraph {
     uint64_t key;
     std::vector<cudaGraphExec_t> execs;
@@ -742,7 +743,8 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
                     &h->tZ, &h->tOm, &h->tIOm, &h->tP, &h->tS, &h->tV, &h->tT, &h->tTIT, &h->tVt, &h->tW, &h->tU,
                     &h->tRU, &h->tSmall, &h->tPerm, &h->bDesc, &h->bRes, &h->gY, &h->gD,
                     &h->xM, &h->eW, &h->eA, &h->eZ, &h->thZ, &h->thXa, &h->thXi, &h->thYX, &h->thR,
-                    &h->jU, &h->jL, &h->jX, &h->jPno, &h->jWork})
+                    &h->jU, &h->jL, &h->jX, &h->jPno, &h->jWork,
+                    &h->jPack, &h->jQS, &h->jS, &h->jD})
     release(*b);
   for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
   if (h->err_dev) cudaFree(h->err_dev);
@@ -1820,6 +1822,32 @@ int rpa_b200_jctc2024(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOc
   }
   RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
   const double* pno = static_cast<const double*>(h->jPno.p);
+  // per-orbital packs (rpa_JCTC2024_PackTransfMatrices): pack[o] = the [U | s V] blocks of the
+  // pairs {k, o}, k = 0 .. NOcc-1, side by side; kcol[o * no + k] = first column of pair {k, o}
+  std::vector<int64_t> pack_off(no + 1, 0);
+  std::vector<int> ncol(no, 0), kcol((size_t)no * no, 0);
+  for (int o = 0; o < no; ++o) {
+    for (int k = 0; k < no; ++k) {
+      kcol[(size_t)o * no + k] = ncol[o];
+      ncol[o] += 2 * pn[(size_t)k + (size_t)no * o];
+    }
+    pack_off[o + 1] = pack_off[o] + ncol[o];
+  }
+  int maxcol = 1;
+  for (int o = 0; o < no; ++o) maxcol = std::max(maxcol, ncol[o]);
+  RPA_CUDA(h, ensure(h->jPack, (size_t)std::max<int64_t>(pack_off[no], 1) * nv * 8));
+  double* pack = static_cast<double*>(h->jPack.p);
+  for (int o = 0; o < no; ++o)
+    for (int k = 0; k < no; ++k) {
+      const int n = pn[(size_t)k + (size_t)no * o];
+      if (n > 0)
+        RPA_CUDA(h, cudaMemcpyAsync(pack + (size_t)nv * (pack_off[o] + kcol[(size_t)o * no + k]),
+                                    pno + poff[(size_t)k + (size_t)no * o], (size_t)nv * 2 * n * 8,
+                                    cudaMemcpyDeviceToDevice, h->stream));
+    }
+  RPA_CUDA(h, ensure(h->jQS, (size_t)nv * maxcol * 2 * 8));
+  RPA_CUDA(h, ensure(h->jS, (size_t)4 * no * std::max<int64_t>(max_n * max_n, 1) * 8));
+  RPA_CUDA(h, ensure(h->jD, (size_t)(8 * no + 8) * sizeof(rpa::GemmF64Args) + (size_t)(8 * no + 16) * sizeof(int)));
 
   // ---- energy terms (rpa_JCTC2024_Gaibj_Gabij_v2)
   const double c2b = -2.0, c2c = -2.0, c2d = 2.0, c2g = -4.0, c2h = -4.0, c2i = 2.0, c2j = 2.0;
@@ -1857,56 +1885,66 @@ int rpa_b200_jctc2024(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOc
                                                h->stream));
         }
       }
-      // G(ba; ji) for 2g..2j and G(bj; ai) for 2b..2d, accumulated over k
-      RPA_CUDA(h, cudaMemsetAsync(Gg, 0, nvv * 8, h->stream));
-      RPA_CUDA(h, cudaMemsetAsync(Gb, 0, nvv * 8, h->stream));
+      // G(ba; ji) for 2g..2j and G(bj; ai) for 2b..2d: the k sum becomes one GEMM over the
+      // packed PNO blocks of orbital j against per-k QS slots (zero where a pair has no PNOs)
+      const int ncj = ncol[j];
+      double* QSg = static_cast<double*>(h->jQS.p);
+      double* QSb = QSg + (size_t)nv * maxcol;
+      RPA_CUDA(h, cudaMemsetAsync(QSg, 0, (size_t)nv * maxcol * 2 * 8, h->stream));
+      std::vector<rpa::GemmF64Args> sp, q1, q2;
+      double* Sbase = static_cast<double*>(h->jS.p);
+      size_t soff = 0;
+      const double* pj = pack + (size_t)nv * pack_off[j];
+      const double* pi_ = pack + (size_t)nv * pack_off[i];
       for (int k = 0; k < no; ++k) {
         const int nkj = pn[(size_t)k + (size_t)no * j], nki = pn[(size_t)k + (size_t)no * i];
         if (nkj == 0 || nki == 0) continue;
-        const double* kj[2] = {pno + poff[(size_t)k + (size_t)no * j], nullptr};
+        const double* kj[2] = {pj + (size_t)nv * kcol[(size_t)j * no + k], nullptr};
         kj[1] = kj[0] + (size_t)nv * nkj;
-        const double* ki[2] = {pno + poff[(size_t)k + (size_t)no * i], nullptr};
+        const double* ki[2] = {pi_ + (size_t)nv * kcol[(size_t)i * no + k], nullptr};
         ki[1] = ki[0] + (size_t)nv * nki;
         int Pki, Qki, Pik, Qik, Pkj, Qkj, Pjk, Qjk;
         if (k >= i) { Pki = 0; Qki = 1; Pik = 1; Qik = 0; } else { Pki = 1; Qki = 0; Pik = 0; Qik = 1; }
         if (k >= j) { Pkj = 0; Qkj = 1; Pjk = 1; Qjk = 0; } else { Pkj = 1; Qkj = 0; Pjk = 0; Qjk = 1; }
-        double* S_jk_ki = Sm;
-        double* S_jk_ik = Sm + nvv;
-        double* S_kj_ki = Sm + 2 * nvv;
-        double* S_kj_ik = Sm + 3 * nvv;
-        RPA_CUDA(h, G(gemm_g(nkj, nki, nv, kj[Qjk], nv, true, ki[Pki], nv, false, S_jk_ki, nkj)));
-        RPA_CUDA(h, G(gemm_g(nkj, nki, nv, kj[Qjk], nv, true, ki[Pik], nv, false, S_jk_ik, nkj)));
-        RPA_CUDA(h, G(gemm_g(nkj, nki, nv, kj[Qkj], nv, true, ki[Pki], nv, false, S_kj_ki, nkj)));
-        RPA_CUDA(h, G(gemm_g(nkj, nki, nv, kj[Qkj], nv, true, ki[Pik], nv, false, S_kj_ik, nkj)));
-        double* qs[2] = {QS, QS + (size_t)nv * nkj};
-        // alpha ki[q] S^T (+ beta qs) into qs[x]:  (nv x nki)(nki x nkj)
-        auto qsum = [&](int x, int q, const double* S, double alpha, double beta) {
-          return G(gemm_g(nv, nkj, nki, ki[q], nv, false, S, nkj, true, qs[x], nv, alpha, beta));
+        double* S_jk_ki = Sbase + soff;
+        double* S_jk_ik = S_jk_ki + (size_t)nkj * nki;
+        double* S_kj_ki = S_jk_ik + (size_t)nkj * nki;
+        double* S_kj_ik = S_kj_ki + (size_t)nkj * nki;
+        soff += 4 * (size_t)nkj * nki;
+        sp.push_back(gemm_g(nkj, nki, nv, kj[Qjk], nv, true, ki[Pki], nv, false, S_jk_ki, nkj));
+        sp.push_back(gemm_g(nkj, nki, nv, kj[Qjk], nv, true, ki[Pik], nv, false, S_jk_ik, nkj));
+        sp.push_back(gemm_g(nkj, nki, nv, kj[Qkj], nv, true, ki[Pki], nv, false, S_kj_ki, nkj));
+        sp.push_back(gemm_g(nkj, nki, nv, kj[Qkj], nv, true, ki[Pik], nv, false, S_kj_ik, nkj));
+        const size_t c0 = (size_t)kcol[(size_t)j * no + k];
+        double* qg[2] = {QSg + (size_t)nv * c0, QSg + (size_t)nv * (c0 + nkj)};
+        double* qb[2] = {QSb + (size_t)nv * c0, QSb + (size_t)nv * (c0 + nkj)};
+        // alpha ki[q] S^T (+ beta slot)
+        auto qs = [&](double* dst, int q, const double* S, double alpha, double beta) {
+          return gemm_g(nv, nkj, nki, ki[q], nv, false, S, nkj, true, dst, nv, alpha, beta);
         };
-        // 2g..2j (always formed; the screening drops its trace at the end)
         if (i != j) {
-          RPA_CUDA(h, qsum(Pjk, Qki, S_jk_ki, 2.0 * c2g, 0.0));
-          RPA_CUDA(h, qsum(Pjk, Qik, S_jk_ik, c2i + c2j, 1.0));
-          RPA_CUDA(h, qsum(Pkj, Qik, S_kj_ik, 2.0 * c2h, 0.0));
-          RPA_CUDA(h, qsum(Pkj, Qki, S_kj_ki, c2i + c2j, 1.0));
+          q1.push_back(qs(qg[Pjk], Qki, S_jk_ki, 2.0 * c2g, 0.0));
+          q2.push_back(qs(qg[Pjk], Qik, S_jk_ik, c2i + c2j, 1.0));
+          q1.push_back(qs(qg[Pkj], Qik, S_kj_ik, 2.0 * c2h, 0.0));
+          q2.push_back(qs(qg[Pkj], Qki, S_kj_ki, c2i + c2j, 1.0));
+          q1.push_back(qs(qb[Pkj], Qik, S_kj_ik, 2.0 * c2d, 0.0));
+          q2.push_back(qs(qb[Pkj], Qki, S_kj_ki, c2b + c2c, 1.0));
+          q1.push_back(qs(qb[Pjk], Qik, S_jk_ik, c2b + c2c, 0.0));
         } else {
-          RPA_CUDA(h, qsum(Pjk, Qki, S_jk_ki, c2g, 0.0));
-          RPA_CUDA(h, qsum(Pjk, Qik, S_jk_ik, c2i + c2j, 1.0));
-          RPA_CUDA(h, qsum(Pkj, Qik, S_kj_ik, c2h, 0.0));
-        }
-        RPA_CUDA(h, G(gemm_g(nv, nv, 2 * nkj, kj[0], nv, false, QS, nv, true, Gg, nv, 1.0, 1.0)));
-        // 2b..2d
-        if (i != j) {
-          RPA_CUDA(h, qsum(Pkj, Qik, S_kj_ik, 2.0 * c2d, 0.0));
-          RPA_CUDA(h, qsum(Pkj, Qki, S_kj_ki, c2b + c2c, 1.0));
-          RPA_CUDA(h, qsum(Pjk, Qik, S_jk_ik, c2b + c2c, 0.0));
-          RPA_CUDA(h, G(gemm_g(nv, nv, 2 * nkj, kj[0], nv, false, QS, nv, true, Gb, nv, 1.0, 1.0)));
-        } else {
-          RPA_CUDA(h, qsum(Pkj, Qik, S_kj_ik, c2d, 0.0));
-          RPA_CUDA(h, qsum(Pkj, Qki, S_kj_ki, c2b + c2c, 1.0));
-          RPA_CUDA(h, G(gemm_g(nv, nv, nkj, kj[Pkj], nv, false, qs[Pkj], nv, true, Gb, nv, 1.0, 1.0)));
+          q1.push_back(qs(qg[Pjk], Qki, S_jk_ki, c2g, 0.0));
+          q2.push_back(qs(qg[Pjk], Qik, S_jk_ik, c2i + c2j, 1.0));
+          q1.push_back(qs(qg[Pkj], Qik, S_kj_ik, c2h, 0.0));
+          q1.push_back(qs(qb[Pkj], Qik, S_kj_ik, c2d, 0.0));  // the other slot of 2b..2d stays zero
+          q2.push_back(qs(qb[Pkj], Qki, S_kj_ki, c2b + c2c, 1.0));
         }
       }
+      if (!sp.empty()) {
+        RPA_CUDA(h, rpa::launch_gemm_f64_grouped(sp, h->jD.p, h->jD.bytes, h->stream));
+        RPA_CUDA(h, rpa::launch_gemm_f64_grouped(q1, h->jD.p, h->jD.bytes, h->stream));
+        RPA_CUDA(h, rpa::launch_gemm_f64_grouped(q2, h->jD.p, h->jD.bytes, h->stream));
+      }
+      RPA_CUDA(h, G(gemm_g(nv, nv, ncj, pj, nv, false, QSg, nv, true, Gg, nv, 1.0, 0.0)));
+      RPA_CUDA(h, G(gemm_g(nv, nv, ncj, pj, nv, false, QSb, nv, true, Gb, nv, 1.0, 0.0)));
       // Tr V G: sum_ga Y(g,a) ZXX(g) (Y G)(g,a)  and  sum_ga (ZYX G)(g,a) X(g,i) Y(g,a)
       rpa::GemmF64Args gg = gemm_g(ng, nv, nv, Yd, ldy, false, Gg, nv, false, Wg, ng);
       gg.rowscale = zg;

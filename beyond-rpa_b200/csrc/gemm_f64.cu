@@ -49,14 +49,13 @@ __device__ __forceinline__ int tile_off(int r, int k) {
   return kMC ? k * LDM + r : r * LDK + k;
 }
 
+// One 64 x 64 output tile (m0, n0) of problem g; b is the batch index (or the split-K index).
 template <bool kAM, bool kBN>
-__global__ void __launch_bounds__(kThreads, 4) gemm_f64_kernel(const GemmF64Args g) {
+__device__ __forceinline__ void gemm_tile(const GemmF64Args& g, const int m0, const int n0, const int b) {
   extern __shared__ double smem[];
   double* As = smem;                              // [kStages][kTileWords]
   double* Bs = smem + kStages * kTileWords;       // [kStages][kTileWords]
   double* Ss = smem + 2 * kStages * kTileWords;   // [kStages][BK]
-  const int b = blockIdx.z;
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BM;
   const bool split = g.splitk > 1;
   // split-K: blockIdx.z selects the K range [kbeg, kend) and its partial-product buffer
   int64_t kbeg = 0, kend = g.K;
@@ -156,6 +155,30 @@ __global__ void __launch_bounds__(kThreads, 4) gemm_f64_kernel(const GemmF64Args
   }
 }
 
+template <bool kAM, bool kBN>
+__global__ void __launch_bounds__(kThreads, 4) gemm_f64_kernel(const GemmF64Args g) {
+  gemm_tile<kAM, kBN>(g, blockIdx.y * BM, blockIdx.x * BM, blockIdx.z);
+}
+
+// Many independent problems of one operand layout in one launch: CTA x works on tile
+// x - tile_start[p] of the problem p with tile_start[p] <= x < tile_start[p + 1].
+template <bool kAM, bool kBN>
+__global__ void __launch_bounds__(kThreads, 4) gemm_f64_grouped_kernel(const GemmF64Args* __restrict__ probs,
+                                                                       const int* __restrict__ tile_start,
+                                                                       int nprob) {
+  const int x = blockIdx.x;
+  int lo = 0, hi = nprob - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (tile_start[mid] <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  const GemmF64Args& g = probs[lo];  // read through L1 when needed (a register copy would spill)
+  const int tiles_n = (g.N + BM - 1) / BM;
+  const int t = x - tile_start[lo];
+  gemm_tile<kAM, kBN>(g, (t / tiles_n) * BM, (t % tiles_n) * BM, 0);
+}
+
 // C = alpha rs(m) sum_s P_s + beta C, partials summed in a fixed order.
 __global__ void splitk_reduce_kernel(const GemmF64Args g) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -191,6 +214,60 @@ cudaError_t launch_variant(const GemmF64Args& g, cudaStream_t stream) {
   return cudaGetLastError();
 }
 }  // namespace
+
+template <bool kAM, bool kBN>
+cudaError_t set_smem_attr() {
+  static uint64_t done = 0;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 64 && (done >> dev & 1)) return cudaSuccess;
+  e = cudaFuncSetAttribute(gemm_f64_grouped_kernel<kAM, kBN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+  if (e == cudaSuccess && dev < 64) done |= 1ull << dev;
+  return e;
+}
+
+template <bool kAM, bool kBN>
+cudaError_t launch_grouped_variant(const GemmF64Args* probs, const int* tile_start, int nprob, int ntiles,
+                                   cudaStream_t stream) {
+  cudaError_t e = set_smem_attr<kAM, kBN>();
+  if (e != cudaSuccess) return e;
+  gemm_f64_grouped_kernel<kAM, kBN><<<ntiles, kThreads, kSmem, stream>>>(probs, tile_start, nprob);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_f64_grouped(const std::vector<GemmF64Args>& probs, void* dev_buf, size_t dev_bytes,
+                                    cudaStream_t stream) {
+  if (probs.empty()) return cudaSuccess;
+  const bool am = (probs[0].a_m == 1), bn = (probs[0].b_n == 1);
+  std::vector<int> start(probs.size() + 1, 0);
+  for (size_t p = 0; p < probs.size(); ++p) {
+    const GemmF64Args& g = probs[p];
+    if ((g.a_m == 1) != am || (g.b_n == 1) != bn || g.batch != 1 || g.splitk > 1) return cudaErrorInvalidValue;
+    const int t = (g.M > 0 && g.N > 0) ? ((g.M + BM - 1) / BM) * ((g.N + BM - 1) / BM) : 0;
+    start[p + 1] = start[p] + t;
+  }
+  const int ntiles = start.back();
+  if (ntiles == 0) return cudaSuccess;
+  const size_t pb = probs.size() * sizeof(GemmF64Args);
+  const size_t need = pb + start.size() * sizeof(int);
+  if (need > dev_bytes) return cudaErrorInvalidValue;
+  // stream-ordered uploads: a later upload into the same buffer waits for this launch
+  char* base = static_cast<char*>(dev_buf);
+  cudaError_t e = cudaMemcpyAsync(base, probs.data(), pb, cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpyAsync(base + pb, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return e;
+  const GemmF64Args* dp = reinterpret_cast<const GemmF64Args*>(base);
+  const int* ds = reinterpret_cast<const int*>(base + pb);
+  const int np = (int)probs.size();
+  if (am) e = bn ? launch_grouped_variant<true, true>(dp, ds, np, ntiles, stream)
+                 : launch_grouped_variant<true, false>(dp, ds, np, ntiles, stream);
+  else e = bn ? launch_grouped_variant<false, true>(dp, ds, np, ntiles, stream)
+              : launch_grouped_variant<false, false>(dp, ds, np, ntiles, stream);
+  ++g_launches;
+  return e;
+}
 
 cudaError_t launch_gemm_f64(const GemmF64Args& g, cudaStream_t stream) {
   if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return cudaSuccess;

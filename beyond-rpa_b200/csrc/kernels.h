@@ -174,6 +174,10 @@ struct GemmF64Args {
   double* work;
 };
 cudaError_t launch_gemm_f64(const GemmF64Args& g, cudaStream_t stream);
+// Independent problems (batch 1, no split-K, one operand layout) in one launch; their descriptors
+// are uploaded (stream-ordered) into dev_buf (probs.size() * sizeof(GemmF64Args) + 4 (n + 1) bytes).
+cudaError_t launch_gemm_f64_grouped(const std::vector<GemmF64Args>& probs, void* dev_buf, size_t dev_bytes,
+                                    cudaStream_t stream);
 
 // ---------------------------------------------------------------- T2 chain
 // Batched forward substitution L_b X_b = B_b in place (L lower, column-major).
