@@ -294,7 +294,8 @@ def run_ours(args):
                 "ms_per_step": t_e2e / e2e_steps},
         "gpu_launches": launches,
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": sustained, "unit": "TFLOP/s",
-                     "frac": achieved / sustained, "traffic": profile_traffic("syrk_split_bf16", WORKLOAD),
+                     "frac": achieved / sustained, "frac_of_burst_peak": achieved / burst,
+                     "traffic": profile_traffic("syrk_split_bf16", WORKLOAD),
                      "kernel": "syrk_split_bf16_kernel",
                      "note": f"peak = bf16_tflops_sustained ({src}); achieved = 3 bf16 SYRK products "
                              f"3*NQ^2*nov*K / contraction time"},

@@ -59,6 +59,8 @@ struct rpa_b200_handle {
   double timings[6] = {0, 0, 0, 0, 0, 0};
   int64_t launches = 0;
   int seg_chunks = 16;  // 512-column accumulation segments of the tensor-core SYRK
+  int sync_every = 32;  // K chunks between the wave-progress milestones of the SYRK (0: off)
+  DevBuf syncBuf;       // milestone counters of the SYRK waves
   // per-call event pairs around the scale/split pass and the contraction kernel
   std::vector<cudaEvent_t> pool;
   size_t pool_used = 0;
@@ -273,6 +275,17 @@ int choose_kg(rpa_b200_handle* h, const Validated& v, int64_t pitch) {
   return (int)std::min<size_t>((size_t)kmax, std::max<size_t>(1, budget / perFreq));
 }
 
+// Zeroed wave-progress counters for one tensor-core SYRK launch (nullptr: no synchronisation).
+int prepare_sync(rpa_b200_handle* h, int NQ, int kg, int64_t nov_part, int** out) {
+  *out = nullptr;
+  const int64_t words = rpa::syrk_tc_sync_words(NQ, kg, nov_part, h->num_sms, h->sync_every);
+  if (words <= 0) return RPA_OK;
+  RPA_CUDA(h, ensure(h->syncBuf, (size_t)words * sizeof(int)));
+  RPA_CUDA(h, cudaMemsetAsync(h->syncBuf.p, 0, (size_t)words * sizeof(int), h->stream));
+  *out = static_cast<int*>(h->syncBuf.p);
+  return RPA_OK;
+}
+
 int build_pi(rpa_b200_handle* h, const Validated& v, const double* Rd, int64_t ldR, double alpha, int64_t prec) {
   const int NQ = v.NQ;
   const int64_t nov = v.nov;
@@ -339,6 +352,9 @@ int build_pi(rpa_b200_handle* h, const Validated& v, const double* Rd, int64_t l
     a.diag = diag;
     a.err = h->err_dev;
     a.seg_chunks = h->seg_chunks;
+    if ((s = prepare_sync(h, NQ, n, nov, &a.sync)) != RPA_OK) return s;
+    a.sync_every = h->sync_every;
+    a.sync_lag = 2;
     RPA_CUDA(h, rpa::launch_syrk_split_bf16(&mAh, &mAl, &mBh, &mBl, a, h->num_sms, h->stream));
     RPA_CUDA(h, cudaEventRecord(e2, h->stream));
     h->tc_ev.push_back({e1, e2});
@@ -354,14 +370,17 @@ int build_pi(rpa_b200_handle* h, const Validated& v, const double* Rd, int64_t l
 // non-finite entries of R; the caller reads it after the stream has been synchronised.
 // Returns 1 (nothing done) when the frequencies do not fit in one group.
 int build_pi_pipelined(rpa_b200_handle* h, const Validated& v, const double* Rh, int64_t ldR, double alpha) {
-  constexpr int kPipe = 4;
+  // pieces of growing size (weights 1, 2, ..., 6): the first copy, which nothing hides, is short,
+  // and each later copy fits under the contraction of the pieces before it
+  constexpr int kPipe = 6;
+  constexpr int kWeightSum = kPipe * (kPipe + 1) / 2;
   const int NQ = v.NQ;
   const int64_t nov = v.nov;
   const int64_t pitch = (nov + 7) / 8 * 8;
   int kg = 0;
   if ((kg = choose_kg(h, v, pitch)) <= 0) return -kg;
   const rpa::SplitPlan plan = rpa::plan_scale_split(NQ, nov, h->num_sms);
-  if (kg < v.K || plan.nsplit < kPipe || plan.ai_per_split % 32 != 0) return 1;
+  if (kg < v.K || plan.nsplit < 4 || plan.ai_per_split % 32 != 0) return 1;
   RPA_CUDA(h, ensure(h->R, (size_t)NQ * nov * 8));
   RPA_CUDA(h, ensure(h->Pi, (size_t)v.K * NQ * NQ * 8));
   RPA_CUDA(h, ensure(h->diag, (size_t)v.K * NQ * 8));
@@ -386,8 +405,10 @@ int build_pi_pipelined(rpa_b200_handle* h, const Validated& v, const double* Rh,
   cudaEvent_t start = pool_event(h);
   RPA_CUDA(h, cudaEventRecord(start, h->stream));
   RPA_CUDA(h, cudaStreamWaitEvent(h->copy_stream, start, 0));
+  bool first = true;  // the first non-empty piece writes Pi, later ones add into it
   for (int c = 0; c < kPipe; ++c) {
-    const int s0 = (int)((int64_t)plan.nsplit * c / kPipe), s1 = (int)((int64_t)plan.nsplit * (c + 1) / kPipe);
+    const int64_t w0 = (int64_t)c * (c + 1) / 2, w1 = (int64_t)(c + 1) * (c + 2) / 2;
+    const int s0 = (int)(plan.nsplit * w0 / kWeightSum), s1 = (int)(plan.nsplit * w1 / kWeightSum);
     const int64_t a0 = (int64_t)s0 * plan.ai_per_split, a1 = std::min(nov, (int64_t)s1 * plan.ai_per_split);
     if (a1 <= a0) continue;
     cudaEvent_t arrived = pool_event(h);
@@ -418,7 +439,11 @@ int build_pi_pipelined(rpa_b200_handle* h, const Validated& v, const double* Rh,
     a.seg_chunks = h->seg_chunks;
     a.chunk0 = (int)(a0 / 32);
     a.nov_part = a1 - a0;
-    a.accumulate = (c > 0) ? 1 : 0;
+    a.accumulate = first ? 0 : 1;
+    first = false;
+    if ((s = prepare_sync(h, NQ, v.K, a1 - a0, &a.sync)) != RPA_OK) return s;
+    a.sync_every = h->sync_every;
+    a.sync_lag = 2;
     RPA_CUDA(h, rpa::launch_syrk_split_bf16(&mAh, &mAl, &mBh, &mBl, a, h->num_sms, h->stream));
     RPA_CUDA(h, cudaEventRecord(e2, h->stream));
     h->tc_ev.push_back({e1, e2});
@@ -720,6 +745,7 @@ int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) {
   }
   h->stream = h->own_stream;
   if (const char* sc = std::getenv("RPA_B200_SEG_CHUNKS")) h->seg_chunks = std::atoi(sc);
+  if (const char* se = std::getenv("RPA_B200_SYNC_EVERY")) h->sync_every = std::atoi(se);
   for (auto& e : h->ev) cudaEventCreate(&e);
   cudaDriverEntryPointQueryResult q;
   void* fn = nullptr;
@@ -744,7 +770,7 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
                     &h->tRU, &h->tSmall, &h->tPerm, &h->bDesc, &h->bRes, &h->gY, &h->gD,
                     &h->xM, &h->eW, &h->eA, &h->eZ, &h->thZ, &h->thXa, &h->thXi, &h->thYX, &h->thR,
                     &h->jU, &h->jL, &h->jX, &h->jPno, &h->jWork,
-                    &h->jPack, &h->jQS, &h->jS, &h->jD})
+                    &h->jPack, &h->jQS, &h->jS, &h->jD, &h->syncBuf})
     release(*b);
   for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
   if (h->err_dev) cudaFree(h->err_dev);

@@ -82,7 +82,16 @@ struct SyrkTcArgs {
   int chunk0;
   int64_t nov_part;
   int accumulate;    // 1: Pi_k += the sub-range's contribution (FP64), 0: Pi_k = it
+  // Optional L2 locality of a wave of persistent CTAs: every sync_every K chunks a producer
+  // announces its progress in sync[wave * nmilestones + milestone] (zeroed before the launch)
+  // and waits, bounded, until every CTA of its wave has passed milestone - sync_lag.  Purely a
+  // performance device: a wait that runs out of time just stops synchronising.
+  int* sync;
+  int sync_every;
+  int sync_lag;
 };
+// Counters needed by SyrkTcArgs::sync for a launch of this shape (0: no synchronisation).
+int64_t syrk_tc_sync_words(int NQ, int kg, int64_t nov_part, int num_sms, int sync_every);
 // Tensor maps: 3-D (ai, Q, k) bf16 views of X_hi / X_lo; A maps use a
 // 128-row box, B maps a 256-row box, 32 ai per box, 64-byte swizzle.
 cudaError_t launch_syrk_split_bf16(const CUtensorMap* tmA_hi, const CUtensorMap* tmA_lo, const CUtensorMap* tmB_hi,

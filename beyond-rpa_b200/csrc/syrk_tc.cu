@@ -91,6 +91,10 @@ struct SingleSource {
   const CUtensorMap* maps[4];
   SyrkTcArgs a;
   int nblocks, ntm, nchunks, nunits;
+  __device__ __forceinline__ int* sync_counters() const { return a.sync; }
+  __device__ __forceinline__ int sync_every() const { return a.sync_every; }
+  __device__ __forceinline__ int sync_lag() const { return a.sync_lag; }
+  __device__ __forceinline__ int max_chunks() const { return nchunks; }
   __device__ __forceinline__ Unit get(int u) const {
     const UnitCoord c = decode_unit(u, nblocks, ntm);
     Unit x;
@@ -114,6 +118,10 @@ struct MultiSource {
   const SyrkInst* insts;
   const uint4* work;  // (instance, k, tm, tn)
   int nunits;
+  __device__ __forceinline__ int* sync_counters() const { return nullptr; }
+  __device__ __forceinline__ int sync_every() const { return 1; }
+  __device__ __forceinline__ int sync_lag() const { return 0; }
+  __device__ __forceinline__ int max_chunks() const { return 0; }
   __device__ __forceinline__ Unit get(int u) const {
     const uint4 w = work[u];
     const SyrkInst& in = insts[w.x];
@@ -135,6 +143,17 @@ struct MultiSource {
     return x;
   }
 };
+
+// Bounded wait until *c >= target (acquire); false when it gave up (~70 ms).
+__device__ __noinline__ bool wait_count(const int* c, int target) {
+  for (uint32_t it = 0; it < (1u << 20); ++it) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(c) : "memory");
+    if (v >= target) return true;
+    __nanosleep(64);
+  }
+  return false;
+}
 
 template <class Source>
 __device__ __forceinline__ void syrk_body(const Source& src, int* err, const int seg_chunks) {
@@ -182,13 +201,25 @@ __device__ __forceinline__ void syrk_body(const Source& src, int* err, const int
       uint32_t issued = 0, issued_par = 0;  // per-stage bit masks: issued, parity of the last issue
       bool ok = true;
       const CUtensorMap* last = nullptr;
+      int* const sync = src.sync_counters();
+      const int sync_every = src.sync_every(), sync_lag = src.sync_lag();
+      const int nmile = sync ? (src.max_chunks() + sync_every - 1) / sync_every : 0;
+      bool sync_wait = true;  // cleared for good if a wait ever runs out of time
       for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
         const Unit x = src.get(u);
         if (x.map[0] != last) {
           for (int i = 0; i < 4; ++i) tma_prefetch_desc(x.map[i]);
           last = x.map[0];
         }
+        const int wave = (u - (int)blockIdx.x) / (int)gridDim.x;
+        const int members = min((int)gridDim.x, nunits - wave * (int)gridDim.x);
         for (int ch = 0; ch < x.nchunks; ++ch) {
+          if (sync && ch % sync_every == 0) {
+            const int mi = ch / sync_every;
+            int* row = sync + (int64_t)wave * nmile;
+            asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(row + mi) : "memory");
+            if (sync_wait && mi >= sync_lag) sync_wait = wait_count(row + mi - sync_lag, members);
+          }
           if (!mbar_wait(&empty[stage], phase ^ 1u, err, kDevTimeoutTmaEmpty)) {
             ok = false;
             break;
@@ -372,6 +403,16 @@ cudaError_t launch_syrk_split_bf16(const CUtensorMap* tmA_hi, const CUtensorMap*
                                                                   ntm, nunits, nchunks, seg_chunks);
   ++g_launches;
   return cudaGetLastError();
+}
+
+int64_t syrk_tc_sync_words(int NQ, int kg, int64_t nov_part, int num_sms, int sync_every) {
+  if (sync_every <= 0) return 0;
+  const int nunits = syrk_tc_blocks(NQ) * kg;
+  const int grid = nunits < num_sms ? nunits : num_sms;
+  if (grid <= 0) return 0;
+  const int64_t waves = (nunits + grid - 1) / grid;
+  const int64_t nchunks = (nov_part + TK - 1) / TK;
+  return waves * ((nchunks + sync_every - 1) / sync_every);
 }
 
 int syrk_tc_blocks(int NQ) {

@@ -159,8 +159,12 @@ def test_host_r_pipelined_staging_matches_device_r(handle):
     host = handle.ec_rpa(s.R, s.eps_o, s.eps_v, x, w, prec="split")
     Rt = torch.from_numpy(np.ascontiguousarray(s.R.T)).cuda()
     dev = handle.ec_rpa(Rt.T, s.eps_o, s.eps_v, x, w, prec="split")
-    assert abs(host[0] - dev[0]) < 1e-9
-    assert np.max(np.abs(host[1] - dev[1])) < 1e-9
+    # the pieces are summed in FP64 (the one-shot build keeps one FP32 running sum per tile):
+    # both are within the split-precision budget and the piecewise sum is no farther from FP64
+    assert abs(host[0] - dev[0]) < 1e-7
+    assert np.max(np.abs(host[1] - dev[1])) < 1e-7
+    e64, _ = handle.ec_rpa(Rt.T, s.eps_o, s.eps_v, x, w, prec="fp64")
+    assert abs(host[0] - e64) <= abs(dev[0] - e64) + 1e-9
     ref, _ = O.ec_rpa(s.R, s.eps_o, s.eps_v, x, w)
     assert abs(host[0] - ref) < 1e-6
 
