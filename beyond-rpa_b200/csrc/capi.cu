@@ -46,6 +46,7 @@ struct rpa_b200_handle {
   DevBuf thZ, thXa, thXi, thYX, thR;  // THC factors, Khatri-Rao block, Cholesky vectors formed from them
   DevBuf jU, jL, jX, jPno, jWork;      // particle-hole corrections: localised T2 vectors, PNOs, scratch
   DevBuf jPack, jQS, jS, jD;           // per-orbital PNO packs, QS slots, S blocks, grouped-GEMM descriptors
+  DevBuf jT, jM, jV, jMap;             // batched PNO stage: T_ij, T T^T, eigenvectors, column map
   struct BatchGraph {
     uint64_t key;
     std::vector<cudaGraphExec_t> execs;
@@ -770,7 +771,8 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
                     &h->tRU, &h->tSmall, &h->tPerm, &h->bDesc, &h->bRes, &h->gY, &h->gD,
                     &h->xM, &h->eW, &h->eA, &h->eZ, &h->thZ, &h->thXa, &h->thXi, &h->thYX, &h->thR,
                     &h->jU, &h->jL, &h->jX, &h->jPno, &h->jWork,
-                    &h->jPack, &h->jQS, &h->jS, &h->jD, &h->syncBuf})
+                    &h->jPack, &h->jQS, &h->jS, &h->jD, &h->syncBuf,
+                    &h->jT, &h->jM, &h->jV, &h->jMap})
     release(*b);
   for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
   if (h->err_dev) cudaFree(h->err_dev);
@@ -1801,45 +1803,95 @@ int rpa_b200_jctc2024(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOc
     }
   }
 
-  // ---- pair-natural orbitals of every pair i >= j: packed [U | s V] (nv x 2n) per pair
+  // ---- pair-natural orbitals of every pair i >= j: packed [U | s V] (nv x 2n) per pair.  Pairs
+  // run in batches: one grouped GEMM forms every T_ij, one batched GEMM every T T^T, one batched
+  // eigensolver call diagonalises them, one column map gathers the kept singular vectors and one
+  // grouped GEMM forms every s V = T^T U.
   std::vector<int64_t> poff((size_t)no * no, -1);
   std::vector<int> pn((size_t)no * no, 0);
   size_t pno_used = 0;
   const double thr2 = CutoffThreshPNO * CutoffThreshPNO;
   int64_t max_n = 0, sum_n = 0, zero_pairs = 0;
-  RPA_CUDA(h, ensure(h->tPerm, (size_t)nv * sizeof(int)));
-  RPA_CUDA(h, ensure(h->tSmall, (size_t)std::max(nv, 256) * 8 + 64));
-  for (int j = 0; j < no; ++j) {
-    for (int i = j; i < no; ++i) {
-      // T(a, b) = sum_mu U(a, i, mu) A_mu U(b, j, mu)
-      rpa::GemmF64Args gt = gemm_g(nv, nv, nt, Ud + (int64_t)nv * i, ldu, false, Ud + (int64_t)nv * j, ldu, true, Tm, nv);
+  std::vector<std::pair<int, int>> plist;
+  for (int j = 0; j < no; ++j)
+    for (int i = j; i < no; ++i) plist.push_back({i, j});
+  const size_t per_pair = 3 * nvv * 8 + (rpa::syevd_workspace_bytes(nv, 2) - rpa::syevd_workspace_bytes(nv, 1));
+  const int bmax = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)plist.size(),
+                                                               (int64_t)((size_t)4 << 30) / (int64_t)per_pair));
+  RPA_CUDA(h, ensure(h->jD, (size_t)(std::max(8 * no, bmax) + 8) * sizeof(rpa::GemmF64Args) +
+                                (size_t)(std::max(8 * no, bmax) + 16) * sizeof(int)));
+  for (size_t b0 = 0; b0 < plist.size(); b0 += bmax) {
+    const int nbat = (int)std::min<size_t>(bmax, plist.size() - b0);
+    RPA_CUDA(h, ensure(h->jT, (size_t)nbat * nvv * 8));
+    RPA_CUDA(h, ensure(h->jM, (size_t)nbat * nvv * 8));
+    RPA_CUDA(h, ensure(h->jV, (size_t)nbat * nvv * 8));
+    RPA_CUDA(h, ensure(h->eW, rpa::syevd_workspace_bytes(nv, nbat)));
+    double* Tb = static_cast<double*>(h->jT.p);
+    double* Mb = static_cast<double*>(h->jM.p);
+    double* Vb = static_cast<double*>(h->jV.p);
+    std::vector<rpa::GemmF64Args> tp;
+    for (int q = 0; q < nbat; ++q) {  // T(a, b) = sum_mu U(a, i, mu) A_mu U(b, j, mu)
+      const int i = plist[b0 + q].first, j = plist[b0 + q].second;
+      rpa::GemmF64Args gt =
+          gemm_g(nv, nv, nt, Ud + (int64_t)nv * i, ldu, false, Ud + (int64_t)nv * j, ldu, true, Tb + nvv * q, nv);
       gt.kscale = Ad;
-      RPA_CUDA(h, rpa::launch_gemm_f64(gt, h->stream));
-      RPA_CUDA(h, rpa::launch_gemm_f64(gemm_g(nv, nv, nv, Tm, nv, false, Tm, nv, true, Mm, nv), h->stream));
-      std::vector<double> ev;
-      std::vector<int> order;
-      if ((s = sym_eig(h, Mm, Vm, nv, ev, order))) return s;
-      std::vector<int> keep;
-      for (int q = nv - 1; q >= 0; --q)  // descending singular values
-        if (ev[order[q]] > thr2) keep.push_back(order[q]);
-        else break;
-      const int n = (int)keep.size();
+      tp.push_back(gt);
+    }
+    RPA_CUDA(h, rpa::launch_gemm_f64_grouped(tp, h->jD.p, h->jD.bytes, h->stream));
+    rpa::GemmF64Args gm = gemm_g(nv, nv, nv, Tb, nv, false, Tb, nv, true, Mb, nv);
+    gm.batch = nbat;
+    gm.sA = gm.sB = gm.sC = (int64_t)nvv;
+    RPA_CUDA(h, rpa::launch_gemm_f64(gm, h->stream));
+    std::vector<double> ev;
+    bool conv = false;
+    RPA_CUDA(h, rpa::syevd_batched(Mb, nv, nbat, Vb, h->eW.p, h->eW.bytes, ev, conv, h->stream));
+    if (!conv) return fail(h, RPA_ERR_NOT_CONVERGED, "PNO eigensolver: a leaf did not converge");
+    // keep singular values above the cutoff (eigenvalues of T T^T above its square), descending
+    std::vector<int64_t> map;
+    std::vector<rpa::GemmF64Args> sv;
+    size_t need = pno_used;
+    std::vector<std::pair<int, size_t>> placed(nbat, {0, 0});
+    for (int q = 0; q < nbat; ++q) {
+      std::vector<int> order(nv);
+      for (int c = 0; c < nv; ++c) order[c] = c;
+      const double* evq = ev.data() + (size_t)nv * q;
+      std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return evq[a] > evq[b]; });
+      int n = 0;
+      while (n < nv && evq[order[n]] > thr2) ++n;
       max_n = std::max<int64_t>(max_n, n);
       sum_n += n;
       if (n == 0) {
         ++zero_pairs;
         continue;
       }
-      const size_t bytes = (size_t)nv * 2 * n * 8;
-      if ((s = grow_keep(h, h->jPno, pno_used + bytes, pno_used))) return s;
-      double* dst = reinterpret_cast<double*>(static_cast<char*>(h->jPno.p) + pno_used);
-      if ((s = gather(h, Vm, nv, dst, keep, nullptr))) return s;  // U
-      RPA_CUDA(h, rpa::launch_gemm_f64(gemm_g(nv, n, nv, Tm, nv, true, dst, nv, false, dst + (size_t)nv * n, nv),
-                                       h->stream));  // s V = T^T U
-      poff[(size_t)i + (size_t)no * j] = poff[(size_t)j + (size_t)no * i] = (int64_t)(pno_used / 8);
-      pn[(size_t)i + (size_t)no * j] = pn[(size_t)j + (size_t)no * i] = n;
-      pno_used += bytes;
+      placed[q] = {n, need};
+      for (int c = 0; c < n; ++c) {
+        map.push_back((int64_t)q * nv + order[c]);
+        map.push_back((int64_t)(need / 8 / nv) + c);
+      }
+      need += (size_t)nv * 2 * n * 8;
     }
+    if ((s = grow_keep(h, h->jPno, std::max<size_t>(need, 8), pno_used))) return s;
+    double* pnob = static_cast<double*>(h->jPno.p);
+    RPA_CUDA(h, ensure(h->jMap, std::max<size_t>(map.size(), 2) * sizeof(int64_t)));
+    if (!map.empty()) {
+      RPA_CUDA(h, cudaMemcpyAsync(h->jMap.p, map.data(), map.size() * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                  h->stream));
+      RPA_CUDA(h, rpa::launch_copy_columns(Vb, pnob, static_cast<const int64_t*>(h->jMap.p),
+                                           (int64_t)(map.size() / 2), nv, h->stream));  // U
+    }
+    for (int q = 0; q < nbat; ++q) {
+      const int n = placed[q].first;
+      if (n == 0) continue;
+      const int i = plist[b0 + q].first, j = plist[b0 + q].second;
+      double* dst = pnob + placed[q].second / 8;
+      sv.push_back(gemm_g(nv, n, nv, Tb + nvv * q, nv, true, dst, nv, false, dst + (size_t)nv * n, nv));  // s V
+      poff[(size_t)i + (size_t)no * j] = poff[(size_t)j + (size_t)no * i] = (int64_t)(placed[q].second / 8);
+      pn[(size_t)i + (size_t)no * j] = pn[(size_t)j + (size_t)no * i] = n;
+    }
+    RPA_CUDA(h, rpa::launch_gemm_f64_grouped(sv, h->jD.p, h->jD.bytes, h->stream));
+    pno_used = need;
+    RPA_CUDA(h, cudaStreamSynchronize(h->stream));  // map and the descriptors must outlive their uploads
   }
   if (PNOStats) {
     PNOStats[0] = max_n;

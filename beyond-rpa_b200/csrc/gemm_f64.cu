@@ -243,7 +243,9 @@ cudaError_t launch_gemm_f64_grouped(const std::vector<GemmF64Args>& probs, void*
   std::vector<int> start(probs.size() + 1, 0);
   for (size_t p = 0; p < probs.size(); ++p) {
     const GemmF64Args& g = probs[p];
-    if ((g.a_m == 1) != am || (g.b_n == 1) != bn || g.batch != 1 || g.splitk > 1) return cudaErrorInvalidValue;
+    // the layout template only chooses the load mapping (loads use the general strides), so
+    // problems whose unit strides differ from the first one's stay correct, just less coalesced
+    if (g.batch != 1 || g.splitk > 1) return cudaErrorInvalidValue;
     const int t = (g.M > 0 && g.N > 0) ? ((g.M + BM - 1) / BM) * ((g.N + BM - 1) / BM) : 0;
     start[p + 1] = start[p] + t;
   }

@@ -183,7 +183,8 @@ struct GemmF64Args {
   double* work;
 };
 cudaError_t launch_gemm_f64(const GemmF64Args& g, cudaStream_t stream);
-// Independent problems (batch 1, no split-K, one operand layout) in one launch; their descriptors
+// Independent problems (batch 1, no split-K; the first problem's operand layout picks the load
+// mapping) in one launch; their descriptors
 // are uploaded (stream-ordered) into dev_buf (probs.size() * sizeof(GemmF64Args) + 4 (n + 1) bytes).
 cudaError_t launch_gemm_f64_grouped(const std::vector<GemmF64Args>& probs, void* dev_buf, size_t dev_bytes,
                                     cudaStream_t stream);
@@ -233,6 +234,9 @@ cudaError_t launch_symmetrize_avg(double* A, int64_t lda, int n, cudaStream_t st
 cudaError_t launch_sosex(const double* R, int64_t ldR, int NQ, int no, int nv, const double* U, int64_t ldU,
                          const double* U2, int64_t ldU2, int NT, const double* Bmu, double* partial, int64_t* npartial,
                          cudaStream_t stream);
+// dst column map[2c+1] <- src column map[2c] for c < ncols (columns of `rows` contiguous doubles).
+cudaError_t launch_copy_columns(const double* src, double* dst, const int64_t* map, int64_t ncols, int rows,
+                                cudaStream_t stream);
 // C = A o B (element-wise).
 cudaError_t launch_hadamard(const double* A, int64_t lda, const double* B, int64_t ldb, int rows, int cols,
                             double* C, int64_t ldc, cudaStream_t stream);
@@ -272,6 +276,11 @@ cudaError_t launch_logdet_varlen(const MatDesc* mats, int nmat, int nmax, int* e
 // ---------------------------------------------------------------- symmetric eigensolver
 // Householder tridiagonalisation + divide and conquer + WY back-transformation (syevd.cu).
 size_t syevd_workspace_bytes(int n);
+size_t syevd_workspace_bytes(int n, int nmat);
+// nmat matrices of order n at stride n^2 (A destroyed), eigenvectors into Z at the same stride,
+// evals (host) nmat x n; all matrices run in the same launches.
+cudaError_t syevd_batched(double* A, int n, int nmat, double* Z, void* work, size_t work_bytes,
+                          std::vector<double>& evals, bool& converged, cudaStream_t stream);
 // A (n x n, ld n) is destroyed; Z (n x n, ld n) receives the eigenvectors and evals (host) the
 // eigenvalues in the order of Z's columns; converged is false if a leaf solve failed.
 // Synchronises the stream.

@@ -10,6 +10,8 @@
 // A non-positive pivot is reported as an error, never as a NaN energy.
 #include <algorithm>
 
+#include <cstdlib>
+
 #include "kernels.h"
 
 namespace rpa {
@@ -244,10 +246,21 @@ __global__ void copy_lower_kernel(const double* src, int64_t lds, int64_t stride
 // factorization + panel solve + update of the rest of the 256-wide outer
 // block), then one rank-256 update of the trailing matrix per outer block.
 
+// Outer block width: NB2 unless RPA_B200_CHOL_NB2 (a multiple of NB) says otherwise.
+int outer_block() {
+  static int nb2 = [] {
+    const char* e = std::getenv("RPA_B200_CHOL_NB2");
+    const int v = e ? std::atoi(e) : NB2;
+    return (v >= NB && v % NB == 0) ? v : NB2;
+  }();
+  return nb2;
+}
+
 cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag, int* err,
                                   cudaStream_t stream) {
-  for (int J0 = 0; J0 < n; J0 += NB2) {
-    const int J1 = min(n, J0 + NB2);
+  const int nb2 = outer_block();
+  for (int J0 = 0; J0 < n; J0 += nb2) {
+    const int J1 = min(n, J0 + nb2);
     for (int j0 = J0; j0 < J1; j0 += NB) {
       potrf_diag_kernel<<<nmat, 256, 0, stream>>>(A, ld, stride, n, j0, Ldiag, err);
       ++g_launches;

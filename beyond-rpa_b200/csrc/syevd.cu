@@ -103,9 +103,19 @@ __device__ __forceinline__ void cluster_sum(cg::cluster_group& cl, double (*part
 //            trailing matrix by panel columns < fin is applied here), store W(:, fin).
 //  nxt >= 0: bring column p+nxt up to date, generate its reflector (tau, d, e, V(:, p+nxt)).
 __global__ void __cluster_dims__(kCS, 1, 1) __launch_bounds__(kCT)
-    house_kernel(double* A, int n, double* V, double* Wp, int p, int fin, int nxt, const double* y, double* tau,
-                 double* d, double* e) {
+    house_kernel(double* A, int n, int64_t mstride, double* V, double* Wp, int p, int fin, int nxt, const double* y,
+                 double* tau, double* d, double* e) {
   cg::cluster_group cl = cg::this_cluster();
+  {  // matrix of this cluster
+    const int64_t z = (int64_t)blockIdx.x / kCS;
+    A += mstride * z;
+    V += mstride * z;
+    Wp += (int64_t)n * kNB * z;
+    y += (int64_t)n * z;
+    tau += (int64_t)n * z;
+    d += (int64_t)n * z;
+    e += (int64_t)n * z;
+  }
   const int rank = (int)cl.block_rank();
   __shared__ double part[2][2 * kNB];
   __shared__ double tot[2 * kNB];
@@ -199,8 +209,11 @@ __global__ void __cluster_dims__(kCS, 1, 1) __launch_bounds__(kCT)
 
 // y(c) = sum_{r > j} A(r, c) v(r) for c > j: one warp per column, four independent
 // accumulators per lane so that four loads of each lane are in flight.
-__global__ void __launch_bounds__(256) trailing_gemv_kernel(const double* A, int n, const double* v, int j,
-                                                            double* y) {
+__global__ void __launch_bounds__(256) trailing_gemv_kernel(const double* A, int n, int64_t mstride, const double* v,
+                                                            int j, double* y) {
+  A += mstride * blockIdx.y;
+  v += mstride * blockIdx.y;
+  y += (int64_t)n * blockIdx.y;
   const int c = j + 1 + (int)blockIdx.x * 8 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (c >= n) return;
@@ -222,8 +235,11 @@ __global__ void __launch_bounds__(256) trailing_gemv_kernel(const double* A, int
 
 // T (upper triangular, nb x nb, ld kNB) of the block reflector H_p ... H_{p+nb-1} = I - V T V^T,
 // from G = V^T V (ld kNB): T(i,i) = tau_i, T(0:i, i) = -tau_i T(0:i, 0:i) G(0:i, i).
-__global__ void build_t_kernel(const double* G, const double* tau, int nb, double* T) {
+__global__ void build_t_kernel(const double* G, const double* tau, int nb, double* T, int n) {
   __shared__ double Gs[kNB][kNB + 1], Ts[kNB][kNB + 1], ts[kNB];
+  G += (int64_t)kNB * kNB * blockIdx.x;  // one matrix of the batch per CTA
+  T += (int64_t)kNB * kNB * blockIdx.x;
+  tau += (int64_t)n * blockIdx.x;
   const int r = threadIdx.x;  // row of T
   for (int c = 0; c < kNB; ++c) {
     Gs[r][c] = (r < nb && c < nb) ? G[r + kNB * c] : 0.0;
@@ -249,10 +265,13 @@ __global__ void build_t_kernel(const double* G, const double* tau, int nb, doubl
 // ---------------------------------------------------------------- stage 2: divide and conquer
 
 // Cuppen tearing: for every internal boundary b (between rows b-1 and b), d(b-1), d(b) -= |e(b-1)|.
-__global__ void tear_kernel(double* d, const double* e, const int* bounds, int nb) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nb) return;
-  const int b = bounds[i];
+__global__ void tear_kernel(double* d, const double* e, const int* bounds, int nb, int n, int nmat) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)nb * nmat) return;
+  const int64_t z = idx / nb;
+  d += (int64_t)n * z;
+  e += (int64_t)n * z;
+  const int b = bounds[idx % nb];
   const double r = fabs(e[b - 1]);
   d[b - 1] -= r;
   d[b] -= r;
@@ -266,7 +285,12 @@ struct Leaf {
 // leaf is held densely in shared memory; each sweep is m'-1 rounds of m'/2 disjoint rotations
 // (round-robin pairing, m' = m rounded up to even); lane l owns row/column l for the updates.
 __global__ void __launch_bounds__(32) leaf_jacobi_kernel(const Leaf* leaves, const double* dIn, const double* eIn,
-                                                         double* D, double* Q, int64_t ldq, int* err) {
+                                                         double* D, double* Q, int64_t ldq, int* err, int n,
+                                                         int64_t mstride) {
+  dIn += (int64_t)n * blockIdx.y;
+  eIn += (int64_t)n * blockIdx.y;
+  D += (int64_t)n * blockIdx.y;
+  Q += mstride * blockIdx.y;
   constexpr int P = kLeaf + 1;
   __shared__ double a[kLeaf * P], z[kLeaf * P];  // a[r * P + c]
   __shared__ double rc[kLeaf / 2], rs[kLeaf / 2];
@@ -370,11 +394,38 @@ struct DcScratch {
   int *kidx, *colS, *colk, *coldef, *rp, *ri, *org, *cnt;
 };
 
+// The scratch of matrix z of a batch (cnt and rho are indexed by merge + nm * z instead).
+__device__ __forceinline__ DcScratch sc_at(DcScratch sc, int64_t z, int64_t n) {
+  sc.keys += 2 * n * z;
+  sc.kidx += 2 * n * z;
+  sc.ds += n * z;
+  sc.zs += n * z;
+  sc.dk += n * z;
+  sc.zk += n * z;
+  sc.ddef += n * z;
+  sc.rc += n * z;
+  sc.rs += n * z;
+  sc.tau += n * z;
+  sc.colS += n * z;
+  sc.colk += n * z;
+  sc.coldef += n * z;
+  sc.rp += n * z;
+  sc.ri += n * z;
+  sc.org += n * z;
+  return sc;
+}
+
 // Sort the poles, form z from the children's boundary rows, deflate (one CTA per merge).
 __global__ void __launch_bounds__(1024) merge_prepare_kernel(const Merge* merges, const double* D, const double* Q,
-                                                             int64_t ldq, const double* e, DcScratch sc) {
+                                                             int64_t ldq, const double* e, DcScratch sc, int nfull,
+                                                             int64_t mstride, int nm) {
   __shared__ double red[33];
   const Merge M = merges[blockIdx.x];
+  const int64_t mz = blockIdx.x + (int64_t)nm * blockIdx.y;  // (merge, matrix)
+  D += (int64_t)nfull * blockIdx.y;
+  Q += mstride * blockIdx.y;
+  e += (int64_t)nfull * blockIdx.y;
+  sc = sc_at(sc, blockIdx.y, nfull);
   const int n = M.n1 + M.n2, s = M.s, t = threadIdx.x;
   int P = 1;
   while (P < n) P <<= 1;
@@ -473,19 +524,24 @@ __global__ void __launch_bounds__(1024) merge_prepare_kernel(const Merge* merges
     sc.colk[s + k] = pcol;
     ++k;
   }
-  sc.cnt[2 * blockIdx.x] = k;
-  sc.cnt[2 * blockIdx.x + 1] = nr;
-  sc.rho[blockIdx.x] = rho;
+  sc.cnt[2 * mz] = k;
+  sc.cnt[2 * mz + 1] = nr;
+  sc.rho[mz] = rho;
 }
 
 // Apply the deflation rotations to the merge's block of Q (thread per row) and gather its
 // columns as [non-deflated (k) | deflated] into Qp (n x n, ld n).
-__global__ void merge_gather_kernel(const Merge* merges, double* Q, int64_t ldq, double* Qp_base, DcScratch sc) {
+__global__ void merge_gather_kernel(const Merge* merges, double* Q, int64_t ldq, double* Qp_base, DcScratch sc,
+                                    int nfull, int64_t mstride, int nm) {
   const Merge M = merges[blockIdx.y];
   const int n = M.n1 + M.n2, s = M.s;
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
-  const int k = sc.cnt[2 * blockIdx.y], nr = sc.cnt[2 * blockIdx.y + 1];
+  const int64_t mz = blockIdx.y + (int64_t)nm * blockIdx.z;
+  Q += mstride * blockIdx.z;
+  Qp_base += mstride * blockIdx.z;
+  sc = sc_at(sc, blockIdx.z, nfull);
+  const int k = sc.cnt[2 * mz], nr = sc.cnt[2 * mz + 1];
   double* row = Q + (int64_t)(s + r) + ldq * s;  // row r of the block: row[ldq * col]
   for (int q = 0; q < nr; ++q) {
     const int64_t a = ldq * sc.rp[s + q], b = ldq * sc.ri[s + q];
@@ -501,13 +557,15 @@ __global__ void merge_gather_kernel(const Merge* merges, double* Q, int64_t ldq,
 
 // Roots of 1 + rho sum_i z_i^2 / (d_i - lambda) = 0 by bisection on tau = lambda - d_org, with
 // d_org the pole nearer to the root (warp per root).
-__global__ void __launch_bounds__(256) secular_kernel(const Merge* merges, DcScratch sc) {
+__global__ void __launch_bounds__(256) secular_kernel(const Merge* merges, DcScratch sc, int nfull, int nm) {
   const Merge M = merges[blockIdx.y];
   const int s = M.s;
-  const int k = sc.cnt[2 * blockIdx.y];
+  const int64_t mz = blockIdx.y + (int64_t)nm * blockIdx.z;
+  sc = sc_at(sc, blockIdx.z, nfull);
+  const int k = sc.cnt[2 * mz];
   const int j = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (j >= k) return;
-  const double rho = sc.rho[blockIdx.y];
+  const double rho = sc.rho[mz];
   const double* dk = sc.dk + s;
   const double* zk = sc.zk + s;
   double z2 = 0.0;
@@ -556,10 +614,13 @@ __global__ void __launch_bounds__(256) secular_kernel(const Merge* merges, DcScr
 
 // Loewner formula: zhat_i = sign(z_i) sqrt(-prod_j (d_i - lambda_j) / prod_{j != i} (d_i - d_j) / rho);
 // overwrites zk (the secular roots are already fixed).
-__global__ void lowner_kernel(const Merge* merges, DcScratch sc, double* zhat) {
+__global__ void lowner_kernel(const Merge* merges, DcScratch sc, double* zhat, int nfull, int nm) {
   const Merge M = merges[blockIdx.y];
   const int s = M.s;
-  const int k = sc.cnt[2 * blockIdx.y];
+  const int64_t mz = blockIdx.y + (int64_t)nm * blockIdx.z;
+  sc = sc_at(sc, blockIdx.z, nfull);
+  zhat += (int64_t)nfull * blockIdx.z;
+  const int k = sc.cnt[2 * mz];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= k) return;
   const double* dk = sc.dk + s;
@@ -569,17 +630,23 @@ __global__ void lowner_kernel(const Merge* merges, DcScratch sc, double* zhat) {
     const double delta = (di - dk[sc.org[s + j]]) - sc.tau[s + j];
     w *= (j == i) ? delta : delta / (di - dk[j]);
   }
-  zhat[s + i] = copysign(sqrt(fmax(-w, 0.0) / sc.rho[blockIdx.y]), sc.zk[s + i]);
+  zhat[s + i] = copysign(sqrt(fmax(-w, 0.0) / sc.rho[mz]), sc.zk[s + i]);
 }
 
 // Columns of the rank-one problem's eigenvectors, u_j(i) = zhat_i / (d_i - lambda_j) normalised
 // (block per column), and the merged eigenvalues (non-deflated roots, then the deflated poles).
 __global__ void __launch_bounds__(256) merge_vectors_kernel(const Merge* merges, DcScratch sc, const double* zhat,
-                                                            double* Uk_base, double* D) {
+                                                            double* Uk_base, double* D, int nfull, int64_t mstride,
+                                                            int nm) {
   __shared__ double red[33];
   const Merge M = merges[blockIdx.y];
   const int n = M.n1 + M.n2, s = M.s;
-  const int k = sc.cnt[2 * blockIdx.y];
+  const int64_t mz = blockIdx.y + (int64_t)nm * blockIdx.z;
+  sc = sc_at(sc, blockIdx.z, nfull);
+  zhat += (int64_t)nfull * blockIdx.z;
+  Uk_base += mstride * blockIdx.z;
+  D += (int64_t)nfull * blockIdx.z;
+  const int k = sc.cnt[2 * mz];
   const int j = blockIdx.x;
   if (j >= n) return;
   if (j >= k) {
@@ -598,6 +665,24 @@ __global__ void __launch_bounds__(256) merge_vectors_kernel(const Merge* merges,
   const double inv = 1.0 / sqrt(block_sum(part, red));
   for (int i = threadIdx.x; i < k; i += blockDim.x) u[i] *= inv;
   if (threadIdx.x == 0) D[s + j] = dorg + tau;
+}
+
+// Deflated columns of every (merge, matrix): Q(block)(:, k ..) = Qp(:, k ..) (the rank-one
+// problem's eigenvectors replace columns 0 .. k-1 through a GEMM).
+__global__ void copy_deflated_kernel(const Merge* merges, const double* Qp_base, double* Q, int64_t ldq,
+                                     const int* cnt, int64_t mstride, int nm) {
+  const Merge M = merges[blockIdx.y];
+  const int n = M.n1 + M.n2, s = M.s;
+  const int64_t mz = blockIdx.y + (int64_t)nm * blockIdx.z;
+  const int k = cnt[2 * mz];
+  const int64_t total = (int64_t)n * (n - k);
+  const double* Qp = Qp_base + mstride * blockIdx.z + M.qp_off;
+  double* blk = Q + mstride * blockIdx.z + s + ldq * s;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = idx % n, c = k + idx / n;
+    blk[r + ldq * c] = Qp[r + (int64_t)n * c];
+  }
 }
 
 GemmF64Args gemm_args(int M, int N, int64_t K, const double* A, int64_t a_m, int64_t a_k, const double* B,
@@ -636,94 +721,107 @@ inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 }  // namespace
 
-size_t syevd_workspace_bytes(int n) {
-  const size_t nn = (size_t)n * n;
+size_t syevd_workspace_bytes(int n, int nmat) {
+  const size_t nn = (size_t)n * n, B = (size_t)std::max(nmat, 1);
   size_t b = 0;
-  b += align256(nn * 8);            // V (Householder vectors)
-  b += align256(nn * 8);            // Qp
-  b += align256(nn * 8);            // Uk
-  b += align256((size_t)n * kNB * 8);  // Wp
-  b += 2 * align256((size_t)kNB * n * 8);  // Y, Y2
-  b += 2 * align256((size_t)kNB * kNB * 8);  // G, T
-  b += align256(std::max((size_t)16 * kNB * n, (size_t)64 * kNB * kNB) * 8);  // split-K partials
-  b += 6 * align256((size_t)n * 8);  // y, tau, d, e, zhat, D
-  b += align256((size_t)2 * n * 8) + align256((size_t)2 * n * 4);  // sort keys
-  b += 9 * align256((size_t)n * 8);  // ds zs dk zk ddef rc rs tau rho
-  b += 7 * align256((size_t)n * 4);  // colS colk coldef rp ri org cnt
+  b += 3 * align256(B * nn * 8);                    // V (Householder vectors), Qp, Uk
+  b += align256(B * n * kNB * 8);                   // Wp
+  b += 2 * align256(B * kNB * n * 8);               // Y, Y2
+  b += 2 * align256(B * kNB * kNB * 8);             // G, T
+  b += align256(std::max((size_t)16 * kNB * n, (size_t)64 * kNB * kNB) * 8);  // split-K partials (one matrix)
+  b += 6 * align256(B * n * 8);                     // y, tau, d, e, zhat, D
+  b += align256(B * 2 * n * 8) + align256(B * 2 * n * 4);  // sort keys
+  b += 8 * align256(B * n * 8);                     // ds zs dk zk ddef rc rs tau
+  b += 6 * align256(B * n * 4);                     // colS colk coldef rp ri org
+  b += align256(B * n * 8) + align256(B * n * 4);   // rho, cnt (per merge and matrix)
   b += 2 * align256((size_t)n * sizeof(Merge)) + align256((size_t)n * sizeof(Leaf)) + align256((size_t)n * 4);
+  b += align256((B * ((size_t)n / kLeaf + 2)) * (sizeof(GemmF64Args) + 8) + 64);  // grouped-GEMM descriptors
   return b + 4096 + 256;
 }
 
-// Eigen-decomposition of the symmetric n x n matrix A (column-major, ld n; destroyed).  Z (n x n, ld n)
-// receives the eigenvectors, evals (host) the eigenvalues in the order of Z's columns (not sorted).
-cudaError_t syevd(double* A, int n, double* Z, void* work, size_t work_bytes, std::vector<double>& evals,
-                  bool& converged, cudaStream_t stream) {
+size_t syevd_workspace_bytes(int n) { return syevd_workspace_bytes(n, 1); }
+
+// Eigen-decompositions of nmat symmetric n x n matrices A_z = A + z n^2 (column-major, ld n;
+// destroyed).  Z_z = Z + z n^2 receives the eigenvectors, evals (host, nmat x n) the eigenvalues in
+// the order of the columns (not sorted).  Every stage runs all matrices in the same launches.
+cudaError_t syevd_batched(double* A, int n, int nmat, double* Z, void* work, size_t work_bytes,
+                          std::vector<double>& evals, bool& converged, cudaStream_t stream) {
   converged = false;
-  if (n < 1) return cudaErrorInvalidValue;
-  if (work_bytes < syevd_workspace_bytes(n)) return cudaErrorInvalidValue;
+  if (n < 1 || nmat < 1) return cudaErrorInvalidValue;
+  if (work_bytes < syevd_workspace_bytes(n, nmat)) return cudaErrorInvalidValue;
   const int64_t ld = n;
-  const size_t nn = (size_t)n * n;
+  const size_t nn = (size_t)n * n, B = (size_t)nmat;
+  const int64_t ms = (int64_t)nn;  // matrix stride
   char* w = static_cast<char*>(work);
   auto take = [&](size_t bytes) {
     void* p = w;
     w += align256(bytes);
     return p;
   };
-  double* V = (double*)take(nn * 8);
-  double* Qp = (double*)take(nn * 8);
-  double* Uk = (double*)take(nn * 8);
-  double* Wp = (double*)take((size_t)n * kNB * 8);
-  double* Y = (double*)take((size_t)kNB * n * 8);
-  double* Y2 = (double*)take((size_t)kNB * n * 8);
-  double* Gm = (double*)take((size_t)kNB * kNB * 8);
-  double* Tb = (double*)take((size_t)kNB * kNB * 8);
+  double* V = (double*)take(B * nn * 8);
+  double* Qp = (double*)take(B * nn * 8);
+  double* Uk = (double*)take(B * nn * 8);
+  double* Wp = (double*)take(B * n * kNB * 8);
+  double* Y = (double*)take(B * kNB * n * 8);
+  double* Y2 = (double*)take(B * kNB * n * 8);
+  double* Gm = (double*)take(B * kNB * kNB * 8);
+  double* Tb = (double*)take(B * kNB * kNB * 8);
   double* Pk = (double*)take(std::max((size_t)16 * kNB * n, (size_t)64 * kNB * kNB) * 8);
-  double* y = (double*)take((size_t)n * 8);
-  double* tau = (double*)take((size_t)n * 8);
-  double* d = (double*)take((size_t)n * 8);
-  double* e = (double*)take((size_t)n * 8);
-  double* zhat = (double*)take((size_t)n * 8);
-  double* D = (double*)take((size_t)n * 8);
+  double* y = (double*)take(B * n * 8);
+  double* tau = (double*)take(B * n * 8);
+  double* d = (double*)take(B * n * 8);
+  double* e = (double*)take(B * n * 8);
+  double* zhat = (double*)take(B * n * 8);
+  double* D = (double*)take(B * n * 8);
   DcScratch sc;
-  sc.keys = (double*)take((size_t)2 * n * 8);
-  sc.kidx = (int*)take((size_t)2 * n * 4);
-  sc.ds = (double*)take((size_t)n * 8);
-  sc.zs = (double*)take((size_t)n * 8);
-  sc.dk = (double*)take((size_t)n * 8);
-  sc.zk = (double*)take((size_t)n * 8);
-  sc.ddef = (double*)take((size_t)n * 8);
-  sc.rc = (double*)take((size_t)n * 8);
-  sc.rs = (double*)take((size_t)n * 8);
-  sc.tau = (double*)take((size_t)n * 8);
-  sc.rho = (double*)take((size_t)n * 8);
-  sc.colS = (int*)take((size_t)n * 4);
-  sc.colk = (int*)take((size_t)n * 4);
-  sc.coldef = (int*)take((size_t)n * 4);
-  sc.rp = (int*)take((size_t)n * 4);
-  sc.ri = (int*)take((size_t)n * 4);
-  sc.org = (int*)take((size_t)n * 4);
-  sc.cnt = (int*)take((size_t)n * 4);
+  sc.keys = (double*)take(B * 2 * n * 8);
+  sc.kidx = (int*)take(B * 2 * n * 4);
+  sc.ds = (double*)take(B * n * 8);
+  sc.zs = (double*)take(B * n * 8);
+  sc.dk = (double*)take(B * n * 8);
+  sc.zk = (double*)take(B * n * 8);
+  sc.ddef = (double*)take(B * n * 8);
+  sc.rc = (double*)take(B * n * 8);
+  sc.rs = (double*)take(B * n * 8);
+  sc.tau = (double*)take(B * n * 8);
+  sc.colS = (int*)take(B * n * 4);
+  sc.colk = (int*)take(B * n * 4);
+  sc.coldef = (int*)take(B * n * 4);
+  sc.rp = (int*)take(B * n * 4);
+  sc.ri = (int*)take(B * n * 4);
+  sc.org = (int*)take(B * n * 4);
+  sc.rho = (double*)take(B * n * 8);
+  sc.cnt = (int*)take(B * n * 4);
   Merge* dMerges = (Merge*)take((size_t)n * sizeof(Merge));
   Leaf* dLeaves = (Leaf*)take((size_t)n * sizeof(Leaf));
   int* dBounds = (int*)take((size_t)n * 4);
+  const size_t desc_bytes = (B * ((size_t)n / kLeaf + 2)) * (sizeof(GemmF64Args) + 8) + 64;
+  void* dDesc = take(desc_bytes);
   int* err_dev = (int*)take(sizeof(int));
   cudaError_t err;
-#define SY_CHECK(x)                       \
-  do {                                    \
+#define SY_CHECK(x)                             \
+  do {                                          \
     if ((err = (x)) != cudaSuccess) return err; \
   } while (0)
+  auto batched = [&](GemmF64Args g, int64_t sA, int64_t sB, int64_t sC) {
+    g.batch = nmat;
+    g.sA = sA;
+    g.sB = sB;
+    g.sC = sC;
+    return g;
+  };
 
-  // ---- stage 1: tridiagonal reduction
+  // ---- stage 1: tridiagonal reduction (one 8-CTA cluster per matrix per column step)
   for (int p = 0; p <= n - 2; p += kNB) {
     const int nb = std::min(kNB, n - 1 - p);
-    house_kernel<<<kCS, kCT, 0, stream>>>(A, n, V, Wp, p, -1, 0, y, tau, d, e);
+    house_kernel<<<kCS * nmat, kCT, 0, stream>>>(A, n, ms, V, Wp, p, -1, 0, y, tau, d, e);
     ++g_launches;
     for (int i = 0; i < nb; ++i) {
       const int j = p + i;
       const int m = n - 1 - j;
-      trailing_gemv_kernel<<<(m + 7) / 8, 256, 0, stream>>>(A, n, V + ld * j, j, y);
+      trailing_gemv_kernel<<<dim3((m + 7) / 8, nmat), 256, 0, stream>>>(A, n, ms, V + ld * j, j, y);
       ++g_launches;
-      house_kernel<<<kCS, kCT, 0, stream>>>(A, n, V, Wp, p, i, i + 1 < nb ? i + 1 : -1, y, tau, d, e);
+      house_kernel<<<kCS * nmat, kCT, 0, stream>>>(A, n, ms, V, Wp, p, i, i + 1 < nb ? i + 1 : -1, y, tau, d, e);
       ++g_launches;
     }
     SY_CHECK(cudaGetLastError());
@@ -731,18 +829,21 @@ cudaError_t syevd(double* A, int n, double* Z, void* work, size_t work_bytes, st
     if (pe < n) {
       const int mt = n - pe;
       // A(pe:, pe:) -= V W^T + W V^T   (panel columns p..p+nb-1)
-      SY_CHECK(launch_gemm_f64(gemm_args(mt, mt, nb, V + pe + ld * p, 1, ld, Wp + pe, ld, 1, A + pe + ld * pe, ld,
-                                         -1.0, 1.0),
+      SY_CHECK(launch_gemm_f64(batched(gemm_args(mt, mt, nb, V + pe + ld * p, 1, ld, Wp + pe, ld, 1, A + pe + ld * pe,
+                                                 ld, -1.0, 1.0),
+                                       ms, (int64_t)n * kNB, ms),
                                stream));
-      SY_CHECK(launch_gemm_f64(gemm_args(mt, mt, nb, Wp + pe, 1, ld, V + pe + ld * p, ld, 1, A + pe + ld * pe, ld,
-                                         -1.0, 1.0),
+      SY_CHECK(launch_gemm_f64(batched(gemm_args(mt, mt, nb, Wp + pe, 1, ld, V + pe + ld * p, ld, 1, A + pe + ld * pe,
+                                                 ld, -1.0, 1.0),
+                                       (int64_t)n * kNB, ms, ms),
                                stream));
     }
   }
-  SY_CHECK(cudaMemcpyAsync(d + (n - 1), A + (n - 1) + ld * (n - 1), 8, cudaMemcpyDeviceToDevice, stream));
+  SY_CHECK(cudaMemcpy2DAsync(d + (n - 1), (size_t)n * 8, A + (n - 1) + ld * (n - 1), nn * 8, 8, B,
+                             cudaMemcpyDeviceToDevice, stream));
 
-  // ---- stage 2: divide and conquer on (d, e)
-  SY_CHECK(cudaMemsetAsync(Z, 0, nn * 8, stream));
+  // ---- stage 2: divide and conquer on (d, e), the same tree for every matrix
+  SY_CHECK(cudaMemsetAsync(Z, 0, B * nn * 8, stream));
   SY_CHECK(cudaMemsetAsync(err_dev, 0, sizeof(int), stream));
   std::vector<Node> nodes;
   build_tree(0, n, 0, nodes);
@@ -762,49 +863,51 @@ cudaError_t syevd(double* A, int n, double* Z, void* work, size_t work_bytes, st
   }
   if (!bounds.empty()) {
     SY_CHECK(cudaMemcpyAsync(dBounds, bounds.data(), bounds.size() * 4, cudaMemcpyHostToDevice, stream));
-    tear_kernel<<<(unsigned)((bounds.size() + 255) / 256), 256, 0, stream>>>(d, e, dBounds, (int)bounds.size());
+    const int64_t tot = (int64_t)bounds.size() * nmat;
+    tear_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, stream>>>(d, e, dBounds, (int)bounds.size(), n, nmat);
     ++g_launches;
   }
   SY_CHECK(cudaMemcpyAsync(dLeaves, leaves.data(), leaves.size() * sizeof(Leaf), cudaMemcpyHostToDevice, stream));
-  leaf_jacobi_kernel<<<(unsigned)leaves.size(), 32, 0, stream>>>(dLeaves, d, e, D, Z, ld, err_dev);
+  leaf_jacobi_kernel<<<dim3((unsigned)leaves.size(), nmat), 32, 0, stream>>>(dLeaves, d, e, D, Z, ld, err_dev, n, ms);
   ++g_launches;
   SY_CHECK(cudaGetLastError());
   std::vector<int> cnt;
   for (int depth = maxdepth; depth >= 0; --depth) {
-    std::vector<Merge>& ms = levels[depth];
-    if (ms.empty()) continue;
+    std::vector<Merge>& mv = levels[depth];
+    if (mv.empty()) continue;
     int64_t off = 0;
     int nmax = 0;
-    for (Merge& m : ms) {
+    for (Merge& m : mv) {
       const int nm = m.n1 + m.n2;
       m.qp_off = off;
       m.uk_off = off;
       off += (int64_t)nm * nm;
       nmax = std::max(nmax, nm);
     }
-    const int nm_ = (int)ms.size();
-    SY_CHECK(cudaMemcpyAsync(dMerges, ms.data(), ms.size() * sizeof(Merge), cudaMemcpyHostToDevice, stream));
-    merge_prepare_kernel<<<nm_, 1024, 0, stream>>>(dMerges, D, Z, ld, e, sc);
-    merge_gather_kernel<<<dim3((nmax + 127) / 128, nm_), 128, 0, stream>>>(dMerges, Z, ld, Qp, sc);
-    secular_kernel<<<dim3((nmax + 7) / 8, nm_), 256, 0, stream>>>(dMerges, sc);
-    lowner_kernel<<<dim3((nmax + 127) / 128, nm_), 128, 0, stream>>>(dMerges, sc, zhat);
-    merge_vectors_kernel<<<dim3(nmax, nm_), 256, 0, stream>>>(dMerges, sc, zhat, Uk, D);
-    g_launches += 5;
+    const int nm_ = (int)mv.size();
+    SY_CHECK(cudaMemcpyAsync(dMerges, mv.data(), mv.size() * sizeof(Merge), cudaMemcpyHostToDevice, stream));
+    merge_prepare_kernel<<<dim3(nm_, nmat), 1024, 0, stream>>>(dMerges, D, Z, ld, e, sc, n, ms, nm_);
+    merge_gather_kernel<<<dim3((nmax + 127) / 128, nm_, nmat), 128, 0, stream>>>(dMerges, Z, ld, Qp, sc, n, ms, nm_);
+    secular_kernel<<<dim3((nmax + 7) / 8, nm_, nmat), 256, 0, stream>>>(dMerges, sc, n, nm_);
+    lowner_kernel<<<dim3((nmax + 127) / 128, nm_, nmat), 128, 0, stream>>>(dMerges, sc, zhat, n, nm_);
+    merge_vectors_kernel<<<dim3(nmax, nm_, nmat), 256, 0, stream>>>(dMerges, sc, zhat, Uk, D, n, ms, nm_);
+    copy_deflated_kernel<<<dim3((unsigned)std::min<int64_t>(((int64_t)nmax * nmax + 255) / 256, 1024), nm_, nmat), 256,
+                           0, stream>>>(dMerges, Qp, Z, ld, sc.cnt, ms, nm_);
+    g_launches += 6;
     SY_CHECK(cudaGetLastError());
-    cnt.resize(2 * ms.size());
+    cnt.resize(2 * (size_t)nm_ * nmat);
     SY_CHECK(cudaMemcpyAsync(cnt.data(), sc.cnt, cnt.size() * 4, cudaMemcpyDeviceToHost, stream));
-    SY_CHECK(cudaStreamSynchronize(stream));  // ms and cnt must outlive their copies
-    for (int q = 0; q < nm_; ++q) {
-      const Merge& m = ms[q];
-      const int nm = m.n1 + m.n2, k = cnt[2 * q];
-      double* blk = Z + m.s + ld * m.s;
-      if (k > 0)
-        SY_CHECK(launch_gemm_f64(gemm_args(nm, k, k, Qp + m.qp_off, 1, nm, Uk + m.uk_off, 1, k, blk, ld, 1.0, 0.0),
-                                 stream));
-      if (k < nm)
-        SY_CHECK(cudaMemcpy2DAsync(blk + ld * k, (size_t)ld * 8, Qp + m.qp_off + (int64_t)nm * k, (size_t)nm * 8,
-                                   (size_t)nm * 8, (size_t)(nm - k), cudaMemcpyDeviceToDevice, stream));
-    }
+    SY_CHECK(cudaStreamSynchronize(stream));  // mv and cnt must outlive their copies
+    std::vector<GemmF64Args> probs;
+    for (int z = 0; z < nmat; ++z)
+      for (int q = 0; q < nm_; ++q) {
+        const Merge& m = mv[q];
+        const int nm = m.n1 + m.n2, k = cnt[2 * ((size_t)q + (size_t)nm_ * z)];
+        if (k > 0)
+          probs.push_back(gemm_args(nm, k, k, Qp + ms * z + m.qp_off, 1, nm, Uk + ms * z + m.uk_off, 1, k,
+                                    Z + ms * z + m.s + ld * m.s, ld, 1.0, 0.0));
+      }
+    SY_CHECK(launch_gemm_f64_grouped(probs, dDesc, desc_bytes, stream));
   }
 
   // ---- stage 3: Z <- Q_H Z, panels in reverse order
@@ -813,29 +916,43 @@ cudaError_t syevd(double* A, int n, double* Z, void* work, size_t work_bytes, st
     const int nb = std::min(kNB, n - 1 - p);
     const int mr = n - 1 - p;  // rows p+1 .. n-1
     const double* Vb = V + (p + 1) + ld * p;
-    // G = V_b^T V_b and Y = V_b^T Z have few output tiles and K = mr: split K
     GemmF64Args gg = gemm_args(nb, nb, mr, Vb, ld, 1, Vb, 1, ld, Gm, kNB, 1.0, 0.0);
-    gg.splitk = std::max(1, std::min(64, mr / 256));
-    gg.work = Pk;
-    SY_CHECK(launch_gemm_f64(gg, stream));
-    build_t_kernel<<<1, 32, 0, stream>>>(Gm, tau + p, nb, Tb);
-    ++g_launches;
     GemmF64Args gy = gemm_args(nb, n, mr, Vb, ld, 1, Z + (p + 1), 1, ld, Y, kNB, 1.0, 0.0);
-    const int ytiles = (n + 63) / 64;  // about 600 CTA slots (148 SMs x 4), K chunks >= 256
-    gy.splitk = std::max(1, std::min(16, std::min(mr / 256, 600 / ytiles)));
-    gy.work = Pk;
+    if (nmat == 1) {
+      // G = V_b^T V_b and Y = V_b^T Z have few output tiles and K = mr: split K
+      gg.splitk = std::max(1, std::min(64, mr / 256));
+      gg.work = Pk;
+      const int ytiles = (n + 63) / 64;  // about 600 CTA slots (148 SMs x 4), K chunks >= 256
+      gy.splitk = std::max(1, std::min(16, std::min(mr / 256, 600 / ytiles)));
+      gy.work = Pk;
+    } else {
+      gg = batched(gg, ms, ms, (int64_t)kNB * kNB);
+      gy = batched(gy, ms, ms, (int64_t)kNB * n);
+    }
+    SY_CHECK(launch_gemm_f64(gg, stream));
+    build_t_kernel<<<nmat, 32, 0, stream>>>(Gm, tau + p, nb, Tb, n);
+    ++g_launches;
     SY_CHECK(launch_gemm_f64(gy, stream));
-    SY_CHECK(launch_gemm_f64(gemm_args(nb, n, nb, Tb, 1, kNB, Y, 1, kNB, Y2, kNB, 1.0, 0.0), stream));
-    SY_CHECK(launch_gemm_f64(gemm_args(mr, n, nb, Vb, 1, ld, Y2, 1, kNB, Z + (p + 1), ld, -1.0, 1.0), stream));
+    SY_CHECK(launch_gemm_f64(batched(gemm_args(nb, n, nb, Tb, 1, kNB, Y, 1, kNB, Y2, kNB, 1.0, 0.0),
+                                     (int64_t)kNB * kNB, (int64_t)kNB * n, (int64_t)kNB * n),
+                             stream));
+    SY_CHECK(launch_gemm_f64(batched(gemm_args(mr, n, nb, Vb, 1, ld, Y2, 1, kNB, Z + (p + 1), ld, -1.0, 1.0), ms,
+                                     (int64_t)kNB * n, ms),
+                             stream));
   }
-  evals.resize(n);
-  SY_CHECK(cudaMemcpyAsync(evals.data(), D, (size_t)n * 8, cudaMemcpyDeviceToHost, stream));
+  evals.resize(B * n);
+  SY_CHECK(cudaMemcpyAsync(evals.data(), D, B * n * 8, cudaMemcpyDeviceToHost, stream));
   int herr = 0;
   SY_CHECK(cudaMemcpyAsync(&herr, err_dev, sizeof(int), cudaMemcpyDeviceToHost, stream));
   SY_CHECK(cudaStreamSynchronize(stream));
   converged = (herr == 0);  // a leaf's Jacobi iteration can fail to converge
   return cudaSuccess;
 #undef SY_CHECK
+}
+
+cudaError_t syevd(double* A, int n, double* Z, void* work, size_t work_bytes, std::vector<double>& evals,
+                  bool& converged, cudaStream_t stream) {
+  return syevd_batched(A, n, 1, Z, work, work_bytes, evals, converged, stream);
 }
 
 }  // namespace rpa

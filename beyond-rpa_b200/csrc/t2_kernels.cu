@@ -4,6 +4,8 @@
 //     factors of rpa_CC_IM_v5 come from the Cholesky factors of the energy);
 //   * guess-vector generation, column normalisation (rpa_CC_NormalizeColumns,
 //     rpa_CC_Doubles.f90:80-91), scalings, gathers and column norms.
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace rpa {
@@ -281,6 +283,15 @@ __global__ void lyap_scale_kernel(double* Y, const double* mu, int n, int* bad) 
   Y[idx] /= den;
 }
 
+// dst column map[2c+1] = src column map[2c] (columns of `rows` doubles, contiguous), c < ncols.
+__global__ void copy_columns_kernel(const double* src, double* dst, const int64_t* map, int64_t ncols, int rows) {
+  const int64_t c = blockIdx.y * (int64_t)gridDim.x + blockIdx.x;
+  if (c >= ncols) return;
+  const double* s = src + map[2 * c] * rows;
+  double* d = dst + map[2 * c + 1] * rows;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) d[r] = s[r];
+}
+
 // C = A o B (element-wise, rows x cols, column-major)
 __global__ void hadamard_kernel(const double* A, int64_t lda, const double* B, int64_t ldb, int rows, int cols,
                                 double* C, int64_t ldc) {
@@ -439,6 +450,16 @@ cudaError_t launch_grad_accum(const double* R, int64_t ldR, const double* Y, int
 cudaError_t launch_replicate(const double* R, int64_t ldR, int NQ, int64_t nov, double* Y, int64_t ldy, int64_t sY,
                              int nb, cudaStream_t stream) {
   replicate_kernel<<<blocks_for((int64_t)NQ * nov), 256, 0, stream>>>(R, ldR, NQ, nov, Y, ldy, sY, nb);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_copy_columns(const double* src, double* dst, const int64_t* map, int64_t ncols, int rows,
+                                cudaStream_t stream) {
+  if (ncols <= 0) return cudaSuccess;
+  const unsigned gx = (unsigned)std::min<int64_t>(ncols, 65535);
+  const unsigned gy = (unsigned)((ncols + gx - 1) / gx);
+  copy_columns_kernel<<<dim3(gx, gy), 128, 0, stream>>>(src, dst, map, ncols, rows);
   ++g_launches;
   return cudaGetLastError();
 }
