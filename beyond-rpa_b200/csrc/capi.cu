@@ -47,6 +47,7 @@ struct rpa_b200_handle {
   DevBuf jU, jL, jX, jPno, jWork;      // particle-hole corrections: localised T2 vectors, PNOs, scratch
   DevBuf jPack, jQS, jS, jD;           // per-orbital PNO packs, QS slots, S blocks, grouped-GEMM descriptors
   DevBuf jT, jM, jV, jMap;             // batched PNO stage: T_ij, T T^T, eigenvectors, column map
+  DevBuf jSK;                          // split-K partials of the G products
   struct BatchGraph {
     uint64_t key;
     std::vector<cudaGraphExec_t> execs;
@@ -772,7 +773,7 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
                     &h->xM, &h->eW, &h->eA, &h->eZ, &h->thZ, &h->thXa, &h->thXi, &h->thYX, &h->thR,
                     &h->jU, &h->jL, &h->jX, &h->jPno, &h->jWork,
                     &h->jPack, &h->jQS, &h->jS, &h->jD, &h->syncBuf,
-                    &h->jT, &h->jM, &h->jV, &h->jMap})
+                    &h->jT, &h->jM, &h->jV, &h->jMap, &h->jSK})
     release(*b);
   for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
   if (h->err_dev) cudaFree(h->err_dev);
@@ -1924,6 +1925,7 @@ int rpa_b200_jctc2024(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOc
                                     cudaMemcpyDeviceToDevice, h->stream));
     }
   RPA_CUDA(h, ensure(h->jQS, (size_t)nv * maxcol * 2 * 8));
+  RPA_CUDA(h, ensure(h->jSK, (size_t)64 * nvv * 8));
   RPA_CUDA(h, ensure(h->jS, (size_t)4 * no * std::max<int64_t>(max_n * max_n, 1) * 8));
   RPA_CUDA(h, ensure(h->jD, (size_t)(8 * no + 8) * sizeof(rpa::GemmF64Args) + (size_t)(8 * no + 16) * sizeof(int)));
 
@@ -1931,6 +1933,98 @@ int rpa_b200_jctc2024(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOc
   const double c2b = -2.0, c2c = -2.0, c2d = 2.0, c2g = -4.0, c2h = -4.0, c2i = 2.0, c2j = 2.0;
   auto slot = [&](int64_t pair, int term) { return part + (size_t)(5 * pair + term) * rpa::kDotPartials; };
   auto G = [&](const rpa::GemmF64Args& g) { return rpa::launch_gemm_f64(g, h->stream); };
+  // grouped-GEMM descriptors of every pair, built once and uploaded in one copy: the k sum of a
+  // pair is one grouped launch for its S blocks and two for its QS slots
+  struct GroupRef {
+    int64_t desc, start;
+    int nprob, ntiles;
+    bool am, bn;
+  };
+  std::vector<rpa::GemmF64Args> all_desc;
+  std::vector<int> all_start;
+  std::vector<GroupRef> groups;
+  {
+    double* QSg = static_cast<double*>(h->jQS.p);
+    double* QSb = QSg + (size_t)nv * maxcol;
+    double* Sbase = static_cast<double*>(h->jS.p);
+    auto add_group = [&](const std::vector<rpa::GemmF64Args>& v) {
+      GroupRef gr{(int64_t)all_desc.size(), (int64_t)all_start.size(), (int)v.size(), 0, true, true};
+      if (!v.empty()) {
+        gr.am = (v[0].a_m == 1);
+        gr.bn = (v[0].b_n == 1);
+      }
+      all_start.push_back(0);
+      for (const auto& g : v) {
+        all_desc.push_back(g);
+        gr.ntiles += rpa::gemm_f64_tiles(g);
+        all_start.push_back(gr.ntiles);
+      }
+      groups.push_back(gr);
+    };
+    for (int j = 0; j < no; ++j)
+      for (int i = j; i < no; ++i) {
+        std::vector<rpa::GemmF64Args> sp, q1, q2;
+        size_t soff = 0;
+        const double* pj = pack + (size_t)nv * pack_off[j];
+        const double* pi_ = pack + (size_t)nv * pack_off[i];
+        for (int k = 0; k < no; ++k) {
+          const int nkj = pn[(size_t)k + (size_t)no * j], nki = pn[(size_t)k + (size_t)no * i];
+          if (nkj == 0 || nki == 0) continue;
+          const double* kj[2] = {pj + (size_t)nv * kcol[(size_t)j * no + k], nullptr};
+          kj[1] = kj[0] + (size_t)nv * nkj;
+          const double* ki[2] = {pi_ + (size_t)nv * kcol[(size_t)i * no + k], nullptr};
+          ki[1] = ki[0] + (size_t)nv * nki;
+          int Pki, Qki, Pik, Qik, Pkj, Qkj, Pjk, Qjk;
+          if (k >= i) { Pki = 0; Qki = 1; Pik = 1; Qik = 0; } else { Pki = 1; Qki = 0; Pik = 0; Qik = 1; }
+          if (k >= j) { Pkj = 0; Qkj = 1; Pjk = 1; Qjk = 0; } else { Pkj = 1; Qkj = 0; Pjk = 0; Qjk = 1; }
+          double* S_jk_ki = Sbase + soff;
+          double* S_jk_ik = S_jk_ki + (size_t)nkj * nki;
+          double* S_kj_ki = S_jk_ik + (size_t)nkj * nki;
+          double* S_kj_ik = S_kj_ki + (size_t)nkj * nki;
+          soff += 4 * (size_t)nkj * nki;
+          sp.push_back(gemm_g(nkj, nki, nv, kj[Qjk], nv, true, ki[Pki], nv, false, S_jk_ki, nkj));
+          sp.push_back(gemm_g(nkj, nki, nv, kj[Qjk], nv, true, ki[Pik], nv, false, S_jk_ik, nkj));
+          sp.push_back(gemm_g(nkj, nki, nv, kj[Qkj], nv, true, ki[Pki], nv, false, S_kj_ki, nkj));
+          sp.push_back(gemm_g(nkj, nki, nv, kj[Qkj], nv, true, ki[Pik], nv, false, S_kj_ik, nkj));
+          const size_t c0 = (size_t)kcol[(size_t)j * no + k];
+          double* qg[2] = {QSg + (size_t)nv * c0, QSg + (size_t)nv * (c0 + nkj)};
+          double* qb[2] = {QSb + (size_t)nv * c0, QSb + (size_t)nv * (c0 + nkj)};
+          // alpha ki[q] S^T (+ beta slot)
+          auto qs = [&](double* dst, int q, const double* S, double alpha, double beta) {
+            return gemm_g(nv, nkj, nki, ki[q], nv, false, S, nkj, true, dst, nv, alpha, beta);
+          };
+          if (i != j) {
+            q1.push_back(qs(qg[Pjk], Qki, S_jk_ki, 2.0 * c2g, 0.0));
+            q2.push_back(qs(qg[Pjk], Qik, S_jk_ik, c2i + c2j, 1.0));
+            q1.push_back(qs(qg[Pkj], Qik, S_kj_ik, 2.0 * c2h, 0.0));
+            q2.push_back(qs(qg[Pkj], Qki, S_kj_ki, c2i + c2j, 1.0));
+            q1.push_back(qs(qb[Pkj], Qik, S_kj_ik, 2.0 * c2d, 0.0));
+            q2.push_back(qs(qb[Pkj], Qki, S_kj_ki, c2b + c2c, 1.0));
+            q1.push_back(qs(qb[Pjk], Qik, S_jk_ik, c2b + c2c, 0.0));
+          } else {
+            q1.push_back(qs(qg[Pjk], Qki, S_jk_ki, c2g, 0.0));
+            q2.push_back(qs(qg[Pjk], Qik, S_jk_ik, c2i + c2j, 1.0));
+            q1.push_back(qs(qg[Pkj], Qik, S_kj_ik, c2h, 0.0));
+            q1.push_back(qs(qb[Pkj], Qik, S_kj_ik, c2d, 0.0));  // the other slot of 2b..2d stays zero
+            q2.push_back(qs(qb[Pkj], Qki, S_kj_ki, c2b + c2c, 1.0));
+          }
+        }
+
+        add_group(sp);
+        add_group(q1);
+        add_group(q2);
+      }
+  }
+  RPA_CUDA(h, ensure(h->jD, std::max<size_t>(all_desc.size(), 1) * sizeof(rpa::GemmF64Args) +
+                                std::max<size_t>(all_start.size(), 1) * sizeof(int) + 256));
+  rpa::GemmF64Args* dprob = static_cast<rpa::GemmF64Args*>(h->jD.p);
+  int* dstart = reinterpret_cast<int*>(static_cast<char*>(h->jD.p) +
+                                       ((std::max<size_t>(all_desc.size(), 1) * sizeof(rpa::GemmF64Args) + 255) & ~(size_t)255));
+  if (!all_desc.empty())
+    RPA_CUDA(h, cudaMemcpyAsync(dprob, all_desc.data(), all_desc.size() * sizeof(rpa::GemmF64Args),
+                                cudaMemcpyHostToDevice, h->stream));
+  RPA_CUDA(h, cudaMemcpyAsync(dstart, all_start.data(), all_start.size() * sizeof(int), cudaMemcpyHostToDevice,
+                              h->stream));
   int64_t pair = 0;
   std::vector<std::pair<int, int>> pair_ij;
   for (int j = 0; j < no; ++j) {
@@ -1966,63 +2060,23 @@ int rpa_b200_jctc2024(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOc
       // G(ba; ji) for 2g..2j and G(bj; ai) for 2b..2d: the k sum becomes one GEMM over the
       // packed PNO blocks of orbital j against per-k QS slots (zero where a pair has no PNOs)
       const int ncj = ncol[j];
+      const double* pj = pack + (size_t)nv * pack_off[j];
       double* QSg = static_cast<double*>(h->jQS.p);
       double* QSb = QSg + (size_t)nv * maxcol;
       RPA_CUDA(h, cudaMemsetAsync(QSg, 0, (size_t)nv * maxcol * 2 * 8, h->stream));
-      std::vector<rpa::GemmF64Args> sp, q1, q2;
-      double* Sbase = static_cast<double*>(h->jS.p);
-      size_t soff = 0;
-      const double* pj = pack + (size_t)nv * pack_off[j];
-      const double* pi_ = pack + (size_t)nv * pack_off[i];
-      for (int k = 0; k < no; ++k) {
-        const int nkj = pn[(size_t)k + (size_t)no * j], nki = pn[(size_t)k + (size_t)no * i];
-        if (nkj == 0 || nki == 0) continue;
-        const double* kj[2] = {pj + (size_t)nv * kcol[(size_t)j * no + k], nullptr};
-        kj[1] = kj[0] + (size_t)nv * nkj;
-        const double* ki[2] = {pi_ + (size_t)nv * kcol[(size_t)i * no + k], nullptr};
-        ki[1] = ki[0] + (size_t)nv * nki;
-        int Pki, Qki, Pik, Qik, Pkj, Qkj, Pjk, Qjk;
-        if (k >= i) { Pki = 0; Qki = 1; Pik = 1; Qik = 0; } else { Pki = 1; Qki = 0; Pik = 0; Qik = 1; }
-        if (k >= j) { Pkj = 0; Qkj = 1; Pjk = 1; Qjk = 0; } else { Pkj = 1; Qkj = 0; Pjk = 0; Qjk = 1; }
-        double* S_jk_ki = Sbase + soff;
-        double* S_jk_ik = S_jk_ki + (size_t)nkj * nki;
-        double* S_kj_ki = S_jk_ik + (size_t)nkj * nki;
-        double* S_kj_ik = S_kj_ki + (size_t)nkj * nki;
-        soff += 4 * (size_t)nkj * nki;
-        sp.push_back(gemm_g(nkj, nki, nv, kj[Qjk], nv, true, ki[Pki], nv, false, S_jk_ki, nkj));
-        sp.push_back(gemm_g(nkj, nki, nv, kj[Qjk], nv, true, ki[Pik], nv, false, S_jk_ik, nkj));
-        sp.push_back(gemm_g(nkj, nki, nv, kj[Qkj], nv, true, ki[Pki], nv, false, S_kj_ki, nkj));
-        sp.push_back(gemm_g(nkj, nki, nv, kj[Qkj], nv, true, ki[Pik], nv, false, S_kj_ik, nkj));
-        const size_t c0 = (size_t)kcol[(size_t)j * no + k];
-        double* qg[2] = {QSg + (size_t)nv * c0, QSg + (size_t)nv * (c0 + nkj)};
-        double* qb[2] = {QSb + (size_t)nv * c0, QSb + (size_t)nv * (c0 + nkj)};
-        // alpha ki[q] S^T (+ beta slot)
-        auto qs = [&](double* dst, int q, const double* S, double alpha, double beta) {
-          return gemm_g(nv, nkj, nki, ki[q], nv, false, S, nkj, true, dst, nv, alpha, beta);
-        };
-        if (i != j) {
-          q1.push_back(qs(qg[Pjk], Qki, S_jk_ki, 2.0 * c2g, 0.0));
-          q2.push_back(qs(qg[Pjk], Qik, S_jk_ik, c2i + c2j, 1.0));
-          q1.push_back(qs(qg[Pkj], Qik, S_kj_ik, 2.0 * c2h, 0.0));
-          q2.push_back(qs(qg[Pkj], Qki, S_kj_ki, c2i + c2j, 1.0));
-          q1.push_back(qs(qb[Pkj], Qik, S_kj_ik, 2.0 * c2d, 0.0));
-          q2.push_back(qs(qb[Pkj], Qki, S_kj_ki, c2b + c2c, 1.0));
-          q1.push_back(qs(qb[Pjk], Qik, S_jk_ik, c2b + c2c, 0.0));
-        } else {
-          q1.push_back(qs(qg[Pjk], Qki, S_jk_ki, c2g, 0.0));
-          q2.push_back(qs(qg[Pjk], Qik, S_jk_ik, c2i + c2j, 1.0));
-          q1.push_back(qs(qg[Pkj], Qik, S_kj_ik, c2h, 0.0));
-          q1.push_back(qs(qb[Pkj], Qik, S_kj_ik, c2d, 0.0));  // the other slot of 2b..2d stays zero
-          q2.push_back(qs(qb[Pkj], Qki, S_kj_ki, c2b + c2c, 1.0));
-        }
+      for (int gi = 0; gi < 3; ++gi) {
+        const GroupRef& gr = groups[(size_t)3 * pair + gi];
+        RPA_CUDA(h, rpa::launch_gemm_f64_grouped_dev(dprob + gr.desc, dstart + gr.start, gr.nprob, gr.ntiles,
+                                                     gr.am, gr.bn, h->stream));
       }
-      if (!sp.empty()) {
-        RPA_CUDA(h, rpa::launch_gemm_f64_grouped(sp, h->jD.p, h->jD.bytes, h->stream));
-        RPA_CUDA(h, rpa::launch_gemm_f64_grouped(q1, h->jD.p, h->jD.bytes, h->stream));
-        RPA_CUDA(h, rpa::launch_gemm_f64_grouped(q2, h->jD.p, h->jD.bytes, h->stream));
+      // the G products have few output tiles and K = sum_k 2 Nkj: split K (about 600 CTA slots)
+      for (int t = 0; t < 2; ++t) {
+        rpa::GemmF64Args gk = gemm_g(nv, nv, ncj, pj, nv, false, t == 0 ? QSg : QSb, nv, true, t == 0 ? Gg : Gb, nv,
+                                     1.0, 0.0);
+        gk.splitk = std::max(1, std::min({64, ncj / 256, 600 / std::max(1, rpa::gemm_f64_tiles(gk))}));
+        gk.work = static_cast<double*>(h->jSK.p);
+        RPA_CUDA(h, G(gk));
       }
-      RPA_CUDA(h, G(gemm_g(nv, nv, ncj, pj, nv, false, QSg, nv, true, Gg, nv, 1.0, 0.0)));
-      RPA_CUDA(h, G(gemm_g(nv, nv, ncj, pj, nv, false, QSb, nv, true, Gb, nv, 1.0, 0.0)));
       // Tr V G: sum_ga Y(g,a) ZXX(g) (Y G)(g,a)  and  sum_ga (ZYX G)(g,a) X(g,i) Y(g,a)
       rpa::GemmF64Args gg = gemm_g(ng, nv, nv, Yd, ldy, false, Gg, nv, false, Wg, ng);
       gg.rowscale = zg;

@@ -271,6 +271,22 @@ cudaError_t launch_gemm_f64_grouped(const std::vector<GemmF64Args>& probs, void*
   return e;
 }
 
+cudaError_t launch_gemm_f64_grouped_dev(const GemmF64Args* probs_dev, const int* tile_start_dev, int nprob,
+                                        int ntiles, bool a_m_unit, bool b_n_unit, cudaStream_t stream) {
+  if (nprob <= 0 || ntiles <= 0) return cudaSuccess;
+  cudaError_t e;
+  if (a_m_unit) e = b_n_unit ? launch_grouped_variant<true, true>(probs_dev, tile_start_dev, nprob, ntiles, stream)
+                             : launch_grouped_variant<true, false>(probs_dev, tile_start_dev, nprob, ntiles, stream);
+  else e = b_n_unit ? launch_grouped_variant<false, true>(probs_dev, tile_start_dev, nprob, ntiles, stream)
+                    : launch_grouped_variant<false, false>(probs_dev, tile_start_dev, nprob, ntiles, stream);
+  ++g_launches;
+  return e;
+}
+
+int gemm_f64_tiles(const GemmF64Args& g) {
+  return (g.M > 0 && g.N > 0) ? ((g.M + BM - 1) / BM) * ((g.N + BM - 1) / BM) : 0;
+}
+
 cudaError_t launch_gemm_f64(const GemmF64Args& g, cudaStream_t stream) {
   if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return cudaSuccess;
   if (g.splitk > 1 && (g.batch != 1 || !g.work)) return cudaErrorInvalidValue;

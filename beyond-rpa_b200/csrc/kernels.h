@@ -188,6 +188,11 @@ cudaError_t launch_gemm_f64(const GemmF64Args& g, cudaStream_t stream);
 // are uploaded (stream-ordered) into dev_buf (probs.size() * sizeof(GemmF64Args) + 4 (n + 1) bytes).
 cudaError_t launch_gemm_f64_grouped(const std::vector<GemmF64Args>& probs, void* dev_buf, size_t dev_bytes,
                                     cudaStream_t stream);
+// The same with descriptors already on the device: tile_start_dev holds the nprob + 1 prefix sums
+// of gemm_f64_tiles (ntiles = the last); a_m_unit / b_n_unit pick the load mapping.
+cudaError_t launch_gemm_f64_grouped_dev(const GemmF64Args* probs_dev, const int* tile_start_dev, int nprob,
+                                        int ntiles, bool a_m_unit, bool b_n_unit, cudaStream_t stream);
+int gemm_f64_tiles(const GemmF64Args& g);
 
 // ---------------------------------------------------------------- T2 chain
 // Batched forward substitution L_b X_b = B_b in place (L lower, column-major).
