@@ -2167,8 +2167,25 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
     }
     RPA_CUDA(h, cudaMemcpyAsync(h->D.p, Dh.data(), total_nov * 8, cudaMemcpyHostToDevice, h->stream));
     RPA_CUDA(h, cudaMemsetAsync(h->count_dev, 0, sizeof(int), h->stream));
-    for (int i = 0; i < n; ++i)
-      RPA_CUDA(h, rpa::launch_count_nonfinite(Rd[i], ldR[i] * (v[i].nov - 1) + v[i].NQ, h->count_dev, h->stream));
+    {  // one screening launch for every instance
+      std::vector<const double*> ptrs(n);
+      std::vector<int64_t> lens(n);
+      int64_t longest = 0;
+      for (int i = 0; i < n; ++i) {
+        ptrs[i] = Rd[i];
+        lens[i] = ldR[i] * (v[i].nov - 1) + v[i].NQ;
+        longest = std::max(longest, lens[i]);
+      }
+      RPA_CUDA(h, ensure(h->bRes, (size_t)n * 16 + 64));
+      char* scr = static_cast<char*>(h->bRes.p);
+      RPA_CUDA(h, cudaMemcpyAsync(scr, ptrs.data(), (size_t)n * 8, cudaMemcpyHostToDevice, h->stream));
+      RPA_CUDA(h, cudaMemcpyAsync(scr + (size_t)n * 8, lens.data(), (size_t)n * 8, cudaMemcpyHostToDevice, h->stream));
+      const int per = (int)std::min<int64_t>(1024, std::max<int64_t>(1, (longest + 256 * 8 - 1) / (256 * 8)));
+      RPA_CUDA(h, rpa::launch_count_nonfinite_multi(reinterpret_cast<const double* const*>(scr),
+                                                    reinterpret_cast<const int64_t*>(scr + (size_t)n * 8), n, per,
+                                                    h->count_dev, h->stream));
+      RPA_CUDA(h, cudaStreamSynchronize(h->stream));  // ptrs and lens must outlive their copies
+    }
     int cnt = 0;
     RPA_CUDA(h, cudaMemcpyAsync(&cnt, h->count_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     RPA_CUDA(h, cudaStreamSynchronize(h->stream));  // Dh must outlive its copy
@@ -2250,12 +2267,29 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
   RPA_CUDA(h, ensure(h->bDesc, desc_off.back() + 256));
   RPA_CUDA(h, ensure(h->bRes, res_off.back() * 8 + 256));
 
+  // wave-milestone counters of every batch's multi-instance SYRK, allocated once for the call
+  std::vector<int64_t> sync_off(batches.size() + 1, 0);
+  std::vector<int> sync_max_chunks(batches.size(), 0);
+  for (size_t b = 0; b < batches.size(); ++b) {
+    size_t nu = 0;
+    int mc = 0;
+    for (int i = batches[b].first; i < batches[b].second; ++i) {
+      nu += (size_t)v[i].K * rpa::syrk_tc_blocks(v[i].NQ);
+      mc = std::max(mc, (int)((v[i].nov + rpa::kSyrkTcTK - 1) / rpa::kSyrkTcTK));
+    }
+    sync_max_chunks[b] = mc;
+    const int64_t words =
+        prec == RPA_PREC_SPLIT_BF16 ? rpa::syrk_tc_multi_sync_words((int)nu, mc, h->num_sms, h->sync_every) : 0;
+    sync_off[b + 1] = sync_off[b] + words;
+  }
+  if (sync_off.back() > 0) RPA_CUDA(h, ensure(h->syncBuf, (size_t)sync_off.back() * sizeof(int)));
   // graph cache key: shapes, pointers and workspace addresses of this call
   uint64_t key = 1469598103934665603ull;
   auto mix = [&](uint64_t x) { key = (key ^ x) * 1099511628211ull; };
   mix((uint64_t)prec);
   mix((uint64_t)h->seg_chunks);
-  for (void* p : {h->Xhi.p, h->Xlo.p, h->Pi.p, h->Ldiag.p, h->bDesc.p, h->bRes.p, h->D.p, (void*)h->stream})
+  for (void* p : {h->Xhi.p, h->Xlo.p, h->Pi.p, h->Ldiag.p, h->bDesc.p, h->bRes.p, h->D.p, h->syncBuf.p,
+                  (void*)h->stream})
     mix((uint64_t)(uintptr_t)p);
   for (int i = 0; i < n; ++i) {
     mix((uint64_t)(uintptr_t)Rd[i]);
@@ -2291,6 +2325,7 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
     std::vector<rpa::SplitJob> jobs(ni);
     std::vector<int64_t> offs(ni + 1, 0);
     std::vector<uint4> units;
+    std::vector<int> unit_len;  // K chunks of each instance's units
     std::vector<int4> work;
     std::vector<rpa::MatDesc> mats;
     std::vector<uint2> coords;
@@ -2347,6 +2382,7 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
         rpa::syrk_tc_block_coords(NQ, coords);
         for (int k = 0; k < K; ++k)
           for (const uint2& c : coords) units.push_back(make_uint4((unsigned)t, (unsigned)k, c.x, c.y));
+        unit_len.push_back(si.nchunks);
       }
       for (int k = 0; k < K; ++k) {
         rpa::MatDesc md;
@@ -2359,6 +2395,10 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
         mats.push_back(md);
       }
     }
+    // longest units first: the persistent CTAs take units round robin, so a descending order
+    // leaves the short units for the end of the launch (stable: an instance's units stay together)
+    std::stable_sort(units.begin(), units.end(),
+                     [&](const uint4& a, const uint4& b) { return unit_len[a.x] > unit_len[b.x]; });
     // descriptors -> device (laid out as in desc_off)
     uint8_t* d = descBase + desc_off[b];
     auto put = [&](const void* src, size_t bytes) {
@@ -2375,17 +2415,24 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
     auto* dMats = reinterpret_cast<rpa::MatDesc*>(put(mats.data(), sizeof(rpa::MatDesc) * mats.size()));
     RPA_CUDA(h, cudaGetLastError());
     RPA_CUDA(h, cudaStreamSynchronize(h->stream));  // host vectors must outlive their copies
+    // wave milestones of the multi-instance SYRK (counters zeroed inside the captured sequence)
+    const int max_chunks = sync_max_chunks[b];
+    const int64_t sync_words = sync_off[b + 1] - sync_off[b];
+    int* msync = sync_words > 0 ? static_cast<int*>(h->syncBuf.p) + sync_off[b] : nullptr;
     // capture the batch's launch sequence
     const int64_t before = rpa::g_launches;
     cudaGraph_t graph = nullptr;
     RPA_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
     if (prec == RPA_PREC_SPLIT_BF16) {
-      e = rpa::launch_scale_split_multi(dJobs, dWork, (int)work.size(), dOffs, ni, offs.back(), h->stream);
+      if (sync_words > 0) e = cudaMemsetAsync(msync, 0, (size_t)sync_words * sizeof(int), h->stream);
+      if (e == cudaSuccess)
+        e = rpa::launch_scale_split_multi(dJobs, dWork, (int)work.size(), dOffs, ni, offs.back(), h->stream);
       if (e == cudaSuccess)
         e = rpa::launch_syrk_split_bf16_multi(dSinst, dUnits, (int)units.size(),
                                               h->seg_chunks > 0 ? h->seg_chunks : 1 << 30, h->err_dev, h->num_sms,
-                                              h->stream);
+                                              h->stream, sync_words > 0 ? msync : nullptr, h->sync_every, 2,
+                                              max_chunks);
     } else {
       for (int t = 0; t < ni && e == cudaSuccess; ++t) {
         const int i = i0 + t;

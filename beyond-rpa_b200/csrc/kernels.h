@@ -106,8 +106,12 @@ struct SyrkInst {
   int NQ;
   int nchunks;  // ceil(nov / 32)
 };
+// sync (optional, zeroed, syrk_tc_multi_sync_words ints): wave milestones as in SyrkTcArgs; a unit
+// shorter than max_chunks releases its wave's remaining milestones when it ends.
 cudaError_t launch_syrk_split_bf16_multi(const SyrkInst* insts, const uint4* work, int nunits, int seg_chunks,
-                                         int* err, int num_sms, cudaStream_t stream);
+                                         int* err, int num_sms, cudaStream_t stream, int* sync = nullptr,
+                                         int sync_every = 0, int sync_lag = 2, int max_chunks = 0);
+int64_t syrk_tc_multi_sync_words(int nunits, int max_chunks, int num_sms, int sync_every);
 int syrk_tc_blocks(int NQ);
 // (tm, tn) of the lower-triangle 128 x 256 tiles in the kernel's unit order
 void syrk_tc_block_coords(int NQ, std::vector<uint2>& out);
@@ -157,6 +161,9 @@ cudaError_t launch_dai(const double* eps_o, const double* eps_v, int64_t no, int
 cudaError_t launch_symmetrize(double* A, int64_t ld, int64_t stride, int n, int nmat, cudaStream_t stream);
 // Count non-finite entries of a device array (result accumulated into *count).
 cudaError_t launch_count_nonfinite(const double* x, int64_t n, int* count, cudaStream_t stream);
+// The same over narr arrays (device arrays of pointers and lengths), blocks_per CTAs each.
+cudaError_t launch_count_nonfinite_multi(const double* const* ptrs, const int64_t* counts, int narr, int blocks_per,
+                                         int* count, cudaStream_t stream);
 // Strided 2-D copy of a column-major matrix block (device to device).
 cudaError_t launch_copy_lower(const double* src, int64_t lds, int64_t strideS, double* dst, int64_t ldd,
                               int64_t strideD, int n, int nmat, cudaStream_t stream);

@@ -232,6 +232,16 @@ __global__ void count_nonfinite_kernel(const double* x, int64_t n, int* count) {
   if (local) atomicAdd(count, local);
 }
 
+// Many arrays at once: blockIdx.y selects array (ptrs[y], counts[y]).
+__global__ void count_nonfinite_multi_kernel(const double* const* ptrs, const int64_t* counts, int* count) {
+  const double* x = ptrs[blockIdx.y];
+  const int64_t n = counts[blockIdx.y];
+  int local = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (!isfinite(x[i])) ++local;
+  if (local) atomicAdd(count, local);
+}
+
 __global__ void copy_lower_kernel(const double* src, int64_t lds, int64_t strideS, double* dst, int64_t ldd,
                                   int64_t strideD, int n) {
   const int z = blockIdx.z;
@@ -384,6 +394,15 @@ cudaError_t launch_count_nonfinite(const double* x, int64_t n, int* count, cudaS
   int64_t blocks = (n + 255) / 256;
   if (blocks > 4096) blocks = 4096;
   count_nonfinite_kernel<<<(unsigned)blocks, 256, 0, stream>>>(x, n, count);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_count_nonfinite_multi(const double* const* ptrs, const int64_t* counts, int narr, int blocks_per,
+                                         int* count, cudaStream_t stream) {
+  if (narr <= 0) return cudaSuccess;
+  count_nonfinite_multi_kernel<<<dim3((unsigned)std::max(1, blocks_per), (unsigned)narr), 256, 0, stream>>>(ptrs, counts,
+                                                                                                         count);
   ++g_launches;
   return cudaGetLastError();
 }

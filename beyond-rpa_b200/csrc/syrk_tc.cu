@@ -118,10 +118,12 @@ struct MultiSource {
   const SyrkInst* insts;
   const uint4* work;  // (instance, k, tm, tn)
   int nunits;
-  __device__ __forceinline__ int* sync_counters() const { return nullptr; }
-  __device__ __forceinline__ int sync_every() const { return 1; }
-  __device__ __forceinline__ int sync_lag() const { return 0; }
-  __device__ __forceinline__ int max_chunks() const { return 0; }
+  int* sync;
+  int sync_every_, sync_lag_, max_chunks_;
+  __device__ __forceinline__ int* sync_counters() const { return sync; }
+  __device__ __forceinline__ int sync_every() const { return sync_every_; }
+  __device__ __forceinline__ int sync_lag() const { return sync_lag_; }
+  __device__ __forceinline__ int max_chunks() const { return max_chunks_; }
   __device__ __forceinline__ Unit get(int u) const {
     const uint4 w = work[u];
     const SyrkInst& in = insts[w.x];
@@ -236,6 +238,11 @@ __device__ __forceinline__ void syrk_body(const Source& src, int* err, const int
             stage = 0;
             phase ^= 1u;
           }
+        }
+        if (sync && ok) {  // a unit shorter than the longest of the launch: release the later milestones
+          int* row = sync + (int64_t)wave * nmile;
+          for (int mi = (x.nchunks + sync_every - 1) / sync_every; mi < nmile; ++mi)
+            asm volatile("red.release.gpu.global.add.s32 [%0], 1;" ::"l"(row + mi) : "memory");
         }
       }
       // make sure no bulk copy is still landing in shared memory at exit
@@ -373,11 +380,16 @@ __global__ void __launch_bounds__(kThreads, 1)
 // Many instances (fragments) in one persistent launch.
 __global__ void __launch_bounds__(kThreads, 1)
     syrk_split_bf16_multi_kernel(const SyrkInst* __restrict__ insts, const uint4* __restrict__ work, const int nunits,
-                                 int* err, const int seg_chunks) {
+                                 int* err, const int seg_chunks, int* sync, const int sync_every, const int sync_lag,
+                                 const int max_chunks) {
   MultiSource src;
   src.insts = insts;
   src.work = work;
   src.nunits = nunits;
+  src.sync = sync;
+  src.sync_every_ = sync_every > 0 ? sync_every : 1;
+  src.sync_lag_ = sync_lag;
+  src.max_chunks_ = max_chunks;
   syrk_body(src, err, seg_chunks);
 }
 }  // namespace
@@ -431,14 +443,23 @@ void syrk_tc_block_coords(int NQ, std::vector<uint2>& out) {
     for (int tm = 2 * tn; tm < ntm; ++tm) out.push_back(make_uint2((unsigned)tm, (unsigned)tn));
 }
 
+int64_t syrk_tc_multi_sync_words(int nunits, int max_chunks, int num_sms, int sync_every) {
+  if (sync_every <= 0 || nunits <= 0) return 0;
+  const int grid = nunits < num_sms ? nunits : num_sms;
+  const int64_t waves = (nunits + grid - 1) / grid;
+  return waves * ((max_chunks + sync_every - 1) / sync_every);
+}
+
 cudaError_t launch_syrk_split_bf16_multi(const SyrkInst* insts, const uint4* work, int nunits, int seg_chunks,
-                                         int* err, int num_sms, cudaStream_t stream) {
+                                         int* err, int num_sms, cudaStream_t stream, int* sync, int sync_every,
+                                         int sync_lag, int max_chunks) {
   if (nunits == 0) return cudaSuccess;
   cudaError_t e =
       cudaFuncSetAttribute(syrk_split_bf16_multi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
   if (e != cudaSuccess) return e;
   const int grid = nunits < num_sms ? nunits : num_sms;
-  syrk_split_bf16_multi_kernel<<<grid, kThreads, kSmemBytes, stream>>>(insts, work, nunits, err, seg_chunks);
+  syrk_split_bf16_multi_kernel<<<grid, kThreads, kSmemBytes, stream>>>(insts, work, nunits, err, seg_chunks, sync,
+                                                                       sync_every, sync_lag, max_chunks);
   ++g_launches;
   return cudaGetLastError();
 }
