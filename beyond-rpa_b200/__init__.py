@@ -107,6 +107,10 @@ def load_library(path: str | os.PathLike | None = None):
     lib.rpa_b200_project_basis.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64]
     lib.rpa_b200_exchange_mbpt3.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _i64, _vp, _vp,
                                             _vp, _i64]
+    lib.rpa_b200_tune_logdet.argtypes = [_vp, _i64, _i64, _vp, _vp, _vp]
+    lib.rpa_b200_set_logdet_plan.argtypes = [_vp, _i64, _i64, _i64]
+    lib.rpa_b200_get_logdet_plan.argtypes = [_vp, _i64, _vp, _vp]
+    lib.rpa_b200_set_autotune.argtypes = [_vp, _i64]
     if path is None:
         _lib = lib
     return lib
@@ -221,6 +225,32 @@ class Handle:
     def set_stream(self, stream=None):
         """Run calls on a cudaStream_t (e.g. torch.cuda.current_stream().cuda_stream)."""
         self._check(self.lib.rpa_b200_set_stream(self._h, stream))
+
+    # ------------------------------------------------------------------ log-det tile plans
+    LOGDET_CANDIDATES = ((128, 64), (256, 64), (512, 64), (128, 128), (256, 128), (512, 128))
+
+    def tune_logdet(self, nq, nmat):
+        """Time every log-det tile plan (outer block, CTA tile) on `nmat` seeded SPD matrices of
+        order `nq`; keep the fastest for nq's bucket.  Returns ((nb2, tile), {candidate: ms})."""
+        nb2, tile = ctypes.c_int64(), ctypes.c_int64()
+        ms = (ctypes.c_double * 6)()
+        self._check(self.lib.rpa_b200_tune_logdet(self._h, int(nq), int(nmat), ctypes.byref(nb2), ctypes.byref(tile),
+                                                  ctypes.cast(ms, _vp)))
+        return (nb2.value, tile.value), dict(zip(self.LOGDET_CANDIDATES, list(ms)))
+
+    def set_logdet_plan(self, nq, nb2, tile):
+        """Store the log-det tile plan for nq's bucket of 256 orders."""
+        self._check(self.lib.rpa_b200_set_logdet_plan(self._h, int(nq), int(nb2), int(tile)))
+
+    def logdet_plan(self, nq):
+        """(nb2, tile) used for matrices of order nq."""
+        nb2, tile = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.rpa_b200_get_logdet_plan(self._h, int(nq), ctypes.byref(nb2), ctypes.byref(tile)))
+        return nb2.value, tile.value
+
+    def set_autotune(self, on=True):
+        """Tune unseen order buckets inside ec_batched (on by default)."""
+        self._check(self.lib.rpa_b200_set_autotune(self._h, 1 if on else 0))
 
     # ------------------------------------------------------------------ Pi(u)
     def pi_u(self, R, eps_o, eps_v, freqs, alpha=4.0, prec="split", out=None):

@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -74,10 +75,20 @@ struct rpa_b200_handle {
     int n, nmat;
     double* Ldiag;
     cudaStream_t stream;
+    int nb2, tile_w;
     cudaGraphExec_t exec;
     int64_t launches;
   };
   std::vector<CholGraph> chol_graphs;
+  // tile plans of the FP64 log-det per bucket of 256 matrix orders (tuned or set)
+  std::map<int, rpa::LogdetPlan> logdet_plans;
+  uint64_t plans_version = 0;  // bumped on every change (part of the batched graph key)
+  int autotune = 1;            // tune unseen order buckets on their first batched use (RPA_B200_AUTOTUNE=0: off)
+  size_t batch_bytes = 0;      // device bytes per batch of the batched entry (0: 60% of free memory)
+  DevBuf tune;                 // tuner workspace: descriptors and pivots of its test matrices
+  // fork/join branches of the batched graph: [0] the next batch's scale/split pass, [1..2] log-det buckets
+  cudaStream_t aux[3] = {};
+  cudaEvent_t fork_ev[6] = {};
 };
 
 namespace {
@@ -453,13 +464,59 @@ int build_pi_pipelined(rpa_b200_handle* h, const Validated& v, const double* Rh,
   return RPA_OK;
 }
 
+// ---- tile plans of the FP64 log-det
+// A plan is kept per bucket of 256 matrix orders; the tuner times every candidate on the
+// matrices it is given and keeps the fastest (measured, not modelled: the best outer block and
+// CTA tile depend on the order, the batch width and what runs beside the log-det).
+constexpr int kPlanBucket = 256;
+const rpa::LogdetPlan kLogdetCands[6] = {{128, 2}, {256, 2}, {512, 2}, {128, 4}, {256, 4}, {512, 4}};
+
+int plan_bucket(int n) { return (n + kPlanBucket - 1) / kPlanBucket; }
+
+rpa::LogdetPlan plan_for(const rpa_b200_handle* h, int n) {
+  auto it = h->logdet_plans.find(plan_bucket(n));
+  return it != h->logdet_plans.end() ? it->second : rpa::default_logdet_plan();
+}
+
+// Time every candidate on nmat matrices of orders <= nmax (device descriptors; contents are
+// overwritten with seeded SPD test matrices), two runs each (the first also loads the variant's
+// kernels), keep the fastest for the bucket of nmax.  ms (6 entries or null): each candidate's time.
+int tune_logdet_on(rpa_b200_handle* h, const rpa::MatDesc* dmats, int nmat, int nmax, double* ms) {
+  cudaEvent_t t0 = pool_event(h), t1 = pool_event(h);
+  if (!t0 || !t1) return fail(h, RPA_ERR_CUDA, "event creation failed");
+  int best = 0;
+  float best_ms = 0.0f;
+  for (int c = 0; c < 6; ++c) {
+    float t = 0.0f;
+    for (int rep = 0; rep < 2; ++rep) {
+      RPA_CUDA(h, rpa::launch_fill_spd_varlen(dmats, nmat, nmax, 0x5eedull + (uint64_t)rep, h->stream));
+      RPA_CUDA(h, cudaEventRecord(t0, h->stream));
+      RPA_CUDA(h, rpa::launch_logdet_varlen(dmats, nmat, nmax, h->err_dev, h->stream, kLogdetCands[c]));
+      RPA_CUDA(h, cudaEventRecord(t1, h->stream));
+      RPA_CUDA(h, cudaEventSynchronize(t1));
+      RPA_CUDA(h, cudaEventElapsedTime(&t, t0, t1));
+    }
+    if (ms) ms[c] = t;
+    if (c == 0 || t < best_ms) {
+      best_ms = t;
+      best = c;
+    }
+  }
+  int s = check_device_error(h);  // the test matrices are positive definite: a flag is a real fault
+  if (s != RPA_OK) return s;
+  h->logdet_plans[plan_bucket(nmax)] = kLogdetCands[best];
+  ++h->plans_version;
+  return RPA_OK;
+}
+
 // Blocked Cholesky of nmat matrices through a cached CUDA graph (the launch
 // sequence depends only on the arguments; ~6 launches per 64 columns would
 // otherwise leave the GPU idle between the small late-step kernels).
 int cholesky(rpa_b200_handle* h, double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag) {
+  const rpa::LogdetPlan plan = plan_for(h, n);
   for (auto& g : h->chol_graphs) {
     if (g.A == A && g.ld == ld && g.stride == stride && g.n == n && g.nmat == nmat && g.Ldiag == Ldiag &&
-        g.stream == h->stream) {
+        g.stream == h->stream && g.nb2 == plan.nb2 && g.tile_w == plan.tile_w) {
       RPA_CUDA(h, cudaGraphLaunch(g.exec, h->stream));
       rpa::g_launches += g.launches;
       return RPA_OK;
@@ -468,7 +525,7 @@ int cholesky(rpa_b200_handle* h, double* A, int64_t ld, int64_t stride, int n, i
   const int64_t before = rpa::g_launches;
   cudaGraph_t graph = nullptr;
   if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-    cudaError_t e = rpa::launch_cholesky_lower(A, ld, stride, n, nmat, Ldiag, h->err_dev, h->stream);
+    cudaError_t e = rpa::launch_cholesky_lower(A, ld, stride, n, nmat, Ldiag, h->err_dev, h->stream, plan);
     cudaError_t e2 = cudaStreamEndCapture(h->stream, &graph);
     const int64_t count = rpa::g_launches - before;
     rpa::g_launches = before;
@@ -480,7 +537,7 @@ int cholesky(rpa_b200_handle* h, double* A, int64_t ld, int64_t stride, int n, i
         cudaGraphExecDestroy(h->chol_graphs.front().exec);
         h->chol_graphs.erase(h->chol_graphs.begin());
       }
-      h->chol_graphs.push_back({A, ld, stride, n, nmat, Ldiag, h->stream, exec, count});
+      h->chol_graphs.push_back({A, ld, stride, n, nmat, Ldiag, h->stream, plan.nb2, plan.tile_w, exec, count});
       RPA_CUDA(h, cudaGraphLaunch(exec, h->stream));
       rpa::g_launches += count;
       return RPA_OK;
@@ -491,7 +548,7 @@ int cholesky(rpa_b200_handle* h, double* A, int64_t ld, int64_t stride, int n, i
     cudaGetLastError();
   }
   // capture unavailable on this stream: launch the same kernels directly
-  RPA_CUDA(h, rpa::launch_cholesky_lower(A, ld, stride, n, nmat, Ldiag, h->err_dev, h->stream));
+  RPA_CUDA(h, rpa::launch_cholesky_lower(A, ld, stride, n, nmat, Ldiag, h->err_dev, h->stream, plan));
   return RPA_OK;
 }
 
@@ -741,6 +798,9 @@ int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) {
   if (cudaSetDevice(h->device) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->aux[0], cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->aux[1], cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&h->aux[2], cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&h->err_dev, sizeof(int)) != cudaSuccess || cudaMalloc(&h->count_dev, sizeof(int)) != cudaSuccess) {
     delete h;
     return RPA_ERR_CUDA;
@@ -748,7 +808,10 @@ int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) {
   h->stream = h->own_stream;
   if (const char* sc = std::getenv("RPA_B200_SEG_CHUNKS")) h->seg_chunks = std::atoi(sc);
   if (const char* se = std::getenv("RPA_B200_SYNC_EVERY")) h->sync_every = std::atoi(se);
+  if (const char* at = std::getenv("RPA_B200_AUTOTUNE")) h->autotune = std::atoi(at) != 0;
+  if (const char* bb = std::getenv("RPA_B200_BATCH_BYTES")) h->batch_bytes = (size_t)std::atoll(bb);
   for (auto& e : h->ev) cudaEventCreate(&e);
+  for (auto& e : h->fork_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   cudaDriverEntryPointQueryResult q;
   void* fn = nullptr;
   if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
@@ -773,7 +836,7 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
                     &h->xM, &h->eW, &h->eA, &h->eZ, &h->thZ, &h->thXa, &h->thXi, &h->thYX, &h->thR,
                     &h->jU, &h->jL, &h->jX, &h->jPno, &h->jWork,
                     &h->jPack, &h->jQS, &h->jS, &h->jD, &h->syncBuf,
-                    &h->jT, &h->jM, &h->jV, &h->jMap, &h->jSK})
+                    &h->jT, &h->jM, &h->jV, &h->jMap, &h->jSK, &h->tune})
     release(*b);
   for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
   if (h->err_dev) cudaFree(h->err_dev);
@@ -782,6 +845,13 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
     if (e) cudaEventDestroy(e);
   for (auto& e : h->pool) cudaEventDestroy(e);
   for (auto& g : h->chol_graphs) cudaGraphExecDestroy(g.exec);
+  for (auto& e : h->fork_ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& st : h->aux)
+    if (st) {
+      cudaStreamSynchronize(st);
+      cudaStreamDestroy(st);
+    }
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   delete h;
@@ -817,6 +887,59 @@ int64_t rpa_b200_last_launches(const rpa_b200_handle* h) { return h ? h->launche
 int rpa_b200_set_stream(rpa_b200_handle* h, void* stream) {
   if (!h) return RPA_ERR_INVALID_ARG;
   h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+  return RPA_OK;
+}
+
+int rpa_b200_tune_logdet(rpa_b200_handle* h, int64_t NQ, int64_t NMat, int64_t* Nb2, int64_t* Tile, double* Ms) {
+  int s = begin_call(h);
+  if (s != RPA_OK) return s;
+  if (NQ < 1 || NQ > (1 << 20) || NMat < 1 || NMat > (1 << 20))
+    return fail(h, RPA_ERR_INVALID_ARG, "invalid tuning case NQ=%lld NMat=%lld", (long long)NQ, (long long)NMat);
+  const int n = (int)NQ, nmat = (int)NMat;
+  RPA_CUDA(h, ensure(h->Pi, (size_t)nmat * n * n * 8));
+  RPA_CUDA(h, ensure(h->tune, (size_t)nmat * (sizeof(rpa::MatDesc) + 8 * ((size_t)n + 4)) + 512));
+  std::vector<rpa::MatDesc> mats(nmat);
+  rpa::MatDesc* dmats = static_cast<rpa::MatDesc*>(h->tune.p);
+  double* scratch = reinterpret_cast<double*>(static_cast<uint8_t*>(h->tune.p) +
+                                              ((size_t)nmat * sizeof(rpa::MatDesc) + 255) / 256 * 256);
+  for (int z = 0; z < nmat; ++z) {
+    mats[z].A = static_cast<double*>(h->Pi.p) + (size_t)z * n * n;
+    mats[z].ld = n;
+    mats[z].n = n;
+    mats[z].Ldiag = scratch + (size_t)z * n;
+    mats[z].tr_dd = scratch + (size_t)nmat * n + 4 * (size_t)z;
+    mats[z].ld_dd = mats[z].tr_dd + 2;
+  }
+  RPA_CUDA(h, cudaMemcpyAsync(dmats, mats.data(), sizeof(rpa::MatDesc) * nmat, cudaMemcpyHostToDevice, h->stream));
+  if ((s = tune_logdet_on(h, dmats, nmat, n, Ms))) return s;
+  const rpa::LogdetPlan p = plan_for(h, n);
+  if (Nb2) *Nb2 = p.nb2;
+  if (Tile) *Tile = 32 * p.tile_w;
+  h->launches = rpa::g_launches;
+  return RPA_OK;
+}
+
+int rpa_b200_set_logdet_plan(rpa_b200_handle* h, int64_t NQ, int64_t Nb2, int64_t Tile) {
+  if (!h || NQ < 1) return RPA_ERR_INVALID_ARG;
+  const rpa::LogdetPlan p{(int)Nb2, (int)(Tile / 32)};
+  if ((Nb2 != 128 && Nb2 != 256 && Nb2 != 512) || (Tile != 64 && Tile != 128) || !rpa::valid_logdet_plan(p))
+    return fail(h, RPA_ERR_INVALID_ARG, "invalid log-det plan Nb2=%lld Tile=%lld", (long long)Nb2, (long long)Tile);
+  h->logdet_plans[plan_bucket((int)std::min<int64_t>(NQ, 1 << 30))] = p;
+  ++h->plans_version;
+  return RPA_OK;
+}
+
+int rpa_b200_get_logdet_plan(const rpa_b200_handle* h, int64_t NQ, int64_t* Nb2, int64_t* Tile) {
+  if (!h || NQ < 1) return RPA_ERR_INVALID_ARG;
+  const rpa::LogdetPlan p = plan_for(h, (int)std::min<int64_t>(NQ, 1 << 30));
+  if (Nb2) *Nb2 = p.nb2;
+  if (Tile) *Tile = 32 * p.tile_w;
+  return RPA_OK;
+}
+
+int rpa_b200_set_autotune(rpa_b200_handle* h, int64_t on) {
+  if (!h) return RPA_ERR_INVALID_ARG;
+  h->autotune = on != 0;
   return RPA_OK;
 }
 
@@ -2218,7 +2341,7 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
   RPA_CUDA(h, cudaMemGetInfo(&freeB, &totalB));
   // buffers that ensure() below may free and reallocate count as available
   const size_t have = h->Xhi.bytes + h->Xlo.bytes + h->Pi.bytes + h->Ldiag.bytes;
-  const size_t budget = (size_t)(0.6 * (double)(freeB + have));
+  const size_t budget = h->batch_bytes > 0 ? h->batch_bytes : (size_t)(0.6 * (double)(freeB + have));
   std::vector<std::pair<int, int>> batches;  // [b0, b1)
   {
     size_t acc = 0;
@@ -2234,7 +2357,7 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
     }
     batches.push_back({b0, n});
   }
-  size_t maxX = 0, maxPi = 0, maxSmall = 0, maxDesc = 0;
+  size_t maxX = 0, maxPi = 0, maxSmall = 0;
   std::vector<size_t> desc_off(batches.size() + 1, 0), res_off(batches.size() + 1, 0);
   for (size_t b = 0; b < batches.size(); ++b) {
     size_t x = 0, pi = 0, sm = 0, units = 0, work = 0, mats = 0;
@@ -2257,13 +2380,15 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
     maxPi = std::max(maxPi, pi);
     maxSmall = std::max(maxSmall, sm);
   }
-  (void)maxDesc;
   if (prec == RPA_PREC_SPLIT_BF16) {
     RPA_CUDA(h, ensure(h->Xhi, maxX + 256));
     RPA_CUDA(h, ensure(h->Xlo, maxX + 256));
   }
   RPA_CUDA(h, ensure(h->Pi, maxPi + 256));
-  RPA_CUDA(h, ensure(h->Ldiag, maxSmall + 256));
+  // small per-batch buffers (exact diagonals, pivots, split partials) alternate between two halves:
+  // the next batch's scale/split pass runs while this batch's log-det still reads its pivots
+  const size_t smallStride = (maxSmall + 255) / 256 * 256;
+  RPA_CUDA(h, ensure(h->Ldiag, 2 * smallStride + 256));
   RPA_CUDA(h, ensure(h->bDesc, desc_off.back() + 256));
   RPA_CUDA(h, ensure(h->bRes, res_off.back() * 8 + 256));
 
@@ -2305,7 +2430,9 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
     std::memcpy(&ab, &inst[i].alpha, 8);
     mix(ab);
   }
-  const bool cached = (h->bgraph.key == key && h->bgraph.execs.size() == batches.size());
+  // the key also covers the log-det tile plans (the tuner below may add some)
+  auto keyed = [&](uint64_t version) { return (key ^ version) * 1099511628211ull; };
+  const bool cached = (h->bgraph.key == keyed(h->plans_version) && h->bgraph.execs.size() == 1);
   if (!cached) {
     for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
     h->bgraph.execs.clear();
@@ -2314,153 +2441,255 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
   }
   uint8_t* descBase = static_cast<uint8_t*>(h->bDesc.p);
   double* resBase = static_cast<double*>(h->bRes.p);
-  for (size_t b = 0; b < batches.size(); ++b) {
-    if (cached) {
-      RPA_CUDA(h, cudaGraphLaunch(h->bgraph.execs[b], h->stream));
-      rpa::g_launches += h->bgraph.launches[b];
-      continue;
-    }
-    const int i0 = batches[b].first, i1 = batches[b].second, ni = i1 - i0;
-    std::vector<rpa::SyrkInst> sinst(ni);
-    std::vector<rpa::SplitJob> jobs(ni);
-    std::vector<int64_t> offs(ni + 1, 0);
-    std::vector<uint4> units;
-    std::vector<int> unit_len;  // K chunks of each instance's units
-    std::vector<int4> work;
-    std::vector<rpa::MatDesc> mats;
-    std::vector<uint2> coords;
-    size_t xo = 0, po = 0, so = 0;
-    double* res = resBase + res_off[b];
-    int nmax = 0;
-    for (int t = 0; t < ni; ++t) {
-      const int i = i0 + t;
-      const int NQ = v[i].NQ, K = v[i].K;
-      const int64_t nov = v[i].nov;
-      __nv_bfloat16* xh = reinterpret_cast<__nv_bfloat16*>(static_cast<uint8_t*>(h->Xhi.p) + xo);
-      __nv_bfloat16* xl = reinterpret_cast<__nv_bfloat16*>(static_cast<uint8_t*>(h->Xlo.p) + xo);
-      double* Pi = reinterpret_cast<double*>(static_cast<uint8_t*>(h->Pi.p) + po);
-      double* smallp = reinterpret_cast<double*>(static_cast<uint8_t*>(h->Ldiag.p) + so);
-      double* diag = smallp;                          // K*NQ
-      double* Ldiag = diag + (size_t)K * NQ;          // K*NQ
-      double* dpart = Ldiag + (size_t)K * NQ;         // nsplit*K*NQ
-      xo += (per[i].xb + 255) / 256 * 256;
-      po += (per[i].pib + 255) / 256 * 256;
-      so += (per[i].smallb + 255) / 256 * 256;
-      nmax = std::max(nmax, NQ);
-      if (prec == RPA_PREC_SPLIT_BF16) {
-        rpa::SplitJob& j = jobs[t];
-        j.R = Rd[i];
-        j.ldR = ldR[i];
-        j.NQ = NQ;
-        j.nov = nov;
-        j.D = D + Doff[i];
-        j.fg.n = K;
-        for (int k = 0; k < K; ++k) j.fg.u2[k] = v[i].freqs[k] * v[i].freqs[k];
-        j.alpha = inst[i].alpha;
-        j.Xhi = xh;
-        j.Xlo = xl;
-        j.pitch = per[i].pitch;
-        j.kstride = (int64_t)NQ * per[i].pitch;
-        j.diag_part = dpart;
-        j.ai_per_split = per[i].plan.ai_per_split;
-        j.nsplit = per[i].plan.nsplit;
-        j.diag = diag;
-        offs[t + 1] = offs[t] + (int64_t)K * NQ;
-        for (int q = 0; q < per[i].plan.qtiles; ++q)
-          for (int sp = 0; sp < per[i].plan.nsplit; ++sp) work.push_back(make_int4(t, q, sp, 0));
-        rpa::SyrkInst& si = sinst[t];
-        if ((s = encode_map(h, &si.tmAh, xh, nov, NQ, K, per[i].pitch, rpa::kSyrkTcTM))) return s;
-        if ((s = encode_map(h, &si.tmAl, xl, nov, NQ, K, per[i].pitch, rpa::kSyrkTcTM))) return s;
-        if ((s = encode_map(h, &si.tmBh, xh, nov, NQ, K, per[i].pitch, rpa::kSyrkTcTN))) return s;
-        if ((s = encode_map(h, &si.tmBl, xl, nov, NQ, K, per[i].pitch, rpa::kSyrkTcTN))) return s;
-        si.Pi = Pi;
-        si.ldPi = NQ;
-        si.piStride = (int64_t)NQ * NQ;
-        si.diag = diag;
-        si.NQ = NQ;
-        si.nchunks = (int)((nov + rpa::kSyrkTcTK - 1) / rpa::kSyrkTcTK);
-        rpa::syrk_tc_block_coords(NQ, coords);
-        for (int k = 0; k < K; ++k)
-          for (const uint2& c : coords) units.push_back(make_uint4((unsigned)t, (unsigned)k, c.x, c.y));
-        unit_len.push_back(si.nchunks);
-      }
-      for (int k = 0; k < K; ++k) {
-        rpa::MatDesc md;
-        md.A = Pi + (size_t)k * NQ * NQ;
-        md.ld = NQ;
-        md.n = NQ;
-        md.Ldiag = Ldiag + (size_t)k * NQ;
-        md.tr_dd = res + 4 * mats.size();
-        md.ld_dd = md.tr_dd + 2;
-        mats.push_back(md);
-      }
-    }
-    // longest units first: the persistent CTAs take units round robin, so a descending order
-    // leaves the short units for the end of the launch (stable: an instance's units stay together)
-    std::stable_sort(units.begin(), units.end(),
-                     [&](const uint4& a, const uint4& b) { return unit_len[a.x] > unit_len[b.x]; });
-    // descriptors -> device (laid out as in desc_off)
-    uint8_t* d = descBase + desc_off[b];
-    auto put = [&](const void* src, size_t bytes) {
-      uint8_t* at = d;
-      if (bytes) cudaMemcpyAsync(at, src, bytes, cudaMemcpyHostToDevice, h->stream);
-      d += (bytes + 255) / 256 * 256;
-      return at;
+  if (cached) {
+    RPA_CUDA(h, cudaGraphLaunch(h->bgraph.execs[0], h->stream));
+    rpa::g_launches += h->bgraph.launches[0];
+  } else {
+    // ---- per batch: descriptors on the device, log-det order buckets, milestone counters
+    struct Bucket {
+      int first, count, nmax;  // matrices [first, first + count) of the batch's (bucket-sorted) list
+      int tune_count, tune_nmax;  // the tuner's subset: the first tune_count of them
+      double cost;                // sum of n^3
     };
-    auto* dSinst = reinterpret_cast<rpa::SyrkInst*>(put(sinst.data(), sizeof(rpa::SyrkInst) * sinst.size()));
-    auto* dJobs = reinterpret_cast<rpa::SplitJob*>(put(jobs.data(), sizeof(rpa::SplitJob) * jobs.size()));
-    auto* dOffs = reinterpret_cast<int64_t*>(put(offs.data(), sizeof(int64_t) * offs.size()));
-    auto* dUnits = reinterpret_cast<uint4*>(put(units.data(), sizeof(uint4) * units.size()));
-    auto* dWork = reinterpret_cast<int4*>(put(work.data(), sizeof(int4) * work.size()));
-    auto* dMats = reinterpret_cast<rpa::MatDesc*>(put(mats.data(), sizeof(rpa::MatDesc) * mats.size()));
-    RPA_CUDA(h, cudaGetLastError());
-    RPA_CUDA(h, cudaStreamSynchronize(h->stream));  // host vectors must outlive their copies
-    // wave milestones of the multi-instance SYRK (counters zeroed inside the captured sequence)
-    const int max_chunks = sync_max_chunks[b];
-    const int64_t sync_words = sync_off[b + 1] - sync_off[b];
-    int* msync = sync_words > 0 ? static_cast<int*>(h->syncBuf.p) + sync_off[b] : nullptr;
-    // capture the batch's launch sequence
+    struct BatchDev {
+      rpa::SyrkInst* sinst = nullptr;
+      uint4* units = nullptr;
+      int nunits = 0;
+      rpa::SplitJob* jobs = nullptr;
+      int4* work = nullptr;
+      int nwork = 0;
+      int64_t* offs = nullptr;
+      int ni = 0;
+      int64_t offs_total = 0;
+      rpa::MatDesc* mats = nullptr;
+      std::vector<Bucket> buckets;
+      std::vector<rpa::DsyrkArgs> fp64;  // FP64 form: one scaled SYRK per instance
+      int* msync = nullptr;
+      int64_t sync_words = 0;
+      int max_chunks = 0;
+    };
+    std::vector<BatchDev> bd(batches.size());
+    for (size_t b = 0; b < batches.size(); ++b) {
+      const int i0 = batches[b].first, i1 = batches[b].second, ni = i1 - i0;
+      std::vector<rpa::SyrkInst> sinst(ni);
+      std::vector<rpa::SplitJob> jobs(ni);
+      std::vector<int64_t> offs(ni + 1, 0);
+      std::vector<uint4> units;
+      std::vector<int> unit_len;  // K chunks of each instance's units
+      std::vector<int4> work;
+      std::vector<rpa::MatDesc> mats;
+      std::vector<uint2> coords;
+      size_t xo = 0, po = 0, so = smallStride * (b & 1);
+      double* res = resBase + res_off[b];
+      BatchDev& dv = bd[b];
+      for (int t = 0; t < ni; ++t) {
+        const int i = i0 + t;
+        const int NQ = v[i].NQ, K = v[i].K;
+        const int64_t nov = v[i].nov;
+        __nv_bfloat16* xh = reinterpret_cast<__nv_bfloat16*>(static_cast<uint8_t*>(h->Xhi.p) + xo);
+        __nv_bfloat16* xl = reinterpret_cast<__nv_bfloat16*>(static_cast<uint8_t*>(h->Xlo.p) + xo);
+        double* Pi = reinterpret_cast<double*>(static_cast<uint8_t*>(h->Pi.p) + po);
+        double* smallp = reinterpret_cast<double*>(static_cast<uint8_t*>(h->Ldiag.p) + so);
+        double* diag = smallp;                          // K*NQ
+        double* Ldiag = diag + (size_t)K * NQ;          // K*NQ
+        double* dpart = Ldiag + (size_t)K * NQ;         // nsplit*K*NQ
+        xo += (per[i].xb + 255) / 256 * 256;
+        po += (per[i].pib + 255) / 256 * 256;
+        so += (per[i].smallb + 255) / 256 * 256;
+        if (prec == RPA_PREC_SPLIT_BF16) {
+          rpa::SplitJob& j = jobs[t];
+          j.R = Rd[i];
+          j.ldR = ldR[i];
+          j.NQ = NQ;
+          j.nov = nov;
+          j.D = D + Doff[i];
+          j.fg.n = K;
+          for (int k = 0; k < K; ++k) j.fg.u2[k] = v[i].freqs[k] * v[i].freqs[k];
+          j.alpha = inst[i].alpha;
+          j.Xhi = xh;
+          j.Xlo = xl;
+          j.pitch = per[i].pitch;
+          j.kstride = (int64_t)NQ * per[i].pitch;
+          j.diag_part = dpart;
+          j.ai_per_split = per[i].plan.ai_per_split;
+          j.nsplit = per[i].plan.nsplit;
+          j.diag = diag;
+          offs[t + 1] = offs[t] + (int64_t)K * NQ;
+          for (int q = 0; q < per[i].plan.qtiles; ++q)
+            for (int sp = 0; sp < per[i].plan.nsplit; ++sp) work.push_back(make_int4(t, q, sp, 0));
+          rpa::SyrkInst& si = sinst[t];
+          if ((s = encode_map(h, &si.tmAh, xh, nov, NQ, K, per[i].pitch, rpa::kSyrkTcTM))) return s;
+          if ((s = encode_map(h, &si.tmAl, xl, nov, NQ, K, per[i].pitch, rpa::kSyrkTcTM))) return s;
+          if ((s = encode_map(h, &si.tmBh, xh, nov, NQ, K, per[i].pitch, rpa::kSyrkTcTN))) return s;
+          if ((s = encode_map(h, &si.tmBl, xl, nov, NQ, K, per[i].pitch, rpa::kSyrkTcTN))) return s;
+          si.Pi = Pi;
+          si.ldPi = NQ;
+          si.piStride = (int64_t)NQ * NQ;
+          si.diag = diag;
+          si.NQ = NQ;
+          si.nchunks = (int)((nov + rpa::kSyrkTcTK - 1) / rpa::kSyrkTcTK);
+          rpa::syrk_tc_block_coords(NQ, coords);
+          for (int k = 0; k < K; ++k)
+            for (const uint2& c : coords) units.push_back(make_uint4((unsigned)t, (unsigned)k, c.x, c.y));
+          unit_len.push_back(si.nchunks);
+        } else {
+          rpa::DsyrkArgs a{};
+          a.A = Rd[i];
+          a.lda = ldR[i];
+          a.strideA = 0;
+          a.C = Pi;
+          a.ldc = NQ;
+          a.strideC = (int64_t)NQ * NQ;
+          a.n = NQ;
+          a.kdim = nov;
+          a.batch = K;
+          a.D = D + Doff[i];
+          a.alpha = inst[i].alpha;
+          for (int k = 0; k < K; ++k) a.u2[k] = v[i].freqs[k] * v[i].freqs[k];
+          dv.fp64.push_back(a);
+        }
+        for (int k = 0; k < K; ++k) {
+          rpa::MatDesc md;
+          md.A = Pi + (size_t)k * NQ * NQ;
+          md.ld = NQ;
+          md.n = NQ;
+          md.Ldiag = Ldiag + (size_t)k * NQ;
+          md.tr_dd = res + 4 * mats.size();
+          md.ld_dd = md.tr_dd + 2;
+          mats.push_back(md);
+        }
+      }
+      // longest units first: the persistent CTAs take units round robin, so a descending order
+      // leaves the short units for the end of the launch (stable: an instance's units stay together)
+      std::stable_sort(units.begin(), units.end(),
+                       [&](const uint4& a, const uint4& c) { return unit_len[a.x] > unit_len[c.x]; });
+      // log-det matrices grouped by order bucket (each keeps its own result slots)
+      std::stable_sort(mats.begin(), mats.end(),
+                       [](const rpa::MatDesc& a, const rpa::MatDesc& c) { return plan_bucket(a.n) < plan_bucket(c.n); });
+      for (int m = 0; m < (int)mats.size(); ++m) {
+        if (dv.buckets.empty() || plan_bucket(mats[m].n) != plan_bucket(mats[dv.buckets.back().first].n))
+          dv.buckets.push_back({m, 0, 0, 0, 0, 0.0});
+        Bucket& bk = dv.buckets.back();
+        ++bk.count;
+        bk.nmax = std::max(bk.nmax, mats[m].n);
+        bk.cost += std::pow((double)mats[m].n, 3);
+        if (bk.tune_count < 128) {
+          ++bk.tune_count;
+          bk.tune_nmax = std::max(bk.tune_nmax, mats[m].n);
+        }
+      }
+      // descriptors -> device (laid out as in desc_off)
+      uint8_t* d = descBase + desc_off[b];
+      auto put = [&](const void* src, size_t bytes) {
+        uint8_t* at = d;
+        if (bytes) cudaMemcpyAsync(at, src, bytes, cudaMemcpyHostToDevice, h->stream);
+        d += (bytes + 255) / 256 * 256;
+        return at;
+      };
+      dv.sinst = reinterpret_cast<rpa::SyrkInst*>(put(sinst.data(), sizeof(rpa::SyrkInst) * sinst.size()));
+      dv.jobs = reinterpret_cast<rpa::SplitJob*>(put(jobs.data(), sizeof(rpa::SplitJob) * jobs.size()));
+      dv.offs = reinterpret_cast<int64_t*>(put(offs.data(), sizeof(int64_t) * offs.size()));
+      dv.units = reinterpret_cast<uint4*>(put(units.data(), sizeof(uint4) * units.size()));
+      dv.work = reinterpret_cast<int4*>(put(work.data(), sizeof(int4) * work.size()));
+      dv.mats = reinterpret_cast<rpa::MatDesc*>(put(mats.data(), sizeof(rpa::MatDesc) * mats.size()));
+      RPA_CUDA(h, cudaGetLastError());
+      RPA_CUDA(h, cudaStreamSynchronize(h->stream));  // host vectors must outlive their copies
+      dv.nunits = (int)units.size();
+      dv.nwork = (int)work.size();
+      dv.ni = ni;
+      dv.offs_total = offs.back();
+      dv.max_chunks = sync_max_chunks[b];
+      dv.sync_words = sync_off[b + 1] - sync_off[b];
+      dv.msync = dv.sync_words > 0 ? static_cast<int*>(h->syncBuf.p) + sync_off[b] : nullptr;
+    }
+    // ---- tile plans of order buckets met for the first time, tuned on this call's own buffers
+    if (h->autotune) {
+      for (const BatchDev& dv : bd)
+        for (const Bucket& bk : dv.buckets)
+          if (!h->logdet_plans.count(plan_bucket(bk.nmax)))
+            if ((s = tune_logdet_on(h, dv.mats + bk.first, bk.tune_count, bk.tune_nmax, nullptr))) return s;
+      RPA_CUDA(h, cudaMemsetAsync(h->err_dev, 0, sizeof(int), h->stream));
+    }
+    // ---- one graph for the whole call.  Split form: batch b+1's scale/split pass (branch aux[0])
+    // overlaps batch b's log-det; its SYRK waits for both.  Log-det order buckets run on up to
+    // three branches, longest first.
+    cudaStream_t S0 = h->stream, S1 = h->aux[0];
+    cudaStream_t br[3] = {h->stream, h->aux[1], h->aux[2]};
+    auto split_pass = [&](const BatchDev& dv, cudaStream_t st) {
+      cudaError_t r = cudaSuccess;
+      if (dv.sync_words > 0) r = cudaMemsetAsync(dv.msync, 0, (size_t)dv.sync_words * sizeof(int), st);
+      if (r == cudaSuccess) r = rpa::launch_scale_split_multi(dv.jobs, dv.work, dv.nwork, dv.offs, dv.ni, dv.offs_total, st);
+      return r;
+    };
+    auto logdet = [&](const BatchDev& dv) {
+      const int nb = (int)dv.buckets.size();
+      const int nbr = std::min(3, nb);
+      std::vector<int> order(nb);
+      for (int i = 0; i < nb; ++i) order[i] = i;
+      std::stable_sort(order.begin(), order.end(),
+                       [&](int a, int c) { return dv.buckets[a].cost > dv.buckets[c].cost; });
+      double load[3] = {0.0, 0.0, 0.0};
+      std::vector<int> branch(nb, 0);
+      for (int i : order) {
+        int j = 0;
+        for (int q = 1; q < nbr; ++q)
+          if (load[q] < load[j]) j = q;
+        branch[i] = j;
+        load[j] += dv.buckets[i].cost;
+      }
+      cudaError_t r = cudaSuccess;
+      if (nbr > 1) {
+        r = cudaEventRecord(h->fork_ev[0], S0);
+        for (int j = 1; j < nbr && r == cudaSuccess; ++j) r = cudaStreamWaitEvent(br[j], h->fork_ev[0], 0);
+      }
+      for (int i : order) {
+        if (r != cudaSuccess) break;
+        const Bucket& bk = dv.buckets[i];
+        r = rpa::launch_logdet_varlen(dv.mats + bk.first, bk.count, bk.nmax, h->err_dev, br[branch[i]],
+                                      plan_for(h, bk.nmax));
+      }
+      for (int j = 1; j < nbr && r == cudaSuccess; ++j) {
+        r = cudaEventRecord(h->fork_ev[j], br[j]);
+        if (r == cudaSuccess) r = cudaStreamWaitEvent(S0, h->fork_ev[j], 0);
+      }
+      return r;
+    };
     const int64_t before = rpa::g_launches;
     cudaGraph_t graph = nullptr;
-    RPA_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    RPA_CUDA(h, cudaStreamBeginCapture(S0, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
+    const int nbatch = (int)bd.size();
     if (prec == RPA_PREC_SPLIT_BF16) {
-      if (sync_words > 0) e = cudaMemsetAsync(msync, 0, (size_t)sync_words * sizeof(int), h->stream);
-      if (e == cudaSuccess)
-        e = rpa::launch_scale_split_multi(dJobs, dWork, (int)work.size(), dOffs, ni, offs.back(), h->stream);
-      if (e == cudaSuccess)
-        e = rpa::launch_syrk_split_bf16_multi(dSinst, dUnits, (int)units.size(),
+      e = split_pass(bd[0], S0);
+      for (int b = 0; b < nbatch && e == cudaSuccess; ++b) {
+        const BatchDev& dv = bd[b];
+        e = rpa::launch_syrk_split_bf16_multi(dv.sinst, dv.units, dv.nunits,
                                               h->seg_chunks > 0 ? h->seg_chunks : 1 << 30, h->err_dev, h->num_sms,
-                                              h->stream, sync_words > 0 ? msync : nullptr, h->sync_every, 2,
-                                              max_chunks);
+                                              S0, dv.msync, h->sync_every, 2, dv.max_chunks);
+        const bool next = b + 1 < nbatch;
+        if (next && e == cudaSuccess) e = cudaEventRecord(h->fork_ev[3], S0);
+        if (next && e == cudaSuccess) e = cudaStreamWaitEvent(S1, h->fork_ev[3], 0);
+        if (next && e == cudaSuccess) e = split_pass(bd[b + 1], S1);
+        if (next && e == cudaSuccess) e = cudaEventRecord(h->fork_ev[4], S1);
+        if (e == cudaSuccess) e = logdet(dv);
+        if (next && e == cudaSuccess) e = cudaStreamWaitEvent(S0, h->fork_ev[4], 0);
+      }
     } else {
-      for (int t = 0; t < ni && e == cudaSuccess; ++t) {
-        const int i = i0 + t;
-        rpa::DsyrkArgs a{};
-        a.A = Rd[i];
-        a.lda = ldR[i];
-        a.strideA = 0;
-        size_t mi = 0;  // first matrix of instance t in this batch
-        for (int u = 0; u < t; ++u) mi += (size_t)v[i0 + u].K;
-        a.C = mats[mi].A;
-        a.ldc = v[i].NQ;
-        a.strideC = (int64_t)v[i].NQ * v[i].NQ;
-        a.n = v[i].NQ;
-        a.kdim = v[i].nov;
-        a.batch = v[i].K;
-        a.D = D + Doff[i];
-        a.alpha = inst[i].alpha;
-        for (int k = 0; k < v[i].K; ++k) a.u2[k] = v[i].freqs[k] * v[i].freqs[k];
-        e = rpa::launch_dsyrk_lower(a, h->stream);
+      for (int b = 0; b < nbatch && e == cudaSuccess; ++b) {
+        for (const rpa::DsyrkArgs& a : bd[b].fp64) {
+          e = rpa::launch_dsyrk_lower(a, S0);
+          if (e != cudaSuccess) break;
+        }
+        if (e == cudaSuccess) e = logdet(bd[b]);
       }
     }
-    if (e == cudaSuccess) e = rpa::launch_logdet_varlen(dMats, (int)mats.size(), nmax, h->err_dev, h->stream);
-    cudaError_t e2 = cudaStreamEndCapture(h->stream, &graph);
+    cudaError_t e2 = cudaStreamEndCapture(S0, &graph);
     const int64_t count = rpa::g_launches - before;
     rpa::g_launches = before;
     if (e != cudaSuccess || e2 != cudaSuccess || !graph) {
       if (graph) cudaGraphDestroy(graph);
-      return fail(h, RPA_ERR_CUDA, "capture of batch %zu failed: %s", b, cudaGetErrorString(e != cudaSuccess ? e : e2));
+      return fail(h, RPA_ERR_CUDA, "capture of the batched launch sequence failed: %s",
+                  cudaGetErrorString(e != cudaSuccess ? e : e2));
     }
     cudaGraphExec_t exec = nullptr;
     cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
@@ -2470,8 +2699,8 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
     h->bgraph.launches.push_back(count);
     RPA_CUDA(h, cudaGraphLaunch(exec, h->stream));
     rpa::g_launches += count;
+    h->bgraph.key = keyed(h->plans_version);
   }
-  if (!cached) h->bgraph.key = key;
   RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
   RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
   std::vector<double> res(res_off.back());

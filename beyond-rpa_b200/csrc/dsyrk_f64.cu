@@ -8,17 +8,29 @@
 //  * the trailing update of the blocked Cholesky (C -= P P^T).
 // A is column-major (rows contiguous), exactly the Cholesky-vector layout
 // R(Q, ai) and the panel layout of a column-major lower Cholesky factor.
-// CTA tile 64 x 64, 4 warps in 2 x 2, warp tile 32 x 32 (4 x 4 DMMA tiles),
-// 16-deep K chunks streamed through a 3-stage cp.async pipeline.
+// Two CTA tiles (the tile tuner picks one per matrix-size bucket):
+//   kW = 2: 64 x 64, 4 warps (2 x 2), 4 CTAs per SM;
+//   kW = 4: 128 x 128, 16 warps (4 x 4), 1 CTA per SM (half the operand
+//           traffic per flop, coarser tiles on the triangle's diagonal).
+// Warp tile 32 x 32 (4 x 4 DMMA tiles) in both; 16-deep K chunks streamed
+// through a 3-stage cp.async pipeline.
+#include <algorithm>
+
 #include "kernels.h"
 
 namespace rpa {
 
 namespace {
-constexpr int BM = 64;
 constexpr int BK = 16;
-constexpr int LDS = BM + 8;  // 72 doubles: fragment loads hit each bank pair twice (optimal)
-constexpr int kThreads = 128;
+// Tile geometry of the kW x kW-warp CTA.  Row pitch BM + 8 doubles (72 or 136): the m8n8k4
+// fragment loads hit each bank pair twice (optimal) in both.
+template <int kW>
+struct Geo {
+  static constexpr int BM = 32 * kW;
+  static constexpr int LDS = BM + 8;
+  static constexpr int kThreads = 32 * kW * kW;
+  static constexpr int kMinBlocks = kW == 2 ? 4 : 1;
+};
 
 __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
@@ -40,9 +52,11 @@ __device__ __forceinline__ void trap_decode(int b, int T, int Tc, int& tm, int& 
   tm = tn + (b - (tn * T - tn * (tn - 1) / 2));
 }
 
-// One 64 x 64 tile (tm, tn) of C(lower trapezoid, ncols columns) for matrix z.
 constexpr int kStages = 3;  // cp.async pipeline depth
-constexpr size_t kTileSmem = sizeof(double) * (size_t)kStages * (2 * BK * LDS + BK);
+template <int kW>
+constexpr size_t tile_smem() {
+  return sizeof(double) * (size_t)kStages * (2 * BK * Geo<kW>::LDS + BK);
+}
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
@@ -53,21 +67,23 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
-// One 64 x 64 tile (tm, tn) of C(lower trapezoid, ncols columns) for matrix z.
+// One BM x BM tile (tm, tn) of C(lower trapezoid, ncols columns) for matrix z.
 // Operands stream global -> shared through a kStages-deep cp.async pipeline
 // (out-of-range elements zero-filled); one barrier per 16-deep K chunk.
-template <bool kScaled>
+template <bool kScaled, int kW>
 __device__ __forceinline__ void dsyrk_tile(const DsyrkArgs& a, const double* A, double* C, int ncols, int tm, int tn,
                                            int z) {
-  extern __shared__ double tile_smem[];
-  auto As = reinterpret_cast<double(*)[BK][LDS]>(tile_smem);                        // [kStages]
-  auto Bs = reinterpret_cast<double(*)[BK][LDS]>(tile_smem + kStages * BK * LDS);   // [kStages]
-  auto sS = reinterpret_cast<double(*)[BK]>(tile_smem + 2 * kStages * BK * LDS);    // [kStages]
+  constexpr int BM = Geo<kW>::BM, LDS = Geo<kW>::LDS, kThreads = Geo<kW>::kThreads;
+  constexpr int kLoads = BK * BM / kThreads;  // elements of each operand per thread and stage
+  extern __shared__ double dyn_smem[];
+  auto As = reinterpret_cast<double(*)[BK][LDS]>(dyn_smem);                        // [kStages]
+  auto Bs = reinterpret_cast<double(*)[BK][LDS]>(dyn_smem + kStages * BK * LDS);   // [kStages]
+  auto sS = reinterpret_cast<double(*)[BK]>(dyn_smem + 2 * kStages * BK * LDS);    // [kStages]
 
   const int m0 = tm * BM, n0 = tn * BM;
   const int t = threadIdx.x;
   const int lane = t & 31, warp = t >> 5;
-  const int wm = warp >> 1, wn = warp & 1;
+  const int wm = warp / kW, wn = warp % kW;
   const double u2 = kScaled ? a.u2[z] : 0.0;
 
   double acc[4][4][2];
@@ -78,7 +94,7 @@ __device__ __forceinline__ void dsyrk_tile(const DsyrkArgs& a, const double* A, 
 
   auto load_stage = [&](int st, int64_t k0) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
+    for (int i = 0; i < kLoads; ++i) {
       const int idx = t + kThreads * i;
       const int col = idx / BM, row = idx % BM;
       const int64_t k = k0 + col;
@@ -146,76 +162,116 @@ __device__ __forceinline__ void dsyrk_tile(const DsyrkArgs& a, const double* A, 
   }
 }
 
-template <bool kScaled>
-__global__ void __launch_bounds__(kThreads, 4) dsyrk_lower_kernel(const DsyrkArgs a, const int T, const int Tc) {
+template <bool kScaled, int kW>
+__global__ void __launch_bounds__(Geo<kW>::kThreads, Geo<kW>::kMinBlocks)
+    dsyrk_lower_kernel(const DsyrkArgs a, const int T, const int Tc) {
   int tm, tn;
   trap_decode(blockIdx.x, T, Tc, tm, tn);
   const int ncols = a.ncols > 0 ? a.ncols : a.n;
   const int z = blockIdx.y;
-  dsyrk_tile<kScaled>(a, a.A + (int64_t)z * a.strideA, a.C + (int64_t)z * a.strideC, ncols, tm, tn, z);
+  dsyrk_tile<kScaled, kW>(a, a.A + (int64_t)z * a.strideA, a.C + (int64_t)z * a.strideC, ncols, tm, tn, z);
 }
 
-// Variable-size batch: step of the two-level blocked Cholesky.
-//   mode 0 (panel update): C = A[j0+64:, j0+64:], n = N - j0 - 64, ncols = min(N, J0+256) - (j0+64), K = 64
-//   mode 1 (trailing):     C = A[J1:, J1:],       n = N - J1, J1 = min(N, J0+256), K = J1 - J0
-__global__ void __launch_bounds__(kThreads, 4) dsyrk_varlen_kernel(const MatDesc* mats, int mode, int J0, int j0) {
-  const MatDesc md = mats[blockIdx.y];
-  const int N = md.n;
-  const int J1 = min(N, J0 + 256);
-  DsyrkArgs a{};
-  int ncols;
+// Shape of one step of the two-level blocked Cholesky for a matrix of order N
+// (outer block nb2, inner block kCholNB):
+//   mode 0 (panel update): C = A[j0+NB:, j0+NB:], n = N - j0 - NB, ncols = min(N, J0+nb2) - (j0+NB), K = NB
+//   mode 1 (trailing):     C = A[J1:, J1:],       n = N - J1, J1 = min(N, J0+nb2), K = J1 - J0
+__host__ __device__ __forceinline__ void varlen_step(int N, int mode, int J0, int j0, int nb2, int& n, int& ncols,
+                                                     int& kdim, int& arow, int& acol) {
+  const int J1 = N < J0 + nb2 ? N : J0 + nb2;
   if (mode == 0) {
-    a.n = N - j0 - BM;
-    ncols = J1 - (j0 + BM);
-    a.kdim = BM;
-    a.A = md.A + (int64_t)(j0 + BM) + md.ld * (int64_t)j0;
-    a.C = md.A + (int64_t)(j0 + BM) + md.ld * (int64_t)(j0 + BM);
+    n = N - j0 - kCholNB;
+    ncols = J1 - (j0 + kCholNB);
+    kdim = kCholNB;
+    arow = j0 + kCholNB;
+    acol = j0;
   } else {
-    a.n = N - J1;
-    ncols = a.n;
-    a.kdim = J1 - J0;
-    a.A = md.A + (int64_t)J1 + md.ld * (int64_t)J0;
-    a.C = md.A + (int64_t)J1 + md.ld * (int64_t)J1;
+    n = N - J1;
+    ncols = n;
+    kdim = J1 - J0;
+    arow = J1;
+    acol = J0;
   }
-  if (a.n <= 0 || ncols <= 0 || a.kdim <= 0) return;
-  a.lda = md.ld;
-  a.ldc = md.ld;
-  const int T = (a.n + BM - 1) / BM;
-  const int Tc = (min(ncols, a.n) + BM - 1) / BM;
+  if (ncols > n) ncols = n;
+}
+
+template <int kW>
+__global__ void __launch_bounds__(Geo<kW>::kThreads, Geo<kW>::kMinBlocks)
+    dsyrk_varlen_kernel(const MatDesc* mats, int mode, int J0, int j0, int nb2) {
+  constexpr int BM = Geo<kW>::BM;
+  const MatDesc md = mats[blockIdx.y];
+  int n, ncols, kdim, arow, acol;
+  varlen_step(md.n, mode, J0, j0, nb2, n, ncols, kdim, arow, acol);
+  if (n <= 0 || ncols <= 0 || kdim <= 0) return;
+  const int T = (n + BM - 1) / BM;
+  const int Tc = (ncols + BM - 1) / BM;
   const int tiles = Tc * T - Tc * (Tc - 1) / 2;
   if ((int)blockIdx.x >= tiles) return;
+  DsyrkArgs a{};
+  a.n = n;
+  a.kdim = kdim;
+  a.A = md.A + (int64_t)arow + md.ld * (int64_t)acol;
+  a.C = md.A + (int64_t)arow + md.ld * (int64_t)arow;
+  a.lda = md.ld;
+  a.ldc = md.ld;
   int tm, tn;
   trap_decode(blockIdx.x, T, Tc, tm, tn);
-  dsyrk_tile<false>(a, a.A, a.C, min(ncols, a.n), tm, tn, 0);
+  dsyrk_tile<false, kW>(a, a.A, a.C, ncols, tm, tn, 0);
 }
-}  // namespace
 
-cudaError_t launch_dsyrk_varlen(const MatDesc* mats, int nmat, int mode, int J0, int j0, int max_tiles,
-                                cudaStream_t stream) {
-  if (nmat <= 0 || max_tiles <= 0) return cudaSuccess;
-  cudaError_t e0 = cudaFuncSetAttribute(dsyrk_varlen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTileSmem);
+int trap_tiles(int n, int ncols, int bm) {
+  if (n <= 0 || ncols <= 0) return 0;
+  const int T = (n + bm - 1) / bm, Tc = (std::min(ncols, n) + bm - 1) / bm;
+  return Tc * T - Tc * (Tc - 1) / 2;
+}
+
+template <int kW>
+cudaError_t launch_varlen_w(const MatDesc* mats, int nmat, int mode, int J0, int j0, int nb2, int nmax,
+                            cudaStream_t stream) {
+  int n, ncols, kdim, arow, acol;
+  varlen_step(nmax, mode, J0, j0, nb2, n, ncols, kdim, arow, acol);  // the largest order has the most tiles
+  const int tiles = trap_tiles(n, ncols, Geo<kW>::BM);
+  if (tiles <= 0 || kdim <= 0) return cudaSuccess;
+  constexpr size_t smem = tile_smem<kW>();
+  cudaError_t e0 = cudaFuncSetAttribute(dsyrk_varlen_kernel<kW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem);
   if (e0 != cudaSuccess) return e0;
-  dsyrk_varlen_kernel<<<dim3((unsigned)max_tiles, (unsigned)nmat), kThreads, kTileSmem, stream>>>(mats, mode, J0, j0);
+  dsyrk_varlen_kernel<kW><<<dim3((unsigned)tiles, (unsigned)nmat), Geo<kW>::kThreads, smem, stream>>>(mats, mode, J0,
+                                                                                                     j0, nb2);
   ++g_launches;
   return cudaGetLastError();
 }
 
-cudaError_t launch_dsyrk_lower(const DsyrkArgs& a, cudaStream_t stream) {
-  if (a.n <= 0 || a.batch <= 0) return cudaSuccess;
+template <bool kScaled, int kW>
+cudaError_t launch_lower_w(const DsyrkArgs& a, cudaStream_t stream) {
+  constexpr int BM = Geo<kW>::BM;
   const int T = (a.n + BM - 1) / BM;
   const int nc = (a.ncols > 0 && a.ncols < a.n) ? a.ncols : a.n;
   const int Tc = (nc + BM - 1) / BM;
   const int64_t tiles = (int64_t)Tc * T - (int64_t)Tc * (Tc - 1) / 2;
-  dim3 grid((unsigned)tiles, (unsigned)a.batch);
-  cudaError_t e0 = a.D ? cudaFuncSetAttribute(dsyrk_lower_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)kTileSmem)
-                       : cudaFuncSetAttribute(dsyrk_lower_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)kTileSmem);
+  constexpr size_t smem = tile_smem<kW>();
+  cudaError_t e0 = cudaFuncSetAttribute(dsyrk_lower_kernel<kScaled, kW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem);
   if (e0 != cudaSuccess) return e0;
-  if (a.D) dsyrk_lower_kernel<true><<<grid, kThreads, kTileSmem, stream>>>(a, T, Tc);
-  else dsyrk_lower_kernel<false><<<grid, kThreads, kTileSmem, stream>>>(a, T, Tc);
+  dsyrk_lower_kernel<kScaled, kW><<<dim3((unsigned)tiles, (unsigned)a.batch), Geo<kW>::kThreads, smem, stream>>>(
+      a, T, Tc);
   ++g_launches;
   return cudaGetLastError();
+}
+}  // namespace
+
+// One step of the variable-size blocked Cholesky over nmat matrices of orders <= nmax.
+cudaError_t launch_dsyrk_varlen(const MatDesc* mats, int nmat, int mode, int J0, int j0, int nb2, int tile_w,
+                                int nmax, cudaStream_t stream) {
+  if (nmat <= 0) return cudaSuccess;
+  return tile_w == 4 ? launch_varlen_w<4>(mats, nmat, mode, J0, j0, nb2, nmax, stream)
+                     : launch_varlen_w<2>(mats, nmat, mode, J0, j0, nb2, nmax, stream);
+}
+
+cudaError_t launch_dsyrk_lower(const DsyrkArgs& a, cudaStream_t stream) {
+  if (a.n <= 0 || a.batch <= 0) return cudaSuccess;
+  if (a.tile_w == 4) return a.D ? launch_lower_w<true, 4>(a, stream) : launch_lower_w<false, 4>(a, stream);
+  return a.D ? launch_lower_w<true, 2>(a, stream) : launch_lower_w<false, 2>(a, stream);
 }
 
 }  // namespace rpa

@@ -140,14 +140,24 @@ struct DsyrkArgs {
   const double* D;  // nullptr -> subtract mode
   double alpha;
   double u2[64];
+  int tile_w;       // warps per CTA-tile side: 2 (64 x 64 tiles, 128 threads) or 4 (128 x 128, 512); 0 = 2
 };
 cudaError_t launch_dsyrk_lower(const DsyrkArgs& a, cudaStream_t stream);
 
 // ---------------------------------------------------------------- log-det
 // Batched lower Cholesky of nmat matrices (column-major, ld, stride),
 // on entry A = 1 + Pi (lower triangle), on exit L; Ldiag[z*n + i] = L_ii.
+// Tile plan of the blocked Cholesky: the outer block (columns per trailing update, a multiple
+// of kCholNB) and the CTA tile of its FP64 SYRK updates (DsyrkArgs::tile_w).
+constexpr int kCholNB = 64;  // inner block: diagonal factorization and panel solve
+struct LogdetPlan {
+  int nb2;
+  int tile_w;
+};
+LogdetPlan default_logdet_plan();  // 256-column outer block (RPA_B200_CHOL_NB2 overrides), 64 x 64 tiles
+bool valid_logdet_plan(const LogdetPlan& p);
 cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag, int* err,
-                                  cudaStream_t stream);
+                                  cudaStream_t stream, const LogdetPlan& plan);
 // tr[z] = sum_i A_z(i,i) (double-double, deterministic); then A_z(i,i) += 1.
 // If `diag` is non-null the diagonal is first overwritten with diag[z*n+i].
 cudaError_t launch_trace_shift(double* A, int64_t ld, int64_t stride, int n, int nmat, const double* diag,
@@ -283,7 +293,14 @@ struct MatDesc {
   double* ld_dd;   // 2 doubles: 2 sum log L_ii (double-double)
 };
 // trace_shift + blocked Cholesky + log sums for nmat matrices of orders <= nmax.
-cudaError_t launch_logdet_varlen(const MatDesc* mats, int nmat, int nmax, int* err, cudaStream_t stream);
+cudaError_t launch_logdet_varlen(const MatDesc* mats, int nmat, int nmax, int* err, cudaStream_t stream,
+                                 const LogdetPlan& plan);
+// Overwrite the lower triangles of the matrices with a seeded, strictly diagonally dominant
+// symmetric test matrix (unit diagonal, |off-diagonal row sums| < 1/2): the input of the tile tuner.
+// One SYRK step (mode 0: panel update, mode 1: trailing update) of the variable-size schedule.
+cudaError_t launch_dsyrk_varlen(const MatDesc* mats, int nmat, int mode, int J0, int j0, int nb2, int tile_w,
+                                int nmax, cudaStream_t stream);
+cudaError_t launch_fill_spd_varlen(const MatDesc* mats, int nmat, int nmax, uint64_t seed, cudaStream_t stream);
 
 // ---------------------------------------------------------------- symmetric eigensolver
 // Householder tridiagonalisation + divide and conquer + WY back-transformation (syevd.cu).

@@ -242,6 +242,20 @@ __global__ void count_nonfinite_multi_kernel(const double* const* ptrs, const in
   if (local) atomicAdd(count, local);
 }
 
+// Tile-tuner input: unit diagonal, off-diagonal entries uniform in (-1/(2n), 1/(2n)), so every
+// off-diagonal row sum is below 1/2 and the matrix (and 1 + it) is symmetric positive definite.
+__global__ void fill_spd_varlen_kernel(const MatDesc* mats, uint64_t seed) {
+  const MatDesc md = mats[blockIdx.y];
+  const double scale = 1.0 / (double)max(md.n, 1);
+  for (int c = blockIdx.x; c < md.n; c += gridDim.x) {
+    double* col = md.A + md.ld * (int64_t)c;
+    for (int r = c + threadIdx.x; r < md.n; r += blockDim.x) {
+      const uint64_t h = splitmix64(seed ^ splitmix64(((uint64_t)blockIdx.y << 40) ^ ((uint64_t)c << 20) ^ (uint64_t)r));
+      col[r] = r == c ? 1.0 : ((double)(h >> 11) * (1.0 / 9007199254740992.0) - 0.5) * scale;
+    }
+  }
+}
+
 __global__ void copy_lower_kernel(const double* src, int64_t lds, int64_t strideS, double* dst, int64_t ldd,
                                   int64_t strideD, int n) {
   const int z = blockIdx.z;
@@ -253,10 +267,10 @@ __global__ void copy_lower_kernel(const double* src, int64_t lds, int64_t stride
 }  // namespace
 
 // Two-level blocked right-looking Cholesky: 64-wide column panels (diagonal
-// factorization + panel solve + update of the rest of the 256-wide outer
-// block), then one rank-256 update of the trailing matrix per outer block.
+// factorization + panel solve + update of the rest of the outer block), then
+// one rank-nb2 update of the trailing matrix per outer block.
 
-// Outer block width: NB2 unless RPA_B200_CHOL_NB2 (a multiple of NB) says otherwise.
+// Default outer block width: NB2 unless RPA_B200_CHOL_NB2 (a multiple of NB) says otherwise.
 int outer_block() {
   static int nb2 = [] {
     const char* e = std::getenv("RPA_B200_CHOL_NB2");
@@ -266,9 +280,16 @@ int outer_block() {
   return nb2;
 }
 
+LogdetPlan default_logdet_plan() { return LogdetPlan{outer_block(), 2}; }
+
+bool valid_logdet_plan(const LogdetPlan& p) {
+  return p.nb2 >= NB && p.nb2 <= 1024 && p.nb2 % NB == 0 && (p.tile_w == 2 || p.tile_w == 4);
+}
+
 cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag, int* err,
-                                  cudaStream_t stream) {
-  const int nb2 = outer_block();
+                                  cudaStream_t stream, const LogdetPlan& plan) {
+  if (!valid_logdet_plan(plan)) return cudaErrorInvalidValue;
+  const int nb2 = plan.nb2;
   for (int J0 = 0; J0 < n; J0 += nb2) {
     const int J1 = min(n, J0 + nb2);
     for (int j0 = J0; j0 < J1; j0 += NB) {
@@ -296,6 +317,7 @@ cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, 
       u.kdim = NB;
       u.batch = nmat;
       u.D = nullptr;
+      u.tile_w = plan.tile_w;
       e = launch_dsyrk_lower(u, stream);
       if (e != cudaSuccess) return e;
     }
@@ -313,31 +335,27 @@ cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, 
     u.kdim = J1 - J0;
     u.batch = nmat;
     u.D = nullptr;
+    u.tile_w = plan.tile_w;
     cudaError_t e = launch_dsyrk_lower(u, stream);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
 }
 
-cudaError_t launch_dsyrk_varlen(const MatDesc* mats, int nmat, int mode, int J0, int j0, int max_tiles,
-                                cudaStream_t stream);
-
 // Same schedule as launch_cholesky_lower over matrices of different orders:
 // every step is launched for the largest order and matrices that are already
 // finished (or too small for the step) leave at once.
-cudaError_t launch_logdet_varlen(const MatDesc* mats, int nmat, int nmax, int* err, cudaStream_t stream) {
+cudaError_t launch_logdet_varlen(const MatDesc* mats, int nmat, int nmax, int* err, cudaStream_t stream,
+                                 const LogdetPlan& plan) {
   if (nmat <= 0) return cudaSuccess;
+  if (!valid_logdet_plan(plan)) return cudaErrorInvalidValue;
   trace_shift_varlen_kernel<<<nmat, 256, 0, stream>>>(mats);
   ++g_launches;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  auto tiles = [](int n, int ncols) {
-    if (n <= 0 || ncols <= 0) return 0;
-    const int T = (n + 63) / 64, Tc = (std::min(ncols, n) + 63) / 64;
-    return Tc * T - Tc * (Tc - 1) / 2;
-  };
-  for (int J0 = 0; J0 < nmax; J0 += NB2) {
-    const int J1 = std::min(nmax, J0 + NB2);
+  const int nb2 = plan.nb2;
+  for (int J0 = 0; J0 < nmax; J0 += nb2) {
+    const int J1 = std::min(nmax, J0 + nb2);
     for (int j0 = J0; j0 < J1; j0 += NB) {
       potrf_varlen_kernel<<<nmat, 256, 0, stream>>>(mats, j0, err);
       ++g_launches;
@@ -345,17 +363,21 @@ cudaError_t launch_logdet_varlen(const MatDesc* mats, int nmat, int nmax, int* e
       if (below <= 0) break;
       trsm_varlen_kernel<<<dim3((below + 127) / 128, nmat), 128, 0, stream>>>(mats, j0);
       ++g_launches;
-      // the largest tile count of this step is reached by the largest matrix
-      const int ncols = std::min(nmax, J0 + NB2) - (j0 + NB);
-      e = launch_dsyrk_varlen(mats, nmat, 0, J0, j0, tiles(below, ncols), stream);
+      e = launch_dsyrk_varlen(mats, nmat, 0, J0, j0, nb2, plan.tile_w, nmax, stream);
       if (e != cudaSuccess) return e;
     }
-    const int trail = nmax - J1;
-    if (trail <= 0) break;
-    e = launch_dsyrk_varlen(mats, nmat, 1, J0, 0, tiles(trail, trail), stream);
+    if (nmax - J1 <= 0) break;
+    e = launch_dsyrk_varlen(mats, nmat, 1, J0, 0, nb2, plan.tile_w, nmax, stream);
     if (e != cudaSuccess) return e;
   }
   logdet_sum_varlen_kernel<<<nmat, 256, 0, stream>>>(mats);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fill_spd_varlen(const MatDesc* mats, int nmat, int nmax, uint64_t seed, cudaStream_t stream) {
+  if (nmat <= 0 || nmax <= 0) return cudaSuccess;
+  fill_spd_varlen_kernel<<<dim3((unsigned)std::min(nmax, 1024), (unsigned)nmat), 256, 0, stream>>>(mats, seed);
   ++g_launches;
   return cudaGetLastError();
 }

@@ -118,8 +118,8 @@ extern "C" int rpa_b200_ec_from_pi_noalloc(int64_t device, void* stream_ptr, int
     }
     if (rpa::launch_count_nonfinite(Pi, (int64_t)(K * n * n), flags + 1, st) != cudaSuccess ||
         rpa::launch_trace_shift(Pi, (int64_t)n, (int64_t)(n * n), (int)n, (int)K, nullptr, tr, st) != cudaSuccess ||
-        rpa::launch_cholesky_lower(Pi, (int64_t)n, (int64_t)(n * n), (int)n, (int)K, Ldiag, flags, st) !=
-            cudaSuccess ||
+        rpa::launch_cholesky_lower(Pi, (int64_t)n, (int64_t)(n * n), (int)n, (int)K, Ldiag, flags, st,
+                                   rpa::default_logdet_plan()) != cudaSuccess ||
         rpa::launch_logdet_sum(Ldiag, (int)n, (int)K, ld, st) != cudaSuccess) {
       status = RPA_ERR_CUDA;
       break;

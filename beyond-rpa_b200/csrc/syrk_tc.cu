@@ -14,7 +14,9 @@
 //   warps 2..17 epilogue: TMEM -> registers -> FP64 global stores
 //               (warp w reads TMEM lanes 32*(w%4).. and 64 accumulator columns)
 // Work unit = (frequency k, 128-row tile tm, 256-column tile tn) with
-// tm*128 + 127 >= tn*256 (touches the lower triangle).  Segmented
+// tm*128 + 127 >= tn*256 (touches the lower triangle); a unit whose last
+// columns lie above the diagonal or beyond NQ issues a narrower MMA (N = the
+// columns that can hold lower-triangle entries, rounded up to 16).  Segmented
 // accumulation: the ai range of a unit is cut into segments of
 // `seg_chunks` x 32 columns; each segment accumulates into a fresh 128 x 256
 // FP32 TMEM accumulator (two of them, 512 columns, alternate), and the
@@ -40,7 +42,6 @@ constexpr int kThreads = 576;
 constexpr int kEpiWarps = 16;
 constexpr int kEpiCols = TN / 4;  // accumulator columns per epilogue warp
 constexpr uint32_t kTmemCols = 512;
-constexpr uint32_t kIdesc = umma_idesc_bf16_f32(TM, TN);
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align slack*/ + 256 /*barriers*/;
 
 // 32 lanes x 8 consecutive 32-bit TMEM columns per warp, added into acc[0..7]
@@ -257,7 +258,14 @@ __device__ __forceinline__ void syrk_body(const Source& src, int* err, const int
       int it = 0;  // segment counter (selects the TMEM accumulator)
       bool ok = true;
       for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
-        const int nchunks = src.get(u).nchunks;
+        const Unit x = src.get(u);
+        const int nchunks = x.nchunks;
+        // MMA width of this unit: only columns n < min(NQ, (tm+1)*TM) can hold lower-triangle
+        // entries (the first 128 rows of a 256-column block on the diagonal, the ragged last
+        // block), rounded up to the N granularity (16) of a 128-row MMA
+        const int live = min(x.NQ, (x.tm + 1) * TM) - x.tn * TN;
+        const int nmma = min(TN, max(16, (live + 15) & ~15));
+        const uint32_t idesc = umma_idesc_bf16_f32(TM, nmma);
         for (int c0 = 0; c0 < nchunks && ok; c0 += seg_chunks, ++it) {
           const int b = it & 1;
           const uint32_t acc_phase = (uint32_t)((it >> 1) & 1);
@@ -281,9 +289,9 @@ __device__ __forceinline__ void syrk_body(const Source& src, int* err, const int
               const uint32_t off = (uint32_t)(kk * 32);  // 16 bf16 = 32 bytes along K
               const uint64_t dah = umma_desc_k_sw64(ah + off), dal = umma_desc_k_sw64(al + off);
               const uint64_t dbh = umma_desc_k_sw64(bh + off), dbl = umma_desc_k_sw64(bl + off);
-              tc_mma_bf16(d_tmem, dah, dbh, kIdesc, (ch > c0 || kk > 0) ? 1u : 0u);
-              tc_mma_bf16(d_tmem, dah, dbl, kIdesc, 1u);
-              tc_mma_bf16(d_tmem, dal, dbh, kIdesc, 1u);
+              tc_mma_bf16(d_tmem, dah, dbh, idesc, (ch > c0 || kk > 0) ? 1u : 0u);
+              tc_mma_bf16(d_tmem, dah, dbl, idesc, 1u);
+              tc_mma_bf16(d_tmem, dal, dbh, idesc, 1u);
             }
             tc_commit(&empty[stage]);
             if (++stage == kStages) {

@@ -179,13 +179,6 @@ __global__ void offdiag_final_kernel(double* out) {
 }
 
 // ----------------------------------------------------------------- vectors
-__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
-  x += 0x9E3779B97F4A7C15ull;
-  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
-  x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
-  return x ^ (x >> 31);
-}
-
 // uniform [-1/2, 1/2) guess vectors (the reference: random_number - 1/2)
 __global__ void fill_uniform_kernel(double* X, int64_t rows, int64_t cols, int64_t ldx, uint64_t seed) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;

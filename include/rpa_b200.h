@@ -69,6 +69,31 @@ int64_t rpa_b200_last_launches(const rpa_b200_handle* handle);
 int rpa_b200_set_stream(rpa_b200_handle* handle, void* stream);
 
 /*
+ * Tile plans of the FP64 log-det (the blocked Cholesky of 1 + Pi(u)), kept per
+ * bucket of 256 matrix orders on the handle.  A plan is the outer block Nb2
+ * (columns per trailing update: 128, 256 or 512) and the CTA tile edge of its
+ * FP64 SYRK updates (64 or 128).  No reference counterpart: the reference
+ * calls DGEQRF (src/linear-algebra/real_linalg.f90:815), whose blocking MKL
+ * picks internally.
+ *   rpa_b200_tune_logdet: time the six candidates on NMat seeded positive
+ *     definite matrices of order NQ (handle workspace NMat*NQ*NQ doubles), keep
+ *     the fastest for NQ's bucket, return it in *Nb2, *Tile; Ms (6 doubles or
+ *     NULL) receives each candidate's time in the order (128,64) (256,64)
+ *     (512,64) (128,128) (256,128) (512,128).
+ *   rpa_b200_set_logdet_plan: store a plan (e.g. one a previous run tuned).
+ *   rpa_b200_get_logdet_plan: the plan used for order NQ (256/64 if none).
+ *   rpa_b200_set_autotune: 1 (default; 0 if RPA_B200_AUTOTUNE=0 at create)
+ *     lets rpa_b200_ec_batched tune each bucket it meets for the first time,
+ *     on the call's own Pi buffers (up to 128 matrices per bucket); 0 uses
+ *     the stored or default plans only.
+ */
+int rpa_b200_tune_logdet(rpa_b200_handle* handle, int64_t NQ, int64_t NMat, int64_t* Nb2, int64_t* Tile,
+                         double* Ms);
+int rpa_b200_set_logdet_plan(rpa_b200_handle* handle, int64_t NQ, int64_t Nb2, int64_t Tile);
+int rpa_b200_get_logdet_plan(const rpa_b200_handle* handle, int64_t NQ, int64_t* Nb2, int64_t* Tile);
+int rpa_b200_set_autotune(rpa_b200_handle* handle, int64_t on);
+
+/*
  * Pi(u) matrices:  PiU(:,:,u) = alpha * sum_ai R(:,ai) Chi_u(ai) R(:,ai)^T,
  * Chi_u(ai) = D(ai) / (D(ai)^2 + u^2), D(ai) = VirtEnergies(a) - OccEnergies(i).
  * Replaces rpa_THC_PiU / rpa_THC_PiU_BlockAlgo / rpa_THC_ChiRkai

@@ -58,3 +58,11 @@ def test_freq_grid_rejects_bad_gap(pkg):
     e = np.array([-1.0, 0.5, 0.2, 1.0])  # HOMO above LUMO
     with pytest.raises(pkg.RPAError):
         pkg.freq_grid(e, 2, 2)
+
+
+def test_plan_entry_points_reject_a_null_handle(pkg):
+    lib = pkg.load_library()
+    assert lib.rpa_b200_tune_logdet(None, 512, 4, None, None, None) == pkg.RPA_ERR_INVALID_ARG
+    assert lib.rpa_b200_set_logdet_plan(None, 512, 256, 64) == pkg.RPA_ERR_INVALID_ARG
+    assert lib.rpa_b200_get_logdet_plan(None, 512, None, None) == pkg.RPA_ERR_INVALID_ARG
+    assert lib.rpa_b200_set_autotune(None, 1) == pkg.RPA_ERR_INVALID_ARG
