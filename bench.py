@@ -474,37 +474,43 @@ def run_cc(args):
     eo = torch.from_numpy(s.eps_o).cuda()
     ev = torch.from_numpy(s.eps_v).cuda()
     u_out = torch.empty((G, nov), dtype=torch.float64, device="cuda").T
-    ev_ = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    times = {"t2": [], "sosex": [], "mbpt3": []}
-    res = ex_s = ex_m = None
+    ev_ = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    times = {"t2": [], "sosex": [], "mbpt3": [], "sosex_fp64": [], "mbpt3_fp64": []}
+    res = ex_s = ex_m = ex_s64 = ex_m64 = None
     for it in range(args.warmup + args.steps):
         ev_[0].record(stream)
         res = h.dring_t2(s.R, eo, ev, s.freqs, s.weights, prec="split", n_guess=G, seed=5, cutoff_thresh=1e-4,
                          u_out=u_out)
         ev_[1].record(stream)
-        ex_s = h.exchange_sosex(s.R, no, nv, res["U"], res["A"], alpha=1.0)
+        ex_s = h.exchange_sosex(s.R, no, nv, res["U"], res["A"], alpha=1.0, prec="split")
         ev_[2].record(stream)
-        ex_m = h.exchange_mbpt3(s.R, eo, ev, res["U"], res["A"])
+        ex_m = h.exchange_mbpt3(s.R, eo, ev, res["U"], res["A"], prec="split")
         ev_[3].record(stream)
+        ex_s64 = h.exchange_sosex(s.R, no, nv, res["U"], res["A"], alpha=1.0, prec="fp64")
+        ev_[4].record(stream)
+        ex_m64 = h.exchange_mbpt3(s.R, eo, ev, res["U"], res["A"], prec="fp64")
+        ev_[5].record(stream)
         torch.cuda.synchronize()
         if it >= args.warmup:
-            times["t2"].append(ev_[0].elapsed_time(ev_[1]))
-            times["sosex"].append(ev_[1].elapsed_time(ev_[2]))
-            times["mbpt3"].append(ev_[2].elapsed_time(ev_[3]))
+            for k, (a, b) in {"t2": (0, 1), "sosex": (1, 2), "mbpt3": (2, 3), "sosex_fp64": (3, 4),
+                              "mbpt3_fp64": (4, 5)}.items():
+                times[k].append(ev_[a].elapsed_time(ev_[b]))
     NT = res["NT"]
     ms = {k: statistics.mean(v) for k, v in times.items()}
-    flops = {"t2": K * (4.0 * nq * nov * G + 2.0 * nq * nq * nov),
-             "sosex": 2.0 * no * no * nq * nv * NT,
-             "mbpt3": 2.0 * nq * nov * NT + 2.0 * NT * NT * (nq + nov) + 2.0 * nov * NT * NT
-             + 2.0 * no * no * nq * nv * NT}
-    total = sum(ms.values())
+    pair = 2.0 * no * no * nq * nv * NT
+    flops = {"t2": K * (4.0 * nq * nov * G + 2.0 * nq * nq * nov), "sosex": pair, "sosex_fp64": pair,
+             "mbpt3": 2.0 * nq * nov * NT + 2.0 * NT * NT * (nq + nov) + 2.0 * nov * NT * NT + pair}
+    flops["mbpt3_fp64"] = flops["mbpt3"]
+    total = ms["t2"] + ms["sosex"] + ms["mbpt3"]
     print(json.dumps({"metric": "CC-path energies (direct-ring T2 + SOSEX + MBPT3 exchange)",
                       "workload": f"{args.workload}: NQ={nq} NOcc={no} NVirt={nv} nov={nov} K={K} G={G}",
-                      "value": 1e3 / total, "unit": "CC-path evaluations/s", "steps": args.steps,
-                      "warmup": args.warmup, "ms": ms, "NT": NT,
+                      "value": 1e3 / total, "unit": "CC-path evaluations/s (split Pi, split exchange contractions)",
+                      "steps": args.steps, "warmup": args.warmup, "ms": ms, "NT": NT,
                       "algorithmic_tflops": {k: flops[k] / (ms[k] * 1e-3) / 1e12 for k in ms},
+                      "pair_contraction_flops": pair,
                       "Ec_logdet": res["Ec"], "Ec_T2_eig": float(np.sum(res["EigRPA"])),
-                      "Ex_sosex": ex_s, "Ex_mbpt3": ex_m}), flush=True)
+                      "Ex_sosex": ex_s, "Ex_sosex_fp64": ex_s64, "dEx_sosex": ex_s - ex_s64,
+                      "Ex_mbpt3": ex_m, "Ex_mbpt3_fp64": ex_m64, "dEx_mbpt3": ex_m - ex_m64}), flush=True)
     h.close()
 
 

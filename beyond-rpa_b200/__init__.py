@@ -95,7 +95,8 @@ def load_library(path: str | os.PathLike | None = None):
     lib.rpa_b200_ec_batched.argtypes = [_vp, _i64, _vp, _i64, _vp, _vp]
     lib.rpa_b200_ec_grad.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _vp, _dbl, _i64, _vp,
                                      _vp, _i64, _vp, _vp]
-    lib.rpa_b200_exchange_sosex.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _dbl, _i64, _vp]
+    lib.rpa_b200_exchange_sosex.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _dbl, _i64, _i64,
+                                            _vp]
     lib.rpa_b200_syevd.argtypes = [_vp, _i64, _vp, _i64, _vp]
     lib.rpa_b200_jctc2024.argtypes = [_vp, _i64, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64, _i64, _vp, _i64,
                                       _vp, _vp, _i64, _dbl, _i64, _dbl, _vp, _vp]
@@ -105,8 +106,8 @@ def load_library(path: str | os.PathLike | None = None):
     lib.rpa_b200_piu_basis.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _dbl, _dbl, _i64, _i64, _dbl,
                                        _vp, _i64, ctypes.c_uint64, _vp, _i64, _vp, _vp, _vp]
     lib.rpa_b200_project_basis.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64]
-    lib.rpa_b200_exchange_mbpt3.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _i64, _vp, _vp,
-                                            _vp, _i64]
+    lib.rpa_b200_exchange_mbpt3.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _i64, _vp, _i64,
+                                            _vp, _vp, _i64]
     lib.rpa_b200_tune_logdet.argtypes = [_vp, _i64, _i64, _vp, _vp, _vp]
     lib.rpa_b200_set_logdet_plan.argtypes = [_vp, _i64, _i64, _i64]
     lib.rpa_b200_get_logdet_plan.argtypes = [_vp, _i64, _vp, _vp]
@@ -375,8 +376,9 @@ class Handle:
         return {"A": A[:n].copy(), "U": Uo, "EigRPA": eig[:n].copy(), "NT": n,
                 "common_thresh": ct.value, "Ec": ec.value}
 
-    def exchange_sosex(self, R, nocc, nvirt, U, A, alpha=1.0, s2_operator=False):
-        """SOSEX exchange energy -alpha sum (aj|bi) T_aibj (rpa_b200_exchange_sosex)."""
+    def exchange_sosex(self, R, nocc, nvirt, U, A, alpha=1.0, s2_operator=False, prec="fp64"):
+        """SOSEX exchange energy -alpha sum (aj|bi) T_aibj (rpa_b200_exchange_sosex); prec "split"
+        runs the pair contraction as split-BF16 on the tensor cores."""
         nq = int(R.shape[0])
         nov = nocc * nvirt
         r = _colmajor(R, nq)
@@ -384,7 +386,7 @@ class Handle:
         a = _vec(A)
         ex = ctypes.c_double()
         self._check(self.lib.rpa_b200_exchange_sosex(self._h, nq, nocc, nvirt, r.ptr, r.ld, int(U.shape[1]), u.ptr,
-                                                     u.ld, a.ptr, float(alpha), int(bool(s2_operator)),
+                                                     u.ld, a.ptr, float(alpha), int(bool(s2_operator)), _PREC[prec],
                                                      ctypes.byref(ex)))
         return ex.value
 
@@ -475,9 +477,9 @@ class Handle:
                                                float(cutoff_vabij), en.ctypes.data, st.ctypes.data))
         return tuple(en), tuple(int(x) for x in st)
 
-    def exchange_mbpt3(self, R, eps_o, eps_v, U, A, return_x=False):
+    def exchange_mbpt3(self, R, eps_o, eps_v, U, A, return_x=False, prec="fp64"):
         """MBPT3 exchange energy -Tr(X K) (rpa_b200_exchange_mbpt3); with return_x also the
-        Lyapunov solution X."""
+        Lyapunov solution X; prec "split" runs the Tr(XK) pair contraction as split-BF16."""
         nq = int(R.shape[0])
         no, nv = len(eps_o), len(eps_v)
         nov = no * nv
@@ -488,7 +490,7 @@ class Handle:
         ex = ctypes.c_double()
         X = np.zeros((nt, nt), order="F") if return_x else None
         self._check(self.lib.rpa_b200_exchange_mbpt3(self._h, nq, no, nv, r.ptr, r.ld, eo.ptr, ev.ptr, nt, u.ptr, u.ld,
-                                                     a.ptr, ctypes.byref(ex),
+                                                     a.ptr, _PREC[prec], ctypes.byref(ex),
                                                      X.ctypes.data if return_x else None, nt))
         return (ex.value, X) if return_x else ex.value
 

@@ -49,6 +49,7 @@ struct rpa_b200_handle {
   DevBuf jPack, jQS, jS, jD;           // per-orbital PNO packs, QS slots, S blocks, grouped-GEMM descriptors
   DevBuf jT, jM, jV, jMap;             // batched PNO stage: T_ij, T T^T, eigenvectors, column map
   DevBuf jSK;                          // split-K partials of the G products
+  DevBuf sxR, sxU, sxP;                // split-BF16 exchange: R and U (U2) hi/lo rows, partial sums
   struct BatchGraph {
     uint64_t key;
     std::vector<cudaGraphExec_t> execs;
@@ -85,6 +86,7 @@ struct rpa_b200_handle {
   uint64_t plans_version = 0;  // bumped on every change (part of the batched graph key)
   int autotune = 1;            // tune unseen order buckets on their first batched use (RPA_B200_AUTOTUNE=0: off)
   size_t batch_bytes = 0;      // device bytes per batch of the batched entry (0: 60% of free memory)
+  int sosex_seg = 2;           // 32-column chunks per accumulation segment of the split exchange contraction
   DevBuf tune;                 // tuner workspace: descriptors and pivots of its test matrices
   // fork/join branches of the batched graph: [0] the next batch's scale/split pass, [1..2] log-det buckets
   cudaStream_t aux[3] = {};
@@ -810,6 +812,7 @@ int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) {
   if (const char* se = std::getenv("RPA_B200_SYNC_EVERY")) h->sync_every = std::atoi(se);
   if (const char* at = std::getenv("RPA_B200_AUTOTUNE")) h->autotune = std::atoi(at) != 0;
   if (const char* bb = std::getenv("RPA_B200_BATCH_BYTES")) h->batch_bytes = (size_t)std::atoll(bb);
+  if (const char* sg = std::getenv("RPA_B200_SOSEX_SEG")) h->sosex_seg = std::max(1, std::atoi(sg));
   for (auto& e : h->ev) cudaEventCreate(&e);
   for (auto& e : h->fork_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   cudaDriverEntryPointQueryResult q;
@@ -836,7 +839,7 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
                     &h->xM, &h->eW, &h->eA, &h->eZ, &h->thZ, &h->thXa, &h->thXi, &h->thYX, &h->thR,
                     &h->jU, &h->jL, &h->jX, &h->jPno, &h->jWork,
                     &h->jPack, &h->jQS, &h->jS, &h->jD, &h->syncBuf,
-                    &h->jT, &h->jM, &h->jV, &h->jMap, &h->jSK, &h->tune})
+                    &h->jT, &h->jM, &h->jV, &h->jMap, &h->jSK, &h->tune, &h->sxR, &h->sxU, &h->sxP})
     release(*b);
   for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
   if (h->err_dev) cudaFree(h->err_dev);
@@ -1224,13 +1227,74 @@ int rpa_b200_dring_t2(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVir
   return RPA_OK;
 }
 
+// Split-BF16 pair contraction on the tensor cores: *out = sum_{i>=j} (2 - delta_ij) sum_{Q,mu} B_mu
+// W_ij W_ji with W_ij = R_i U_j^T and W_ji = R_j U2_i^T (U2 null: U).  R, U (and U2) are split into
+// bf16 hi/lo rows once per call; the unit partials are summed in a fixed order (deterministic).
+int sosex_split(rpa_b200_handle* h, const double* R, int64_t ldR, int NQ, int no, int nv, const double* U,
+                int64_t ldU, const double* U2, int64_t ldU2, int NT, const double* Bd, double* out) {
+  const int nvp = rpa::sosex_tc_nvp(nv);
+  const size_t P = (size_t)no * nvp;
+  const size_t rb = (size_t)NQ * P * 2, ub = (size_t)NT * P * 2;  // bytes of one bf16 part
+  RPA_CUDA(h, ensure(h->sxR, 2 * rb + 256));
+  RPA_CUDA(h, ensure(h->sxU, (U2 ? 4 : 2) * ub + 256));
+  auto* Rh = static_cast<__nv_bfloat16*>(h->sxR.p);
+  auto* Rl = Rh + (size_t)NQ * P;
+  auto* Uh = static_cast<__nv_bfloat16*>(h->sxU.p);
+  auto* Ul = Uh + (size_t)NT * P;
+  auto* U2h = U2 ? Ul + (size_t)NT * P : Uh;
+  auto* U2l = U2 ? U2h + (size_t)NT * P : Ul;
+  RPA_CUDA(h, rpa::launch_split_rows(R, ldR, NQ, no, nv, Rh, Rl, h->stream));
+  RPA_CUDA(h, rpa::launch_split_cols(U, ldU, NT, no, nv, Uh, Ul, h->stream));
+  if (U2) RPA_CUDA(h, rpa::launch_split_cols(U2, ldU2, NT, no, nv, U2h, U2l, h->stream));
+  CUtensorMap maps[6];
+  int s;
+  if ((s = encode_map(h, &maps[0], Rh, (int64_t)P, NQ, 1, (int64_t)P, 128))) return s;
+  if ((s = encode_map(h, &maps[1], Rl, (int64_t)P, NQ, 1, (int64_t)P, 128))) return s;
+  if ((s = encode_map(h, &maps[2], Uh, (int64_t)P, NT, 1, (int64_t)P, 128))) return s;
+  if ((s = encode_map(h, &maps[3], Ul, (int64_t)P, NT, 1, (int64_t)P, 128))) return s;
+  if ((s = encode_map(h, &maps[4], U2h, (int64_t)P, NT, 1, (int64_t)P, 128))) return s;
+  if ((s = encode_map(h, &maps[5], U2l, (int64_t)P, NT, 1, (int64_t)P, 128))) return s;
+  rpa::SosexTcArgs a{};
+  a.NQ = NQ;
+  a.no = no;
+  a.nvp = nvp;
+  a.NT = NT;
+  a.nqt = (NQ + 127) / 128;
+  a.nmt = (NT + 127) / 128;
+  const int64_t units = rpa::sosex_tc_units(NQ, no, NT);
+  if (units > (int64_t)INT32_MAX) return fail(h, RPA_ERR_INVALID_ARG, "exchange contraction too large (%lld units)",
+                                              (long long)units);
+  a.nunits = (int)units;
+  a.same = U2 ? 0 : 1;
+  a.seg_chunks = h->sosex_seg;
+  a.Bmu = Bd;
+  a.err = h->err_dev;
+  const int64_t np = rpa::sosex_tc_partials(NQ, no, NT);
+  const int64_t chunk = 4096;
+  const int64_t nsum = (np + chunk - 1) / chunk;
+  RPA_CUDA(h, ensure(h->sxP, (size_t)(np + nsum) * 8 + 256));
+  a.partial = static_cast<double*>(h->sxP.p);
+  double* sums = a.partial + np;
+  RPA_CUDA(h, rpa::launch_sosex_split_bf16(maps, a, h->num_sms, h->stream));
+  int64_t nout = 0;
+  RPA_CUDA(h, rpa::launch_chunk_sum(a.partial, np, chunk, sums, &nout, h->stream));
+  std::vector<double> hs((size_t)nout);
+  RPA_CUDA(h, cudaMemcpyAsync(hs.data(), sums, (size_t)nout * 8, cudaMemcpyDeviceToHost, h->stream));
+  if ((s = check_device_error(h))) return s;  // also synchronises the stream
+  dd acc{0.0, 0.0};
+  for (double x : hs) acc = rpa::dd_add(acc, x);
+  *out = acc.hi + acc.lo;
+  return RPA_OK;
+}
+
 int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R,
                             int64_t ldR, int64_t NVecsT2, const double* U, int64_t ldU, const double* A, double Alpha,
-                            int64_t S2Operator, double* Ex) {
+                            int64_t S2Operator, int64_t Prec, double* Ex) {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   const int64_t nov = NOcc * NVirt;
-  if (NQ < 1 || NOcc < 1 || NVirt < 1 || NVecsT2 < 1 || ldR < NQ || ldU < nov || !R || !U || !A || !Ex)
+  if (NQ < 1 || NOcc < 1 || NVirt < 1 || NVecsT2 < 1 || ldR < NQ || ldU < nov || !R || !U || !A || !Ex ||
+      (Prec != RPA_PREC_FP64 && Prec != RPA_PREC_SPLIT_BF16))
     return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_exchange_sosex");
   const int NT = (int)NVecsT2;
   std::vector<double> Ah;
@@ -1265,6 +1329,16 @@ int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
   double* part = Bd + NT;
   RPA_CUDA(h, cudaMemcpyAsync(Bd, B.data(), (size_t)NT * 8, cudaMemcpyHostToDevice, h->stream));
   RPA_CUDA(h, cudaEventRecord(h->ev[1], h->stream));
+  if (Prec == RPA_PREC_SPLIT_BF16) {
+    double sum = 0.0;
+    if ((s = sosex_split(h, Rd, ldr, (int)NQ, (int)NOcc, (int)NVirt, Ud, ldu, nullptr, 0, NT, Bd, &sum))) return s;
+    RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
+    RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
+    RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+    *Ex = -Alpha * sum;
+    finish_timings(h);
+    return RPA_OK;
+  }
   int64_t npart = 0;
   RPA_CUDA(h, rpa::launch_sosex(Rd, ldr, (int)NQ, (int)NOcc, (int)NVirt, Ud, ldu, nullptr, 0, NT, Bd, part, &npart,
                                 h->stream));
@@ -1291,12 +1365,13 @@ int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
 // contracts by about three orders of magnitude per step.  All matrix products are FP64 DMMA GEMMs.
 int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R,
                             int64_t ldR, const double* OccEnergies, const double* VirtEnergies, int64_t NVecsT2,
-                            const double* U, int64_t ldU, const double* A, double* Ex, double* X, int64_t ldX) {
+                            const double* U, int64_t ldU, const double* A, int64_t Prec, double* Ex, double* X,
+                            int64_t ldX) {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   const int64_t nov = NOcc * NVirt;
   if (NQ < 1 || NOcc < 1 || NVirt < 1 || NVecsT2 < 1 || ldR < NQ || ldU < nov || !R || !U || !A || !Ex ||
-      !OccEnergies || !VirtEnergies || (X && ldX < NVecsT2))
+      !OccEnergies || !VirtEnergies || (X && ldX < NVecsT2) || (Prec != RPA_PREC_FP64 && Prec != RPA_PREC_SPLIT_BF16))
     return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_exchange_mbpt3");
   if (NQ > INT32_MAX || nov > INT32_MAX || NVecsT2 > 65535)
     return fail(h, RPA_ERR_TOO_LARGE, "rpa_b200_exchange_mbpt3: dimensions too large");
@@ -1442,11 +1517,17 @@ int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
   RPA_CUDA(h, rpa::launch_gemm_f64(gemm_nn((int)nov, NT, NT, Ud, ldu, Xd, NT, UX, nov), h->stream));
   RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
   int64_t npart = 0;
-  RPA_CUDA(h, rpa::launch_sosex(Rd, ldr, (int)NQ, (int)NOcc, (int)NVirt, Ud, ldu, UX, nov, NT, ones, part, &npart,
-                                h->stream));
+  double split_sum = 0.0;
+  if (Prec == RPA_PREC_SPLIT_BF16) {
+    if ((s = sosex_split(h, Rd, ldr, (int)NQ, (int)NOcc, (int)NVirt, Ud, ldu, UX, nov, NT, ones, &split_sum)))
+      return s;
+  } else {
+    RPA_CUDA(h, rpa::launch_sosex(Rd, ldr, (int)NQ, (int)NOcc, (int)NVirt, Ud, ldu, UX, nov, NT, ones, part, &npart,
+                                  h->stream));
+  }
   RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
   std::vector<double> hp((size_t)npart);
-  RPA_CUDA(h, cudaMemcpyAsync(hp.data(), part, (size_t)npart * 8, cudaMemcpyDeviceToHost, h->stream));
+  if (npart) RPA_CUDA(h, cudaMemcpyAsync(hp.data(), part, (size_t)npart * 8, cudaMemcpyDeviceToHost, h->stream));
   if (X) {
     if (is_device_ptr(X))
       RPA_CUDA(h, cudaMemcpy2DAsync(X, (size_t)ldX * 8, Xd, (size_t)NT * 8, (size_t)NT * 8, (size_t)NT,
@@ -1457,7 +1538,7 @@ int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
   }
   RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
   RPA_CUDA(h, cudaStreamSynchronize(h->stream));
-  dd acc{0.0, 0.0};
+  dd acc{split_sum, 0.0};
   for (double x : hp) acc = rpa::dd_add(acc, x);
   *Ex = -(acc.hi + acc.lo);
   finish_timings(h);

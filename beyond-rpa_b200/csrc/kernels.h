@@ -282,6 +282,32 @@ cudaError_t launch_mbpt3_build(const double* Ukl, const double* Dkl, const doubl
 cudaError_t launch_lyap_scale(double* Y, const double* mu, int n, int* bad, cudaStream_t stream);
 int64_t sosex_partials(int NQ, int no, int NT);
 
+// ---------------------------------------------------------------- split-BF16 SOSEX (sosex_tc.cu)
+// Operands split once into bf16 hi/lo rows of P = no * nvp columns (each occupied block padded
+// to nvp = sosex_tc_nvp(nv), a multiple of 32): R -> NQ rows (launch_split_rows), U and U2 ->
+// NT rows (launch_split_cols).  maps[6]: 3-D tensor maps (P, rows, 1) with 32 x 128 boxes of
+// Rh, Rl, Uh, Ul, U2h, U2l.  partial: 16 FP64 values per unit, (2 - delta_ij) sum B W_ij W_ji.
+struct SosexTcArgs {
+  int NQ, no, nvp, NT;
+  int nqt, nmt, nunits;  // 128-row Q tiles, 128-column mu tiles, pairs x nqt x nmt
+  int same;              // U2 is U: the diagonal pairs need W_ii only
+  int seg_chunks;        // 32-column chunks per TMEM accumulation segment
+  const double* Bmu;
+  double* partial;
+  int* err;
+};
+int sosex_tc_nvp(int nv);
+int64_t sosex_tc_units(int NQ, int no, int NT);
+int64_t sosex_tc_partials(int NQ, int no, int NT);
+cudaError_t launch_split_rows(const double* R, int64_t ldR, int NQ, int no, int nv, __nv_bfloat16* Xh,
+                              __nv_bfloat16* Xl, cudaStream_t stream);
+cudaError_t launch_split_cols(const double* U, int64_t ldU, int NT, int no, int nv, __nv_bfloat16* Xh,
+                              __nv_bfloat16* Xl, cudaStream_t stream);
+cudaError_t launch_sosex_split_bf16(const CUtensorMap* maps, const SosexTcArgs& a, int num_sms, cudaStream_t stream);
+// out[b] = fixed-order sum of x[b*chunk .. (b+1)*chunk); *nout = number of chunks.
+cudaError_t launch_chunk_sum(const double* x, int64_t n, int64_t chunk, double* out, int64_t* nout,
+                             cudaStream_t stream);
+
 // ---------------------------------------------------------------- variable-size batches
 // One matrix of a batch of matrices of different orders (fragments).
 struct MatDesc {

@@ -122,6 +122,17 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
                : "memory");
 }
+// 32 lanes x 8 consecutive 32-bit TMEM columns per warp, added into acc[0..7]
+// (first == true: assigned).
+__device__ __forceinline__ void tmem_ld_add_x8(uint32_t taddr, float* acc, bool first) {
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc[i] = first ? __uint_as_float(r[i]) : acc[i] + __uint_as_float(r[i]);
+}
 // 32 lanes x 32 consecutive 32-bit columns per warp.
 __device__ __forceinline__ void tmem_ld_32x32b_x32(uint32_t taddr, float* v) {
   uint32_t r[32];

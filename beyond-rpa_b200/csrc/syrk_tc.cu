@@ -44,18 +44,6 @@ constexpr int kEpiCols = TN / 4;  // accumulator columns per epilogue warp
 constexpr uint32_t kTmemCols = 512;
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align slack*/ + 256 /*barriers*/;
 
-// 32 lanes x 8 consecutive 32-bit TMEM columns per warp, added into acc[0..7]
-// (first == true: assigned).
-__device__ __forceinline__ void tmem_ld_add_x8(uint32_t taddr, float* acc, bool first) {
-  uint32_t r[8];
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-               : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 8; ++i) acc[i] = first ? __uint_as_float(r[i]) : acc[i] + __uint_as_float(r[i]);
-}
-
 struct UnitCoord {
   int k, tm, tn;
 };

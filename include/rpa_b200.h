@@ -220,10 +220,13 @@ int rpa_b200_dring_t2(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVir
  * Replaces rpa_CC_Exchange_SOSEX + rpa_CC_EcExchange1
  * (src/rpa/rpa_CC_Exchange.f90:36-116).  U is (nov x NVecsT2) column-major
  * (ldU >= nov), i.e. the transpose of that routine's Vkai(NVecsT2, NVirt, NOcc).
+ * Prec: RPA_PREC_FP64 (the pair GEMMs on FP64 DMMA) or RPA_PREC_SPLIT_BF16
+ * (R and U split into bf16 hi/lo, three tcgen05 products per W tile, FP32
+ * accumulation in 64-column segments, FP64 Hadamard sums).
  */
 int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R,
                             int64_t ldR, int64_t NVecsT2, const double* U, int64_t ldU, const double* A, double Alpha,
-                            int64_t S2Operator, double* Ex);
+                            int64_t S2Operator, int64_t Prec, double* Ex);
 
 /*
  * Cholesky vectors from THC factors: R(k, ai) = sum_g Zgk(g, k) Xga(g, a) Xgi(g, i),
@@ -314,11 +317,14 @@ int rpa_b200_syevd(rpa_b200_handle* h, int64_t N, double* A, int64_t ldA, double
  * (src/rpa/rpa_CC_Exchange.f90:177-336; the Lyapunov solve replaces
  * real_Lyapunov, src/linear-algebra/real_linalg.f90:125-171).  U and A are
  * the outputs of rpa_b200_dring_t2.  X (may be NULL, ldX >= NVecsT2) receives
- * the Lyapunov solution.  RPA_ERR_NOT_CONVERGED if the solve fails.
+ * the Lyapunov solution.  RPA_ERR_NOT_CONVERGED if the solve fails.  Prec
+ * selects the Tr(XK) pair contraction as in rpa_b200_exchange_sosex (the
+ * Lyapunov solve is FP64 in both).
  */
 int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R,
                             int64_t ldR, const double* OccEnergies, const double* VirtEnergies, int64_t NVecsT2,
-                            const double* U, int64_t ldU, const double* A, double* Ex, double* X, int64_t ldX);
+                            const double* U, int64_t ldU, const double* A, int64_t Prec, double* Ex, double* X,
+                            int64_t ldX);
 
 /*
  * Allocation-free energy from given Pi(u) matrices.  No counterpart in the

@@ -102,6 +102,50 @@ def test_sosex_ragged_shapes(handle):
     assert abs(got - ref) < 1e-12 * max(1.0, abs(ref))
 
 
+# Split-BF16 pair contraction (tcgen05): R and U as bf16 hi/lo pairs, three products, FP32
+# accumulation in 64-column segments.  The accumulator's round-toward-zero bias leaves a
+# relative error of ~1e-6 in E_x on physical amplitudes (a numpy emulation of the
+# accumulation gives 6e-7); the bound below is 5e-6 relative.  Random (unphysical) data
+# cancels more and is checked to 1e-4 relative.
+
+@pytest.mark.parametrize("s2", [False, True])
+def test_sosex_split_matches_oracle(handle, s2):
+    s, x, w, pi, vals, vecs, omega = t2_case(16, 150, 6, 50, 12)
+    A_ref, U_ref, _ = O.t2_direct_ring(s.R, s.eps_o, s.eps_v, x, w, vals, vecs, omega, cutoff_thresh=1e-4)
+    ref = O.exchange_sosex(np.ascontiguousarray(U_ref.T), A_ref, s.R, s.no, s.nv, alpha=1.0, s2_operator=s2)
+    got = handle.exchange_sosex(s.R, s.no, s.nv, U_ref, A_ref, alpha=1.0, s2_operator=s2, prec="split")
+    assert abs(got - ref) < 5e-6 * abs(ref)
+    again = handle.exchange_sosex(s.R, s.no, s.nv, U_ref, A_ref, alpha=1.0, s2_operator=s2, prec="split")
+    assert again == got  # fixed-order reductions: bit-identical
+
+
+def test_sosex_split_ragged_shapes(handle):
+    # nv = 19 (padded to 32), NQ = 77 and NT = 45 (partial 128-row tiles)
+    rng = np.random.default_rng(3)
+    nq, no, nv, nt = 77, 5, 19, 45
+    R = rng.standard_normal((nq, no * nv)) * 0.1
+    U = rng.standard_normal((no * nv, nt)) * 0.2
+    A = -0.05 * rng.uniform(size=nt)
+    ref = O.exchange_sosex(np.ascontiguousarray(U.T), A, R, no, nv, alpha=2.0)
+    got = handle.exchange_sosex(R, no, nv, U, A, alpha=2.0, prec="split")
+    assert abs(got - ref) < 1e-4 * abs(ref)
+
+
+def test_sosex_split_device_inputs_and_many_tiles(handle):
+    # NQ = 300 (3 row tiles), NT = 260 (3 column tiles), nv = 80 (padded to 96: three chunks,
+    # two accumulation segments)
+    import torch
+    rng = np.random.default_rng(8)
+    s = O.make_system(300, 4, 80, 31, decay=50.0, lam0=0.7)
+    U, _ = np.linalg.qr(rng.standard_normal((s.no * s.nv, 260)))
+    A = -0.1 * rng.uniform(size=260)
+    ref = O.exchange_sosex(np.ascontiguousarray(U.T), A, s.R, s.no, s.nv)
+    Rd = torch.from_numpy(np.ascontiguousarray(s.R.T)).cuda().T
+    Ud = torch.from_numpy(np.ascontiguousarray(U.T)).cuda().T
+    got = handle.exchange_sosex(Rd, s.no, s.nv, Ud, A, prec="split")
+    assert abs(got - ref) < 5e-6 * abs(ref)
+
+
 # ----------------------------------------------------------------------------- MBPT3 exchange
 # Tolerances: E_x to 1e-11 relative (FP64 throughout; the GPU Lyapunov solve
 # stops at |res| <= 1e-13 |A|); X to 1e-10 relative to max|X|.
@@ -135,6 +179,15 @@ def test_mbpt3_after_gpu_t2(handle):
     ref, _ = O.exchange_mbpt3_1(res["U"], res["A"], s.R, s.eps_o, s.eps_v)
     got = handle.exchange_mbpt3(s.R, s.eps_o, s.eps_v, res["U"], res["A"])
     assert abs(got - ref) < 1e-11 * max(1.0, abs(ref))
+
+
+def test_mbpt3_split_contraction_matches_oracle(handle):
+    s, x, w, pi, vals, vecs, omega = t2_case(17, 150, 6, 50, 12)
+    A_ref, U_ref, _ = O.t2_direct_ring(s.R, s.eps_o, s.eps_v, x, w, vals, vecs, omega, cutoff_thresh=1e-4)
+    ref, X_ref = O.exchange_mbpt3_1(U_ref, A_ref, s.R, s.eps_o, s.eps_v)
+    got, X = handle.exchange_mbpt3(s.R, s.eps_o, s.eps_v, U_ref, A_ref, return_x=True, prec="split")
+    assert abs(got - ref) < 5e-6 * abs(ref)
+    assert np.max(np.abs(X - X_ref)) < 1e-10 * np.max(np.abs(X_ref))  # the Lyapunov solve stays FP64
 
 
 def test_mbpt3_indefinite_operator_is_reported(handle, pkg):
