@@ -91,6 +91,10 @@ struct rpa_b200_handle {
   // fork/join branches of the batched graph: [0] the next batch's scale/split pass, [1..2] log-det buckets
   cudaStream_t aux[3] = {};
   cudaEvent_t fork_ev[6] = {};
+  // lookahead Cholesky schedules (one per log-det branch): high-priority critical-path stream,
+  // default-priority stream for the rest of each trailing update (RPA_B200_LOOKAHEAD=0: off)
+  bool lookahead = true;
+  rpa::Lookahead la[3] = {};
 };
 
 namespace {
@@ -493,7 +497,8 @@ int tune_logdet_on(rpa_b200_handle* h, const rpa::MatDesc* dmats, int nmat, int 
     for (int rep = 0; rep < 2; ++rep) {
       RPA_CUDA(h, rpa::launch_fill_spd_varlen(dmats, nmat, nmax, 0x5eedull + (uint64_t)rep, h->stream));
       RPA_CUDA(h, cudaEventRecord(t0, h->stream));
-      RPA_CUDA(h, rpa::launch_logdet_varlen(dmats, nmat, nmax, h->err_dev, h->stream, kLogdetCands[c]));
+      RPA_CUDA(h, rpa::launch_logdet_varlen(dmats, nmat, nmax, h->err_dev, h->stream, kLogdetCands[c],
+                                            h->lookahead ? &h->la[0] : nullptr));
       RPA_CUDA(h, cudaEventRecord(t1, h->stream));
       RPA_CUDA(h, cudaEventSynchronize(t1));
       RPA_CUDA(h, cudaEventElapsedTime(&t, t0, t1));
@@ -527,13 +532,14 @@ int cholesky(rpa_b200_handle* h, double* A, int64_t ld, int64_t stride, int n, i
   const int64_t before = rpa::g_launches;
   cudaGraph_t graph = nullptr;
   if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-    cudaError_t e = rpa::launch_cholesky_lower(A, ld, stride, n, nmat, Ldiag, h->err_dev, h->stream, plan);
+    cudaError_t e = rpa::launch_cholesky_lower(A, ld, stride, n, nmat, Ldiag, h->err_dev, h->stream, plan,
+                                               h->lookahead ? &h->la[0] : nullptr);
     cudaError_t e2 = cudaStreamEndCapture(h->stream, &graph);
     const int64_t count = rpa::g_launches - before;
     rpa::g_launches = before;
     cudaGraphExec_t exec = nullptr;
     if (e == cudaSuccess && e2 == cudaSuccess && graph &&
-        cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) {
+        cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority) == cudaSuccess) {
       cudaGraphDestroy(graph);
       if (h->chol_graphs.size() >= 8) {
         cudaGraphExecDestroy(h->chol_graphs.front().exec);
@@ -815,6 +821,19 @@ int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) {
   if (const char* sg = std::getenv("RPA_B200_SOSEX_SEG")) h->sosex_seg = std::max(1, std::atoi(sg));
   for (auto& e : h->ev) cudaEventCreate(&e);
   for (auto& e : h->fork_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  if (const char* la = std::getenv("RPA_B200_LOOKAHEAD")) h->lookahead = std::atoi(la) != 0;
+  {
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    for (auto& l : h->la) {
+      if (cudaStreamCreateWithPriority(&l.crit, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+          cudaStreamCreateWithPriority(&l.rest, cudaStreamNonBlocking, least) != cudaSuccess) {
+        rpa_b200_destroy(h);
+        return RPA_ERR_CUDA;
+      }
+      for (auto& e : l.ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    }
+  }
   cudaDriverEntryPointQueryResult q;
   void* fn = nullptr;
   if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
@@ -855,6 +874,15 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
       cudaStreamSynchronize(st);
       cudaStreamDestroy(st);
     }
+  for (auto& l : h->la) {
+    for (cudaStream_t st : {l.crit, l.rest})
+      if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+      }
+    for (auto& e : l.ev)
+      if (e) cudaEventDestroy(e);
+  }
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   delete h;
@@ -2727,7 +2755,7 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
         if (r != cudaSuccess) break;
         const Bucket& bk = dv.buckets[i];
         r = rpa::launch_logdet_varlen(dv.mats + bk.first, bk.count, bk.nmax, h->err_dev, br[branch[i]],
-                                      plan_for(h, bk.nmax));
+                                      plan_for(h, bk.nmax), h->lookahead ? &h->la[branch[i]] : nullptr);
       }
       for (int j = 1; j < nbr && r == cudaSuccess; ++j) {
         r = cudaEventRecord(h->fork_ev[j], br[j]);
@@ -2773,7 +2801,7 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
                   cudaGetErrorString(e != cudaSuccess ? e : e2));
     }
     cudaGraphExec_t exec = nullptr;
-    cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
+    cudaError_t ei = cudaGraphInstantiate(&exec, graph, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(graph);
     if (ei != cudaSuccess) return fail(h, RPA_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(ei));
     h->bgraph.execs.push_back(exec);

@@ -173,21 +173,31 @@ __global__ void __launch_bounds__(Geo<kW>::kThreads, Geo<kW>::kMinBlocks)
 }
 
 // Shape of one step of the two-level blocked Cholesky for a matrix of order N
-// (outer block nb2, inner block kCholNB):
-//   mode 0 (panel update): C = A[j0+NB:, j0+NB:], n = N - j0 - NB, ncols = min(N, J0+nb2) - (j0+NB), K = NB
-//   mode 1 (trailing):     C = A[J1:, J1:],       n = N - J1, J1 = min(N, J0+nb2), K = J1 - J0
+// (outer block nb2, inner block kCholNB; J1 = min(N, J0+nb2), J2 = min(N, J1+nb2)):
+//   mode 0 (panel update):  C = A[j0+NB:, j0+NB:], n = N - j0 - NB, ncols = J1 - (j0+NB), K = NB
+//   mode 1 (trailing):      C = A[J1:, J1:],       n = N - J1, ncols = n,       K = J1 - J0
+//   mode 2 (next block):    C = A[J1:, J1:J2],     n = N - J1, ncols = J2 - J1, K = J1 - J0
+//   mode 3 (rest):          C = A[J2:, J2:],       n = N - J2, ncols = n,       K = J1 - J0
+// with the panel A[row0:, J0:J1] (row0 = the first row of C) as the SYRK operand.
 __host__ __device__ __forceinline__ void varlen_step(int N, int mode, int J0, int j0, int nb2, int& n, int& ncols,
                                                      int& kdim, int& arow, int& acol) {
   const int J1 = N < J0 + nb2 ? N : J0 + nb2;
+  const int J2 = N < J1 + nb2 ? N : J1 + nb2;
   if (mode == 0) {
     n = N - j0 - kCholNB;
     ncols = J1 - (j0 + kCholNB);
     kdim = kCholNB;
     arow = j0 + kCholNB;
     acol = j0;
+  } else if (mode == 3) {
+    n = N - J2;
+    ncols = n;
+    kdim = J1 - J0;
+    arow = J2;
+    acol = J0;
   } else {
     n = N - J1;
-    ncols = n;
+    ncols = mode == 2 ? J2 - J1 : n;
     kdim = J1 - J0;
     arow = J1;
     acol = J0;

@@ -156,8 +156,15 @@ struct LogdetPlan {
 };
 LogdetPlan default_logdet_plan();  // 256-column outer block (RPA_B200_CHOL_NB2 overrides), 64 x 64 tiles
 bool valid_logdet_plan(const LogdetPlan& p);
+// Lookahead schedule of the blocked Cholesky: the critical path (diagonal blocks, panel solves,
+// the update of the next outer block) on `crit`, the update of the rest of the trailing matrix on
+// `rest`; ev: 4 events without timing.  Both streams join the caller's stream before return.
+struct Lookahead {
+  cudaStream_t crit, rest;
+  cudaEvent_t ev[4];
+};
 cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag, int* err,
-                                  cudaStream_t stream, const LogdetPlan& plan);
+                                  cudaStream_t stream, const LogdetPlan& plan, const Lookahead* la = nullptr);
 // tr[z] = sum_i A_z(i,i) (double-double, deterministic); then A_z(i,i) += 1.
 // If `diag` is non-null the diagonal is first overwritten with diag[z*n+i].
 cudaError_t launch_trace_shift(double* A, int64_t ld, int64_t stride, int n, int nmat, const double* diag,
@@ -320,10 +327,12 @@ struct MatDesc {
 };
 // trace_shift + blocked Cholesky + log sums for nmat matrices of orders <= nmax.
 cudaError_t launch_logdet_varlen(const MatDesc* mats, int nmat, int nmax, int* err, cudaStream_t stream,
-                                 const LogdetPlan& plan);
+                                 const LogdetPlan& plan, const Lookahead* la = nullptr);
 // Overwrite the lower triangles of the matrices with a seeded, strictly diagonally dominant
 // symmetric test matrix (unit diagonal, |off-diagonal row sums| < 1/2): the input of the tile tuner.
-// One SYRK step (mode 0: panel update, mode 1: trailing update) of the variable-size schedule.
+// One SYRK step of the variable-size schedule: mode 0 panel update, mode 1 trailing update,
+// modes 2 and 3 the two halves of the trailing update under lookahead (the next outer block's
+// columns; everything right of them).
 cudaError_t launch_dsyrk_varlen(const MatDesc* mats, int nmat, int mode, int J0, int j0, int nb2, int tile_w,
                                 int nmax, cudaStream_t stream);
 cudaError_t launch_fill_spd_varlen(const MatDesc* mats, int nmat, int nmax, uint64_t seed, cudaStream_t stream);

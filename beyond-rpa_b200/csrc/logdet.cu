@@ -286,67 +286,116 @@ bool valid_logdet_plan(const LogdetPlan& p) {
   return p.nb2 >= NB && p.nb2 <= 1024 && p.nb2 % NB == 0 && (p.tile_w == 2 || p.tile_w == 4);
 }
 
+// Lookahead (la non-null): after the panel of outer block t is factored, the trailing update is
+// split into (a) the columns of block t+1, on the critical stream, and (b) everything right of
+// block t+1, on la->rest.  Block t+1 (diagonal factorizations, panel solves, in-block updates:
+// latency-bound launches) then runs beside (b) of block t, which touches disjoint columns; (a) of
+// block t+1 waits for (b) of block t, whose columns it overlaps.
+namespace {
+struct LookaheadState {
+  const Lookahead* la;
+  cudaStream_t S;  // critical-path stream
+  bool rest_pending = false;
+  cudaError_t begin(cudaStream_t stream) {
+    S = la ? la->crit : stream;
+    if (!la) return cudaSuccess;
+    cudaError_t e = cudaEventRecord(la->ev[0], stream);
+    return e == cudaSuccess ? cudaStreamWaitEvent(la->crit, la->ev[0], 0) : e;
+  }
+  // before (a) of block t: (b) of block t-1 done; the panel of block t is final
+  cudaError_t before_next_block() {
+    cudaError_t e = cudaSuccess;
+    if (rest_pending) e = cudaStreamWaitEvent(S, la->ev[2], 0);
+    if (e == cudaSuccess) e = cudaEventRecord(la->ev[1], S);
+    return e;
+  }
+  cudaError_t fork_rest() { return cudaStreamWaitEvent(la->rest, la->ev[1], 0); }
+  cudaError_t rest_done() {
+    rest_pending = true;
+    return cudaEventRecord(la->ev[2], la->rest);
+  }
+  cudaError_t end(cudaStream_t stream) {
+    if (!la) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    if (rest_pending) e = cudaStreamWaitEvent(S, la->ev[2], 0);
+    if (e == cudaSuccess) e = cudaEventRecord(la->ev[3], S);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, la->ev[3], 0);
+    return e;
+  }
+};
+
+DsyrkArgs update_args(double* A, int64_t ld, int64_t stride, int nmat, int row0, int col0, int n, int ncols,
+                      int kdim, int tile_w) {
+  DsyrkArgs u{};
+  u.A = A + (int64_t)row0 + ld * (int64_t)col0;
+  u.lda = ld;
+  u.strideA = stride;
+  u.C = A + (int64_t)row0 + ld * (int64_t)row0;
+  u.ldc = ld;
+  u.strideC = stride;
+  u.n = n;
+  u.ncols = ncols;
+  u.kdim = kdim;
+  u.batch = nmat;
+  u.D = nullptr;
+  u.tile_w = tile_w;
+  return u;
+}
+}  // namespace
+
 cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag, int* err,
-                                  cudaStream_t stream, const LogdetPlan& plan) {
+                                  cudaStream_t stream, const LogdetPlan& plan, const Lookahead* la) {
   if (!valid_logdet_plan(plan)) return cudaErrorInvalidValue;
   const int nb2 = plan.nb2;
+  LookaheadState st{la, stream};
+  cudaError_t e = st.begin(stream);
+  if (e != cudaSuccess) return e;
+  const cudaStream_t S = st.S;
   for (int J0 = 0; J0 < n; J0 += nb2) {
     const int J1 = min(n, J0 + nb2);
     for (int j0 = J0; j0 < J1; j0 += NB) {
-      potrf_diag_kernel<<<nmat, 256, 0, stream>>>(A, ld, stride, n, j0, Ldiag, err);
+      potrf_diag_kernel<<<nmat, 256, 0, S>>>(A, ld, stride, n, j0, Ldiag, err);
       ++g_launches;
-      cudaError_t e = cudaGetLastError();
+      e = cudaGetLastError();
       if (e != cudaSuccess) return e;
       const int below = n - j0 - NB;
       if (below <= 0) break;
-      trsm_panel_kernel<<<dim3((below + 127) / 128, nmat), 128, 0, stream>>>(A, ld, stride, n, j0);
+      trsm_panel_kernel<<<dim3((below + 127) / 128, nmat), 128, 0, S>>>(A, ld, stride, n, j0);
       ++g_launches;
       e = cudaGetLastError();
       if (e != cudaSuccess) return e;
       const int ncols = J1 - (j0 + NB);  // columns of this outer block right of the panel
       if (ncols <= 0) continue;
-      DsyrkArgs u{};
-      u.A = A + (int64_t)(j0 + NB) + ld * (int64_t)j0;
-      u.lda = ld;
-      u.strideA = stride;
-      u.C = A + (int64_t)(j0 + NB) + ld * (int64_t)(j0 + NB);
-      u.ldc = ld;
-      u.strideC = stride;
-      u.n = below;
-      u.ncols = ncols;
-      u.kdim = NB;
-      u.batch = nmat;
-      u.D = nullptr;
-      u.tile_w = plan.tile_w;
-      e = launch_dsyrk_lower(u, stream);
+      e = launch_dsyrk_lower(update_args(A, ld, stride, nmat, j0 + NB, j0, below, ncols, NB, plan.tile_w), S);
       if (e != cudaSuccess) return e;
     }
     const int trail = n - J1;
     if (trail <= 0) break;
-    DsyrkArgs u{};
-    u.A = A + (int64_t)J1 + ld * (int64_t)J0;
-    u.lda = ld;
-    u.strideA = stride;
-    u.C = A + (int64_t)J1 + ld * (int64_t)J1;
-    u.ldc = ld;
-    u.strideC = stride;
-    u.n = trail;
-    u.ncols = trail;
-    u.kdim = J1 - J0;
-    u.batch = nmat;
-    u.D = nullptr;
-    u.tile_w = plan.tile_w;
-    cudaError_t e = launch_dsyrk_lower(u, stream);
+    if (!la) {
+      e = launch_dsyrk_lower(update_args(A, ld, stride, nmat, J1, J0, trail, trail, J1 - J0, plan.tile_w), S);
+      if (e != cudaSuccess) return e;
+      continue;
+    }
+    const int J2 = min(n, J1 + nb2);
+    if ((e = st.before_next_block()) != cudaSuccess) return e;
+    e = launch_dsyrk_lower(update_args(A, ld, stride, nmat, J1, J0, trail, J2 - J1, J1 - J0, plan.tile_w), S);
     if (e != cudaSuccess) return e;
+    if (n - J2 > 0) {
+      if ((e = st.fork_rest()) != cudaSuccess) return e;
+      e = launch_dsyrk_lower(update_args(A, ld, stride, nmat, J2, J0, n - J2, n - J2, J1 - J0, plan.tile_w),
+                             la->rest);
+      if (e != cudaSuccess) return e;
+      if ((e = st.rest_done()) != cudaSuccess) return e;
+    }
   }
-  return cudaSuccess;
+  return st.end(stream);
 }
 
 // Same schedule as launch_cholesky_lower over matrices of different orders:
 // every step is launched for the largest order and matrices that are already
 // finished (or too small for the step) leave at once.
 cudaError_t launch_logdet_varlen(const MatDesc* mats, int nmat, int nmax, int* err, cudaStream_t stream,
-                                 const LogdetPlan& plan) {
+                                 const LogdetPlan& plan, const Lookahead* la) {
   if (nmat <= 0) return cudaSuccess;
   if (!valid_logdet_plan(plan)) return cudaErrorInvalidValue;
   trace_shift_varlen_kernel<<<nmat, 256, 0, stream>>>(mats);
@@ -354,22 +403,38 @@ cudaError_t launch_logdet_varlen(const MatDesc* mats, int nmat, int nmax, int* e
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const int nb2 = plan.nb2;
+  LookaheadState st{la, stream};
+  if ((e = st.begin(stream)) != cudaSuccess) return e;
+  const cudaStream_t S = st.S;
   for (int J0 = 0; J0 < nmax; J0 += nb2) {
     const int J1 = std::min(nmax, J0 + nb2);
     for (int j0 = J0; j0 < J1; j0 += NB) {
-      potrf_varlen_kernel<<<nmat, 256, 0, stream>>>(mats, j0, err);
+      potrf_varlen_kernel<<<nmat, 256, 0, S>>>(mats, j0, err);
       ++g_launches;
       const int below = nmax - j0 - NB;
       if (below <= 0) break;
-      trsm_varlen_kernel<<<dim3((below + 127) / 128, nmat), 128, 0, stream>>>(mats, j0);
+      trsm_varlen_kernel<<<dim3((below + 127) / 128, nmat), 128, 0, S>>>(mats, j0);
       ++g_launches;
-      e = launch_dsyrk_varlen(mats, nmat, 0, J0, j0, nb2, plan.tile_w, nmax, stream);
+      e = launch_dsyrk_varlen(mats, nmat, 0, J0, j0, nb2, plan.tile_w, nmax, S);
       if (e != cudaSuccess) return e;
     }
     if (nmax - J1 <= 0) break;
-    e = launch_dsyrk_varlen(mats, nmat, 1, J0, 0, nb2, plan.tile_w, nmax, stream);
+    if (!la) {
+      e = launch_dsyrk_varlen(mats, nmat, 1, J0, 0, nb2, plan.tile_w, nmax, S);
+      if (e != cudaSuccess) return e;
+      continue;
+    }
+    if ((e = st.before_next_block()) != cudaSuccess) return e;
+    e = launch_dsyrk_varlen(mats, nmat, 2, J0, 0, nb2, plan.tile_w, nmax, S);
     if (e != cudaSuccess) return e;
+    if (nmax - std::min(nmax, J1 + nb2) > 0) {
+      if ((e = st.fork_rest()) != cudaSuccess) return e;
+      e = launch_dsyrk_varlen(mats, nmat, 3, J0, 0, nb2, plan.tile_w, nmax, la->rest);
+      if (e != cudaSuccess) return e;
+      if ((e = st.rest_done()) != cudaSuccess) return e;
+    }
   }
+  if ((e = st.end(stream)) != cudaSuccess) return e;
   logdet_sum_varlen_kernel<<<nmat, 256, 0, stream>>>(mats);
   ++g_launches;
   return cudaGetLastError();

@@ -117,3 +117,25 @@ def test_batched_autotune_tunes_each_bucket_once(pkg):
         assert np.array_equal(on, again)
     for a, b in zip(on, off):
         assert abs(a - b) <= 1e-12 * abs(b)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "split"])
+def test_lookahead_schedule_is_bit_identical(pkg, prec, monkeypatch):
+    # the lookahead splits each trailing update into two launches over disjoint columns: every
+    # element takes the same products in the same order, so energies must not move at all
+    s = O.make_system(1100, 6, 60, 41, decay=180.0, lam0=0.8)  # five 256-column outer blocks
+    x, w = O.casimir_polder(8, 0.7)
+    sys_ = _fragments(seed=500, n=5) + [(s.R, s.eps_o, s.eps_v, x, w)]
+    out = {}
+    for la in ("0", "1"):
+        monkeypatch.setenv("RPA_B200_LOOKAHEAD", la)
+        with pkg.Handle(0) as h:
+            h.set_autotune(False)
+            ec, eu = h.ec_rpa(s.R, s.eps_o, s.eps_v, x, w, prec=prec)
+            eb, _ = h.ec_batched(sys_, prec=prec)
+            out[la] = (ec, eu, eb)
+    assert out["0"][0] == out["1"][0]
+    assert np.array_equal(out["0"][1], out["1"][1])
+    assert np.array_equal(out["0"][2], out["1"][2])
+    ref, _ = O.ec_rpa(s.R, s.eps_o, s.eps_v, x, w)
+    assert abs(out["1"][0] - ref) < (1e-10 if prec == "fp64" else 1e-6)
