@@ -1716,8 +1716,13 @@ int rpa_b200_piu_basis(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVi
           if ((s = cholesky(h, S, n, (int64_t)nn, n, 1, static_cast<double*>(h->Ldiag.p)))) return s;
           RPA_CUDA(h, rpa::launch_trsm_lower_left(S, n, (int64_t)nn, Yt, n, (int64_t)nn, n, n, 1, h->stream));
         }
+        // the last pass factors the Gram matrix of an (almost) orthonormal Q: its pivots are ~1
+        // unless the columns of Pi G were numerically dependent
+        std::vector<double> piv(n);
+        RPA_CUDA(h, cudaMemcpyAsync(piv.data(), h->Ldiag.p, (size_t)n * 8, cudaMemcpyDeviceToHost, h->stream));
         RPA_CUDA(h, cudaStreamSynchronize(h->stream));
-        if (check_device_error(h) != RPA_OK)
+        const auto mm = std::minmax_element(piv.begin(), piv.end());
+        if (check_device_error(h) != RPA_OK || !(*mm.first > 0.5) || !(*mm.second < 2.0))
           return fail(h, RPA_ERR_NOT_SPD, "random Pi basis: Pi G is numerically rank deficient (CholeskyQR)");
         RPA_CUDA(h, cudaMemcpyAsync(Gd, Yt, nn * 8, cudaMemcpyDeviceToDevice, h->stream));  // Gd <- Q^T
       }

@@ -20,60 +20,79 @@ namespace {
 constexpr int NB = 64;  // Cholesky block size
 constexpr int NB2 = 256;  // outer block of the two-level schedule
 
-// Factor the NB x NB diagonal block of each matrix in shared memory.
-// Column j is used unscaled in step j (update of the columns right of it by
-// a_rj a_cj / d_j) and scaled by 1/sqrt(d_j) in step j+1, when nobody reads
-// it any more: one barrier per column.
+// Factor the NB x NB diagonal block of each matrix (blockDim = 256): thread (r, q) = (t / 4,
+// t % 4) keeps columns q, q+4, ..., q+60 of row r in registers.  Step j: the owners of column j
+// scale it by 1/sqrt(pivot) and publish it in shared memory (double-buffered); every thread
+// subtracts l_rj l_cj from its columns c in (j, r]; the owner of entry (j+1, j+1) then takes its
+// square root.  Two barriers per column and no shared-memory copy of the block.
+__device__ __forceinline__ double reg_get(const double (&v)[NB / 4], int i) {
+  double x = 0.0;
+#pragma unroll
+  for (int k = 0; k < NB / 4; ++k)
+    if (k == i) x = v[k];
+  return x;
+}
+__device__ __forceinline__ void reg_set(double (&v)[NB / 4], int i, double x) {
+#pragma unroll
+  for (int k = 0; k < NB / 4; ++k)
+    if (k == i) v[k] = x;
+}
+
 __device__ __forceinline__ void potrf_diag_body(double* Az, int64_t ld, int n, int j0, double* Ldz, int* err) {
-  __shared__ double L[NB][NB + 1];
+  __shared__ double col[2][NB];
+  __shared__ double piv[NB], pinv[NB];
   const int nbe = min(NB, n - j0);
   const int t = threadIdx.x;
-  for (int idx = t; idx < NB * NB; idx += blockDim.x) {
-    const int r = idx % NB, c = idx / NB;
-    L[r][c] = (r >= c && r < nbe && c < nbe) ? Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] : 0.0;
+  const int r = t >> 2, q = t & 3;
+  const bool live = r < nbe;
+  double v[NB / 4];
+#pragma unroll
+  for (int i = 0; i < NB / 4; ++i) {
+    const int c = q + 4 * i;
+    v[i] = (live && c <= r) ? Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] : 0.0;
   }
-  __syncthreads();
   bool bad = false;
-  for (int j = 0; j < nbe; ++j) {
-    double d = L[j][j];
-    if (!(d > 0.0)) {  // also catches NaN; keep going with a unit pivot, report the error
+  // owner of (j, j): square root of the updated pivot (a non-positive or NaN pivot is replaced
+  // by 1 so that the factorization finishes; the error is reported)
+  auto take_pivot = [&](int j) {
+    double d = reg_get(v, j >> 2);
+    if (!(d > 0.0)) {
       bad = true;
       d = 1.0;
     }
-    const double inv = 1.0 / d;
-    // scale the previous column (nobody reads it in this step)
-    if (j > 0) {
-      double dp = L[j - 1][j - 1];
-      if (!(dp > 0.0)) dp = 1.0;
-      const double s = rsqrt(dp);
-      for (int r = j + t; r < nbe; r += blockDim.x) L[r][j - 1] *= s;
+    const double sq = sqrt(d);
+    reg_set(v, j >> 2, sq);
+    piv[j] = sq;
+    pinv[j] = 1.0 / sq;
+  };
+  if (t == 0 && nbe > 0) take_pivot(0);
+  __syncthreads();
+  for (int j = 0; j < nbe; ++j) {
+    const int buf = j & 1;
+    if (live && r > j && q == (j & 3)) {
+      const double l = reg_get(v, j >> 2) * pinv[j];
+      reg_set(v, j >> 2, l);
+      col[buf][r] = l;
     }
-    const int m = nbe - j - 1;
-    for (int idx = t; idx < m * m; idx += blockDim.x) {
-      const int r = j + 1 + idx % m, c = j + 1 + idx / m;
-      if (r >= c) L[r][c] -= L[r][j] * L[c][j] * inv;
+    __syncthreads();
+    if (live && r > j) {
+      const double lr = col[buf][r];
+#pragma unroll
+      for (int i = 0; i < NB / 4; ++i) {
+        const int c = q + 4 * i;
+        if (c > j && c <= r) v[i] -= lr * col[buf][c];
+      }
+      if (r == j + 1 && q == ((j + 1) & 3)) take_pivot(j + 1);
     }
     __syncthreads();
   }
-  {  // scale the last column and take the square roots of the pivots
-    const int j = nbe - 1;
-    double dp = L[j][j];
-    if (!(dp > 0.0)) dp = 1.0;
-    if (t == 0) L[j][j] = sqrt(dp);
+  if (bad) atomicCAS(err, 0, (int)kDevNotSPD);
+#pragma unroll
+  for (int i = 0; i < NB / 4; ++i) {
+    const int c = q + 4 * i;
+    if (live && c <= r) Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] = v[i];
   }
-  __syncthreads();
-  for (int j = t; j < nbe - 1; j += blockDim.x) {
-    double d = L[j][j];
-    if (!(d > 0.0)) d = 1.0;
-    L[j][j] = sqrt(d);
-  }
-  if (bad && t == 0) atomicCAS(err, 0, (int)kDevNotSPD);
-  __syncthreads();
-  for (int idx = t; idx < NB * NB; idx += blockDim.x) {
-    const int r = idx % NB, c = idx / NB;
-    if (r >= c && r < nbe && c < nbe) Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] = L[r][c];
-  }
-  for (int j = t; j < nbe; j += blockDim.x) Ldz[j0 + j] = L[j][j];
+  if (t < nbe) Ldz[j0 + t] = piv[t];
 }
 
 __global__ void __launch_bounds__(256) potrf_diag_kernel(double* A, int64_t ld, int64_t stride, int n, int j0,
@@ -82,7 +101,9 @@ __global__ void __launch_bounds__(256) potrf_diag_kernel(double* A, int64_t ld, 
   potrf_diag_body(A + (int64_t)z * stride, ld, n, j0, Ldiag + (int64_t)z * n, err);
 }
 
-// Panel solve: rows below the diagonal block, X L_jj^T = A_panel.
+// Panel solve: rows below the diagonal block, X L_jj^T = A_panel, one row per thread.  Column c
+// of X is final once it is scaled by 1/L_cc; it is then subtracted from the later columns of the
+// row (right-looking within the row: 64 short dependency chains instead of one long one).
 __device__ __forceinline__ void trsm_panel_body(double* Az, int64_t ld, int n, int j0, int rblock) {
   __shared__ double Ls[NB][NB + 1];
   __shared__ double inv[NB];
@@ -101,10 +122,9 @@ __device__ __forceinline__ void trsm_panel_body(double* Az, int64_t ld, int n, i
   for (int c = 0; c < NB; ++c) x[c] = Az[(int64_t)r + ld * (int64_t)(j0 + c)];
 #pragma unroll
   for (int c = 0; c < NB; ++c) {
-    double s = x[c];
+    x[c] *= inv[c];
 #pragma unroll
-    for (int m = 0; m < c; ++m) s -= x[m] * Ls[c][m];
-    x[c] = s * inv[c];
+    for (int m = c + 1; m < NB; ++m) x[m] -= x[c] * Ls[m][c];
   }
 #pragma unroll
   for (int c = 0; c < NB; ++c) Az[(int64_t)r + ld * (int64_t)(j0 + c)] = x[c];
