@@ -516,10 +516,52 @@ int tune_logdet_on(rpa_b200_handle* h, const rpa::MatDesc* dmats, int nmat, int 
   return RPA_OK;
 }
 
+// Tune the bucket of order n on nmat test matrices of that order stored at base (n*n doubles each).
+int tune_uniform(rpa_b200_handle* h, int n, int nmat, double* base, double* ms) {
+  RPA_CUDA(h, ensure(h->tune, (size_t)nmat * (sizeof(rpa::MatDesc) + 8 * ((size_t)n + 4)) + 512));
+  std::vector<rpa::MatDesc> mats(nmat);
+  rpa::MatDesc* dmats = static_cast<rpa::MatDesc*>(h->tune.p);
+  double* scratch = reinterpret_cast<double*>(static_cast<uint8_t*>(h->tune.p) +
+                                              ((size_t)nmat * sizeof(rpa::MatDesc) + 255) / 256 * 256);
+  for (int z = 0; z < nmat; ++z) {
+    mats[z].A = base + (size_t)z * n * n;
+    mats[z].ld = n;
+    mats[z].n = n;
+    mats[z].Ldiag = scratch + (size_t)z * n;
+    mats[z].tr_dd = scratch + (size_t)nmat * n + 4 * (size_t)z;
+    mats[z].ld_dd = mats[z].tr_dd + 2;
+  }
+  RPA_CUDA(h, cudaMemcpyAsync(dmats, mats.data(), sizeof(rpa::MatDesc) * nmat, cudaMemcpyHostToDevice, h->stream));
+  int s = tune_logdet_on(h, dmats, nmat, n, ms);
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));  // mats must outlive its copy
+  return s;
+}
+
+// First use of an order bucket by a single-system log-det (autotune on, order >= 512): tune it
+// on as many test matrices as the call factors, in a temporary buffer (fewer, down to 4, when
+// memory is short; the default plan stays when even that fails).  Returns a status.
+int tune_single(rpa_b200_handle* h, int n, int nmat) {
+  if (!h->autotune || n < 512 || h->logdet_plans.count(plan_bucket(n))) return RPA_OK;
+  for (int m = nmat; m >= 1; m = m > 4 ? 4 : 0) {
+    void* tmp = nullptr;
+    if (cudaMalloc(&tmp, (size_t)m * n * n * 8) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    int s = tune_uniform(h, n, m, static_cast<double*>(tmp), nullptr);
+    cudaStreamSynchronize(h->stream);
+    cudaFree(tmp);
+    if (s == RPA_OK) RPA_CUDA(h, cudaMemsetAsync(h->err_dev, 0, sizeof(int), h->stream));
+    return s;
+  }
+  return RPA_OK;
+}
+
 // Blocked Cholesky of nmat matrices through a cached CUDA graph (the launch
 // sequence depends only on the arguments; ~6 launches per 64 columns would
 // otherwise leave the GPU idle between the small late-step kernels).
 int cholesky(rpa_b200_handle* h, double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag) {
+  if (int ts = tune_single(h, n, nmat)) return ts;
   const rpa::LogdetPlan plan = plan_for(h, n);
   for (auto& g : h->chol_graphs) {
     if (g.A == A && g.ld == ld && g.stride == stride && g.n == n && g.nmat == nmat && g.Ldiag == Ldiag &&
@@ -928,21 +970,7 @@ int rpa_b200_tune_logdet(rpa_b200_handle* h, int64_t NQ, int64_t NMat, int64_t* 
     return fail(h, RPA_ERR_INVALID_ARG, "invalid tuning case NQ=%lld NMat=%lld", (long long)NQ, (long long)NMat);
   const int n = (int)NQ, nmat = (int)NMat;
   RPA_CUDA(h, ensure(h->Pi, (size_t)nmat * n * n * 8));
-  RPA_CUDA(h, ensure(h->tune, (size_t)nmat * (sizeof(rpa::MatDesc) + 8 * ((size_t)n + 4)) + 512));
-  std::vector<rpa::MatDesc> mats(nmat);
-  rpa::MatDesc* dmats = static_cast<rpa::MatDesc*>(h->tune.p);
-  double* scratch = reinterpret_cast<double*>(static_cast<uint8_t*>(h->tune.p) +
-                                              ((size_t)nmat * sizeof(rpa::MatDesc) + 255) / 256 * 256);
-  for (int z = 0; z < nmat; ++z) {
-    mats[z].A = static_cast<double*>(h->Pi.p) + (size_t)z * n * n;
-    mats[z].ld = n;
-    mats[z].n = n;
-    mats[z].Ldiag = scratch + (size_t)z * n;
-    mats[z].tr_dd = scratch + (size_t)nmat * n + 4 * (size_t)z;
-    mats[z].ld_dd = mats[z].tr_dd + 2;
-  }
-  RPA_CUDA(h, cudaMemcpyAsync(dmats, mats.data(), sizeof(rpa::MatDesc) * nmat, cudaMemcpyHostToDevice, h->stream));
-  if ((s = tune_logdet_on(h, dmats, nmat, n, Ms))) return s;
+  if ((s = tune_uniform(h, n, nmat, static_cast<double*>(h->Pi.p), Ms))) return s;
   const rpa::LogdetPlan p = plan_for(h, n);
   if (Nb2) *Nb2 = p.nb2;
   if (Tile) *Tile = 32 * p.tile_w;

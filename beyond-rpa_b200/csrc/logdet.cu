@@ -60,10 +60,13 @@ __device__ __forceinline__ void potrf_diag_body(double* Az, int64_t ld, int n, i
       bad = true;
       d = 1.0;
     }
-    const double sq = sqrt(d);
+    // one reciprocal square root (1 ulp) instead of a square root and a division: the
+    // pivot chain is the kernel's critical path
+    const double ri = rsqrt(d);
+    const double sq = d * ri;
     reg_set(v, j >> 2, sq);
     piv[j] = sq;
-    pinv[j] = 1.0 / sq;
+    pinv[j] = ri;
   };
   if (t == 0 && nbe > 0) take_pivot(0);
   __syncthreads();
