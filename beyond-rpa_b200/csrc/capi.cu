@@ -50,6 +50,7 @@ struct rpa_b200_handle {
   DevBuf jT, jM, jV, jMap;             // batched PNO stage: T_ij, T T^T, eigenvectors, column map
   DevBuf jSK;                          // split-K partials of the G products
   DevBuf sxR, sxU, sxP;                // split-BF16 exchange: R and U (U2) hi/lo rows, partial sums
+  DevBuf t2Z, t2M, t2Sync;             // split-BF16 ring contractions: Z (both layouts), M / P, milestones
   struct BatchGraph {
     uint64_t key;
     std::vector<cudaGraphExec_t> execs;
@@ -87,6 +88,7 @@ struct rpa_b200_handle {
   int autotune = 1;            // tune unseen order buckets on their first batched use (RPA_B200_AUTOTUNE=0: off)
   size_t batch_bytes = 0;      // device bytes per batch of the batched entry (0: 60% of free memory)
   int sosex_seg = 2;           // 32-column chunks per accumulation segment of the split exchange contraction
+  int ring_seg = 2;            // the same for the split ring contractions of the T2 range finder
   DevBuf tune;                 // tuner workspace: descriptors and pivots of its test matrices
   // fork/join branches of the batched graph: [0] the next batch's scale/split pass, [1..2] log-det buckets
   cudaStream_t aux[3] = {};
@@ -653,7 +655,76 @@ struct T2Ctx {
   std::vector<double> u2, w;
   int zk;             // frequencies per Z group
   bool z_resident;    // all groups built once
+  // split-BF16 ring contractions (prec split with Z resident): Z split once in both K-major
+  // layouts, Zt (rows K*NQ, nov contiguous, pitch p1) for P = Z M and Z (rows nov, K*NQ
+  // contiguous, pitch p2) for Z^T P
+  bool split = false;
+  int64_t p1 = 0, p2 = 0;
+  CUtensorMap mZt[2], mZ[2];
 };
+
+// Split-BF16 operands of the ring contractions, once per T2 call (Z resident in h->tZ).
+int prepare_split_z(rpa_b200_handle* h, T2Ctx& c) {
+  const int64_t rows = (int64_t)c.K * c.NQ;
+  if (rows > INT32_MAX || c.nov > INT32_MAX) return fail(h, RPA_ERR_TOO_LARGE, "T2 split operands too large");
+  c.p1 = rpa::sosex_tc_nvp((int)c.nov);
+  c.p2 = rpa::sosex_tc_nvp((int)rows);
+  const size_t b1 = (size_t)rows * c.p1 * 2, b2 = (size_t)c.nov * c.p2 * 2;  // bytes of one bf16 part
+  RPA_CUDA(h, ensure(h->t2Z, 2 * b1 + 2 * b2 + 512));
+  auto* base = static_cast<uint8_t*>(h->t2Z.p);
+  auto* zth = reinterpret_cast<__nv_bfloat16*>(base);
+  auto* ztl = reinterpret_cast<__nv_bfloat16*>(base + b1);
+  auto* zh = reinterpret_cast<__nv_bfloat16*>(base + 2 * b1);
+  auto* zl = reinterpret_cast<__nv_bfloat16*>(base + 2 * b1 + b2);
+  const double* Z = static_cast<const double*>(h->tZ.p);
+  RPA_CUDA(h, rpa::launch_split_rows(Z, rows, (int)rows, 1, (int)c.nov, zth, ztl, h->stream));
+  RPA_CUDA(h, rpa::launch_split_cols(Z, rows, (int)c.nov, 1, (int)rows, zh, zl, h->stream));
+  int s;
+  if ((s = encode_map(h, &c.mZt[0], zth, c.p1, (int)rows, 1, c.p1, rpa::kSyrkTcTM))) return s;
+  if ((s = encode_map(h, &c.mZt[1], ztl, c.p1, (int)rows, 1, c.p1, rpa::kSyrkTcTM))) return s;
+  if ((s = encode_map(h, &c.mZ[0], zh, c.p2, (int)c.nov, 1, c.p2, rpa::kSyrkTcTM))) return s;
+  if ((s = encode_map(h, &c.mZ[1], zl, c.p2, (int)c.nov, 1, c.p2, rpa::kSyrkTcTM))) return s;
+  c.split = true;
+  return RPA_OK;
+}
+
+// C (M x N, ld ldc) = alpha A B^T with A given by two maps (M rows) and B (N x K, column-major
+// K x N in memory, ld ldb) split here into bf16 rows of pitch = the A maps' pitch.
+int gemm_split_t2(rpa_b200_handle* h, const CUtensorMap* amaps, int M, int64_t K, int64_t pitch, const double* B,
+                  int64_t ldb, int N, double* C, int64_t ldc, double alpha) {
+  const size_t bb = (size_t)N * pitch * 2;
+  RPA_CUDA(h, ensure(h->t2M, 2 * bb + 256));
+  auto* bh = static_cast<__nv_bfloat16*>(h->t2M.p);
+  auto* bl = reinterpret_cast<__nv_bfloat16*>(static_cast<uint8_t*>(h->t2M.p) + bb);
+  RPA_CUDA(h, rpa::launch_split_cols(B, ldb, N, 1, (int)K, bh, bl, h->stream));
+  CUtensorMap maps[4] = {amaps[0], amaps[1]};
+  int s;
+  if ((s = encode_map(h, &maps[2], bh, pitch, N, 1, pitch, rpa::kSyrkTcTN))) return s;
+  if ((s = encode_map(h, &maps[3], bl, pitch, N, 1, pitch, rpa::kSyrkTcTN))) return s;
+  rpa::GemmSplitArgs g{};
+  g.M = M;
+  g.N = N;
+  g.K = K;
+  g.C = C;
+  g.ldc = ldc;
+  g.alpha = alpha;
+  g.beta = 0.0;
+  // short accumulation segments: each product feeds the Rayleigh-Ritz matrix, and the
+  // round-toward-zero bias of a tensor-core accumulator grows with the additions it takes
+  // (16-chunk segments bias A by ~3e-6 relative, 2-chunk segments by ~4e-7)
+  g.seg_chunks = h->ring_seg;
+  g.err = h->err_dev;
+  g.sync_every = h->sync_every;
+  g.sync_lag = 2;
+  const int64_t words = rpa::gemm_split_sync_words(M, N, K, h->num_sms, h->sync_every);
+  if (words > 0) {
+    RPA_CUDA(h, ensure(h->t2Sync, (size_t)words * sizeof(int)));
+    RPA_CUDA(h, cudaMemsetAsync(h->t2Sync.p, 0, (size_t)words * sizeof(int), h->stream));
+    g.sync = static_cast<int*>(h->t2Sync.p);
+  }
+  RPA_CUDA(h, rpa::launch_gemm_split_bf16(maps, g, h->num_sms, h->stream));
+  return RPA_OK;
+}
 
 int build_z_group(rpa_b200_handle* h, const T2Ctx& c, int g0, int n, double* Z) {
   rpa::ChiGroup cg{};
@@ -677,6 +748,13 @@ int build_z_group(rpa_b200_handle* h, const T2Ctx& c, int g0, int n, double* Z) 
 int apply_I(rpa_b200_handle* h, const T2Ctx& c, const double* M, int ncols, double* out) {
   double* Z = static_cast<double*>(h->tZ.p);
   double* P = static_cast<double*>(h->tP.p);
+  if (c.split) {  // P = Z M, out = -(1/4 pi) Z^T P as split-BF16 GEMMs on the tensor cores
+    const int64_t rows = (int64_t)c.K * c.NQ;
+    int s = gemm_split_t2(h, c.mZt, (int)rows, c.nov, c.p1, M, c.nov, ncols, P, rows, 1.0);
+    if (s == RPA_OK)
+      s = gemm_split_t2(h, c.mZ, (int)c.nov, rows, c.p2, P, rows, ncols, out, c.nov, -1.0 / (4.0 * kPi));
+    return s;
+  }
   bool first = true;
   for (int g0 = 0; g0 < c.K; g0 += c.zk) {
     const int n = std::min(c.zk, c.K - g0);
@@ -861,6 +939,7 @@ int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) {
   if (const char* at = std::getenv("RPA_B200_AUTOTUNE")) h->autotune = std::atoi(at) != 0;
   if (const char* bb = std::getenv("RPA_B200_BATCH_BYTES")) h->batch_bytes = (size_t)std::atoll(bb);
   if (const char* sg = std::getenv("RPA_B200_SOSEX_SEG")) h->sosex_seg = std::max(1, std::atoi(sg));
+  if (const char* rg = std::getenv("RPA_B200_RING_SEG")) h->ring_seg = std::max(1, std::atoi(rg));
   for (auto& e : h->ev) cudaEventCreate(&e);
   for (auto& e : h->fork_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   if (const char* la = std::getenv("RPA_B200_LOOKAHEAD")) h->lookahead = std::atoi(la) != 0;
@@ -900,7 +979,8 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
                     &h->xM, &h->eW, &h->eA, &h->eZ, &h->thZ, &h->thXa, &h->thXi, &h->thYX, &h->thR,
                     &h->jU, &h->jL, &h->jX, &h->jPno, &h->jWork,
                     &h->jPack, &h->jQS, &h->jS, &h->jD, &h->syncBuf,
-                    &h->jT, &h->jM, &h->jV, &h->jMap, &h->jSK, &h->tune, &h->sxR, &h->sxU, &h->sxP})
+                    &h->jT, &h->jM, &h->jV, &h->jMap, &h->jSK, &h->tune, &h->sxR, &h->sxU, &h->sxP,
+                    &h->t2Z, &h->t2M, &h->t2Sync})
     release(*b);
   for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
   if (h->err_dev) cudaFree(h->err_dev);
@@ -1164,6 +1244,8 @@ int rpa_b200_dring_t2(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVir
   if (c.z_resident)
     for (int g0 = 0; g0 < v.K; g0 += c.zk)
       if ((s = build_z_group(h, c, g0, std::min(c.zk, v.K - g0), static_cast<double*>(h->tZ.p)))) return s;
+  if (prec == RPA_PREC_SPLIT_BF16 && c.z_resident)
+    if ((s = prepare_split_z(h, c))) return s;
 
   // guess vectors (rpa_CC_Doubles.f90:746-763): given, or uniform [-1/2, 1/2) from the seed
   double* Om = static_cast<double*>(h->tOm.p);

@@ -112,6 +112,25 @@ cudaError_t launch_syrk_split_bf16_multi(const SyrkInst* insts, const uint4* wor
                                          int* err, int num_sms, cudaStream_t stream, int* sync = nullptr,
                                          int sync_every = 0, int sync_lag = 2, int max_chunks = 0);
 int64_t syrk_tc_multi_sync_words(int nunits, int max_chunks, int num_sms, int sync_every);
+// General split-BF16 GEMM on the same tensor-core pipeline (128 x 256 tiles over the full grid):
+//   C(m, n) = alpha sum_k A(m, k) B(n, k) + beta C(m, n),  m < M, n < N, FP64 C (column-major, ldc),
+// A = A_hi + A_lo (M rows, K contiguous) and B likewise (N rows): maps[4] = A_hi, A_lo (boxes of
+// 32 x kSyrkTcTM) and B_hi, B_lo (32 x kSyrkTcTN), 3-D (K, rows, 1).  Rows of both must be padded
+// to a multiple of 8 bf16 (16 bytes) with zeros beyond K.
+struct GemmSplitArgs {
+  int M, N;
+  int64_t K;
+  double* C;
+  int64_t ldc;
+  double alpha, beta;
+  int seg_chunks;
+  int* sync;  // optional wave milestones (zeroed, gemm_split_sync_words ints)
+  int sync_every, sync_lag;
+  int* err;
+};
+int64_t gemm_split_sync_words(int M, int N, int64_t K, int num_sms, int sync_every);
+cudaError_t launch_gemm_split_bf16(const CUtensorMap* maps, const GemmSplitArgs& a, int num_sms,
+                                   cudaStream_t stream);
 int syrk_tc_blocks(int NQ);
 // (tm, tn) of the lower-triangle 128 x 256 tiles in the kernel's unit order
 void syrk_tc_block_coords(int NQ, std::vector<uint2>& out);

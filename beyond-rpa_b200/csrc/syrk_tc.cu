@@ -73,6 +73,11 @@ struct Unit {
   int64_t ldPi;
   const double* dk;    // exact diagonal of this frequency
   const CUtensorMap* map[4];  // A_hi, A_lo, B_hi, B_lo
+  // full GEMM units (tri == false): C(m, n) = alpha sum_k A(m,k) B(n,k) + beta C(m, n),
+  // m < NQ (rows of A), n < N (rows of B); C = Pk with leading dimension ldPi
+  bool tri = true;
+  int N = 0;
+  double alpha = 1.0, beta = 0.0;
 };
 
 // Single instance: tensor maps are kernel parameters, units are decoded.
@@ -131,6 +136,37 @@ struct MultiSource {
     x.map[1] = &in.tmAl;
     x.map[2] = &in.tmBh;
     x.map[3] = &in.tmBl;
+    return x;
+  }
+};
+
+// General GEMM: tensor maps are kernel parameters; units (tm, tn) over the full tile grid,
+// tm-major (consecutive units share an A band).
+struct GemmSource {
+  const CUtensorMap* maps[4];
+  GemmSplitArgs a;
+  int ntn, nchunks, nunits;
+  __device__ __forceinline__ int* sync_counters() const { return a.sync; }
+  __device__ __forceinline__ int sync_every() const { return a.sync_every; }
+  __device__ __forceinline__ int sync_lag() const { return a.sync_lag; }
+  __device__ __forceinline__ int max_chunks() const { return nchunks; }
+  __device__ __forceinline__ Unit get(int u) const {
+    Unit x;
+    x.k = 0;
+    x.tm = u / ntn;
+    x.tn = u - x.tm * ntn;
+    x.NQ = a.M;
+    x.N = a.N;
+    x.nchunks = nchunks;
+    x.chunk0 = 0;
+    x.accumulate = false;
+    x.Pk = a.C;
+    x.ldPi = a.ldc;
+    x.dk = nullptr;
+    x.tri = false;
+    x.alpha = a.alpha;
+    x.beta = a.beta;
+    for (int i = 0; i < 4; ++i) x.map[i] = maps[i];
     return x;
   }
 };
@@ -251,7 +287,7 @@ __device__ __forceinline__ void syrk_body(const Source& src, int* err, const int
         // MMA width of this unit: only columns n < min(NQ, (tm+1)*TM) can hold lower-triangle
         // entries (the first 128 rows of a 256-column block on the diagonal, the ragged last
         // block), rounded up to the N granularity (16) of a 128-row MMA
-        const int live = min(x.NQ, (x.tm + 1) * TM) - x.tn * TN;
+        const int live = x.tri ? min(x.NQ, (x.tm + 1) * TM) - x.tn * TN : x.N - x.tn * TN;
         const int nmma = min(TN, max(16, (live + 15) & ~15));
         const uint32_t idesc = umma_idesc_bf16_f32(TM, nmma);
         for (int c0 = 0; c0 < nchunks && ok; c0 += seg_chunks, ++it) {
@@ -318,7 +354,8 @@ __device__ __forceinline__ void syrk_body(const Source& src, int* err, const int
 #pragma unroll
         for (int cc = 0; cc < kEpiCols / 8; ++cc) {
           const int n0 = nbase + cc * 8;
-          if (n0 <= warp_max_m && n0 < x.NQ)  // warp-uniform: skip columns above the diagonal
+          if (x.tri ? (n0 <= warp_max_m && n0 < x.NQ) : n0 < x.N)  // warp-uniform: skip columns above
+                                                                      // the diagonal or beyond N
             tmem_ld_add_x8(tmem_base + (uint32_t)(b * TN + colq * kEpiCols + cc * 8) + ((uint32_t)(quarter * 32) << 16),
                            &run[cc * 8], c0 == 0);
         }
@@ -327,7 +364,17 @@ __device__ __forceinline__ void syrk_body(const Source& src, int* err, const int
         if (lane == 0) mbar_arrive(&acc_empty[b]);
       }
       if (!ok) break;
-      if (m < x.NQ && nbase <= m) {
+      if (!x.tri) {
+        if (m < x.NQ) {
+          double* p = x.Pk + (int64_t)m + (int64_t)nbase * x.ldPi;
+          const int ncol = min(kEpiCols, x.N - nbase);
+#pragma unroll
+          for (int j = 0; j < kEpiCols; ++j) {
+            if (j < ncol) *p = x.beta == 0.0 ? x.alpha * (double)run[j] : fma(x.alpha, (double)run[j], x.beta * *p);
+            p += x.ldPi;
+          }
+        }
+      } else if (m < x.NQ && nbase <= m) {
         double* p = x.Pk + (int64_t)m + (int64_t)nbase * x.ldPi;
         const int jd = m - nbase;  // column index of the diagonal element (may be >= kEpiCols)
         if (x.accumulate) {
@@ -388,7 +435,48 @@ __global__ void __launch_bounds__(kThreads, 1)
   src.max_chunks_ = max_chunks;
   syrk_body(src, err, seg_chunks);
 }
+__global__ void __launch_bounds__(kThreads, 1)
+    gemm_split_bf16_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
+                           const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
+                           const GemmSplitArgs args, const int ntn, const int nunits, const int nchunks) {
+  GemmSource src;
+  src.maps[0] = &tmA_hi;
+  src.maps[1] = &tmA_lo;
+  src.maps[2] = &tmB_hi;
+  src.maps[3] = &tmB_lo;
+  src.a = args;
+  src.ntn = ntn;
+  src.nchunks = nchunks;
+  src.nunits = nunits;
+  syrk_body(src, args.err, args.seg_chunks > 0 ? args.seg_chunks : nchunks);
+}
 }  // namespace
+
+int64_t gemm_split_sync_words(int M, int N, int64_t K, int num_sms, int sync_every) {
+  if (sync_every <= 0) return 0;
+  const int64_t nunits = (int64_t)((M + TM - 1) / TM) * ((N + TN - 1) / TN);
+  const int64_t grid = nunits < num_sms ? nunits : num_sms;
+  if (grid <= 0) return 0;
+  const int64_t nchunks = (K + TK - 1) / TK;
+  return (nunits + grid - 1) / grid * ((nchunks + sync_every - 1) / sync_every);
+}
+
+cudaError_t launch_gemm_split_bf16(const CUtensorMap* maps, const GemmSplitArgs& a, int num_sms,
+                                   cudaStream_t stream) {
+  const int64_t ntm = (a.M + TM - 1) / TM, ntn = (a.N + TN - 1) / TN;
+  const int64_t nunits = ntm * ntn;
+  const int64_t nchunks = (a.K + TK - 1) / TK;
+  if (a.M <= 0 || a.N <= 0 || a.K <= 0) return cudaSuccess;
+  if (nunits > INT32_MAX || nchunks > INT32_MAX) return cudaErrorInvalidValue;
+  cudaError_t e = cudaFuncSetAttribute(gemm_split_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kSmemBytes);
+  if (e != cudaSuccess) return e;
+  const int grid = nunits < num_sms ? (int)nunits : num_sms;
+  gemm_split_bf16_kernel<<<grid, kThreads, kSmemBytes, stream>>>(maps[0], maps[1], maps[2], maps[3], a, (int)ntn,
+                                                                  (int)nunits, (int)nchunks);
+  ++g_launches;
+  return cudaGetLastError();
+}
 
 cudaError_t launch_syrk_split_bf16(const CUtensorMap* tmA_hi, const CUtensorMap* tmA_lo, const CUtensorMap* tmB_hi,
                                    const CUtensorMap* tmB_lo, const SyrkTcArgs& a, int num_sms,

@@ -81,6 +81,22 @@ def test_t2_split_precision_energy(handle):
     assert abs(res["EigRPA"].sum() - O.t2_eig_rpa(U_ref, A_ref, s.R).sum()) < 1e-6
 
 
+def test_t2_split_ring_contractions_track_fp64(handle):
+    # prec split: Pi and the two ring contractions of every I(1) application (P = Z M and
+    # Z^T P) run as split-BF16 tensor-core GEMMs; the Gram and Rayleigh-Ritz matrices and the
+    # eigensolvers stay FP64.  A numpy emulation of the split products gives ~6e-7 relative
+    # error in A and ~4e-8 Eh in EigRPA at these sizes; the bounds below leave 10-30x margin.
+    s, x, w, pi, vals, vecs, omega = t2_case(19, 200, 8, 60, 12)
+    r64 = handle.dring_t2(s.R, s.eps_o, s.eps_v, x, w, prec="fp64", guess=omega, cutoff_thresh=1e-4)
+    r16 = handle.dring_t2(s.R, s.eps_o, s.eps_v, x, w, prec="split", guess=omega, cutoff_thresh=1e-4)
+    assert r16["NT"] == r64["NT"]
+    assert np.max(np.abs(r16["A"] - r64["A"])) < 2e-5 * np.max(np.abs(r64["A"]))
+    assert abs(r16["EigRPA"].sum() - r64["EigRPA"].sum()) < 2e-6 * abs(r64["EigRPA"].sum())
+    ex16 = handle.exchange_sosex(s.R, s.no, s.nv, r16["U"], r16["A"], prec="split")
+    ex64 = handle.exchange_sosex(s.R, s.no, s.nv, r64["U"], r64["A"], prec="fp64")
+    assert abs(ex16 - ex64) < 2e-5 * abs(ex64)
+
+
 @pytest.mark.parametrize("s2", [False, True])
 def test_sosex_matches_oracle(handle, s2):
     s, x, w, pi, vals, vecs, omega = t2_case(16, 150, 6, 50, 12)
