@@ -390,11 +390,30 @@ int build_pi(rpa_b200_handle* h, const Validated& v, const double* Rd, int64_t l
 // by the global split, so the result equals the one-shot build.  count_dev collects the number of
 // non-finite entries of R; the caller reads it after the stream has been synchronised.
 // Returns 1 (nothing done) when the frequencies do not fit in one group.
+// Relative sizes of the pieces R is staged in (RPA_B200_PIECES = comma-separated weights).
+std::vector<int> piece_weights() {
+  std::vector<int> w;
+  if (const char* e = std::getenv("RPA_B200_PIECES")) {
+    for (const char* p = e; *p;) {
+      char* end = nullptr;
+      const long x = std::strtol(p, &end, 10);
+      if (end == p) break;
+      if (x > 0 && x < 1000) w.push_back((int)x);
+      p = (*end == ',') ? end + 1 : end;
+    }
+  }
+  if (w.empty() || w.size() > 32) w = {1, 2, 3, 4, 5, 6};
+  return w;
+}
+
 int build_pi_pipelined(rpa_b200_handle* h, const Validated& v, const double* Rh, int64_t ldR, double alpha) {
-  // pieces of growing size (weights 1, 2, ..., 6): the first copy, which nothing hides, is short,
-  // and each later copy fits under the contraction of the pieces before it
-  constexpr int kPipe = 6;
-  constexpr int kWeightSum = kPipe * (kPipe + 1) / 2;
+  // pieces of growing size (weights 1, 2, ..., 6 by default): the first copy, which nothing
+  // hides, is short, and each later copy runs under the contraction of the pieces before it
+  const std::vector<int> weights = piece_weights();
+  const int kPipe = (int)weights.size();
+  std::vector<int64_t> cum(kPipe + 1, 0);
+  for (int c = 0; c < kPipe; ++c) cum[c + 1] = cum[c] + weights[c];
+  const int64_t kWeightSum = cum[kPipe];
   const int NQ = v.NQ;
   const int64_t nov = v.nov;
   const int64_t pitch = (nov + 7) / 8 * 8;
@@ -428,7 +447,7 @@ int build_pi_pipelined(rpa_b200_handle* h, const Validated& v, const double* Rh,
   RPA_CUDA(h, cudaStreamWaitEvent(h->copy_stream, start, 0));
   bool first = true;  // the first non-empty piece writes Pi, later ones add into it
   for (int c = 0; c < kPipe; ++c) {
-    const int64_t w0 = (int64_t)c * (c + 1) / 2, w1 = (int64_t)(c + 1) * (c + 2) / 2;
+    const int64_t w0 = cum[c], w1 = cum[c + 1];
     const int s0 = (int)(plan.nsplit * w0 / kWeightSum), s1 = (int)(plan.nsplit * w1 / kWeightSum);
     const int64_t a0 = (int64_t)s0 * plan.ai_per_split, a1 = std::min(nov, (int64_t)s1 * plan.ai_per_split);
     if (a1 <= a0) continue;
