@@ -256,7 +256,7 @@ def run_ours(args):
     h2d = nq * nov * 8 + (no + nv + 2 * K) * 8
     d2h = 8 * (1 + K)
 
-    # FP64 form of the same path (the north-star comparison), one call
+    # FP64 form of the same path (the split-vs-FP64 comparison), one call
     ec64, _ = h.ec_rpa(s.R, s.eps_o, s.eps_v, s.freqs, s.weights, prec="fp64")
     t64 = h.timings()
     e4 = torch.cuda.Event(enable_timing=True)

@@ -1,7 +1,7 @@
 """GPU parity tests of the Pi(u) build and the RPA energy through the C ABI,
 against the FP64 oracle and its golden fixtures.
 
-Tolerances (stated per north-star precision budget):
+Tolerances (the precision budget of the split form):
   FP64 path:   Pi entries 1e-12 relative to max|Pi|; E_c 1e-10 Eh.
   split-BF16:  Pi off-diagonal 3e-5 relative to max|Pi| (bf16 hi/lo, FP32
                accumulation), diagonal exact to 1e-12 relative; E_c 1e-6 Eh.
