@@ -63,6 +63,13 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool val
                "l"(gmem), "r"(valid ? 8 : 0)
                : "memory");
 }
+// 16 bytes (two consecutive rows of one column), the first `bytes` of them copied (16, 8 or 0),
+// the rest zero-filled.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem), "r"(bytes)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
@@ -70,7 +77,9 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // One BM x BM tile (tm, tn) of C(lower trapezoid, ncols columns) for matrix z.
 // Operands stream global -> shared through a kStages-deep cp.async pipeline
 // (out-of-range elements zero-filled); one barrier per 16-deep K chunk.
-template <bool kScaled, int kW>
+// kCopy: 8 (8-byte copies), 16 (16-byte copies; the caller checked the alignment) or 0 (decide
+// per operand from its alignment).
+template <bool kScaled, int kW, int kCopy>
 __device__ __forceinline__ void dsyrk_tile(const DsyrkArgs& a, const double* A, double* C, int ncols, int tm, int tn,
                                            int z) {
   constexpr int BM = Geo<kW>::BM, LDS = Geo<kW>::LDS, kThreads = Geo<kW>::kThreads;
@@ -92,16 +101,34 @@ __device__ __forceinline__ void dsyrk_tile(const DsyrkArgs& a, const double* A, 
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
+  // 16-byte copies of row pairs when every column of the operand starts 16-byte aligned (aligned
+  // base, even leading dimension; m0, n0 and the pair index are even): half the copy
+  // instructions, 12-16 % faster than 8-byte copies on B200
+  const bool vec = kCopy == 16 || (kCopy == 0 && ((reinterpret_cast<uintptr_t>(A) & 15) == 0) && ((a.lda & 1) == 0));
   auto load_stage = [&](int st, int64_t k0) {
+    if (vec) {
 #pragma unroll
-    for (int i = 0; i < kLoads; ++i) {
-      const int idx = t + kThreads * i;
-      const int col = idx / BM, row = idx % BM;
-      const int64_t k = k0 + col;
-      const bool kin = k < a.kdim;
-      const bool va = kin && m0 + row < a.n, vb = kin && n0 + row < a.n;
-      cp_async8(&As[st][col][row], va ? A + (int64_t)(m0 + row) + a.lda * k : A, va);
-      cp_async8(&Bs[st][col][row], vb ? A + (int64_t)(n0 + row) + a.lda * k : A, vb);
+      for (int i = 0; i < kLoads / 2; ++i) {
+        const int idx = t + kThreads * i;
+        const int col = idx / (BM / 2), row = 2 * (idx % (BM / 2));
+        const int64_t k = k0 + col;
+        const bool kin = k < a.kdim;
+        const int ba = kin ? 8 * max(0, min(2, a.n - (m0 + row))) : 0;
+        const int bb = kin ? 8 * max(0, min(2, a.n - (n0 + row))) : 0;
+        cp_async16(&As[st][col][row], ba ? A + (int64_t)(m0 + row) + a.lda * k : A, ba);
+        cp_async16(&Bs[st][col][row], bb ? A + (int64_t)(n0 + row) + a.lda * k : A, bb);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < kLoads; ++i) {
+        const int idx = t + kThreads * i;
+        const int col = idx / BM, row = idx % BM;
+        const int64_t k = k0 + col;
+        const bool kin = k < a.kdim;
+        const bool va = kin && m0 + row < a.n, vb = kin && n0 + row < a.n;
+        cp_async8(&As[st][col][row], va ? A + (int64_t)(m0 + row) + a.lda * k : A, va);
+        cp_async8(&Bs[st][col][row], vb ? A + (int64_t)(n0 + row) + a.lda * k : A, vb);
+      }
     }
     if (kScaled && t < BK) {
       const int64_t k = k0 + t;
@@ -162,14 +189,14 @@ __device__ __forceinline__ void dsyrk_tile(const DsyrkArgs& a, const double* A, 
   }
 }
 
-template <bool kScaled, int kW>
+template <bool kScaled, int kW, int kCopy>
 __global__ void __launch_bounds__(Geo<kW>::kThreads, Geo<kW>::kMinBlocks)
     dsyrk_lower_kernel(const DsyrkArgs a, const int T, const int Tc) {
   int tm, tn;
   trap_decode(blockIdx.x, T, Tc, tm, tn);
   const int ncols = a.ncols > 0 ? a.ncols : a.n;
   const int z = blockIdx.y;
-  dsyrk_tile<kScaled, kW>(a, a.A + (int64_t)z * a.strideA, a.C + (int64_t)z * a.strideC, ncols, tm, tn, z);
+  dsyrk_tile<kScaled, kW, kCopy>(a, a.A + (int64_t)z * a.strideA, a.C + (int64_t)z * a.strideC, ncols, tm, tn, z);
 }
 
 // Shape of one step of the two-level blocked Cholesky for a matrix of order N
@@ -226,7 +253,7 @@ __global__ void __launch_bounds__(Geo<kW>::kThreads, Geo<kW>::kMinBlocks)
   a.ldc = md.ld;
   int tm, tn;
   trap_decode(blockIdx.x, T, Tc, tm, tn);
-  dsyrk_tile<false, kW>(a, a.A, a.C, ncols, tm, tn, 0);
+  dsyrk_tile<false, kW, 0>(a, a.A, a.C, ncols, tm, tn, 0);
 }
 
 int trap_tiles(int n, int ncols, int bm) {
@@ -252,21 +279,28 @@ cudaError_t launch_varlen_w(const MatDesc* mats, int nmat, int mode, int J0, int
   return cudaGetLastError();
 }
 
-template <bool kScaled, int kW>
-cudaError_t launch_lower_w(const DsyrkArgs& a, cudaStream_t stream) {
+template <bool kScaled, int kW, int kCopy>
+cudaError_t launch_lower_wc(const DsyrkArgs& a, cudaStream_t stream) {
   constexpr int BM = Geo<kW>::BM;
   const int T = (a.n + BM - 1) / BM;
   const int nc = (a.ncols > 0 && a.ncols < a.n) ? a.ncols : a.n;
   const int Tc = (nc + BM - 1) / BM;
   const int64_t tiles = (int64_t)Tc * T - (int64_t)Tc * (Tc - 1) / 2;
   constexpr size_t smem = tile_smem<kW>();
-  cudaError_t e0 = cudaFuncSetAttribute(dsyrk_lower_kernel<kScaled, kW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem);
+  cudaError_t e0 = cudaFuncSetAttribute(dsyrk_lower_kernel<kScaled, kW, kCopy>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e0 != cudaSuccess) return e0;
-  dsyrk_lower_kernel<kScaled, kW><<<dim3((unsigned)tiles, (unsigned)a.batch), Geo<kW>::kThreads, smem, stream>>>(
-      a, T, Tc);
+  dsyrk_lower_kernel<kScaled, kW, kCopy><<<dim3((unsigned)tiles, (unsigned)a.batch), Geo<kW>::kThreads, smem,
+                                          stream>>>(a, T, Tc);
   ++g_launches;
   return cudaGetLastError();
+}
+
+// 16-byte copies when every column of every matrix of the batch starts 16-byte aligned.
+template <bool kScaled, int kW>
+cudaError_t launch_lower_w(const DsyrkArgs& a, cudaStream_t stream) {
+  const bool vec = ((reinterpret_cast<uintptr_t>(a.A) & 15) == 0) && ((a.lda & 1) == 0) && ((a.strideA & 1) == 0);
+  return vec ? launch_lower_wc<kScaled, kW, 16>(a, stream) : launch_lower_wc<kScaled, kW, 8>(a, stream);
 }
 }  // namespace
 

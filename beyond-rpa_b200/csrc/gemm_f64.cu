@@ -38,6 +38,12 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool val
                "l"(gmem), "r"(valid ? 8 : 0)
                : "memory");
 }
+// 16 bytes (two consecutive elements), the first `bytes` of them copied, the rest zero-filled.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem), "r"(bytes)
+               : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
@@ -50,7 +56,9 @@ __device__ __forceinline__ int tile_off(int r, int k) {
 }
 
 // One 64 x 64 output tile (m0, n0) of problem g; b is the batch index (or the split-K index).
-template <bool kAM, bool kBN>
+// kVec: both operands are copied in 16-byte pairs along their unit-stride index (the launcher
+// checked unit strides, even other strides and 16-byte aligned bases).
+template <bool kAM, bool kBN, bool kVec = false>
 __device__ __forceinline__ void gemm_tile(const GemmF64Args& g, const int m0, const int n0, const int b) {
   extern __shared__ double smem[];
   double* As = smem;                              // [kStages][kTileWords]
@@ -79,20 +87,40 @@ __device__ __forceinline__ void gemm_tile(const GemmF64Args& g, const int m0, co
     for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
   auto load_stage = [&](int st, int64_t k0) {
+    if (kVec) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int idx = t + kThreads * i;
-      // consecutive threads walk the operand's unit-stride index
-      const int ra = kAM ? idx % BM : idx / BK, ca = kAM ? idx / BM : idx % BK;
-      const int64_t ka = k0 + ca;
-      const bool va = (m0 + ra < g.M) && (ka < kend);
-      cp_async8(As + st * kTileWords + tile_off<kAM>(ra, ca),
-                va ? A + (int64_t)(m0 + ra) * g.a_m + ka * g.a_k : A, va);
-      const int rb = kBN ? idx % BM : idx / BK, cb = kBN ? idx / BM : idx % BK;
-      const int64_t kb = k0 + cb;
-      const bool vb = (n0 + rb < g.N) && (kb < kend);
-      cp_async8(Bs + st * kTileWords + tile_off<kBN>(rb, cb),
-                vb ? B + kb * g.b_k + (int64_t)(n0 + rb) * g.b_n : B, vb);
+      for (int i = 0; i < 4; ++i) {
+        const int idx = t + kThreads * i;
+        // pairs along the unit-stride index: (ra, ra+1) or (ca, ca+1)
+        const int ra = kAM ? 2 * (idx % (BM / 2)) : idx / (BK / 2), ca = kAM ? idx / (BM / 2) : 2 * (idx % (BK / 2));
+        const int64_t ka = k0 + ca;
+        const int na = kAM ? ((ka < kend) ? max(0, min(2, g.M - (m0 + ra))) : 0)
+                           : ((m0 + ra < g.M) ? (int)max((int64_t)0, min((int64_t)2, kend - ka)) : 0);
+        cp_async16(As + st * kTileWords + tile_off<kAM>(ra, ca),
+                   na ? A + (int64_t)(m0 + ra) * g.a_m + ka * g.a_k : A, 8 * na);
+        const int rb = kBN ? 2 * (idx % (BM / 2)) : idx / (BK / 2), cb = kBN ? idx / (BM / 2) : 2 * (idx % (BK / 2));
+        const int64_t kb = k0 + cb;
+        const int nb = kBN ? ((kb < kend) ? max(0, min(2, g.N - (n0 + rb))) : 0)
+                           : ((n0 + rb < g.N) ? (int)max((int64_t)0, min((int64_t)2, kend - kb)) : 0);
+        cp_async16(Bs + st * kTileWords + tile_off<kBN>(rb, cb),
+                   nb ? B + kb * g.b_k + (int64_t)(n0 + rb) * g.b_n : B, 8 * nb);
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int idx = t + kThreads * i;
+        // consecutive threads walk the operand's unit-stride index
+        const int ra = kAM ? idx % BM : idx / BK, ca = kAM ? idx / BM : idx % BK;
+        const int64_t ka = k0 + ca;
+        const bool va = (m0 + ra < g.M) && (ka < kend);
+        cp_async8(As + st * kTileWords + tile_off<kAM>(ra, ca),
+                  va ? A + (int64_t)(m0 + ra) * g.a_m + ka * g.a_k : A, va);
+        const int rb = kBN ? idx % BM : idx / BK, cb = kBN ? idx / BM : idx % BK;
+        const int64_t kb = k0 + cb;
+        const bool vb = (n0 + rb < g.N) && (kb < kend);
+        cp_async8(Bs + st * kTileWords + tile_off<kBN>(rb, cb),
+                  vb ? B + kb * g.b_k + (int64_t)(n0 + rb) * g.b_n : B, vb);
+      }
     }
     if (ks && t < BK) {
       const int64_t k = k0 + t;
@@ -155,9 +183,9 @@ __device__ __forceinline__ void gemm_tile(const GemmF64Args& g, const int m0, co
   }
 }
 
-template <bool kAM, bool kBN>
+template <bool kAM, bool kBN, bool kVec>
 __global__ void __launch_bounds__(kThreads, 4) gemm_f64_kernel(const GemmF64Args g) {
-  gemm_tile<kAM, kBN>(g, blockIdx.y * BM, blockIdx.x * BM, blockIdx.z);
+  gemm_tile<kAM, kBN, kVec>(g, blockIdx.y * BM, blockIdx.x * BM, blockIdx.z);
 }
 
 // Many independent problems of one operand layout in one launch: CTA x works on tile
@@ -192,21 +220,22 @@ __global__ void splitk_reduce_kernel(const GemmF64Args g) {
   *p = (g.beta == 0.0) ? val : val + g.beta * *p;
 }
 
-template <bool kAM, bool kBN>
+template <bool kAM, bool kBN, bool kVec>
 cudaError_t launch_variant(const GemmF64Args& g, cudaStream_t stream) {
   static uint64_t attr_set = 0;  // per-variant bit per device: dynamic shared memory opted in
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev >= 64 || !(attr_set >> dev & 1)) {
-    e = cudaFuncSetAttribute(gemm_f64_kernel<kAM, kBN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
+    e = cudaFuncSetAttribute(gemm_f64_kernel<kAM, kBN, kVec>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kSmem);
     if (e != cudaSuccess) return e;
     if (dev < 64) attr_set |= 1ull << dev;
   }
   const bool split = g.splitk > 1;
   dim3 grid((unsigned)((g.N + BM - 1) / BM), (unsigned)((g.M + BM - 1) / BM),
             (unsigned)(split ? g.splitk : g.batch));
-  gemm_f64_kernel<kAM, kBN><<<grid, kThreads, kSmem, stream>>>(g);
+  gemm_f64_kernel<kAM, kBN, kVec><<<grid, kThreads, kSmem, stream>>>(g);
   if (split) {
     const int64_t mn = (int64_t)g.M * g.N;
     splitk_reduce_kernel<<<(unsigned)((mn + 255) / 256), 256, 0, stream>>>(g);
@@ -287,13 +316,29 @@ int gemm_f64_tiles(const GemmF64Args& g) {
   return (g.M > 0 && g.N > 0) ? ((g.M + BM - 1) / BM) * ((g.N + BM - 1) / BM) : 0;
 }
 
+namespace {
+// 16-byte pair copies: unit stride along the pair, the other stride and the batch stride even,
+// a 16-byte aligned base (split-K ranges start at multiples of 16).
+bool pairable(const double* p, int64_t unit, int64_t other, int64_t batch_stride, bool batched) {
+  return unit == 1 && (other & 1) == 0 && (!batched || (batch_stride & 1) == 0) &&
+         (reinterpret_cast<uintptr_t>(p) & 15) == 0;
+}
+template <bool kAM, bool kBN>
+cudaError_t launch_layout(const GemmF64Args& g, cudaStream_t stream) {
+  const bool batched = g.batch > 1 && g.splitk <= 1;
+  const bool vec = pairable(g.A, kAM ? g.a_m : g.a_k, kAM ? g.a_k : g.a_m, g.sA, batched) &&
+                   pairable(g.B, kBN ? g.b_n : g.b_k, kBN ? g.b_k : g.b_n, g.sB, batched);
+  return vec ? launch_variant<kAM, kBN, true>(g, stream) : launch_variant<kAM, kBN, false>(g, stream);
+}
+}  // namespace
+
 cudaError_t launch_gemm_f64(const GemmF64Args& g, cudaStream_t stream) {
   if (g.M <= 0 || g.N <= 0 || g.batch <= 0) return cudaSuccess;
   if (g.splitk > 1 && (g.batch != 1 || !g.work)) return cudaErrorInvalidValue;
   const bool am = (g.a_m == 1), bn = (g.b_n == 1);
   cudaError_t e;
-  if (am) e = bn ? launch_variant<true, true>(g, stream) : launch_variant<true, false>(g, stream);
-  else e = bn ? launch_variant<false, true>(g, stream) : launch_variant<false, false>(g, stream);
+  if (am) e = bn ? launch_layout<true, true>(g, stream) : launch_layout<true, false>(g, stream);
+  else e = bn ? launch_layout<false, true>(g, stream) : launch_layout<false, false>(g, stream);
   g_launches += g.splitk > 1 ? 2 : 1;
   return e;
 }
