@@ -207,28 +207,45 @@ __global__ void __cluster_dims__(kCS, 1, 1) __launch_bounds__(kCT)
   cl.sync();  // no CTA leaves while another may still read its shared memory
 }
 
-// y(c) = sum_{r > j} A(r, c) v(r) for c > j: one warp per column, four independent
-// accumulators per lane so that four loads of each lane are in flight.
+// y(c) = sum_{r > j} A(r, c) v(r) for c > j: kGemvWarps warps per column (two columns per
+// 256-thread block), each lane with four independent accumulators, partial sums added in a
+// fixed order.  The trailing matrix is read once per column step, so the kernel must keep
+// enough loads in flight to run at memory speed: one warp per column left it latency-bound.
+constexpr int kGemvWarps = 4;
 __global__ void __launch_bounds__(256) trailing_gemv_kernel(const double* A, int n, int64_t mstride, const double* v,
                                                             int j, double* y) {
+  __shared__ double part[8];
   A += mstride * blockIdx.y;
   v += mstride * blockIdx.y;
   y += (int64_t)n * blockIdx.y;
-  const int c = j + 1 + (int)blockIdx.x * 8 + (threadIdx.x >> 5);
-  const int lane = threadIdx.x & 31;
-  if (c >= n) return;
-  const double* col = A + (int64_t)n * c;
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-  int r = j + 1 + lane;
-  for (; r + 96 < n; r += 128) {
-    a0 += col[r] * v[r];
-    a1 += col[r + 32] * v[r + 32];
-    a2 += col[r + 64] * v[r + 64];
-    a3 += col[r + 96] * v[r + 96];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = j + 1 + (int)blockIdx.x * (8 / kGemvWarps) + warp / kGemvWarps;
+  const int w = warp % kGemvWarps;
+  double acc = 0.0;
+  if (c < n) {
+    const double* col = A + (int64_t)n * c;
+    constexpr int S = 32 * kGemvWarps;  // rows between consecutive loads of one lane
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int r = j + 1 + w * 32 + lane;
+    for (; r + 3 * S < n; r += 4 * S) {
+      a0 += col[r] * v[r];
+      a1 += col[r + S] * v[r + S];
+      a2 += col[r + 2 * S] * v[r + 2 * S];
+      a3 += col[r + 3 * S] * v[r + 3 * S];
+    }
+    for (; r < n; r += S) a0 += col[r] * v[r];
+    acc = warp_sum((a0 + a1) + (a2 + a3));
   }
-  for (; r < n; r += 32) a0 += col[r] * v[r];
-  const double acc = warp_sum((a0 + a1) + (a2 + a3));
-  if (lane == 0) y[c] = acc;
+  if (lane == 0) part[warp] = acc;
+  __syncthreads();
+  if (threadIdx.x < 8 / kGemvWarps) {
+    const int cc = j + 1 + (int)blockIdx.x * (8 / kGemvWarps) + (int)threadIdx.x;
+    if (cc < n) {
+      double s = 0.0;
+      for (int q = 0; q < kGemvWarps; ++q) s += part[threadIdx.x * kGemvWarps + q];
+      y[cc] = s;
+    }
+  }
 }
 
 // ---------------------------------------------------------------- stage 3: back-transformation
@@ -819,7 +836,8 @@ cudaError_t syevd_batched(double* A, int n, int nmat, double* Z, void* work, siz
     for (int i = 0; i < nb; ++i) {
       const int j = p + i;
       const int m = n - 1 - j;
-      trailing_gemv_kernel<<<dim3((m + 7) / 8, nmat), 256, 0, stream>>>(A, n, ms, V + ld * j, j, y);
+      trailing_gemv_kernel<<<dim3((m + 8 / kGemvWarps - 1) / (8 / kGemvWarps), nmat), 256, 0, stream>>>(
+          A, n, ms, V + ld * j, j, y);
       ++g_launches;
       house_kernel<<<kCS * nmat, kCT, 0, stream>>>(A, n, ms, V, Wp, p, i, i + 1 < nb ? i + 1 : -1, y, tau, d, e);
       ++g_launches;
