@@ -108,6 +108,7 @@ def load_library(path: str | os.PathLike | None = None):
     lib.rpa_b200_project_basis.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _i64, _vp, _i64]
     lib.rpa_b200_exchange_mbpt3.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _i64, _vp, _i64,
                                             _vp, _vp, _i64]
+    lib.rpa_b200_mbe_energy.argtypes = [_i64, _vp, _vp]
     lib.rpa_b200_tune_logdet.argtypes = [_vp, _i64, _i64, _vp, _vp, _vp]
     lib.rpa_b200_set_logdet_plan.argtypes = [_vp, _i64, _i64, _i64]
     lib.rpa_b200_get_logdet_plan.argtypes = [_vp, _i64, _vp, _vp]
@@ -115,6 +116,24 @@ def load_library(path: str | os.PathLike | None = None):
     if path is None:
         _lib = lib
     return lib
+
+
+SUBSYSTEMS = ("total", "A", "B", "C", "AB", "BC", "AC", "D", "AD", "BD", "CD", "ABC", "ABD", "ACD", "BCD")
+
+
+def mbe_energy(energies, nbody):
+    """Interaction (nbody 2) or nonadditive (3, 4) energy of a many-body expansion from the
+    subsystem energies, in the order of SUBSYSTEMS (rpa_b200_mbe_energy; host code, no GPU)."""
+    lib = load_library()
+    need = {2: 3, 3: 7, 4: 15}.get(int(nbody))
+    e = np.ascontiguousarray(energies, dtype=np.float64)
+    if need is None or e.size < need:
+        raise ValueError("nbody must be 2, 3 or 4 with 3, 7 or 15 subsystem energies")
+    out = ctypes.c_double()
+    st = lib.rpa_b200_mbe_energy(int(nbody), e.ctypes.data, ctypes.byref(out))
+    if st != RPA_OK:
+        raise RPAError(st, "rpa_b200_mbe_energy failed")
+    return out.value
 
 
 def freq_grid(orb_energies, nocc, nvirt, nfixed=0, core_thresh=-3.0, target_error=1e-6, target_rel_error=1e-3):

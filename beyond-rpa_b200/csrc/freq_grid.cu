@@ -13,9 +13,11 @@
 // Newton iteration on theta = arccos(t) with the three-term Legendre
 // recurrence (as quad_GaussLegendre, quadratures.f90:418-509, does).
 #include <cmath>
+#include <initializer_list>
 #include <vector>
 
 #include "../../include/rpa_b200.h"
+#include "rpa_common.cuh"
 
 namespace {
 
@@ -187,3 +189,44 @@ extern "C" int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* Orb
   *NFreqs = n;
   return RPA_OK;
 }
+
+// ------------------------------------------------------------------ many-body-expansion energies
+// rpa_Eint2Body / rpa_EintNadd / rpa_EintNadd4Body (src/rpa/rpa_driver.f90:381-433): each group
+// difference in FP64, left to right, as the reference evaluates it; the combination of the groups
+// (REAL(16) there) in double-double.
+extern "C" int rpa_b200_mbe_energy(int64_t NBody, const double* E, double* Eint) {
+  if (!E || !Eint || NBody < 2 || NBody > 4) return RPA_ERR_INVALID_ARG;
+  const double* e = E;
+  if (NBody == 2) {
+    *Eint = e[0] - e[1] - e[2];
+    return RPA_OK;
+  }
+  auto comb = [](std::initializer_list<double> terms) {
+    rpa::dd acc{0.0, 0.0};
+    for (double t : terms) acc = rpa::dd_add(acc, t);
+    return acc.hi + acc.lo;
+  };
+  // subsystem energies (0-based reference order)
+  const double tot = e[0], A = e[1], B = e[2], C = e[3], AB = e[4], BC = e[5], AC = e[6];
+  if (NBody == 3) {
+    const double eabc = tot - A - B - C;
+    const double eab = AB - A - B, ebc = BC - B - C, eac = AC - A - C;
+    *Eint = comb({eabc, -eab, -ebc, -eac});
+    return RPA_OK;
+  }
+  const double D = e[7], AD = e[8], BD = e[9], CD = e[10];
+  const double ABC = e[11], ABD = e[12], ACD = e[13], BCD = e[14];
+  const double eabcd = tot - A - B - C - D;
+  const double eabc = ABC - A - B - C, eabd = ABD - A - B - D, eacd = ACD - A - C - D, ebcd = BCD - B - C - D;
+  const double eab = AB - A - B, ebc = BC - B - C, eac = AC - A - C;
+  const double ead = AD - A - D, ebd = BD - B - D, ecd = CD - C - D;
+  // the reference forms the four three-body nonadditive terms in REAL(16), then subtracts them
+  // Eabcd - sum of pair terms - the four three-body nonadditive terms (Eabc - Eab - Ebc - Eac,
+  // ...), REAL(16) throughout in the reference: expanded here into one double-double sum so that
+  // no intermediate is rounded to FP64
+  *Eint = comb({eabcd, -eab, -ebc, -eac, -ead, -ebd, -ecd,
+                -eabc, eab, ebc, eac, -eabd, eab, ead, ebd,
+                -eacd, eac, ead, ecd, -ebcd, ebc, ebd, ecd});
+  return RPA_OK;
+}
+

@@ -149,6 +149,19 @@ int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* OrbEnergies, d
                        double* FreqWeights, int64_t* NFreqs);
 
 /*
+ * Interaction (NBody = 2) and nonadditive (NBody = 3, 4) energies of a many-body
+ * expansion from the subsystem energies E, in the reference's subsystem order
+ * (src/common/sys_definitions.f90:19-36), 0-based: E[0] whole system, E[1..3]
+ * monomers A, B, C, E[4..6] dimers AB, BC, AC, E[7] monomer D, E[8..10] dimers
+ * AD, BD, CD, E[11..14] trimers ABC, ABD, ACD, BCD; NBody = 2, 3, 4 reads
+ * E[0..2], E[0..6], E[0..14].  Replaces rpa_Eint2Body, rpa_EintNadd and
+ * rpa_EintNadd4Body (src/rpa/rpa_driver.f90:381-433): the group differences in
+ * FP64 as there, their combination in double-double (the reference's REAL(16)).
+ * Host-only; no handle.
+ */
+int rpa_b200_mbe_energy(int64_t NBody, const double* E, double* Eint);
+
+/*
  * Adjoint of the RPA energy: dE_c/dR (NQ x nov, leading dimension lddR),
  * dE_c/dOccEnergies (NOcc) and dE_c/dVirtEnergies (NVirt); Ec (may be NULL)
  * the energy itself.  No counterpart in the reference (it has no gradients):

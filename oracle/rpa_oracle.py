@@ -485,15 +485,39 @@ def ec_grad(R, eps_o, eps_v, freqs, weights, alpha=4.0):
 # --------------------------------------------------------------------------
 
 def eint_2body(e_ab, e_a, e_b):
-    """rpa_Eint2Body, src/rpa/rpa_driver.f90:381-386 (REAL(16) -> exact sums)."""
-    return math.fsum([e_ab, -e_a, -e_b])
+    """rpa_Eint2Body, src/rpa/rpa_driver.f90:381-386 (FP64, left to right)."""
+    return (e_ab - e_a) - e_b
 
 
 def eint_nadd3(e):
     """3-body nonadditive energy from the 7 subsystem energies
-    [ABC, AB, AC, BC, A, B, C]. rpa_EintNadd, src/rpa/rpa_driver.f90:389-400."""
+    [ABC, AB, AC, BC, A, B, C]. rpa_EintNadd, src/rpa/rpa_driver.f90:389-400: the group
+    differences in FP64, their combination in REAL(16) (here: exact sum, rounded once)."""
     abc, ab, ac, bc, a, b, c = e
-    return math.fsum([abc, -ab, -ac, -bc, a, b, c])
+    eabc = ((abc - a) - b) - c
+    eab, ebc, eac = (ab - a) - b, (bc - b) - c, (ac - a) - c
+    return math.fsum([eabc, -eab, -ebc, -eac])
+
+
+def mbe_energy(nbody, e):
+    """Interaction / nonadditive energy from subsystem energies in the reference order
+    (src/common/sys_definitions.f90:19-36, 0-based): total, A, B, C, AB, BC, AC, D, AD, BD, CD,
+    ABC, ABD, ACD, BCD.  rpa_Eint2Body / rpa_EintNadd / rpa_EintNadd4Body,
+    src/rpa/rpa_driver.f90:381-433."""
+    if nbody == 2:
+        return eint_2body(e[0], e[1], e[2])
+    tot, A, B, C, AB, BC, AC = e[:7]
+    if nbody == 3:
+        return eint_nadd3([tot, AB, AC, BC, A, B, C])
+    D, AD, BD, CD, ABC, ABD, ACD, BCD = e[7:15]
+    eabcd = (((tot - A) - B) - C) - D
+    eabc, eabd = ((ABC - A) - B) - C, ((ABD - A) - B) - D
+    eacd, ebcd = ((ACD - A) - C) - D, ((BCD - B) - C) - D
+    eab, ebc, eac = (AB - A) - B, (BC - B) - C, (AC - A) - C
+    ead, ebd, ecd = (AD - A) - D, (BD - B) - D, (CD - C) - D
+    return math.fsum([eabcd, -eab, -ebc, -eac, -ead, -ebd, -ecd,
+                      -eabc, eab, ebc, eac, -eabd, eab, ead, ebd,
+                      -eacd, eac, ead, ecd, -ebcd, ebc, ebd, ecd])
 
 
 # --------------------------------------------------------------------------

@@ -66,3 +66,32 @@ def test_plan_entry_points_reject_a_null_handle(pkg):
     assert lib.rpa_b200_set_logdet_plan(None, 512, 256, 64) == pkg.RPA_ERR_INVALID_ARG
     assert lib.rpa_b200_get_logdet_plan(None, 512, None, None) == pkg.RPA_ERR_INVALID_ARG
     assert lib.rpa_b200_set_autotune(None, 1) == pkg.RPA_ERR_INVALID_ARG
+
+
+@pytest.mark.parametrize("nbody", [2, 3, 4])
+def test_mbe_energy_matches_oracle(pkg, oracle, nbody):
+    # host entry point: interaction / nonadditive energies from subsystem energies of ~-100 Eh
+    rng = np.random.default_rng(40 + nbody)
+    for _ in range(50):
+        e = -100.0 * rng.uniform(0.5, 2.0, 15)
+        e[0] = np.sum(e[1:4]) + rng.uniform(-1e-2, 1e-2)  # a whole system near its parts
+        got = pkg.mbe_energy(e, nbody)
+        assert got == oracle.mbe_energy(nbody, e)
+
+
+def test_mbe_energy_of_additive_subsystems_vanishes(pkg):
+    # exactly additive energies (sums of monomers) give zero interaction at every order
+    a, b, c, d = -76.123456789012345, -40.5, -0.25, -12.0009765625
+    e = [a + b + c + d, a, b, c, a + b, b + c, a + c, d, a + d, b + d, c + d,
+         a + b + c, a + b + d, a + c + d, b + c + d]
+    assert abs(pkg.mbe_energy([a + b, a, b], 2)) <= 1e-14
+    e3 = [a + b + c] + e[1:7]
+    assert abs(pkg.mbe_energy(e3, 3)) <= 1e-13
+    assert abs(pkg.mbe_energy(e, 4)) <= 1e-13
+
+
+def test_mbe_energy_rejects_bad_arguments(pkg):
+    lib = pkg.load_library()
+    assert lib.rpa_b200_mbe_energy(5, None, None) == pkg.RPA_ERR_INVALID_ARG
+    with pytest.raises(ValueError):
+        pkg.mbe_energy([1.0, 2.0], 3)
