@@ -109,6 +109,7 @@ def load_library(path: str | os.PathLike | None = None):
     lib.rpa_b200_exchange_mbpt3.argtypes = [_vp, _i64, _i64, _i64, _vp, _i64, _vp, _vp, _i64, _vp, _i64, _vp, _i64,
                                             _vp, _vp, _i64]
     lib.rpa_b200_mbe_energy.argtypes = [_i64, _vp, _vp]
+    lib.rpa_b200_freq_grid_mbe.argtypes = [_i64, _vp, _vp, _vp, _dbl, _i64, _dbl, _dbl, _i64, _vp, _vp, _vp]
     lib.rpa_b200_tune_logdet.argtypes = [_vp, _i64, _i64, _vp, _vp, _vp]
     lib.rpa_b200_set_logdet_plan.argtypes = [_vp, _i64, _i64, _i64]
     lib.rpa_b200_get_logdet_plan.argtypes = [_vp, _i64, _vp, _vp]
@@ -134,6 +135,29 @@ def mbe_energy(energies, nbody):
     if st != RPA_OK:
         raise RPAError(st, "rpa_b200_mbe_energy failed")
     return out.value
+
+
+def freq_grid_mbe(sets, limit_dai=True, nfixed=0, core_thresh=-3.0, target_error=1e-6, target_rel_error=1e-3):
+    """One grid for the subsystems of a many-body expansion (rpa_b200_freq_grid_mbe; host code):
+    sets = [(orb_energies, nocc, nvirt), ...] with sets[0] the whole complex."""
+    lib = load_library()
+    arrs = [np.ascontiguousarray(e, dtype=np.float64) for e, _, _ in sets]
+    no = np.array([int(n) for _, n, _ in sets], dtype=np.int64)
+    nv = np.array([int(n) for _, _, n in sets], dtype=np.int64)
+    for a, o, v in zip(arrs, no, nv):
+        if a.size != o + v:
+            raise ValueError("each orbital-energy set must hold NOcc + NVirt values")
+    ptrs = (ctypes.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+    x = np.zeros(64)
+    w = np.zeros(64)
+    n = ctypes.c_int64()
+    st = lib.rpa_b200_freq_grid_mbe(len(arrs), no.ctypes.data, nv.ctypes.data, ctypes.cast(ptrs, _vp),
+                                    float(core_thresh), 1 if limit_dai else 0, float(target_error),
+                                    float(target_rel_error), int(nfixed), x.ctypes.data, w.ctypes.data,
+                                    ctypes.byref(n))
+    if st != RPA_OK:
+        raise RPAError(st, "rpa_b200_freq_grid_mbe failed")
+    return x[:n.value].copy(), w[:n.value].copy()
 
 
 def freq_grid(orb_energies, nocc, nvirt, nfixed=0, core_thresh=-3.0, target_error=1e-6, target_rel_error=1e-3):
@@ -324,6 +348,27 @@ class Handle:
         self._check(self.lib.rpa_b200_ec_grad(self._h, nq, no, nv, r.ptr, r.ld, eo.ptr, ev.ptr, K, fr.ptr, w.ptr,
                                               float(alpha), _PREC[prec], ctypes.byref(ec), p_dR, ld_dR, p_dO, p_dV))
         return ec.value, dR, dO, dV
+
+    def mbe_energies(self, subsystems, nbody, prec="split", limit_dai=True, nfixed=0, core_thresh=-3.0):
+        """Many-body-expansion driver (the energy part of rpa_PostSCF, src/rpa/rpa_driver.f90:25-433):
+        one frequency grid shared by all subsystems (freq_grid_mbe), every subsystem's E_c in one
+        batched call, then the interaction (nbody 2) or nonadditive (3, 4) energy (mbe_energy).
+
+        subsystems: (R, eps_occ, eps_virt) per subsystem in the order of SUBSYSTEMS (3, 7 or 15 of
+        them), R over the active occupied orbitals (those with eps >= core_thresh), eps_occ all
+        occupied energies ascending.  Returns (E_c per subsystem, interaction energy, freqs, weights)."""
+        need = {2: 3, 3: 7, 4: 15}.get(int(nbody))
+        if need is None or len(subsystems) != need:
+            raise ValueError("nbody 2, 3 or 4 needs 3, 7 or 15 subsystems")
+        sets = [(np.concatenate([np.asarray(eo, np.float64), np.asarray(ev, np.float64)]), len(eo), len(ev))
+                for _, eo, ev in subsystems]
+        x, w = freq_grid_mbe(sets, limit_dai=limit_dai, nfixed=nfixed, core_thresh=core_thresh)
+        systems = []
+        for R, eo, ev in subsystems:
+            eo = np.asarray(eo, np.float64)
+            systems.append((R, eo[eo >= core_thresh], ev, x, w))
+        ec, _ = self.ec_batched(systems, prec=prec)
+        return ec, mbe_energy(ec, nbody), x, w
 
     def ec_batched(self, systems, prec="split"):
         """Energies of many systems in one call (rpa_b200_ec_batched).

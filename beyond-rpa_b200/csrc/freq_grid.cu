@@ -70,17 +70,32 @@ struct Hist {
   std::vector<double> d, wt;
 };
 
-bool histogram(const double* e, int64_t nocc, int64_t nvirt, double core_thresh, int nbins, Hist& h) {
+int64_t ncore(const double* e, int64_t nocc, double core_thresh) {
   int64_t nc = 0;
   for (int64_t k = 0; k < nocc; ++k) {
     if (e[k] < core_thresh) ++nc;
     else break;
   }
-  if (nc >= nocc) return false;
+  return nc;
+}
+
+// Largest active excitation energy e_a1 - e_i0 (rpa_DaiMaxThresh, OrbDiffHist.f90:10-39); 0 when
+// every occupied orbital is frozen.
+double dai_max(const double* e, int64_t nocc, int64_t nvirt, double core_thresh) {
+  const int64_t nc = ncore(e, nocc, core_thresh);
+  return nc < nocc ? e[nocc + nvirt - 1] - e[nc] : 0.0;
+}
+
+// rpa_DaiHistogram (OrbDiffHist.f90:42-123): bins of the active differences d <= thresh.
+// Returns 1 for a histogram, 0 when every occupied orbital is frozen (the set then takes no part
+// in the error estimate), -1 for a non-positive gap.
+int histogram(const double* e, int64_t nocc, int64_t nvirt, double core_thresh, int nbins, double thresh, Hist& h) {
+  const int64_t nc = ncore(e, nocc, core_thresh);
+  if (nc >= nocc) return 0;
   const int64_t i0 = nc, i1 = nocc - 1, a0 = nocc, a1 = nocc + nvirt - 1;
   const double dmin = e[a0] - e[i1];
-  const double dmax = e[a1] - e[i0];
-  if (!(dmin > 0.0)) return false;
+  const double dmax = std::fmin(thresh, e[a1] - e[i0]);
+  if (!(dmin > 0.0)) return -1;
   const double width = (dmax - dmin) / nbins;
   h.d.resize(nbins);
   h.wt.assign(nbins, 0.0);
@@ -90,6 +105,7 @@ bool histogram(const double* e, int64_t nocc, int64_t nvirt, double core_thresh,
   for (int64_t i = i0; i <= i1; ++i)
     for (int64_t a = a0; a <= a1; ++a) {
       const double d = e[a] - e[i];
+      if (!(d <= thresh)) continue;
       const double x = (d - (dmin + width / 2.0)) / width;
       int64_t k = 1 + (int64_t)(x >= 0 ? std::floor(x + 0.5) : -std::floor(-x + 0.5));  // Fortran nint
       if (k < 1) k = 1;
@@ -98,26 +114,33 @@ bool histogram(const double* e, int64_t nocc, int64_t nvirt, double core_thresh,
       ++total;
     }
   for (int k = 0; k < nbins; ++k) h.wt[k] = std::fabs((double)cnt[k] / (double)total);
-  return true;
+  return 1;
 }
 
-void quad_error(const std::vector<double>& u, const std::vector<double>& w, const Hist& h, double& rel,
-                double& rmsd) {
+// rpa_FreqQuadError (OptFreqQuad.f90:125-169) over several histograms: the RMSD is the root of the
+// largest per-set mean square error, the relative error the largest over all sets.
+void quad_error(const std::vector<double>& u, const std::vector<double>& w, const std::vector<Hist>& hs,
+                double& rel, double& rmsd) {
   rel = 0.0;
-  double err2 = 0.0;
-  for (size_t l = 0; l < h.d.size(); ++l) {
-    if (!(h.wt[l] > 0.0)) continue;
-    const double d = h.d[l];
-    const double exact = kPiG / (2.0 * d);
-    double approx = 0.0;
-    for (size_t k = 0; k < u.size(); ++k) approx += w[k] / (d * d + u[k] * u[k]);
-    rel = std::fmax(rel, std::fabs((approx - exact) / exact));
-    err2 += h.wt[l] * (approx - exact) * (approx - exact);
+  double err2max = 0.0;
+  for (const Hist& h : hs) {
+    double err2 = 0.0;
+    for (size_t l = 0; l < h.d.size(); ++l) {
+      if (!(h.wt[l] > 0.0)) continue;
+      const double d = h.d[l];
+      const double exact = kPiG / (2.0 * d);
+      double approx = 0.0;
+      for (size_t k = 0; k < u.size(); ++k) approx += w[k] / (d * d + u[k] * u[k]);
+      rel = std::fmax(rel, std::fabs((approx - exact) / exact));
+      err2 += h.wt[l] * (approx - exact) * (approx - exact);
+    }
+    err2max = std::fmax(err2max, err2);
   }
-  rmsd = std::sqrt(err2);
+  rmsd = std::sqrt(err2max);
 }
 
-bool opt_scaling(int n, const Hist& h, std::vector<double>& u, std::vector<double>& w, double& rel, double& rmsd) {
+bool opt_scaling(int n, const std::vector<Hist>& h, std::vector<double>& u, std::vector<double>& w, double& rel,
+                 double& rmsd) {
   std::vector<double> t, wgl;
   if (!gauss_legendre(n, t, wgl)) return false;
   std::vector<double> u0(n), w0(n);
@@ -154,27 +177,19 @@ bool opt_scaling(int n, const Hist& h, std::vector<double>& u, std::vector<doubl
   return true;
 }
 
-}  // namespace
-
-extern "C" int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* OrbEnergies, double CoreOrbThresh,
-                                  double TargetError, double TargetRelError, int64_t NFixed, double* Freqs,
-                                  double* FreqWeights, int64_t* NFreqs) {
-  if (NOcc < 1 || NVirt < 1 || !OrbEnergies || !Freqs || !FreqWeights || !NFreqs) return RPA_ERR_INVALID_ARG;
-  if (NFixed < 0 || NFixed > 64) return RPA_ERR_INVALID_ARG;
-  for (int64_t k = 0; k < NOcc + NVirt; ++k)
-    if (!std::isfinite(OrbEnergies[k])) return RPA_ERR_NONFINITE;
-  Hist h;
-  if (!histogram(OrbEnergies, NOcc, NVirt, CoreOrbThresh, 100, h)) return RPA_ERR_INVALID_ARG;
+// The grid for the histograms hs (at least one non-empty).
+int grid_from_histograms(const std::vector<Hist>& hs, double TargetError, double TargetRelError, int64_t NFixed,
+                         double* Freqs, double* FreqWeights, int64_t* NFreqs) {
   std::vector<double> u, w;
   double rel = 0.0, rmsd = 0.0;
   int n = 0;
   if (NFixed > 0) {
     n = (int)NFixed;
-    if (!opt_scaling(n, h, u, w, rel, rmsd)) return RPA_ERR_NOT_CONVERGED;
+    if (!opt_scaling(n, hs, u, w, rel, rmsd)) return RPA_ERR_NOT_CONVERGED;
   } else {
     bool conv = false;
     for (n = 8; n <= 64; ++n) {
-      if (!opt_scaling(n, h, u, w, rel, rmsd)) return RPA_ERR_NOT_CONVERGED;
+      if (!opt_scaling(n, hs, u, w, rel, rmsd)) return RPA_ERR_NOT_CONVERGED;
       if (rmsd < TargetError && rel < TargetRelError) {
         conv = true;
         break;
@@ -188,6 +203,48 @@ extern "C" int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* Orb
   }
   *NFreqs = n;
   return RPA_OK;
+}
+
+}  // namespace
+
+extern "C" int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* OrbEnergies, double CoreOrbThresh,
+                                  double TargetError, double TargetRelError, int64_t NFixed, double* Freqs,
+                                  double* FreqWeights, int64_t* NFreqs) {
+  if (NOcc < 1 || NVirt < 1 || !OrbEnergies || !Freqs || !FreqWeights || !NFreqs) return RPA_ERR_INVALID_ARG;
+  if (NFixed < 0 || NFixed > 64) return RPA_ERR_INVALID_ARG;
+  for (int64_t k = 0; k < NOcc + NVirt; ++k)
+    if (!std::isfinite(OrbEnergies[k])) return RPA_ERR_NONFINITE;
+  std::vector<Hist> hs(1);
+  if (histogram(OrbEnergies, NOcc, NVirt, CoreOrbThresh, 100, HUGE_VAL, hs[0]) != 1) return RPA_ERR_INVALID_ARG;
+  return grid_from_histograms(hs, TargetError, TargetRelError, NFixed, Freqs, FreqWeights, NFreqs);
+}
+
+// One grid shared by the subsystems of a many-body expansion (rpa_PostSCF,
+// src/rpa/rpa_driver.f90:118-175): a histogram per subsystem and spin, optionally capped at the
+// largest excitation energy of set 0 (the whole complex, GridLimitDai), and the errors of the
+// optimiser taken as the worst over the sets.
+extern "C" int rpa_b200_freq_grid_mbe(int64_t NSets, const int64_t* NOcc, const int64_t* NVirt,
+                                      const double* const* OrbEnergies, double CoreOrbThresh, int64_t LimitDai,
+                                      double TargetError, double TargetRelError, int64_t NFixed, double* Freqs,
+                                      double* FreqWeights, int64_t* NFreqs) {
+  if (NSets < 1 || NSets > 4096 || !NOcc || !NVirt || !OrbEnergies || !Freqs || !FreqWeights || !NFreqs)
+    return RPA_ERR_INVALID_ARG;
+  if (NFixed < 0 || NFixed > 64) return RPA_ERR_INVALID_ARG;
+  for (int64_t s = 0; s < NSets; ++s) {
+    if (NOcc[s] < 1 || NVirt[s] < 1 || !OrbEnergies[s]) return RPA_ERR_INVALID_ARG;
+    for (int64_t k = 0; k < NOcc[s] + NVirt[s]; ++k)
+      if (!std::isfinite(OrbEnergies[s][k])) return RPA_ERR_NONFINITE;
+  }
+  const double thresh = LimitDai ? dai_max(OrbEnergies[0], NOcc[0], NVirt[0], CoreOrbThresh) : HUGE_VAL;
+  std::vector<Hist> hs;
+  for (int64_t s = 0; s < NSets; ++s) {
+    Hist h;
+    const int r = histogram(OrbEnergies[s], NOcc[s], NVirt[s], CoreOrbThresh, 100, thresh, h);
+    if (r < 0) return RPA_ERR_INVALID_ARG;
+    if (r > 0) hs.push_back(std::move(h));
+  }
+  if (hs.empty()) return RPA_ERR_INVALID_ARG;
+  return grid_from_histograms(hs, TargetError, TargetRelError, NFixed, Freqs, FreqWeights, NFreqs);
 }
 
 // ------------------------------------------------------------------ many-body-expansion energies

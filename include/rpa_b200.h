@@ -149,6 +149,25 @@ int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* OrbEnergies, d
                        double* FreqWeights, int64_t* NFreqs);
 
 /*
+ * One frequency grid shared by the subsystems of a many-body expansion (so that
+ * their energies differ consistently): NSets orbital-energy sets (one per
+ * subsystem and spin; set s has NOcc[s] occupied then NVirt[s] virtual
+ * energies at OrbEnergies[s]), set 0 being the whole complex.  A Delta
+ * histogram per set; LimitDai != 0 caps every histogram at the largest active
+ * excitation energy of set 0 (GridLimitDai: excitations on ghost atoms of a
+ * monomer must not stretch its histogram); the optimiser's RMSD and relative
+ * error are the worst over the sets.  A set whose occupied orbitals are all
+ * frozen takes no part.  Replaces the grid construction of rpa_PostSCF
+ * (src/rpa/rpa_driver.f90:118-175) with rpa_DaiMaxThresh / rpa_DaiHistogram
+ * (src/rpa/OrbDiffHist.f90:10-123) and the multi-set rpa_FreqQuadError
+ * (src/rpa/OptFreqQuad.f90:125-169).  Other arguments as rpa_b200_freq_grid.
+ */
+int rpa_b200_freq_grid_mbe(int64_t NSets, const int64_t* NOcc, const int64_t* NVirt,
+                           const double* const* OrbEnergies, double CoreOrbThresh, int64_t LimitDai,
+                           double TargetError, double TargetRelError, int64_t NFixed, double* Freqs,
+                           double* FreqWeights, int64_t* NFreqs);
+
+/*
  * Interaction (NBody = 2) and nonadditive (NBody = 3, 4) energies of a many-body
  * expansion from the subsystem energies E, in the reference's subsystem order
  * (src/common/sys_definitions.f90:19-36), 0-based: E[0] whole system, E[1..3]

@@ -80,6 +80,32 @@ def dai(eps_o, eps_v):
     return (eps_v[:, None] - eps_o[None, :]).reshape(-1, order="F")
 
 
+def dai_max_thresh(orb_energies, nocc, nvirt, core_thresh=CORE_ORB_THRESH):
+    """Largest active excitation energy e_a1 - e_i0 (0 when every occupied orbital is frozen).
+
+    rpa_DaiMaxThresh, src/rpa/OrbDiffHist.f90:10-39 (one spin)."""
+    e = np.asarray(orb_energies, np.float64)
+    nc = ncore(e, nocc, core_thresh)
+    return float(e[nocc + nvirt - 1] - e[nc]) if nc < nocc else 0.0
+
+
+def grid_for_cluster(sets, limit_dai=True, n=None, core_thresh=CORE_ORB_THRESH):
+    """One grid for the subsystems of a many-body expansion: sets = [(orb_energies, nocc, nvirt)]
+    with sets[0] the whole complex; histograms capped at its largest excitation energy when
+    limit_dai (rpa_PostSCF, src/rpa/rpa_driver.f90:118-175)."""
+    thresh = dai_max_thresh(*sets[0], core_thresh) if limit_dai else np.inf
+    vals, wts = [], []
+    for e, no, nv in sets:
+        v, w = dai_histogram(e, no, nv, core_thresh, thresh)
+        vals.append(v)
+        wts.append(w)
+    dv, dw = np.array(vals).T, np.array(wts).T
+    if n is not None:
+        x, w, *_ = opt_quad_scaling(n, dv, dw)
+        return x, w
+    return optimize_freq_quad(dv, dw)
+
+
 def dai_histogram(orb_energies, nocc, nvirt, core_thresh=CORE_ORB_THRESH,
                   dai_max_thresh=np.inf, nbins=100):
     """Histogram of orbital-energy differences used by the grid optimiser.

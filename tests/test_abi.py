@@ -95,3 +95,50 @@ def test_mbe_energy_rejects_bad_arguments(pkg):
     assert lib.rpa_b200_mbe_energy(5, None, None) == pkg.RPA_ERR_INVALID_ARG
     with pytest.raises(ValueError):
         pkg.mbe_energy([1.0, 2.0], 3)
+
+
+def _cluster_sets(seed=7):
+    # a dimer AB and its monomers in the dimer basis: the monomers carry ghost virtuals far above
+    # the complex's highest excitation, which the capped histograms must ignore
+    rng = np.random.default_rng(seed)
+    def orbitals(nocc, nvirt, ghosts):
+        occ = np.sort(np.concatenate([[-20.3], rng.uniform(-1.3, -0.4, nocc - 1)]))
+        virt = np.sort(np.concatenate([np.exp(rng.uniform(np.log(0.03), np.log(4.0), nvirt)),
+                                       rng.uniform(8.0, 40.0, ghosts)]))
+        return occ, virt
+    oa, va = orbitals(4, 30, 6)
+    ob, vb = orbitals(3, 26, 8)
+    oab = np.sort(np.concatenate([oa, ob]))
+    vab = np.sort(np.concatenate([va[va < 5.0], vb[vb < 5.0]]))
+    return [(np.concatenate([oab, vab]), len(oab), len(vab)),
+            (np.concatenate([oa, va]), len(oa), len(va)),
+            (np.concatenate([ob, vb]), len(ob), len(vb))]
+
+
+@pytest.mark.parametrize("limit", [True, False])
+def test_freq_grid_mbe_matches_oracle(pkg, oracle, limit):
+    sets = _cluster_sets()
+    x, w = pkg.freq_grid_mbe(sets, limit_dai=limit, nfixed=12)
+    xr, wr = oracle.grid_for_cluster(sets, limit_dai=limit, n=12)
+    assert np.allclose(x, xr, rtol=1e-12) and np.allclose(w, wr, rtol=1e-12)
+    x, w = pkg.freq_grid_mbe(sets, limit_dai=limit)
+    xr, wr = oracle.grid_for_cluster(sets, limit_dai=limit)
+    assert len(x) == len(xr) and np.allclose(x, xr, rtol=1e-12) and np.allclose(w, wr, rtol=1e-12)
+
+
+def test_freq_grid_mbe_of_one_set_is_the_single_grid(pkg):
+    (e, no, nv), = _cluster_sets()[:1]
+    x1, w1 = pkg.freq_grid(e, no, nv, nfixed=10)
+    x2, w2 = pkg.freq_grid_mbe([(e, no, nv)], nfixed=10)
+    assert np.array_equal(x1, x2) and np.array_equal(w1, w2)
+
+
+def test_freq_grid_mbe_skips_all_core_sets_and_rejects_bad_gaps(pkg):
+    sets = _cluster_sets()
+    core_only = (np.array([-25.0, -21.0, 0.5, 1.0, 2.0]), 2, 3)  # every occupied orbital frozen
+    x1, _ = pkg.freq_grid_mbe(sets, nfixed=10)
+    x2, _ = pkg.freq_grid_mbe(sets + [core_only], nfixed=10)
+    assert np.array_equal(x1, x2)
+    bad = (np.array([-1.0, 0.5, 0.2, 1.0]), 2, 2)  # HOMO above LUMO
+    with pytest.raises(pkg.RPAError):
+        pkg.freq_grid_mbe(sets + [bad], nfixed=10)

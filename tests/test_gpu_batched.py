@@ -67,3 +67,29 @@ def test_batched_repeated_call_uses_cached_graph(handle):
     a, _ = handle.ec_batched(sys_, prec="split")
     b, _ = handle.ec_batched(sys_, prec="split")
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-11), ("split", 1e-7)])
+def test_mbe_driver_dimer_of_noninteracting_monomers(handle, prec, tol):
+    # the driver: shared grid over the dimer and its monomers, batched energies, Eint;
+    # two non-interacting monomers (block-diagonal R) must give Eint ~ 0 on the shared grid
+    a = O.make_system(110, 4, 26, 301, decay=30.0, lam0=0.6)
+    b = O.make_system(90, 3, 28, 302, decay=25.0, lam0=0.6)
+    eo = np.concatenate([a.eps_o, b.eps_o])
+    ev = np.concatenate([a.eps_v, b.eps_v])
+    order_o, order_v = np.argsort(eo), np.argsort(ev)
+    no, nv = len(eo), len(ev)
+    R = np.zeros((a.nq + b.nq, no * nv))
+    pos_o, pos_v = np.argsort(order_o), np.argsort(order_v)  # position of each orbital in the sorted lists
+    for (s, q0, i0, a0) in ((a, 0, 0, 0), (b, a.nq, a.no, a.nv)):
+        Rr = s.R.reshape(s.nq, s.nv, s.no, order="F")
+        for i in range(s.no):
+            for aa in range(s.nv):
+                col = pos_v[a0 + aa] + nv * pos_o[i0 + i]
+                R[q0:q0 + s.nq, col] = Rr[:, aa, i]
+    subsystems = [(R, eo[order_o], ev[order_v]), (a.R, a.eps_o, a.eps_v), (b.R, b.eps_o, b.eps_v)]
+    ec, eint, x, w = handle.mbe_energies(subsystems, 2, prec=prec, nfixed=12)
+    assert abs(eint) < tol
+    for (Rs, eos, evs), e in zip(subsystems, ec):
+        ref, _ = O.ec_rpa(Rs, eos, evs, x, w)
+        assert abs(e - ref) < (1e-10 if prec == "fp64" else 1e-6)
