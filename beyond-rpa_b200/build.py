@@ -47,7 +47,7 @@ def build(force: bool = False, verbose_ptxas: bool = False, jobs: int | None = N
         return LIB
     objdir = HERE / "_build"
     objdir.mkdir(exist_ok=True)
-    flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "--expt-relaxed-constexpr",
+    flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O3,-fvisibility=hidden", "--expt-relaxed-constexpr",
                     f"-I{INCLUDE}", f"-I{CSRC}"]
     if verbose_ptxas:
         flags += ["-Xptxas", "-v"]

@@ -1387,7 +1387,7 @@ int rpa_b200_dring_t2(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVir
 // Split-BF16 pair contraction on the tensor cores: *out = sum_{i>=j} (2 - delta_ij) sum_{Q,mu} B_mu
 // W_ij W_ji with W_ij = R_i U_j^T and W_ji = R_j U2_i^T (U2 null: U).  R, U (and U2) are split into
 // bf16 hi/lo rows once per call; the unit partials are summed in a fixed order (deterministic).
-int sosex_split(rpa_b200_handle* h, const double* R, int64_t ldR, int NQ, int no, int nv, const double* U,
+static int sosex_split(rpa_b200_handle* h, const double* R, int64_t ldR, int NQ, int no, int nv, const double* U,
                 int64_t ldU, const double* U2, int64_t ldU2, int NT, const double* Bd, double* out) {
   const int nvp = rpa::sosex_tc_nvp(nv);
   const size_t P = (size_t)no * nvp;
@@ -1942,7 +1942,7 @@ int rpa_b200_project_basis(rpa_b200_handle* h, int64_t NQ, int64_t NVecs, int64_
 
 // Device copy of a column-major (rows x cols) input, or the input itself when it is already on
 // the device; ld receives the leading dimension of the returned pointer.
-int stage_matrix(rpa_b200_handle* h, DevBuf& buf, const double* A, int64_t lda, int64_t rows, int64_t cols,
+static int stage_matrix(rpa_b200_handle* h, DevBuf& buf, const double* A, int64_t lda, int64_t rows, int64_t cols,
                  const double** out, int64_t* ld) {
   if (is_device_ptr(A)) {
     *out = A;
@@ -1959,7 +1959,7 @@ int stage_matrix(rpa_b200_handle* h, DevBuf& buf, const double* A, int64_t lda, 
 
 // R = Z^T (Xa * Xi) into Rout (device, NQ x nov, ld ldR): Khatri-Rao blocks of whole occupied
 // orbitals (<= ~1 GB each) and one FP64 DMMA GEMM per block.
-int form_thc_r(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zd, int64_t ldz,
+static int form_thc_r(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zd, int64_t ldz,
                const double* Xad, int64_t ldxa, const double* Xid, int64_t ldxi, double* Rout, int64_t ldR) {
   const int64_t per_occ = NGrid * NVirt;
   int64_t ib = std::max<int64_t>(1, std::min<int64_t>(NOcc, (int64_t)(1ll << 27) / std::max<int64_t>(per_occ, 1)));
@@ -1975,7 +1975,7 @@ int form_thc_r(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int6
   return RPA_OK;
 }
 
-int check_thc_args(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zgk,
+static int check_thc_args(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zgk,
                    int64_t ldZ, const double* Xga, int64_t ldXa, const double* Xgi, int64_t ldXi) {
   if (NGrid < 1 || NQ < 1 || NOcc < 1 || NVirt < 1 || !Zgk || !Xga || !Xgi || ldZ < NGrid || ldXa < NGrid ||
       ldXi < NGrid)
@@ -2044,7 +2044,7 @@ int rpa_b200_ec_thc(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc,
 }
 
 // Device buffer grown to `bytes` keeping its first `used` bytes.
-int grow_keep(rpa_b200_handle* h, DevBuf& b, size_t bytes, size_t used) {
+static int grow_keep(rpa_b200_handle* h, DevBuf& b, size_t bytes, size_t used) {
   if (b.p && b.bytes >= bytes) return RPA_OK;
   const size_t nb = std::max(bytes, b.bytes * 2);
   void* p = nullptr;
@@ -2059,7 +2059,7 @@ int grow_keep(rpa_b200_handle* h, DevBuf& b, size_t bytes, size_t used) {
 
 // C = alpha A op(B) (+ beta C) with A (M x K) column-major and B given as (K x N) column-major
 // (bt = false) or as (N x K) column-major, i.e. B^T (bt = true).
-rpa::GemmF64Args gemm_g(int M, int N, int64_t K, const double* A, int64_t lda, bool at, const double* B,
+static rpa::GemmF64Args gemm_g(int M, int N, int64_t K, const double* A, int64_t lda, bool at, const double* B,
                         int64_t ldb, bool bt, double* C, int64_t ldc, double alpha = 1.0, double beta = 0.0) {
   rpa::GemmF64Args g = gemm_nn(M, N, K, A, lda, B, ldb, C, ldc);
   if (at) {

@@ -26,6 +26,11 @@
 #ifdef __cplusplus
 extern "C" {
 #endif
+/* The library is built with hidden default visibility: exactly the entry points declared here
+ * are exported. */
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
 
 typedef enum rpa_status {
   RPA_OK = 0,
@@ -383,6 +388,9 @@ int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
 int rpa_b200_ec_from_pi_noalloc(int64_t device, void* stream, int64_t NQ, int64_t NFreqs, const double* PiU,
                                 int64_t ldPi, const double* FreqWeights, double* Ec, double* Eu);
 
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
 #ifdef __cplusplus
 }
 #endif
