@@ -35,6 +35,7 @@ RPA_ERR_TIMEOUT = 6
 RPA_ERR_NO_DEVICE = 7
 RPA_ERR_NOT_CONVERGED = 8
 RPA_ERR_TOO_LARGE = 9
+RPA_ERR_INTERNAL = 10
 
 PREC_FP64 = 0
 PREC_SPLIT_BF16 = 1

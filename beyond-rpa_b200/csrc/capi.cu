@@ -16,6 +16,7 @@
 #include <string>
 #include <vector>
 
+#include "abi_guard.h"
 #include "kernels.h"
 
 using rpa::dd;
@@ -196,6 +197,8 @@ int validate_common(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt,
   if (!h) return RPA_ERR_INVALID_ARG;
   if (NQ < 1 || NQ > (1 << 20)) return fail(h, RPA_ERR_INVALID_ARG, "NQ=%lld out of range", (long long)NQ);
   if (NOcc < 1 || NVirt < 1) return fail(h, RPA_ERR_INVALID_ARG, "NOcc and NVirt must be >= 1");
+  if (NOcc > INT32_MAX / NVirt)
+    return fail(h, RPA_ERR_TOO_LARGE, "NOcc*NVirt=%lld*%lld exceeds 2^31-1", (long long)NOcc, (long long)NVirt);
   if (NFreqs < 1 || NFreqs > 64) return fail(h, RPA_ERR_INVALID_ARG, "NFreqs=%lld not in [1,64]", (long long)NFreqs);
   if (ldR < NQ) return fail(h, RPA_ERR_INVALID_ARG, "ldR < NQ");
   if (!R || !eo || !ev || !freqs) return fail(h, RPA_ERR_INVALID_ARG, "NULL array argument");
@@ -922,11 +925,27 @@ void finish_timings(rpa_b200_handle* h) {
   h->launches = rpa::g_launches;
 }
 
+// Handler of the entry points' function-try-blocks: the status of the exception in flight, its
+// text in last_error, and a stream capture the unwound call left open on the handle's stream ended
+// and discarded, so that the next call on this handle starts clean.
+int exception_status(rpa_b200_handle* h) noexcept {
+  if (!h) return rpa::status_of_exception(nullptr);
+  const int status = rpa::status_of_exception(&h->last_error);
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (h->stream && cudaStreamIsCapturing(h->stream, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(h->stream, &g);
+    if (g) cudaGraphDestroy(g);
+  }
+  cudaGetLastError();
+  return status;
+}
+
 }  // namespace
 
 extern "C" {
 
-int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) {
+int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) try {
   (void)flags;
   if (!handle) return RPA_ERR_INVALID_ARG;
   *handle = nullptr;
@@ -984,9 +1003,11 @@ int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) {
   h->encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   *handle = h;
   return RPA_OK;
+} catch (...) {
+  return rpa::status_of_exception(nullptr);
 }
 
-int rpa_b200_destroy(rpa_b200_handle* h) {
+int rpa_b200_destroy(rpa_b200_handle* h) try {
   if (!h) return RPA_OK;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
@@ -1028,6 +1049,8 @@ int rpa_b200_destroy(rpa_b200_handle* h) {
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   delete h;
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 const char* rpa_b200_status_string(int status) {
@@ -1036,33 +1059,38 @@ const char* rpa_b200_status_string(int status) {
     case RPA_ERR_INVALID_ARG: return "invalid argument";
     case RPA_ERR_NOT_SPD: return "1+Pi(u) is not positive definite";
     case RPA_ERR_NONFINITE: return "non-finite input or result";
-    case RPA_ERR_OOM: return "device out of memory";
+    case RPA_ERR_OOM: return "out of memory";
     case RPA_ERR_CUDA: return "CUDA error";
     case RPA_ERR_TIMEOUT: return "device-side wait timed out";
     case RPA_ERR_NO_DEVICE: return "no sm_100 device";
     case RPA_ERR_NOT_CONVERGED: return "not converged";
-    case RPA_ERR_TOO_LARGE: return "problem exceeds the fixed scratch of the allocation-free entry point";
+    case RPA_ERR_TOO_LARGE: return "problem exceeds a size limit of the entry point";
+    case RPA_ERR_INTERNAL: return "internal error";
     default: return "unknown status";
   }
 }
 
 const char* rpa_b200_last_error(const rpa_b200_handle* h) { return h ? h->last_error.c_str() : "null handle"; }
 
-int rpa_b200_last_timings(const rpa_b200_handle* h, double* out, int64_t n) {
+int rpa_b200_last_timings(const rpa_b200_handle* h, double* out, int64_t n) try {
   if (!h || !out) return RPA_ERR_INVALID_ARG;
   for (int64_t i = 0; i < n && i < 6; ++i) out[i] = h->timings[i];
   return RPA_OK;
+} catch (...) {
+  return rpa::status_of_exception(nullptr);
 }
 
 int64_t rpa_b200_last_launches(const rpa_b200_handle* h) { return h ? h->launches : -1; }
 
-int rpa_b200_set_stream(rpa_b200_handle* h, void* stream) {
+int rpa_b200_set_stream(rpa_b200_handle* h, void* stream) try {
   if (!h) return RPA_ERR_INVALID_ARG;
   h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
-int rpa_b200_tune_logdet(rpa_b200_handle* h, int64_t NQ, int64_t NMat, int64_t* Nb2, int64_t* Tile, double* Ms) {
+int rpa_b200_tune_logdet(rpa_b200_handle* h, int64_t NQ, int64_t NMat, int64_t* Nb2, int64_t* Tile, double* Ms) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   if (NQ < 1 || NQ > (1 << 20) || NMat < 1 || NMat > (1 << 20))
@@ -1075,9 +1103,11 @@ int rpa_b200_tune_logdet(rpa_b200_handle* h, int64_t NQ, int64_t NMat, int64_t* 
   if (Tile) *Tile = 32 * p.tile_w;
   h->launches = rpa::g_launches;
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
-int rpa_b200_set_logdet_plan(rpa_b200_handle* h, int64_t NQ, int64_t Nb2, int64_t Tile) {
+int rpa_b200_set_logdet_plan(rpa_b200_handle* h, int64_t NQ, int64_t Nb2, int64_t Tile) try {
   if (!h || NQ < 1) return RPA_ERR_INVALID_ARG;
   const rpa::LogdetPlan p{(int)Nb2, (int)(Tile / 32)};
   if ((Nb2 != 128 && Nb2 != 256 && Nb2 != 512) || (Tile != 64 && Tile != 128) || !rpa::valid_logdet_plan(p))
@@ -1085,25 +1115,31 @@ int rpa_b200_set_logdet_plan(rpa_b200_handle* h, int64_t NQ, int64_t Nb2, int64_
   h->logdet_plans[plan_bucket((int)std::min<int64_t>(NQ, 1 << 30))] = p;
   ++h->plans_version;
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
-int rpa_b200_get_logdet_plan(const rpa_b200_handle* h, int64_t NQ, int64_t* Nb2, int64_t* Tile) {
+int rpa_b200_get_logdet_plan(const rpa_b200_handle* h, int64_t NQ, int64_t* Nb2, int64_t* Tile) try {
   if (!h || NQ < 1) return RPA_ERR_INVALID_ARG;
   const rpa::LogdetPlan p = plan_for(h, (int)std::min<int64_t>(NQ, 1 << 30));
   if (Nb2) *Nb2 = p.nb2;
   if (Tile) *Tile = 32 * p.tile_w;
   return RPA_OK;
+} catch (...) {
+  return rpa::status_of_exception(nullptr);
 }
 
-int rpa_b200_set_autotune(rpa_b200_handle* h, int64_t on) {
+int rpa_b200_set_autotune(rpa_b200_handle* h, int64_t on) try {
   if (!h) return RPA_ERR_INVALID_ARG;
   h->autotune = on != 0;
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 int rpa_b200_pi(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R, int64_t ldR,
                 const double* OccEnergies, const double* VirtEnergies, int64_t NFreqs, const double* Freqs,
-                double alpha, int64_t prec, double* PiU, int64_t ldPi) {
+                double alpha, int64_t prec, double* PiU, int64_t ldPi) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   Validated v;
@@ -1132,13 +1168,15 @@ int rpa_b200_pi(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, con
   if ((s = check_device_error(h))) return s;
   finish_timings(h);
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 int rpa_b200_ec_from_pi(rpa_b200_handle* h, int64_t NQ, int64_t NFreqs, const double* PiU, int64_t ldPi,
-                        const double* FreqWeights, double* Ec, double* Eu) {
+                        const double* FreqWeights, double* Ec, double* Eu) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
-  if (NQ < 1 || NFreqs < 1 || NFreqs > 64 || ldPi < NQ || !PiU || !FreqWeights || !Ec)
+  if (NQ < 1 || NQ > (1 << 20) || NFreqs < 1 || NFreqs > 64 || ldPi < NQ || !PiU || !FreqWeights || !Ec)
     return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_ec_from_pi");
   std::vector<double> w;
   if ((s = fetch_small(h, FreqWeights, NFreqs, w))) return s;
@@ -1165,11 +1203,13 @@ int rpa_b200_ec_from_pi(rpa_b200_handle* h, int64_t NQ, int64_t NFreqs, const do
   RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
   finish_timings(h);
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 int rpa_b200_ec(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R, int64_t ldR,
                 const double* OccEnergies, const double* VirtEnergies, int64_t NFreqs, const double* Freqs,
-                const double* FreqWeights, double alpha, int64_t prec, double* Ec, double* Eu) {
+                const double* FreqWeights, double alpha, int64_t prec, double* Ec, double* Eu) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   Validated v;
@@ -1204,6 +1244,8 @@ int rpa_b200_ec(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, con
   RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
   finish_timings(h);
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 
@@ -1212,7 +1254,7 @@ int rpa_b200_dring_t2(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVir
                       const double* FreqWeights, double alpha, int64_t prec, int64_t GuessNVecs, const double* Omega,
                       uint64_t seed, double SmallEigenvalsCutoff, double CutoffThresh, int64_t CutoffType,
                       double* CommonThresh, int64_t MaxNVecsT2, double* A, double* U, int64_t ldU,
-                      int64_t* NVecsT2, double* EigRPA, double* Ec) {
+                      int64_t* NVecsT2, double* EigRPA, double* Ec) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   Validated v;
@@ -1382,6 +1424,8 @@ int rpa_b200_dring_t2(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVir
   if (*CommonThresh < 0.0) *CommonThresh = K;
   finish_timings(h);
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 // Split-BF16 pair contraction on the tensor cores: *out = sum_{i>=j} (2 - delta_ij) sum_{Q,mu} B_mu
@@ -1446,7 +1490,7 @@ static int sosex_split(rpa_b200_handle* h, const double* R, int64_t ldR, int NQ,
 
 int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R,
                             int64_t ldR, int64_t NVecsT2, const double* U, int64_t ldU, const double* A, double Alpha,
-                            int64_t S2Operator, int64_t Prec, double* Ex) {
+                            int64_t S2Operator, int64_t Prec, double* Ex) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   const int64_t nov = NOcc * NVirt;
@@ -1510,6 +1554,8 @@ int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
   *Ex = -Alpha * (acc.hi + acc.lo);
   finish_timings(h);
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 // MBPT3 exchange (rpa_CC_Exchange_MBPT3_1, src/rpa/rpa_CC_Exchange.f90:232-272, with rpa_CC_Ukl :177,
@@ -1523,7 +1569,7 @@ int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
 int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R,
                             int64_t ldR, const double* OccEnergies, const double* VirtEnergies, int64_t NVecsT2,
                             const double* U, int64_t ldU, const double* A, int64_t Prec, double* Ex, double* X,
-                            int64_t ldX) {
+                            int64_t ldX) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   const int64_t nov = NOcc * NVirt;
@@ -1700,11 +1746,13 @@ int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
   *Ex = -(acc.hi + acc.lo);
   finish_timings(h);
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 // Replaces real_EVD (src/linear-algebra/real_linalg.f90:1501-1559, LAPACK dsyevd) with
 // ComputeEigenvecs = .true.: eigenvalues ascending, A overwritten by the eigenvectors.
-int rpa_b200_syevd(rpa_b200_handle* h, int64_t N, double* A, int64_t ldA, double* Eigenvals) {
+int rpa_b200_syevd(rpa_b200_handle* h, int64_t N, double* A, int64_t ldA, double* Eigenvals) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   if (N < 1 || ldA < N || !A || !Eigenvals) return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_syevd");
@@ -1742,6 +1790,8 @@ int rpa_b200_syevd(rpa_b200_handle* h, int64_t N, double* A, int64_t ldA, double
   RPA_CUDA(h, cudaStreamSynchronize(h->stream));
   finish_timings(h);
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 // Basis of the effective dielectric matrix from Pi at the lowest frequency: rpa_G
@@ -1753,7 +1803,7 @@ int rpa_b200_piu_basis(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVi
                        const double* OccEnergies, const double* VirtEnergies, double LowestFreq, double alpha,
                        int64_t prec, int64_t BasisType, double TargetError, const double* Guess, int64_t ldGuess,
                        uint64_t seed, double* G, int64_t ldG, int64_t* NVecs, double* TraceError,
-                       double* ExactTrace) {
+                       double* ExactTrace) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   if (BasisType < 1 || BasisType > 3) return fail(h, RPA_ERR_INVALID_ARG, "invalid basis type %lld", (long long)BasisType);
@@ -1890,12 +1940,14 @@ int rpa_b200_piu_basis(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVi
   RPA_CUDA(h, cudaStreamSynchronize(h->stream));
   finish_timings(h);
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 // R' = G^T R (NVecs x nov): the Cholesky vectors in the compressed Pi basis (the Cholesky-path
 // counterpart of THC_ZgkPiU = Zgk G(:, 1:NVecsPiU), src/rpa/rpa.f90:2318-2320).
 int rpa_b200_project_basis(rpa_b200_handle* h, int64_t NQ, int64_t NVecs, int64_t nov, const double* G, int64_t ldG,
-                           const double* R, int64_t ldR, double* Rp, int64_t ldRp) {
+                           const double* R, int64_t ldR, double* Rp, int64_t ldRp) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   if (NQ < 1 || NVecs < 1 || NVecs > NQ || nov < 1 || !G || !R || !Rp || ldG < NQ || ldR < NQ || ldRp < NVecs)
@@ -1938,6 +1990,8 @@ int rpa_b200_project_basis(rpa_b200_handle* h, int64_t NQ, int64_t NVecs, int64_
   RPA_CUDA(h, cudaStreamSynchronize(h->stream));
   finish_timings(h);
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 // Device copy of a column-major (rows x cols) input, or the input itself when it is already on
@@ -1980,7 +2034,7 @@ static int check_thc_args(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t
   if (NGrid < 1 || NQ < 1 || NOcc < 1 || NVirt < 1 || !Zgk || !Xga || !Xgi || ldZ < NGrid || ldXa < NGrid ||
       ldXi < NGrid)
     return fail(h, RPA_ERR_INVALID_ARG, "invalid THC factor dimensions");
-  if (NGrid > INT32_MAX || NQ > INT32_MAX || NOcc * NVirt > INT32_MAX)
+  if (NGrid > INT32_MAX || NQ > INT32_MAX || NOcc > INT32_MAX / NVirt)
     return fail(h, RPA_ERR_TOO_LARGE, "THC dimensions too large");
   return RPA_OK;
 }
@@ -1989,7 +2043,7 @@ static int check_thc_args(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t
 // rpa_THC_Rkab / rpa_THC_Rkai (src/rpa/rpa_THC.f90:374-426).
 int rpa_b200_thc_r(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zgk,
                    int64_t ldZ, const double* Xga, int64_t ldXa, const double* Xgi, int64_t ldXi, double* R,
-                   int64_t ldR) {
+                   int64_t ldR) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   if ((s = check_thc_args(h, NGrid, NQ, NOcc, NVirt, Zgk, ldZ, Xga, ldXa, Xgi, ldXi))) return s;
@@ -2019,6 +2073,8 @@ int rpa_b200_thc_r(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, 
   RPA_CUDA(h, cudaStreamSynchronize(h->stream));
   finish_timings(h);
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 // RPA energy from THC factors (the FullRkai branch of rpa_THC_PiU, src/rpa/rpa_THC.f90:215-329):
@@ -2026,7 +2082,7 @@ int rpa_b200_thc_r(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, 
 int rpa_b200_ec_thc(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zgk,
                     int64_t ldZ, const double* Xga, int64_t ldXa, const double* Xgi, int64_t ldXi,
                     const double* OccEnergies, const double* VirtEnergies, int64_t NFreqs, const double* Freqs,
-                    const double* FreqWeights, double alpha, int64_t prec, double* Ec, double* Eu) {
+                    const double* FreqWeights, double alpha, int64_t prec, double* Ec, double* Eu) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   if ((s = check_thc_args(h, NGrid, NQ, NOcc, NVirt, Zgk, ldZ, Xga, ldXa, Xgi, ldXi))) return s;
@@ -2041,6 +2097,8 @@ int rpa_b200_ec_thc(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc,
   if ((s = form_thc_r(h, NGrid, NQ, NOcc, NVirt, Zd, ldz, Xad, ldxa, Xid, ldxi, Rd, NQ))) return s;
   return rpa_b200_ec(h, NQ, NOcc, NVirt, Rd, NQ, OccEnergies, VirtEnergies, NFreqs, Freqs, FreqWeights, alpha, prec,
                      Ec, Eu);
+} catch (...) {
+  return exception_status(h);
 }
 
 // Device buffer grown to `bytes` keeping its first `used` bytes.
@@ -2085,7 +2143,7 @@ int rpa_b200_jctc2024(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOc
                       int64_t ldZ, const double* Xgi, int64_t ldXi, const double* Yga, int64_t ldYa, int64_t NVecsT2,
                       const double* U, int64_t ldU, const double* Am, const double* Lik, int64_t ldL,
                       double CutoffThreshPNO, int64_t BoysScreening, double CutoffThreshVabij, double* Energies,
-                      int64_t* PNOStats) {
+                      int64_t* PNOStats) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   if (NGrid < 1 || NQ < 1 || NOcc < 1 || NVirt < 1 || NVecsT2 < 1 || !Zgk || !Xgi || !Yga || !U || !Am ||
@@ -2479,13 +2537,16 @@ int rpa_b200_jctc2024(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOc
   Energies[3] = e2ghij.hi + e2ghij.lo;
   finish_timings(h);
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* inst, int64_t prec, double* Ec,
-                        double* Eu) {
+                        double* Eu) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
-  if (ninst < 1 || !inst || !Ec) return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_ec_batched");
+  if (ninst < 1 || ninst > (1 << 24) || !inst || !Ec)
+    return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_ec_batched");
   if (prec != RPA_PREC_FP64 && prec != RPA_PREC_SPLIT_BF16)
     return fail(h, RPA_ERR_INVALID_ARG, "unknown precision mode %lld", (long long)prec);
   const int n = (int)ninst;
@@ -2969,12 +3030,14 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
   }
   finish_timings(h);
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 int rpa_b200_ec_grad(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* R, int64_t ldR,
                      const double* OccEnergies, const double* VirtEnergies, int64_t NFreqs, const double* Freqs,
                      const double* FreqWeights, double alpha, int64_t prec, double* Ec, double* dR, int64_t lddR,
-                     double* dOcc, double* dVirt) {
+                     double* dOcc, double* dVirt) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
   Validated v;
@@ -3059,6 +3122,8 @@ int rpa_b200_ec_grad(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt
   }
   finish_timings(h);
   return RPA_OK;
+} catch (...) {
+  return exception_status(h);
 }
 
 }  // extern "C"

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/rpa_b200.h"
+#include "abi_guard.h"
 #include "rpa_common.cuh"
 
 namespace {
@@ -209,7 +210,7 @@ int grid_from_histograms(const std::vector<Hist>& hs, double TargetError, double
 
 extern "C" int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* OrbEnergies, double CoreOrbThresh,
                                   double TargetError, double TargetRelError, int64_t NFixed, double* Freqs,
-                                  double* FreqWeights, int64_t* NFreqs) {
+                                  double* FreqWeights, int64_t* NFreqs) try {
   if (NOcc < 1 || NVirt < 1 || !OrbEnergies || !Freqs || !FreqWeights || !NFreqs) return RPA_ERR_INVALID_ARG;
   if (NFixed < 0 || NFixed > 64) return RPA_ERR_INVALID_ARG;
   for (int64_t k = 0; k < NOcc + NVirt; ++k)
@@ -217,6 +218,8 @@ extern "C" int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* Orb
   std::vector<Hist> hs(1);
   if (histogram(OrbEnergies, NOcc, NVirt, CoreOrbThresh, 100, HUGE_VAL, hs[0]) != 1) return RPA_ERR_INVALID_ARG;
   return grid_from_histograms(hs, TargetError, TargetRelError, NFixed, Freqs, FreqWeights, NFreqs);
+} catch (...) {
+  return rpa::status_of_exception(nullptr);
 }
 
 // One grid shared by the subsystems of a many-body expansion (rpa_PostSCF,
@@ -226,7 +229,7 @@ extern "C" int rpa_b200_freq_grid(int64_t NOcc, int64_t NVirt, const double* Orb
 extern "C" int rpa_b200_freq_grid_mbe(int64_t NSets, const int64_t* NOcc, const int64_t* NVirt,
                                       const double* const* OrbEnergies, double CoreOrbThresh, int64_t LimitDai,
                                       double TargetError, double TargetRelError, int64_t NFixed, double* Freqs,
-                                      double* FreqWeights, int64_t* NFreqs) {
+                                      double* FreqWeights, int64_t* NFreqs) try {
   if (NSets < 1 || NSets > 4096 || !NOcc || !NVirt || !OrbEnergies || !Freqs || !FreqWeights || !NFreqs)
     return RPA_ERR_INVALID_ARG;
   if (NFixed < 0 || NFixed > 64) return RPA_ERR_INVALID_ARG;
@@ -245,13 +248,15 @@ extern "C" int rpa_b200_freq_grid_mbe(int64_t NSets, const int64_t* NOcc, const 
   }
   if (hs.empty()) return RPA_ERR_INVALID_ARG;
   return grid_from_histograms(hs, TargetError, TargetRelError, NFixed, Freqs, FreqWeights, NFreqs);
+} catch (...) {
+  return rpa::status_of_exception(nullptr);
 }
 
 // ------------------------------------------------------------------ many-body-expansion energies
 // rpa_Eint2Body / rpa_EintNadd / rpa_EintNadd4Body (src/rpa/rpa_driver.f90:381-433): each group
 // difference in FP64, left to right, as the reference evaluates it; the combination of the groups
 // (REAL(16) there) in double-double.
-extern "C" int rpa_b200_mbe_energy(int64_t NBody, const double* E, double* Eint) {
+extern "C" int rpa_b200_mbe_energy(int64_t NBody, const double* E, double* Eint) try {
   if (!E || !Eint || NBody < 2 || NBody > 4) return RPA_ERR_INVALID_ARG;
   const double* e = E;
   if (NBody == 2) {
@@ -285,5 +290,7 @@ extern "C" int rpa_b200_mbe_energy(int64_t NBody, const double* E, double* Eint)
                 -eabc, eab, ebc, eac, -eabd, eab, ead, ebd,
                 -eacd, eac, ead, ecd, -ebcd, ebc, ebd, ecd});
   return RPA_OK;
+} catch (...) {
+  return rpa::status_of_exception(nullptr);
 }
 

@@ -26,6 +26,7 @@
 #include <mutex>
 #include <vector>
 
+#include "abi_guard.h"
 #include "kernels.h"
 
 namespace {
@@ -68,7 +69,7 @@ bool is_device_pointer(const void* p) {
 
 extern "C" int rpa_b200_ec_from_pi_noalloc(int64_t device, void* stream_ptr, int64_t NQ, int64_t NFreqs,
                                            const double* PiU, int64_t ldPi, const double* FreqWeights, double* Ec,
-                                           double* Eu) {
+                                           double* Eu) try {
   if (NQ < 1 || NFreqs < 1 || NFreqs > 64 || ldPi < NQ || !PiU || !FreqWeights || !Ec) return RPA_ERR_INVALID_ARG;
   const size_t n = (size_t)NQ, K = (size_t)NFreqs;
   // layout of the scratch: Pi copy | L_ii | traces + log sums (double-double) | error word, counter
@@ -89,11 +90,11 @@ extern "C" int rpa_b200_ec_from_pi_noalloc(int64_t device, void* stream_ptr, int
   double* tr = Ldiag + K * n;
   double* ld = tr + 2 * K;
   int* flags = reinterpret_cast<int*>(ld + 2 * K);  // flags[0] = device error word, flags[1] = non-finite count
-  std::vector<double> w(K), host(4 * K);
+  double w[64], host[4 * 64];  // K <= 64
   int f[2] = {0, 0};
   do {
     if (is_device_pointer(FreqWeights)) {
-      if (cudaMemcpyAsync(w.data(), FreqWeights, K * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      if (cudaMemcpyAsync(w, FreqWeights, K * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
           cudaStreamSynchronize(st) != cudaSuccess) {
         status = RPA_ERR_CUDA;
         break;
@@ -124,7 +125,7 @@ extern "C" int rpa_b200_ec_from_pi_noalloc(int64_t device, void* stream_ptr, int
       status = RPA_ERR_CUDA;
       break;
     }
-    if (cudaMemcpyAsync(host.data(), tr, 4 * K * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+    if (cudaMemcpyAsync(host, tr, 4 * K * 8, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaMemcpyAsync(f, flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {
       status = RPA_ERR_CUDA;
@@ -161,4 +162,6 @@ extern "C" int rpa_b200_ec_from_pi_noalloc(int64_t device, void* stream_ptr, int
   } while (false);
   cudaSetDevice(prev);
   return status;
+} catch (...) {
+  return rpa::status_of_exception(nullptr);
 }

@@ -37,13 +37,16 @@ typedef enum rpa_status {
   RPA_ERR_INVALID_ARG = 1,  /* bad dimension, NULL pointer, unsupported mode   */
   RPA_ERR_NOT_SPD = 2,      /* 1+Pi(u) not positive definite (Cholesky pivot) */
   RPA_ERR_NONFINITE = 3,    /* NaN/Inf in an input or result                 */
-  RPA_ERR_OOM = 4,          /* device allocation failed                       */
+  RPA_ERR_OOM = 4,          /* device or host allocation failed               */
   RPA_ERR_CUDA = 5,         /* CUDA runtime / driver error                    */
   RPA_ERR_TIMEOUT = 6,      /* a bounded device-side wait expired             */
   RPA_ERR_NO_DEVICE = 7,    /* no sm_100 GPU visible                          */
   RPA_ERR_NOT_CONVERGED = 8, /* quadrature / eigen-solver did not converge    */
-  RPA_ERR_TOO_LARGE = 9      /* problem exceeds the fixed scratch of
-                                rpa_b200_ec_from_pi_noalloc                    */
+  RPA_ERR_TOO_LARGE = 9,    /* problem exceeds a size limit of the entry point
+                                (e.g. the fixed scratch of
+                                rpa_b200_ec_from_pi_noalloc)                   */
+  RPA_ERR_INTERNAL = 10     /* unexpected host-side failure; no entry point
+                                lets a C++ exception escape                    */
 } rpa_status;
 
 /* Precision of the Pi(u) contraction. */

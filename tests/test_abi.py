@@ -22,6 +22,36 @@ def test_status_strings(pkg):
     assert lib.rpa_b200_status_string(999) == b"unknown status"
 
 
+def test_status_codes_match_the_header(pkg):
+    import re
+    text = pkg.HEADER.read_text()
+    enum = dict((m.group(1), int(m.group(2))) for m in re.finditer(r"\b(RPA_(?:OK|ERR_\w+))\s*=\s*(\d+)", text))
+    assert enum["RPA_ERR_INTERNAL"] == 10
+    for name, value in enum.items():
+        assert getattr(pkg, name) == value, name
+    lib = pkg.load_library()
+    strings = [lib.rpa_b200_status_string(v) for v in sorted(enum.values())]
+    assert b"unknown status" not in strings and len(set(strings)) == len(strings)
+
+
+def test_no_entry_point_lets_an_exception_escape(pkg):
+    # every exported int-returning definition is a function-try-block with a catch-all handler
+    import re
+    csrc = pkg.HEADER.parents[1] / "beyond-rpa_b200" / "csrc"
+    seen = 0
+    for path in sorted(csrc.glob("*.cu")):
+        src = path.read_text()
+        for m in re.finditer(r'^(?:extern "C" )?int (rpa_b200_\w+)\(', src, re.M):
+            brace = src.index("{", m.end())
+            assert src[:brace].endswith(") try "), f"{path.name}: {m.group(1)} is not a function-try-block"
+            close = src.index("\n}", brace)
+            assert src.startswith("\n} catch (...) {", close), f"{path.name}: {m.group(1)} has no catch-all"
+            seen += 1
+    declared = [n for n in pkg.declared_functions() if n not in
+                ("rpa_b200_status_string", "rpa_b200_last_error", "rpa_b200_last_launches")]
+    assert seen == len(declared)
+
+
 def test_create_without_gpu_reports_no_device(pkg):
     import torch
     if torch.cuda.is_available():
