@@ -63,4 +63,4 @@ def test_noalloc_rejects_problems_beyond_its_scratch(pkg):
     st = lib.rpa_b200_ec_from_pi_noalloc(0, None, 2100, 1, pi.ctypes.data, 2100, w.ctypes.data,
                                          ctypes.byref(ec), None)
     assert st == pkg.RPA_ERR_TOO_LARGE
-    assert b"scratch" in lib.rpa_b200_status_string(st)
+    assert b"size limit" in lib.rpa_b200_status_string(st)
