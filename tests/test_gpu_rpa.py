@@ -110,6 +110,43 @@ def test_multi_tile_split_against_fp64(handle):
     assert rel_err(psp, p64) < 3e-5
 
 
+EDGE_SIZES = [(1, 1, 1, 1), (7, 1, 3, 2), (64, 2, 32, 1), (65, 3, 21, 3), (129, 2, 64, 5), (257, 4, 65, 17)]
+
+
+def edge_system(nq, no, nv, nf):
+    s = O.make_system(nq, no, nv, 500 + nq, decay=max(nq / 4.0, 1.0), lam0=0.7)
+    x, w = O.casimir_polder(nf, 0.7)
+    return s, x, w
+
+
+@pytest.mark.parametrize("nq,no,nv,nf", EDGE_SIZES)
+def test_minimum_and_block_boundary_sizes(handle, nq, no, nv, nf):
+    # one Cholesky vector, one occupied and one virtual orbital, one frequency; orders at and
+    # just past the 64-column Cholesky block, the 128-row SYRK tile and the 256-column outer
+    # block; 17 frequencies (two split-BF16 groups)
+    s, x, w = edge_system(nq, no, nv, nf)
+    ref, ref_eu = O.ec_rpa(s.R, s.eps_o, s.eps_v, x, w)
+    e64, eu64 = handle.ec_rpa(s.R, s.eps_o, s.eps_v, x, w, prec="fp64")
+    esp, _ = handle.ec_rpa(s.R, s.eps_o, s.eps_v, x, w, prec="split")
+    assert abs(e64 - ref) < 1e-10
+    assert np.max(np.abs(eu64 - ref_eu)) < 1e-10
+    assert abs(esp - ref) < 1e-6
+    pi = handle.pi_u(s.R, s.eps_o, s.eps_v, x[:2], prec="split")
+    assert rel_err(pi, O.pi_matrices(s.R, s.eps_o, s.eps_v, x[:2])) < 3e-5
+
+
+def test_batched_minimum_and_block_boundary_sizes(handle):
+    sys_ = []
+    for nq, no, nv, nf in EDGE_SIZES:
+        if nf <= 16:
+            s, x, w = edge_system(nq, no, nv, nf)
+            sys_.append((s.R, s.eps_o, s.eps_v, x, w))
+    for prec, tol in (("fp64", 1e-10), ("split", 1e-6)):
+        ec, _ = handle.ec_batched(sys_, prec=prec)
+        for (R, eo, ev, x, w), e in zip(sys_, ec):
+            assert abs(e - O.ec_rpa(R, eo, ev, x, w)[0]) < tol
+
+
 # ----------------------------------------------------------------------------- errors
 
 def test_nonfinite_input_is_reported(handle, pkg):
