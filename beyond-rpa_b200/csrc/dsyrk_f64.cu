@@ -171,18 +171,39 @@ __device__ __forceinline__ void dsyrk_tile(const DsyrkArgs& a, const double* A, 
   }
   cp_async_wait<0>();
 
+  // Subtract mode reads the C fragment of two row groups at a time before storing any of it:
+  // a load-subtract-store per element would wait out one memory round trip per element, since
+  // the compiler cannot move a load of C above a store to C.
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int row = m0 + wm * 32 + i * 8 + (lane >> 2);
+  for (int i0 = 0; i0 < 4; i0 += 2) {
+    double cv[2][4][2];
+    if (!kScaled) {
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+      for (int i = 0; i < 2; ++i) {
+        const int row = m0 + wm * 32 + (i0 + i) * 8 + (lane >> 2);
 #pragma unroll
-      for (int v = 0; v < 2; ++v) {
-        const int col = n0 + wn * 32 + j * 8 + 2 * (lane & 3) + v;
-        if (row < a.n && col < ncols && row >= col) {
-          double* p = C + (int64_t)row + a.ldc * (int64_t)col;
-          if (kScaled) *p = acc[i][j][v];
-          else *p -= acc[i][j][v];
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+          for (int v = 0; v < 2; ++v) {
+            const int col = n0 + wn * 32 + j * 8 + 2 * (lane & 3) + v;
+            cv[i][j][v] =
+                (row < a.n && col < ncols && row >= col) ? C[(int64_t)row + a.ldc * (int64_t)col] : 0.0;
+          }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int row = m0 + wm * 32 + (i0 + i) * 8 + (lane >> 2);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+          const int col = n0 + wn * 32 + j * 8 + 2 * (lane & 3) + v;
+          if (row < a.n && col < ncols && row >= col) {
+            double* p = C + (int64_t)row + a.ldc * (int64_t)col;
+            if (kScaled) *p = acc[i0 + i][j][v];
+            else *p = cv[i][j][v] - acc[i0 + i][j][v];
+          }
         }
       }
     }

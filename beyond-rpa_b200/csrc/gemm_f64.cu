@@ -160,23 +160,43 @@ __device__ __forceinline__ void gemm_tile(const GemmF64Args& g, const int m0, co
   }
   cp_async_wait<0>();
 
+  // With beta != 0 the C fragment of a row group is read before any of it is stored: a
+  // load-update-store per element would wait out one memory round trip per element, since the
+  // compiler cannot move a load of C above a store to C.
+  const bool keep = !split && g.beta != 0.0;
+  constexpr int kEpiRows = 1;  // row groups per read-then-write pass (2 spills in the grouped kernel)
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const int m = m0 + wm * 32 + i * 8 + (lane >> 2);
-    if (m >= g.M) continue;
-    const double rsm = g.rowscale ? g.rowscale[m] : 1.0;
+  for (int i0 = 0; i0 < 4; i0 += kEpiRows) {
+    double cv[kEpiRows][4][2];
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int i = 0; i < kEpiRows; ++i) {
+      const int m = m0 + wm * 32 + (i0 + i) * 8 + (lane >> 2);
 #pragma unroll
-      for (int v = 0; v < 2; ++v) {
-        const int n = n0 + wn * 32 + j * 8 + 2 * (lane & 3) + v;
-        if (n >= g.N) continue;
-        double* p = C + (int64_t)m + ldc * (int64_t)n;
-        if (split) {
-          *p = acc[i][j][v];
-        } else {
-          const double val = g.alpha * rsm * acc[i][j][v];
-          *p = (g.beta == 0.0) ? val : val + g.beta * *p;
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+          const int n = n0 + wn * 32 + j * 8 + 2 * (lane & 3) + v;
+          cv[i][j][v] = (keep && m < g.M && n < g.N) ? C[(int64_t)m + ldc * (int64_t)n] : 0.0;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < kEpiRows; ++i) {
+      const int m = m0 + wm * 32 + (i0 + i) * 8 + (lane >> 2);
+      if (m >= g.M) continue;
+      const double rsm = g.rowscale ? g.rowscale[m] : 1.0;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+          const int n = n0 + wn * 32 + j * 8 + 2 * (lane & 3) + v;
+          if (n >= g.N) continue;
+          double* p = C + (int64_t)m + ldc * (int64_t)n;
+          if (split) {
+            *p = acc[i0 + i][j][v];
+          } else {
+            const double val = g.alpha * rsm * acc[i0 + i][j][v];
+            *p = keep ? val + g.beta * cv[i][j][v] : val;
+          }
         }
       }
     }
