@@ -968,7 +968,7 @@ int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) try
       cudaStreamCreateWithFlags(&h->aux[1], cudaStreamNonBlocking) != cudaSuccess ||
       cudaStreamCreateWithFlags(&h->aux[2], cudaStreamNonBlocking) != cudaSuccess ||
       cudaMalloc(&h->err_dev, sizeof(int)) != cudaSuccess || cudaMalloc(&h->count_dev, sizeof(int)) != cudaSuccess) {
-    delete h;
+    rpa_b200_destroy(h);  // releases whatever was created (it skips null members)
     return RPA_ERR_CUDA;
   }
   h->stream = h->own_stream;

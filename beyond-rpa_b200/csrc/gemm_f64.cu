@@ -13,6 +13,8 @@
 // operand's shared-memory tile follows its unit-stride index: [k][m] with row
 // pitch 72 when m (or n) is contiguous, [m][k] with pitch 18 when k is; both
 // pitches make the m8n8k4 fragment loads hit every bank pair exactly twice.
+#include <atomic>
+
 #include "kernels.h"
 
 namespace rpa {
@@ -242,15 +244,17 @@ __global__ void splitk_reduce_kernel(const GemmF64Args g) {
 
 template <bool kAM, bool kBN, bool kVec>
 cudaError_t launch_variant(const GemmF64Args& g, cudaStream_t stream) {
-  static uint64_t attr_set = 0;  // per-variant bit per device: dynamic shared memory opted in
+  // per-variant bit per device: dynamic shared memory opted in (atomic: handles on different
+  // devices may launch from different host threads)
+  static std::atomic<uint64_t> attr_set{0};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (dev >= 64 || !(attr_set >> dev & 1)) {
+  if (dev >= 64 || !(attr_set.load(std::memory_order_relaxed) >> dev & 1)) {
     e = cudaFuncSetAttribute(gemm_f64_kernel<kAM, kBN, kVec>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kSmem);
     if (e != cudaSuccess) return e;
-    if (dev < 64) attr_set |= 1ull << dev;
+    if (dev < 64) attr_set.fetch_or(1ull << dev, std::memory_order_relaxed);
   }
   const bool split = g.splitk > 1;
   dim3 grid((unsigned)((g.N + BM - 1) / BM), (unsigned)((g.M + BM - 1) / BM),
@@ -266,13 +270,13 @@ cudaError_t launch_variant(const GemmF64Args& g, cudaStream_t stream) {
 
 template <bool kAM, bool kBN>
 cudaError_t set_smem_attr() {
-  static uint64_t done = 0;
+  static std::atomic<uint64_t> done{0};
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (dev < 64 && (done >> dev & 1)) return cudaSuccess;
+  if (dev < 64 && (done.load(std::memory_order_relaxed) >> dev & 1)) return cudaSuccess;
   e = cudaFuncSetAttribute(gemm_f64_grouped_kernel<kAM, kBN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmem);
-  if (e == cudaSuccess && dev < 64) done |= 1ull << dev;
+  if (e == cudaSuccess && dev < 64) done.fetch_or(1ull << dev, std::memory_order_relaxed);
   return e;
 }
 
