@@ -22,6 +22,35 @@ def test_status_strings(pkg):
     assert lib.rpa_b200_status_string(999) == b"unknown status"
 
 
+def test_ctypes_signatures_match_the_header(pkg):
+    # every binding's argtypes agree with the prototype in include/rpa_b200.h: same count, and
+    # int64_t -> c_int64, uint64_t -> c_uint64, double -> c_double, int -> c_int, pointer -> pointer
+    import re
+    text = re.sub(r"/\*.*?\*/", " ", pkg.HEADER.read_text(), flags=re.S)
+    lib = pkg.load_library()
+    checked = 0
+    for m in re.finditer(r"^\s*(?:int64_t|int|const char\*)\s+(rpa_b200_\w+)\s*\(([^;]*?)\)\s*;", text, re.M):
+        name, params = m.group(1), " ".join(m.group(2).split())
+        params = [] if params in ("", "void") else [p.strip() for p in params.split(",")]
+        argtypes = getattr(lib, name).argtypes
+        assert argtypes is not None and len(argtypes) == len(params), name
+        for p, t in zip(params, argtypes):
+            if "*" in p:
+                assert t is ctypes.c_void_p or issubclass(t, (ctypes._Pointer, ctypes.c_char_p)), (name, p, t)
+            elif p.startswith("uint64_t"):
+                assert t is ctypes.c_uint64, (name, p, t)
+            elif p.startswith("int64_t"):
+                assert t is ctypes.c_int64, (name, p, t)
+            elif p.startswith("double"):
+                assert t is ctypes.c_double, (name, p, t)
+            elif p.startswith("int "):
+                assert t is ctypes.c_int, (name, p, t)
+            else:
+                raise AssertionError(f"{name}: unhandled parameter type {p!r}")
+        checked += 1
+    assert checked == len(pkg.declared_functions())
+
+
 def test_status_codes_match_the_header(pkg):
     import re
     text = pkg.HEADER.read_text()
