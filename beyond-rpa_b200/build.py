@@ -38,6 +38,7 @@ def needs_build() -> bool:
         return True
     t = LIB.stat().st_mtime
     deps = sources() + list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    deps.append(CSRC / "librpa_b200.map")
     deps.append(Path(__file__))
     return any(p.stat().st_mtime > t for p in deps)
 
@@ -69,7 +70,8 @@ def build(force: bool = False, verbose_ptxas: bool = False, jobs: int | None = N
     if failed:
         raise RuntimeError("nvcc compilation failed")
     tmp = LIB.with_suffix(".so.tmp")
-    link = [nvcc(), *ARCH, "-shared", "-Xlinker", "--no-undefined", "-o", str(tmp), *map(str, objs)]
+    link = [nvcc(), *ARCH, "-shared", "-Xlinker", "--no-undefined", "-Xlinker", f"--version-script={CSRC / 'librpa_b200.map'}",
+            "-o", str(tmp), *map(str, objs)]
     subprocess.run(link, check=True)
     tmp.replace(LIB)
     return LIB

@@ -22,6 +22,19 @@ def test_status_strings(pkg):
     assert lib.rpa_b200_status_string(999) == b"unknown status"
 
 
+def test_library_exports_nothing_but_the_declared_api(pkg):
+    # hidden default visibility: the only exported functions are the rpa_b200_* entry points
+    import shutil
+    import subprocess
+    nm = shutil.which("nm")
+    if nm is None:
+        pytest.skip("nm not available")
+    out = subprocess.run([nm, "-D", "--defined-only", str(pkg.LIB_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    funcs = {line.split()[-1] for line in out.splitlines() if len(line.split()) == 3 and line.split()[1] in "TtWi"}
+    assert funcs == set(pkg.declared_functions()), sorted(funcs ^ set(pkg.declared_functions()))
+
+
 def test_ctypes_signatures_match_the_header(pkg):
     # every binding's argtypes agree with the prototype in include/rpa_b200.h: same count, and
     # int64_t -> c_int64, uint64_t -> c_uint64, double -> c_double, int -> c_int, pointer -> pointer
