@@ -1,6 +1,6 @@
 """FP64 CPU oracle for the Cholesky-vector RPA hot path.
 
-TEST INFRASTRUCTURE ONLY.  This module is the checker: it is imported by
+TEST INFRASTRUCTURE ONLY.  This module checks the library: it is imported by
 ``tests/``, by ``__graft_entry__.smoke()`` and by the ``cpu_baseline`` /
 ``--impl reference`` legs of ``bench.py``, and by nothing else.  The product
 path (``beyond-rpa_b200/``) never imports, links or executes it.

@@ -71,7 +71,7 @@ def test_batched_repeated_call_uses_cached_graph(handle):
 
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-11), ("split", 1e-7)])
 def test_mbe_driver_dimer_of_noninteracting_monomers(handle, prec, tol):
-    # the driver: shared grid over the dimer and its monomers, batched energies, Eint;
+    # the MBE driver (Handle.mbe_energies): shared grid over the dimer and its monomers, batched energies, Eint;
     # two non-interacting monomers (block-diagonal R) must give Eint ~ 0 on the shared grid
     a = O.make_system(110, 4, 26, 301, decay=30.0, lam0=0.6)
     b = O.make_system(90, 3, 28, 302, decay=25.0, lam0=0.6)
