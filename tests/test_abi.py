@@ -64,6 +64,23 @@ def test_ctypes_signatures_match_the_header(pkg):
     assert checked == len(pkg.declared_functions())
 
 
+def test_fortran_interfaces_cover_the_header(pkg):
+    # every C entry point has a bind(C) interface in the Fortran module of INTEGRATION.md, with
+    # as many dummy arguments as the prototype has parameters
+    import re
+    header = re.sub(r"/\*.*?\*/", " ", pkg.HEADER.read_text(), flags=re.S)
+    protos = {m.group(1): [p for p in " ".join(m.group(2).split()).split(",") if p.strip() not in ("", "void")]
+              for m in re.finditer(r"^\s*(?:int64_t|int|const char\*)\s+(rpa_b200_\w+)\s*\(([^;]*?)\)\s*;",
+                                   header, re.M)}
+    doc = (pkg.HEADER.parents[1] / "INTEGRATION.md").read_text()
+    doc = re.sub(r"&\s*\n\s*", " ", doc)  # join Fortran continuation lines
+    binds = {m.group(3): [a for a in m.group(2).split(",") if a.strip()]
+             for m in re.finditer(r"function\s+(\w+)\s*\(([^)]*)\)\s*bind\(C,\s*name=\"(\w+)\"\)", doc)}
+    assert set(protos) <= set(binds), sorted(set(protos) - set(binds))
+    for name, params in protos.items():
+        assert len(binds[name]) == len(params), (name, binds[name], params)
+
+
 def test_status_codes_match_the_header(pkg):
     import re
     text = pkg.HEADER.read_text()
