@@ -81,6 +81,24 @@ def test_fortran_interfaces_cover_the_header(pkg):
         assert len(binds[name]) == len(params), (name, binds[name], params)
 
 
+def test_plain_c_caller(pkg, tmp_path):
+    # the header is valid C99 and the library links and runs from a C program
+    import shutil
+    import subprocess
+    import torch
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    libdir = pkg.LIB_PATH.parent
+    exe = tmp_path / "c_abi_harness"
+    src = pkg.HEADER.parents[1] / "tests" / "c_abi_harness.c"
+    subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", f"-I{pkg.HEADER.parent}", str(src),
+                    f"-L{libdir}", "-lrpa_b200", f"-Wl,-rpath,{libdir}", "-lm", "-o", str(exe)], check=True)
+    args = [str(exe)] + ([] if torch.cuda.is_available() else ["nogpu"])
+    out = subprocess.run(args, capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0 and out.stdout.strip() == "ok", out.stderr
+
+
 def test_status_codes_match_the_header(pkg):
     import re
     text = pkg.HEADER.read_text()
