@@ -108,10 +108,13 @@ int histogram(const double* e, int64_t nocc, int64_t nvirt, double core_thresh, 
       const double d = e[a] - e[i];
       if (!(d <= thresh)) continue;
       const double x = (d - (dmin + width / 2.0)) / width;
-      int64_t k = 1 + (int64_t)(x >= 0 ? std::floor(x + 0.5) : -std::floor(-x + 0.5));  // Fortran nint
-      if (k < 1) k = 1;
-      if (k > nbins) k = nbins;
-      ++cnt[k - 1];
+      // 1 + nint(x) (Fortran nint), clamped to [1, nbins] before the conversion to an integer: with
+      // a single distinct difference the width is 0 and x is 0/0, which lands in bin 1 (gfortran's
+      // nint of a NaN is the most negative integer, which the reference's max(1, k) clamps to 1)
+      double kf = 1.0 + (x >= 0 ? std::floor(x + 0.5) : -std::floor(-x + 0.5));
+      if (!(kf >= 1.0)) kf = 1.0;
+      if (kf > nbins) kf = nbins;
+      ++cnt[(int)kf - 1];
       ++total;
     }
   for (int k = 0; k < nbins; ++k) h.wt[k] = std::fabs((double)cnt[k] / (double)total);

@@ -128,12 +128,16 @@ def dai_histogram(orb_energies, nocc, nvirt, core_thresh=CORE_ORB_THRESH,
     vals = dmin + np.arange(nbins) * width
     d = (e[a0:a1 + 1][None, :] - e[i0:i1 + 1][:, None]).ravel()
     d = d[d <= dai_max_thresh]
-    # nint() is round-half-away-from-zero in Fortran
-    x = (d - (dmin + width / 2.0)) / width
-    k = 1 + np.where(x >= 0, np.floor(x + 0.5), -np.floor(-x + 0.5)).astype(np.int64)
-    k = np.clip(k, 1, nbins)
+    # nint() is round-half-away-from-zero in Fortran; the bin index is clamped to [1, nbins] as
+    # the reference does, in floating point (a zero width, i.e. one distinct difference, gives
+    # 0/0: bin 1, where gfortran's nint of a NaN clamps to)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        x = (d - (dmin + width / 2.0)) / width
+    kf = 1.0 + np.where(x >= 0, np.floor(x + 0.5), -np.floor(-x + 0.5))
+    k = np.where(np.isnan(kf) | (kf < 1.0), 1.0, np.minimum(kf, nbins)).astype(np.int64)
     count = np.bincount(k - 1, minlength=nbins).astype(np.float64)
-    return vals, np.abs(count / count.sum())
+    with np.errstate(invalid="ignore"):  # no difference under the cap: 0/0, as in the reference
+        return vals, np.abs(count / count.sum())
 
 
 # --------------------------------------------------------------------------
@@ -223,6 +227,8 @@ def opt_quad_scaling(n, dai_values, dai_weights, min_alpha=0.1, max_alpha=15.0, 
     rel = np.zeros((nscan, dv.shape[1]))
     for s in range(dv.shape[1]):
         m = dw[:, s] > 0.0
+        if not m.any():  # no bin with weight > 0 (e.g. every difference above the cap): no error
+            continue
         d = dv[m, s]
         exact = PI / (2.0 * d)
         for c0 in range(0, nscan, 1000):

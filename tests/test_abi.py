@@ -161,6 +161,37 @@ def test_freq_grid_matches_oracle(pkg, oracle):
     assert len(x) == len(xr) and np.allclose(x, xr, rtol=1e-12)
 
 
+@pytest.mark.parametrize("seed,no,nv,occ,virt", [
+    (11, 1, 1, (-0.6, -0.5), (0.2, 0.3)),      # one excitation: every histogram bin but one empty
+    (12, 3, 40, (-0.4, -0.35), (0.01, 0.05)),  # small gap, narrow spread
+    (13, 30, 400, (-2.5, -0.2), (0.05, 60.0)),  # wide spread of excitation energies
+    (14, 7, 7, (-1.0, -0.9), (2.0, 2.1)),      # large gap, near-degenerate levels
+])
+def test_freq_grid_matches_oracle_on_varied_spectra(pkg, oracle, seed, no, nv, occ, virt):
+    # Where the best grid of n points still has a quadrature error above rounding, the optimum
+    # scale is unique and the library's grid equals the oracle's.  Where n points integrate every
+    # 1/(D^2 + u^2) to rounding level (many points, narrow spectra), the error is flat in the
+    # scale and its argmin is decided by rounding noise, which differs between implementations
+    # (the reference's included): there the library's grid must reach rounding level too.
+    import math
+    s = oracle.make_system(4, no, nv, seed, occ_range=occ, virt_range=virt)
+    e = np.concatenate([s.eps_o, s.eps_v])
+    d = (s.eps_v[:, None] - s.eps_o[None, :]).ravel()
+
+    def quad_error(x, w):
+        exact = math.pi / (2.0 * d)
+        return float(np.max(np.abs(np.sum(w[None, :] / (d[:, None] ** 2 + x[None, :] ** 2), axis=1) - exact) / exact))
+
+    for nfixed in (8, 20, 64, None):
+        x, w = pkg.freq_grid(e, no, nv, nfixed=nfixed or 0)
+        xr, wr = oracle.grid_for(s, nfixed)
+        assert len(x) == len(xr) and (nfixed is None or len(x) == nfixed)
+        if quad_error(xr, wr) > 1e-12:
+            assert np.allclose(x, xr, rtol=1e-12) and np.allclose(w, wr, rtol=1e-12)
+        else:
+            assert quad_error(x, w) < 1e-13
+
+
 def test_freq_grid_rejects_bad_gap(pkg):
     e = np.array([-1.0, 0.5, 0.2, 1.0])  # HOMO above LUMO
     with pytest.raises(pkg.RPAError):
@@ -238,6 +269,23 @@ def test_freq_grid_mbe_of_one_set_is_the_single_grid(pkg):
     x1, w1 = pkg.freq_grid(e, no, nv, nfixed=10)
     x2, w2 = pkg.freq_grid_mbe([(e, no, nv)], nfixed=10)
     assert np.array_equal(x1, x2) and np.array_equal(w1, w2)
+
+
+def test_freq_grid_mbe_set_above_the_cap_takes_no_part(pkg, oracle):
+    # a subsystem whose smallest excitation energy lies above the complex's largest one has no
+    # difference under the cap (its histogram weights are 0/0, as in the reference) and leaves
+    # the capped grid unchanged; without the cap it counts
+    sets = _cluster_sets()
+    cap = oracle.dai_max_thresh(*sets[0])  # the complex's largest active excitation energy
+    far = (np.array([-0.5, -0.4, cap + 0.1, cap + 0.3]), 2, 2)
+    x1, w1 = pkg.freq_grid_mbe(sets, nfixed=10)
+    x2, w2 = pkg.freq_grid_mbe(sets + [far], nfixed=10)
+    assert np.array_equal(x1, x2) and np.array_equal(w1, w2)
+    xr, wr = oracle.grid_for_cluster(sets + [far], limit_dai=True, n=10)
+    assert np.allclose(x2, xr, rtol=1e-12) and np.allclose(w2, wr, rtol=1e-12)
+    x3, _ = pkg.freq_grid_mbe(sets + [far], limit_dai=False, nfixed=10)
+    xr3, _ = oracle.grid_for_cluster(sets + [far], limit_dai=False, n=10)
+    assert np.allclose(x3, xr3, rtol=1e-12)
 
 
 def test_freq_grid_mbe_skips_all_core_sets_and_rejects_bad_gaps(pkg):
