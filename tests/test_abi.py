@@ -192,6 +192,19 @@ def test_freq_grid_matches_oracle_on_varied_spectra(pkg, oracle, seed, no, nv, o
             assert quad_error(x, w) < 1e-13
 
 
+def test_freq_grid_unreachable_target_is_reported(pkg, oracle):
+    # no grid of up to 64 points meets the targets: the reference stops with "Quadrature did not
+    # converge to specified accuracy" (rpa_OptimizeFreqQuad); the library returns a status
+    s = oracle.make_system(4, 5, 30, 3, occ_range=(-1.0, -0.3), virt_range=(0.05, 3.0))
+    e = np.concatenate([s.eps_o, s.eps_v])
+    with pytest.raises(pkg.RPAError) as err:
+        pkg.freq_grid(e, 5, 30, target_error=1e-30, target_rel_error=1e-30)
+    assert err.value.status == pkg.RPA_ERR_NOT_CONVERGED
+    vals, wts = oracle.dai_histogram(e, 5, 30)
+    with pytest.raises(RuntimeError):
+        oracle.optimize_freq_quad(vals, wts, target_error=1e-30, target_rel_error=1e-30)
+
+
 def test_freq_grid_rejects_bad_gap(pkg):
     e = np.array([-1.0, 0.5, 0.2, 1.0])  # HOMO above LUMO
     with pytest.raises(pkg.RPAError):
