@@ -17,6 +17,17 @@
  * MSG_ERROR); this ABI returns a non-zero status instead, and the Fortran
  * shim maps it back to msg + error stop.
  * A handle must not be shared by two host threads at the same time.
+ * Limits (checked before any GPU work):
+ *   - 1 <= NQ <= 2^20 and 1 <= NFreqs <= 64 (RPA_ERR_INVALID_ARG otherwise);
+ *   - NOcc * NVirt <= 2^31 - 1 (RPA_ERR_TOO_LARGE);
+ *   - at most 16 frequencies per instance in rpa_b200_ec_batched, at most 2^24
+ *     instances per call (RPA_ERR_INVALID_ARG);
+ *   - N <= 46340 in rpa_b200_syevd and NQ <= 46340 in rpa_b200_piu_basis (an
+ *     N x N FP64 matrix indexed in 32-bit); GEMM dimensions of the T2, exchange,
+ *     THC and JCTC paths <= 2^31 - 1 (RPA_ERR_TOO_LARGE);
+ *   - rpa_b200_ec_from_pi_noalloc: the fixed scratch described at its
+ *     declaration (RPA_ERR_TOO_LARGE);
+ *   - device memory: RPA_ERR_OOM when a workspace cannot be allocated.
  */
 #ifndef RPA_B200_H
 #define RPA_B200_H
