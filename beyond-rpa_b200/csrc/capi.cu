@@ -1463,7 +1463,7 @@ static int sosex_split(rpa_b200_handle* h, const double* R, int64_t ldR, int NQ,
   a.nqt = (NQ + 127) / 128;
   a.nmt = (NT + 127) / 128;
   const int64_t units = rpa::sosex_tc_units(NQ, no, NT);
-  if (units > (int64_t)INT32_MAX) return fail(h, RPA_ERR_INVALID_ARG, "exchange contraction too large (%lld units)",
+  if (units > (int64_t)INT32_MAX) return fail(h, RPA_ERR_TOO_LARGE, "exchange contraction too large (%lld units)",
                                               (long long)units);
   a.nunits = (int)units;
   a.same = U2 ? 0 : 1;
