@@ -8,9 +8,12 @@
  *   - Cholesky vectors R(Q, ai) with ai = a + NVirt*(i-1) (a fastest), i.e.
  *     the Rkai(NCholesky, NVirt*NOcc) arrays of src/rpa/rpa_THC.f90:362 and
  *     src/rpa/rpa_core_MO.f90:395;
- *   - array arguments may point to host memory (pageable or pinned) or to
- *     device memory of the handle's GPU; the library detects which
- *     (cudaPointerGetAttributes) and stages host data itself;
+ *   - array arguments may point to host memory (pageable or pinned), to
+ *     managed memory, or to device memory of the handle's GPU; the library
+ *     detects which (cudaPointerGetAttributes) and stages host data itself.
+ *     Device memory of another GPU is not supported: kernels read device
+ *     arguments in place, so copy such data to the handle's GPU (or to the
+ *     host) first;
  *   - scalar outputs (energies) are host pointers;
  *   - every call is synchronous on return and returns an rpa_status.
  * Errors: the Fortran reference stops with `error stop` after msg(...,
