@@ -296,6 +296,9 @@ def run_ours(args):
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": sustained, "unit": "TFLOP/s",
                      "frac": achieved / sustained, "frac_of_burst_peak": achieved / burst,
                      "traffic": profile_traffic("syrk_split_bf16", WORKLOAD),
+                     "traffic_source": f"profiles/syrk_split_bf16_{WORKLOAD}.md: dram__bytes_read.sum + "
+                                       "dram__bytes_write.sum per launch from a committed ncu capture "
+                                       "(not measured by this run)",
                      "kernel": "syrk_split_bf16_kernel",
                      "note": f"peak = bf16_tflops_sustained ({src}); achieved = 3 bf16 SYRK products "
                              f"3*NQ^2*nov*K / contraction time"},

@@ -115,6 +115,9 @@ def load_library(path: str | os.PathLike | None = None):
     lib.rpa_b200_set_logdet_plan.argtypes = [_vp, _i64, _i64, _i64]
     lib.rpa_b200_get_logdet_plan.argtypes = [_vp, _i64, _vp, _vp]
     lib.rpa_b200_set_autotune.argtypes = [_vp, _i64]
+    lib.rpa_b200_set_workspace_limit.argtypes = [_vp, _i64]
+    lib.rpa_b200_workspace_bytes.argtypes = [_vp, _vp, _vp]
+    lib.rpa_b200_selftest_wait_timeout.argtypes = [_vp, _dbl]
     if path is None:
         _lib = lib
     return lib
@@ -296,6 +299,20 @@ class Handle:
     def set_autotune(self, on=True):
         """Tune unseen order buckets inside ec_batched (on by default)."""
         self._check(self.lib.rpa_b200_set_autotune(self._h, 1 if on else 0))
+
+    def set_workspace_limit(self, nbytes=0):
+        """Cap the handle's device workspace at nbytes (0: no cap); over-cap calls raise RPA_ERR_OOM."""
+        self._check(self.lib.rpa_b200_set_workspace_limit(self._h, int(nbytes)))
+
+    def workspace_bytes(self):
+        """(bytes the workspace holds now, cap or 0)."""
+        used, limit = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.rpa_b200_workspace_bytes(self._h, ctypes.byref(used), ctypes.byref(limit)))
+        return used.value, limit.value
+
+    def selftest_wait_timeout(self, limit_ms=20.0):
+        """Run the bounded-wait self-test; returns its status (RPA_ERR_TIMEOUT when detection works)."""
+        return int(self.lib.rpa_b200_selftest_wait_timeout(self._h, float(limit_ms)))
 
     # ------------------------------------------------------------------ Pi(u)
     def pi_u(self, R, eps_o, eps_v, freqs, alpha=4.0, prec="split", out=None):

@@ -40,4 +40,18 @@ inline int status_of_exception(std::string* detail) noexcept {
   return status;
 }
 
+// Where an array argument lives, from the memory type and device that cudaPointerGetAttributes
+// reports for it.  `type` is a cudaMemoryType value (0 unregistered host memory, 1 registered or
+// pinned host memory, 2 device memory, 3 managed memory); `ptr_device` is the device of device
+// memory.  Device memory of a GPU other than the handle's is refused before any launch: the
+// kernels read device arguments in place, and a kernel of one GPU given another GPU's address
+// would fault or read the wrong memory.  Managed memory is reachable from every GPU.
+enum class ArgMemory { Host, HandleDevice, OtherDevice };
+
+inline ArgMemory classify_arg_memory(int type, int ptr_device, int handle_device) noexcept {
+  if (type == 2) return ptr_device == handle_device ? ArgMemory::HandleDevice : ArgMemory::OtherDevice;
+  if (type == 3) return ArgMemory::HandleDevice;
+  return ArgMemory::Host;
+}
+
 }  // namespace rpa

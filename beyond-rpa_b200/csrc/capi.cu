@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <initializer_list>
 #include <map>
 #include <string>
 #include <vector>
@@ -30,6 +31,35 @@ struct DevBuf {
   size_t bytes = 0;
 };
 
+// Device-memory accounting of one handle: bytes its workspace holds, and the cap a caller may set
+// (rpa_b200_set_workspace_limit; 0 = none).  Every workspace allocation of a call goes through
+// dev_alloc / dev_free below, which charge the handle whose call is running on this thread.
+struct WorkspaceAccount {
+  size_t used = 0;
+  size_t limit = 0;
+};
+namespace {
+thread_local WorkspaceAccount* g_account = nullptr;
+
+cudaError_t dev_alloc(void** p, size_t bytes) {
+  WorkspaceAccount* a = g_account;
+  if (a && a->limit && (bytes > a->limit || a->used > a->limit - bytes)) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;  // over the caller's cap: reported like a failed cudaMalloc
+  }
+  const cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaSuccess && a) a->used += bytes;
+  return e;
+}
+
+void dev_free(void* p, size_t bytes) {
+  if (!p) return;
+  cudaFree(p);
+  WorkspaceAccount* a = g_account;
+  if (a) a->used = a->used > bytes ? a->used - bytes : 0;
+}
+}  // namespace
+
 struct rpa_b200_handle {
   int device = 0;
   int num_sms = 0;
@@ -37,6 +67,7 @@ struct rpa_b200_handle {
   cudaStream_t own_stream = nullptr;  // the handle's own stream
   cudaStream_t copy_stream = nullptr;  // host-to-device staging overlapped with compute
   std::string last_error;
+  WorkspaceAccount account;  // device bytes of the workspace below and the caller's cap
   DevBuf R, D, eps, Xhi, Xlo, diag_part, diag, Pi, Ldiag, ddbuf;
   // direct-ring T2 / exchange workspace
   DevBuf tZ, tOm, tIOm, tP, tS, tV, tT, tTIT, tVt, tW, tU, tRU, tSmall, tPerm;
@@ -128,18 +159,18 @@ int fail(rpa_b200_handle* h, int status, const char* fmt, ...) {
 cudaError_t ensure(DevBuf& b, size_t bytes) {
   if (b.bytes >= bytes && b.p) return cudaSuccess;
   if (b.p) {
-    cudaFree(b.p);
+    dev_free(b.p, b.bytes);
     b.p = nullptr;
     b.bytes = 0;
   }
   if (bytes == 0) bytes = 256;
-  cudaError_t e = cudaMalloc(&b.p, bytes);
+  cudaError_t e = dev_alloc(&b.p, bytes);
   if (e == cudaSuccess) b.bytes = bytes;
   return e;
 }
 
 void release(DevBuf& b) {
-  if (b.p) cudaFree(b.p);
+  dev_free(b.p, b.bytes);
   b.p = nullptr;
   b.bytes = 0;
 }
@@ -160,6 +191,27 @@ bool is_device_ptr(const void* p) {
     return false;
   }
   return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+// Refuse array arguments that are device memory of a GPU other than the handle's (see
+// rpa::classify_arg_memory).  Null pointers and pointers the runtime does not know are skipped
+// here (the argument checks of each entry point handle them).
+int check_arrays(rpa_b200_handle* h, std::initializer_list<const void*> arrays) {
+  int index = 0;
+  for (const void* p : arrays) {
+    ++index;
+    if (!p) continue;
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (rpa::classify_arg_memory((int)attr.type, attr.device, h->device) == rpa::ArgMemory::OtherDevice)
+      return fail(h, RPA_ERR_INVALID_ARG,
+                  "array argument %d is device memory of GPU %d; this handle runs on GPU %d (copy it first)", index,
+                  attr.device, h->device);
+  }
+  return RPA_OK;
 }
 
 // Read a small array (host or device) into a host vector.
@@ -568,13 +620,13 @@ int tune_single(rpa_b200_handle* h, int n, int nmat) {
   if (!h->autotune || n < 512 || h->logdet_plans.count(plan_bucket(n))) return RPA_OK;
   for (int m = nmat; m >= 1; m = m > 4 ? 4 : 0) {
     void* tmp = nullptr;
-    if (cudaMalloc(&tmp, (size_t)m * n * n * 8) != cudaSuccess) {
+    if (dev_alloc(&tmp, (size_t)m * n * n * 8) != cudaSuccess) {
       cudaGetLastError();
       continue;
     }
     int s = tune_uniform(h, n, m, static_cast<double*>(tmp), nullptr);
     cudaStreamSynchronize(h->stream);
-    cudaFree(tmp);
+    dev_free(tmp, (size_t)m * n * n * 8);
     if (s == RPA_OK) RPA_CUDA(h, cudaMemsetAsync(h->err_dev, 0, sizeof(int), h->stream));
     return s;
   }
@@ -901,6 +953,7 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
 int begin_call(rpa_b200_handle* h) {
   if (!h) return RPA_ERR_INVALID_ARG;
   h->last_error.clear();
+  g_account = &h->account;
   h->pool_used = 0;
   h->split_ev.clear();
   h->tc_ev.clear();
@@ -1009,6 +1062,7 @@ int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) try
 
 int rpa_b200_destroy(rpa_b200_handle* h) try {
   if (!h) return RPA_OK;
+  g_account = &h->account;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->own_stream) cudaStreamSynchronize(h->own_stream);
@@ -1047,6 +1101,7 @@ int rpa_b200_destroy(rpa_b200_handle* h) try {
   }
   if (h->own_stream) cudaStreamDestroy(h->own_stream);
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  g_account = nullptr;
   delete h;
   return RPA_OK;
 } catch (...) {
@@ -1129,6 +1184,34 @@ int rpa_b200_get_logdet_plan(const rpa_b200_handle* h, int64_t NQ, int64_t* Nb2,
   return rpa::status_of_exception(nullptr);
 }
 
+int rpa_b200_set_workspace_limit(rpa_b200_handle* h, int64_t Bytes) try {
+  if (!h || Bytes < 0) return RPA_ERR_INVALID_ARG;
+  h->account.limit = (size_t)Bytes;
+  return RPA_OK;
+} catch (...) {
+  return exception_status(h);
+}
+
+int rpa_b200_workspace_bytes(const rpa_b200_handle* h, int64_t* Used, int64_t* Limit) try {
+  if (!h) return RPA_ERR_INVALID_ARG;
+  if (Used) *Used = (int64_t)h->account.used;
+  if (Limit) *Limit = (int64_t)h->account.limit;
+  return RPA_OK;
+} catch (...) {
+  return rpa::status_of_exception(nullptr);
+}
+
+int rpa_b200_selftest_wait_timeout(rpa_b200_handle* h, double LimitMs) try {
+  int s = begin_call(h);
+  if (s != RPA_OK) return s;
+  if (!(LimitMs > 0.0) || LimitMs > rpa::kWaitLimitNs * 1e-6)
+    return fail(h, RPA_ERR_INVALID_ARG, "LimitMs must be in (0, %g]", rpa::kWaitLimitNs * 1e-6);
+  RPA_CUDA(h, rpa::launch_wait_timeout_selftest(h->err_dev, (unsigned long long)(LimitMs * 1e6), h->stream));
+  return check_device_error(h);
+} catch (...) {
+  return exception_status(h);
+}
+
 int rpa_b200_set_autotune(rpa_b200_handle* h, int64_t on) try {
   if (!h) return RPA_ERR_INVALID_ARG;
   h->autotune = on != 0;
@@ -1142,6 +1225,7 @@ int rpa_b200_pi(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, con
                 double alpha, int64_t prec, double* PiU, int64_t ldPi) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
+  if ((s = check_arrays(h, {R, OccEnergies, VirtEnergies, Freqs, PiU}))) return s;
   Validated v;
   if ((s = validate_common(h, NQ, NOcc, NVirt, R, ldR, OccEnergies, VirtEnergies, NFreqs, Freqs, alpha, prec, v)))
     return s;
@@ -1176,6 +1260,7 @@ int rpa_b200_ec_from_pi(rpa_b200_handle* h, int64_t NQ, int64_t NFreqs, const do
                         const double* FreqWeights, double* Ec, double* Eu) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
+  if ((s = check_arrays(h, {PiU, FreqWeights}))) return s;
   if (NQ < 1 || NQ > (1 << 20) || NFreqs < 1 || NFreqs > 64 || ldPi < NQ || !PiU || !FreqWeights || !Ec)
     return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_ec_from_pi");
   std::vector<double> w;
@@ -1193,7 +1278,8 @@ int rpa_b200_ec_from_pi(rpa_b200_handle* h, int64_t NQ, int64_t NFreqs, const do
                                     (size_t)ldPi * 8, (size_t)n * 8, (size_t)n, cudaMemcpyHostToDevice, h->stream));
   }
   RPA_CUDA(h, cudaMemsetAsync(h->count_dev, 0, sizeof(int), h->stream));
-  RPA_CUDA(h, rpa::launch_count_nonfinite(Pi, (int64_t)K * n * n, h->count_dev, h->stream));
+  // only the lower triangle is read (a device input copies nothing else; the workspace's upper half holds leftovers)
+  RPA_CUDA(h, rpa::launch_count_nonfinite_lower(Pi, n, (int64_t)n * n, n, K, h->count_dev, h->stream));
   int cnt = 0;
   RPA_CUDA(h, cudaMemcpyAsync(&cnt, h->count_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
   RPA_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -1212,6 +1298,7 @@ int rpa_b200_ec(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt, con
                 const double* FreqWeights, double alpha, int64_t prec, double* Ec, double* Eu) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
+  if ((s = check_arrays(h, {R, OccEnergies, VirtEnergies, Freqs, FreqWeights}))) return s;
   Validated v;
   if ((s = validate_common(h, NQ, NOcc, NVirt, R, ldR, OccEnergies, VirtEnergies, NFreqs, Freqs, alpha, prec, v)))
     return s;
@@ -1257,6 +1344,7 @@ int rpa_b200_dring_t2(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVir
                       int64_t* NVecsT2, double* EigRPA, double* Ec) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
+  if ((s = check_arrays(h, {R, OccEnergies, VirtEnergies, Freqs, FreqWeights, Omega, A, U}))) return s;
   Validated v;
   if ((s = validate_common(h, NQ, NOcc, NVirt, R, ldR, OccEnergies, VirtEnergies, NFreqs, Freqs, alpha, prec, v)))
     return s;
@@ -1493,6 +1581,7 @@ int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
                             int64_t S2Operator, int64_t Prec, double* Ex) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
+  if ((s = check_arrays(h, {R, U, A}))) return s;
   const int64_t nov = NOcc * NVirt;
   if (NQ < 1 || NOcc < 1 || NVirt < 1 || NVecsT2 < 1 || ldR < NQ || ldU < nov || !R || !U || !A || !Ex ||
       (Prec != RPA_PREC_FP64 && Prec != RPA_PREC_SPLIT_BF16))
@@ -1572,6 +1661,7 @@ int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
                             int64_t ldX) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
+  if ((s = check_arrays(h, {R, OccEnergies, VirtEnergies, U, A, X}))) return s;
   const int64_t nov = NOcc * NVirt;
   if (NQ < 1 || NOcc < 1 || NVirt < 1 || NVecsT2 < 1 || ldR < NQ || ldU < nov || !R || !U || !A || !Ex ||
       !OccEnergies || !VirtEnergies || (X && ldX < NVecsT2) || (Prec != RPA_PREC_FP64 && Prec != RPA_PREC_SPLIT_BF16))
@@ -1755,6 +1845,7 @@ int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
 int rpa_b200_syevd(rpa_b200_handle* h, int64_t N, double* A, int64_t ldA, double* Eigenvals) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
+  if ((s = check_arrays(h, {A, Eigenvals}))) return s;
   if (N < 1 || ldA < N || !A || !Eigenvals) return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_syevd");
   if (N > 46340) return fail(h, RPA_ERR_TOO_LARGE, "rpa_b200_syevd: N too large");
   const int n = (int)N;
@@ -1806,6 +1897,7 @@ int rpa_b200_piu_basis(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVi
                        double* ExactTrace) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
+  if ((s = check_arrays(h, {R, OccEnergies, VirtEnergies, Guess, G}))) return s;
   if (BasisType < 1 || BasisType > 3) return fail(h, RPA_ERR_INVALID_ARG, "invalid basis type %lld", (long long)BasisType);
   if (!G || ldG < NQ || !NVecs || !(TargetError >= 0.0) || (Guess && ldGuess < NQ))
     return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_piu_basis");
@@ -1950,6 +2042,7 @@ int rpa_b200_project_basis(rpa_b200_handle* h, int64_t NQ, int64_t NVecs, int64_
                            const double* R, int64_t ldR, double* Rp, int64_t ldRp) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
+  if ((s = check_arrays(h, {G, R, Rp}))) return s;
   if (NQ < 1 || NVecs < 1 || NVecs > NQ || nov < 1 || !G || !R || !Rp || ldG < NQ || ldR < NQ || ldRp < NVecs)
     return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_project_basis");
   if (NQ > INT32_MAX || nov > INT32_MAX) return fail(h, RPA_ERR_TOO_LARGE, "rpa_b200_project_basis: too large");
@@ -2046,6 +2139,7 @@ int rpa_b200_thc_r(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, 
                    int64_t ldR) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
+  if ((s = check_arrays(h, {Zgk, Xga, Xgi, R}))) return s;
   if ((s = check_thc_args(h, NGrid, NQ, NOcc, NVirt, Zgk, ldZ, Xga, ldXa, Xgi, ldXi))) return s;
   if (!R || ldR < NQ) return fail(h, RPA_ERR_INVALID_ARG, "R is NULL or ldR < NQ");
   const int64_t nov = NOcc * NVirt;
@@ -2085,6 +2179,7 @@ int rpa_b200_ec_thc(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc,
                     const double* FreqWeights, double alpha, int64_t prec, double* Ec, double* Eu) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
+  if ((s = check_arrays(h, {Zgk, Xga, Xgi, OccEnergies, VirtEnergies, Freqs, FreqWeights}))) return s;
   if ((s = check_thc_args(h, NGrid, NQ, NOcc, NVirt, Zgk, ldZ, Xga, ldXa, Xgi, ldXi))) return s;
   const int64_t nov = NOcc * NVirt;
   const double *Zd, *Xad, *Xid;
@@ -2106,10 +2201,10 @@ static int grow_keep(rpa_b200_handle* h, DevBuf& b, size_t bytes, size_t used) {
   if (b.p && b.bytes >= bytes) return RPA_OK;
   const size_t nb = std::max(bytes, b.bytes * 2);
   void* p = nullptr;
-  RPA_CUDA(h, cudaMalloc(&p, nb));
+  RPA_CUDA(h, dev_alloc(&p, nb));
   if (b.p && used) RPA_CUDA(h, cudaMemcpyAsync(p, b.p, used, cudaMemcpyDeviceToDevice, h->stream));
   RPA_CUDA(h, cudaStreamSynchronize(h->stream));
-  if (b.p) cudaFree(b.p);
+  dev_free(b.p, b.bytes);
   b.p = p;
   b.bytes = nb;
   return RPA_OK;
@@ -2146,6 +2241,7 @@ int rpa_b200_jctc2024(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOc
                       int64_t* PNOStats) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
+  if ((s = check_arrays(h, {Zgk, Xgi, Yga, U, Am, Lik}))) return s;
   if (NGrid < 1 || NQ < 1 || NOcc < 1 || NVirt < 1 || NVecsT2 < 1 || !Zgk || !Xgi || !Yga || !U || !Am ||
       !Energies || ldZ < NGrid || ldXi < NGrid || ldYa < NGrid || ldU < NOcc * NVirt || (Lik && ldL < NOcc) ||
       !(CutoffThreshPNO >= 0.0))
@@ -2555,6 +2651,8 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
   size_t host_R = 0, total_nov = 0;
   for (int i = 0; i < n; ++i) {
     const rpa_instance& I = inst[i];
+    if ((s = check_arrays(h, {I.R, I.OccEnergies, I.VirtEnergies, I.Freqs, I.FreqWeights})))
+      return fail(h, s, "instance %d: %s", i, h->last_error.c_str());
     if ((s = validate_common(h, I.NQ, I.NOcc, I.NVirt, I.R, I.ldR, I.OccEnergies, I.VirtEnergies, I.NFreqs, I.Freqs,
                              I.alpha, prec, v[i])))
       return fail(h, s, "instance %d: %s", i, h->last_error.c_str());
@@ -3040,6 +3138,7 @@ int rpa_b200_ec_grad(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVirt
                      double* dOcc, double* dVirt) try {
   int s = begin_call(h);
   if (s != RPA_OK) return s;
+  if ((s = check_arrays(h, {R, OccEnergies, VirtEnergies, Freqs, FreqWeights, dR, dOcc, dVirt}))) return s;
   Validated v;
   if ((s = validate_common(h, NQ, NOcc, NVirt, R, ldR, OccEnergies, VirtEnergies, NFreqs, Freqs, alpha, prec, v)))
     return s;

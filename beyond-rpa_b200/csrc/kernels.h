@@ -195,8 +195,14 @@ cudaError_t launch_dai(const double* eps_o, const double* eps_v, int64_t no, int
                        cudaStream_t stream);
 // Copy lower triangle to upper (full symmetric square) for nmat matrices.
 cudaError_t launch_symmetrize(double* A, int64_t ld, int64_t stride, int n, int nmat, cudaStream_t stream);
+// Failure-detection self-test: one bounded wait on an mbarrier nobody arrives on, limit_ns long;
+// it records kDevTimeoutSelfTest in *err when it expires.
+cudaError_t launch_wait_timeout_selftest(int* err, unsigned long long limit_ns, cudaStream_t stream);
 // Count non-finite entries of a device array (result accumulated into *count).
 cudaError_t launch_count_nonfinite(const double* x, int64_t n, int* count, cudaStream_t stream);
+// The same over the lower triangles (diagonal included) of nmat n x n matrices, ld and stride apart.
+cudaError_t launch_count_nonfinite_lower(const double* A, int64_t ld, int64_t stride, int n, int nmat, int* count,
+                                         cudaStream_t stream);
 // The same over narr arrays (device arrays of pointers and lengths), blocks_per CTAs each.
 cudaError_t launch_count_nonfinite_multi(const double* const* ptrs, const int64_t* counts, int narr, int blocks_per,
                                          int* count, cudaStream_t stream);

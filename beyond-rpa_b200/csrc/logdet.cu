@@ -255,6 +255,20 @@ __global__ void count_nonfinite_kernel(const double* x, int64_t n, int* count) {
   if (local) atomicAdd(count, local);
 }
 
+// Lower triangle (diagonal included) of nmat column-major n x n matrices: blockIdx.x strides over
+// columns, blockIdx.y selects the matrix.  Entries above the diagonal are never read, so leftovers
+// there (a reused buffer, a caller's unused upper half) cannot raise a false count.
+__global__ void count_nonfinite_lower_kernel(const double* A, int64_t ld, int64_t stride, int n, int* count) {
+  const double* a = A + (int64_t)blockIdx.y * stride;
+  int local = 0;
+  for (int c = blockIdx.x; c < n; c += gridDim.x) {
+    const double* col = a + ld * (int64_t)c;
+    for (int r = c + threadIdx.x; r < n; r += blockDim.x)
+      if (!isfinite(col[r])) ++local;
+  }
+  if (local) atomicAdd(count, local);
+}
+
 // Many arrays at once: blockIdx.y selects array (ptrs[y], counts[y]).
 __global__ void count_nonfinite_multi_kernel(const double* const* ptrs, const int64_t* counts, int* count) {
   const double* x = ptrs[blockIdx.y];
@@ -504,6 +518,15 @@ cudaError_t launch_count_nonfinite(const double* x, int64_t n, int* count, cudaS
   int64_t blocks = (n + 255) / 256;
   if (blocks > 4096) blocks = 4096;
   count_nonfinite_kernel<<<(unsigned)blocks, 256, 0, stream>>>(x, n, count);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_count_nonfinite_lower(const double* A, int64_t ld, int64_t stride, int n, int nmat, int* count,
+                                         cudaStream_t stream) {
+  if (n <= 0 || nmat <= 0) return cudaSuccess;
+  const int cols = std::min(n, std::max(1, 4096 / nmat));
+  count_nonfinite_lower_kernel<<<dim3((unsigned)cols, (unsigned)nmat), 256, 0, stream>>>(A, ld, stride, n, count);
   ++g_launches;
   return cudaGetLastError();
 }

@@ -21,7 +21,10 @@
 //     threads) race on the array and must be serialised by the caller;
 //   * the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (once per device, with that device current); make
-//     this first call before any stream capture begins.
+//     this first call before any stream capture begins.  Under CUDA's lazy
+//     module loading that first call is also when the array and the kernels
+//     used here are loaded onto the GPU, so a caller that freezes its device
+//     footprint makes one call before freezing it.
 #include <cmath>
 #include <mutex>
 #include <vector>
@@ -70,7 +73,10 @@ bool is_device_pointer(const void* p) {
 extern "C" int rpa_b200_ec_from_pi_noalloc(int64_t device, void* stream_ptr, int64_t NQ, int64_t NFreqs,
                                            const double* PiU, int64_t ldPi, const double* FreqWeights, double* Ec,
                                            double* Eu) try {
-  if (NQ < 1 || NFreqs < 1 || NFreqs > 64 || ldPi < NQ || !PiU || !FreqWeights || !Ec) return RPA_ERR_INVALID_ARG;
+  // the same argument limits as rpa_b200_ec_from_pi; they also keep the size arithmetic below from wrapping
+  if (NQ < 1 || NQ > (1 << 20) || NFreqs < 1 || NFreqs > 64 || ldPi < NQ || !PiU || !FreqWeights || !Ec)
+    return RPA_ERR_INVALID_ARG;
+  if (device < 0 || device >= kMaxDevices) return RPA_ERR_INVALID_ARG;
   const size_t n = (size_t)NQ, K = (size_t)NFreqs;
   // layout of the scratch: Pi copy | L_ii | traces + log sums (double-double) | error word, counter
   const size_t need = K * n * n + K * n + 4 * K + 1;
@@ -117,7 +123,9 @@ extern "C" int rpa_b200_ec_from_pi_noalloc(int64_t device, void* stream_ptr, int
       status = RPA_ERR_CUDA;
       break;
     }
-    if (rpa::launch_count_nonfinite(Pi, (int64_t)(K * n * n), flags + 1, st) != cudaSuccess ||
+    // only the lower triangle is read: the upper half of the shared array may hold an earlier call's data
+    if (rpa::launch_count_nonfinite_lower(Pi, (int64_t)n, (int64_t)(n * n), (int)n, (int)K, flags + 1, st) !=
+            cudaSuccess ||
         rpa::launch_trace_shift(Pi, (int64_t)n, (int64_t)(n * n), (int)n, (int)K, nullptr, tr, st) != cudaSuccess ||
         rpa::launch_cholesky_lower(Pi, (int64_t)n, (int64_t)(n * n), (int)n, (int)K, Ldiag, flags, st,
                                    rpa::default_logdet_plan()) != cudaSuccess ||

@@ -17,6 +17,7 @@ enum DeviceError : int {
   kDevTimeoutAccFull = 103,   // epilogue gave up waiting for the accumulator
   kDevTimeoutAccEmpty = 104,  // MMA issuer gave up waiting for the epilogue
   kDevTimeoutDrain = 105,     // drain of in-flight async work timed out
+  kDevTimeoutSelfTest = 106,  // the failure-detection self-test's wait expired (as it is meant to)
   kDevNotSPD = 201,           // Cholesky pivot <= 0 or NaN: 1+Pi is not SPD
 };
 
@@ -58,13 +59,14 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 }
 // Slow path of the bounded wait (kept out of line so that the fast path of
 // the hot loops needs no extra registers).
-static __device__ __noinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity, int* err, int code) {
+static __device__ __noinline__ bool mbar_wait_slow(uint64_t* bar, uint32_t parity, int* err, int code,
+                                                   unsigned long long limit_ns = kWaitLimitNs) {
   const unsigned long long t0 = globaltimer_ns();
   uint32_t it = 0;
   while (!mbar_try_wait(bar, parity)) {
     if ((++it & 255u) == 0u) {
       if (*reinterpret_cast<volatile int*>(err) != 0) return false;
-      if (globaltimer_ns() - t0 > kWaitLimitNs) {
+      if (globaltimer_ns() - t0 > limit_ns) {
         atomicCAS(err, 0, code);
         return false;
       }

@@ -11,9 +11,9 @@
  *   - array arguments may point to host memory (pageable or pinned), to
  *     managed memory, or to device memory of the handle's GPU; the library
  *     detects which (cudaPointerGetAttributes) and stages host data itself.
- *     Device memory of another GPU is not supported: kernels read device
- *     arguments in place, so copy such data to the handle's GPU (or to the
- *     host) first;
+ *     Device memory of another GPU is refused with RPA_ERR_INVALID_ARG before
+ *     any launch (kernels read device arguments in place): copy such data to
+ *     the handle's GPU (or to the host) first;
  *   - scalar outputs (energies) are host pointers;
  *   - every call is synchronous on return and returns an rpa_status.
  * Errors: the Fortran reference stops with `error stop` after msg(...,
@@ -114,6 +114,32 @@ int rpa_b200_tune_logdet(rpa_b200_handle* handle, int64_t NQ, int64_t NMat, int6
 int rpa_b200_set_logdet_plan(rpa_b200_handle* handle, int64_t NQ, int64_t Nb2, int64_t Tile);
 int rpa_b200_get_logdet_plan(const rpa_b200_handle* handle, int64_t NQ, int64_t* Nb2, int64_t* Tile);
 int rpa_b200_set_autotune(rpa_b200_handle* handle, int64_t on);
+
+/*
+ * Device-memory cap of a handle.  No reference counterpart (the reference
+ * allocates host arrays as it goes).  The handle's workspace grows on demand;
+ * rpa_b200_set_workspace_limit caps it at Bytes (0 = no cap, the default).  An
+ * allocation that would pass the cap fails as a failed cudaMalloc does: the
+ * call returns RPA_ERR_OOM and the handle stays usable (raise the cap, or use
+ * smaller problems).  Lowering the cap frees nothing already held.
+ * rpa_b200_workspace_bytes reports the bytes held now and the cap (either
+ * pointer may be NULL).
+ */
+int rpa_b200_set_workspace_limit(rpa_b200_handle* handle, int64_t Bytes);
+int rpa_b200_workspace_bytes(const rpa_b200_handle* handle, int64_t* Used, int64_t* Limit);
+
+/*
+ * Failure-detection self-test.  No reference counterpart.  Every spin-wait
+ * in this library's kernels is bounded: when its limit (4 s) passes, the
+ * waiting thread records an error code on the device, the kernel returns, and
+ * the call reports RPA_ERR_TIMEOUT with the CUDA context still usable.  This
+ * entry point runs that same bounded wait on a barrier that nothing ever
+ * arrives on, with the limit LimitMs (0 < LimitMs <= 4000), and reports the
+ * result through the same path: it returns RPA_ERR_TIMEOUT when detection
+ * works.  Nothing asynchronous is in flight while it waits, and the next call
+ * on the handle starts clean.
+ */
+int rpa_b200_selftest_wait_timeout(rpa_b200_handle* handle, double LimitMs);
 
 /*
  * Pi(u) matrices:  PiU(:,:,u) = alpha * sum_ai R(:,ai) Chi_u(ai) R(:,ai)^T,
@@ -400,6 +426,14 @@ int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
  *     race on it: serialise them.
  *   - The first call on a device looks the array's address up once
  *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *     That first call is also when the device memory is committed: with CUDA's
+ *     lazy module loading the 32 MiB array and the kernels this entry point
+ *     uses are loaded onto the GPU at that moment, not when the library is
+ *     loaded.  A caller whose device footprint is frozen later should make one
+ *     call (any valid problem) before that point.
+ *   - Only the lower triangle of each PiU(:,:,u) is read, as in
+ *     rpa_b200_ec_from_pi.  Same limits on NQ (<= 2^20) and NFreqs (<= 64);
+ *     device must be a CUDA ordinal below 64 (RPA_ERR_INVALID_ARG otherwise).
  */
 #define RPA_B200_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 int rpa_b200_ec_from_pi_noalloc(int64_t device, void* stream, int64_t NQ, int64_t NFreqs, const double* PiU,

@@ -65,14 +65,14 @@ def test_ctypes_signatures_match_the_header(pkg):
 
 
 def test_fortran_interfaces_cover_the_header(pkg):
-    # every C entry point has a bind(C) interface in the Fortran module of INTEGRATION.md, with
-    # as many dummy arguments as the prototype has parameters
+    # every C entry point has a bind(C) interface in the Fortran module include/rpa_b200_iface.f90,
+    # with as many dummy arguments as the prototype has parameters
     import re
     header = re.sub(r"/\*.*?\*/", " ", pkg.HEADER.read_text(), flags=re.S)
     protos = {m.group(1): [p for p in " ".join(m.group(2).split()).split(",") if p.strip() not in ("", "void")]
               for m in re.finditer(r"^\s*(?:int64_t|int|const char\*)\s+(rpa_b200_\w+)\s*\(([^;]*?)\)\s*;",
                                    header, re.M)}
-    doc = (pkg.HEADER.parents[1] / "INTEGRATION.md").read_text()
+    doc = (pkg.HEADER.parent / "rpa_b200_iface.f90").read_text()
     doc = re.sub(r"&\s*\n\s*", " ", doc)  # join Fortran continuation lines
     binds = {m.group(3): [a for a in m.group(2).split(",") if a.strip()]
              for m in re.finditer(r"function\s+(\w+)\s*\(([^)]*)\)\s*bind\(C,\s*name=\"(\w+)\"\)", doc)}
@@ -310,3 +310,56 @@ def test_freq_grid_mbe_skips_all_core_sets_and_rejects_bad_gaps(pkg):
     bad = (np.array([-1.0, 0.5, 0.2, 1.0]), 2, 2)  # HOMO above LUMO
     with pytest.raises(pkg.RPAError):
         pkg.freq_grid_mbe(sets + [bad], nfixed=10)
+
+
+def test_pointer_classification_refuses_other_gpus(pkg, tmp_path):
+    # the argument check of every entry point: device memory of another GPU is refused, the
+    # handle's own device memory, managed memory and host memory pass (fake attribute values;
+    # a single-GPU box cannot produce a real foreign pointer)
+    import shutil
+    import subprocess
+    cxx = shutil.which("g++")
+    if cxx is None:
+        pytest.skip("no C++ compiler")
+    src = tmp_path / "classify.cpp"
+    src.write_text(r"""
+#include "abi_guard.h"
+#include <cstdio>
+int main() {
+  using rpa::ArgMemory;
+  using rpa::classify_arg_memory;
+  int bad = 0;
+  // type: 0 unregistered host, 1 registered host, 2 device, 3 managed
+  bad += classify_arg_memory(0, -2, 0) != ArgMemory::Host;
+  bad += classify_arg_memory(1, 0, 1) != ArgMemory::Host;
+  bad += classify_arg_memory(2, 0, 0) != ArgMemory::HandleDevice;
+  bad += classify_arg_memory(2, 3, 3) != ArgMemory::HandleDevice;
+  bad += classify_arg_memory(2, 1, 0) != ArgMemory::OtherDevice;
+  bad += classify_arg_memory(2, 0, 7) != ArgMemory::OtherDevice;
+  bad += classify_arg_memory(3, 5, 0) != ArgMemory::HandleDevice;
+  std::printf("%d\n", bad);
+  return bad;
+}
+""")
+    exe = tmp_path / "classify"
+    csrc = pkg.HEADER.parents[1] / "beyond-rpa_b200" / "csrc"
+    subprocess.run([cxx, "-std=c++17", "-Wall", "-Werror", f"-I{csrc}", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=30)
+    assert out.returncode == 0 and out.stdout.strip() == "0", out.stdout
+
+
+def test_every_entry_point_with_arrays_checks_their_device(pkg):
+    # each entry point that takes array arguments runs check_arrays right after begin_call
+    import re
+    src = (pkg.HEADER.parents[1] / "beyond-rpa_b200" / "csrc" / "capi.cu").read_text()
+    header = re.sub(r"/\*.*?\*/", " ", pkg.HEADER.read_text(), flags=re.S)
+    with_arrays = [m.group(1) for m in re.finditer(r"^\s*int\s+(rpa_b200_\w+)\s*\(([^;]*?)\)\s*;", header, re.M)
+                   if re.search(r"double\s*\*|rpa_instance\s*\*", m.group(2))]
+    assert "rpa_b200_ec" in with_arrays
+    for name in with_arrays:
+        if name in ("rpa_b200_tune_logdet", "rpa_b200_freq_grid", "rpa_b200_freq_grid_mbe", "rpa_b200_mbe_energy",
+                    "rpa_b200_last_timings", "rpa_b200_ec_from_pi_noalloc"):
+            continue  # host-only arrays, or no handle (the no-alloc entry point has no handle device)
+        body = src[src.index(f"\nint {name}("):]
+        body = body[:body.index("\n} catch (...)")]
+        assert "check_arrays(h, {" in body, name

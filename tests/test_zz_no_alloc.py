@@ -54,6 +54,63 @@ def test_noalloc_matches_allocating_entry_point_on_consecutive_calls(pkg, handle
     assert abs(ec - ref_b[0]) < 1e-11 and np.max(np.abs(eu - ref_b[1])) < 1e-10
 
 
+def test_noalloc_statuses_leave_no_stale_state(pkg, handle):
+    import torch
+    pi_a, w_a = _case(503, 300, 6, 50, 8)
+    pi_b, w_b = _case(504, 200, 5, 37, 5)
+    ref_a = handle.ec_from_pi(pi_a, w_a)
+    ref_b = handle.ec_from_pi(pi_b, w_b)
+    # pi[k, c, r] is entry (r, c) of the column-major Pi(u_k) the library reads (column c, row r)
+    # NaN in the lower triangle (r >= c): reported, and the next (device-input, other NQ) call is clean
+    bad = pi_a.copy()
+    bad[3, 5, 17] = np.nan
+    st, _, _ = _noalloc(pkg, bad, w_a)
+    assert st == pkg.RPA_ERR_NONFINITE
+    st, ec, _ = _noalloc(pkg, torch.from_numpy(pi_b).cuda(), w_b)
+    assert st == pkg.RPA_OK and abs(ec - ref_b[0]) < 1e-11
+    # NaN only above the diagonal is never read: a host call that copies it into the shared array and
+    # the device-input call after it (which copies only the lower triangle over it) both succeed
+    up = pi_a.copy()
+    up[:, 17, 5] = np.nan
+    st, ec, _ = _noalloc(pkg, up, w_a)
+    assert st == pkg.RPA_OK and abs(ec - ref_a[0]) < 1e-11
+    st, ec, _ = _noalloc(pkg, torch.from_numpy(pi_a).cuda(), w_a)
+    assert st == pkg.RPA_OK and abs(ec - ref_a[0]) < 1e-11
+    # 1 + Pi not positive definite: reported, and the next call is clean
+    nspd = pi_b.copy()
+    nspd[2] -= 3.0 * np.eye(pi_b.shape[1])
+    st, _, _ = _noalloc(pkg, nspd, w_b)
+    assert st == pkg.RPA_ERR_NOT_SPD
+    st, ec, eu = _noalloc(pkg, pi_b, w_b)
+    assert st == pkg.RPA_OK and abs(ec - ref_b[0]) < 1e-11 and np.max(np.abs(eu - ref_b[1])) < 1e-10
+
+
+def test_noalloc_on_a_caller_stream(pkg, handle):
+    import torch
+    pi, w = _case(505, 256, 4, 60, 6)
+    ref = handle.ec_from_pi(pi, w)
+    s = torch.cuda.Stream()
+    d = torch.from_numpy(pi).cuda()
+    torch.cuda.current_stream().synchronize()
+    for _ in range(2):
+        st, ec, eu = _noalloc(pkg, d, w, stream=ctypes.c_void_p(s.cuda_stream))
+        assert st == pkg.RPA_OK
+        assert abs(ec - ref[0]) < 1e-11 and np.max(np.abs(eu - ref[1])) < 1e-10
+
+
+def test_noalloc_rejects_bad_arguments(pkg):
+    lib = pkg.load_library()
+    ec = ctypes.c_double()
+    w = np.ones(1)
+    pi = np.zeros((1, 4, 4))
+    # NQ beyond 2^20 (its size would wrap a 64-bit count) and a negative device are argument errors
+    st = lib.rpa_b200_ec_from_pi_noalloc(0, None, 1 << 62, 4, pi.ctypes.data, 1 << 62, w.ctypes.data,
+                                         ctypes.byref(ec), None)
+    assert st == pkg.RPA_ERR_INVALID_ARG
+    st = lib.rpa_b200_ec_from_pi_noalloc(-1, None, 4, 1, pi.ctypes.data, 4, w.ctypes.data, ctypes.byref(ec), None)
+    assert st == pkg.RPA_ERR_INVALID_ARG
+
+
 def test_noalloc_rejects_problems_beyond_its_scratch(pkg):
     # 1 x 2100^2 doubles exceed the 32 MiB array: refused before any GPU work
     pi = np.zeros((1, 4, 4))
