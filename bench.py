@@ -119,6 +119,57 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows), "power_w_max": max(power) if power else None}
 
 
+# ----------------------------------------------------------------------------- host cores, FP64 peak
+
+def host_cores():
+    """(physical cores, logical CPUs) usable by this process: distinct (core, socket) pairs of
+    lscpu's table restricted to the CPUs in this process's affinity mask."""
+    cpus = sorted(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else list(range(os.cpu_count()))
+    try:
+        out = subprocess.run(["lscpu", "-p=CPU,CORE,SOCKET"], capture_output=True, text=True, timeout=10).stdout
+        table = {int(c): (core, sock) for c, core, sock in
+                 (line.split(",") for line in out.splitlines() if line and not line.startswith("#"))}
+        phys = len({table[c] for c in cpus if c in table}) or len(cpus)
+    except (OSError, ValueError, subprocess.SubprocessError):
+        phys = len(cpus)
+    return phys, len(cpus)
+
+
+def fp64_peak(stream, seconds=4.0):
+    """cuBLAS DGEMM 8192^3 (torch.matmul, float64) on this GPU, the method of the bf16 peaks:
+    best of 10 (burst) and back to back for `seconds` (sustained); TFLOP/s, CUDA events."""
+    import torch
+    n = 8192
+    g = torch.Generator(device="cuda").manual_seed(5)
+    a = torch.randn((n, n), dtype=torch.float64, device="cuda", generator=g)
+    b = torch.randn((n, n), dtype=torch.float64, device="cuda", generator=g)
+    c = torch.empty_like(a)
+    flop = 2.0 * n ** 3
+    for _ in range(2):
+        torch.matmul(a, b, out=c)
+    best = float("inf")
+    for _ in range(10):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        torch.matmul(a, b, out=c)
+        e1.record(stream)
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    reps = max(1, int(seconds * 1e3 / best))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        torch.matmul(a, b, out=c)
+    e1.record(stream)
+    e1.synchronize()
+    sustained = flop * reps / (e0.elapsed_time(e1) / 1e3) / 1e12
+    del a, b, c
+    torch.cuda.empty_cache()
+    return {"burst_tflops": flop / (best / 1e3) / 1e12, "sustained_tflops": sustained,
+            "how": f"torch.matmul float64 {n}^3 (cuBLAS DGEMM, 2 n^3 flop): best of 10 and {reps} back to back, "
+                   "CUDA events"}
+
+
 # ----------------------------------------------------------------------------- CPU restatement timing
 
 def cpu_sample(nq, no, nv, K, budget_s=8.0, seed=0):
@@ -149,11 +200,42 @@ def cpu_sample(nq, no, nv, K, budget_s=8.0, seed=0):
     O.logdet_qr(A)
     t_qr = time.perf_counter() - t1
     t_full = t_blk * nblk_total * K + t_qr * K
-    threads = os.cpu_count()
+    phys, logical = host_cores()
     sample = (f"{done} DGEMM blocks of 500 ai x NQ={nq} (1 frequency) + 1 DGEQRF log-det of {nq}x{nq}; "
               f"extrapolated to {nblk_total} blocks x {K} frequencies + {K} log-dets")
-    return {"value": 1.0 / t_full, "unit": "E_c/s", "cores": threads, "kind": "port", "sample": sample,
-            "seconds_per_Ec": t_full, "t_block_s": t_blk, "t_logdet_s": t_qr}
+    return {"value": 1.0 / t_full, "unit": "E_c/s", "cores": phys, "threads": logical, "kind": "port",
+            "sample": sample, "seconds_per_Ec": t_full, "t_block_s": t_blk, "t_logdet_s": t_qr}
+
+
+# ----------------------------------------------------------------------------- inputs
+
+PINNED = ROOT / "tests" / "golden" / "pinned_golden.json"
+
+
+def pinned_system(pkg, name, rank):
+    """Inputs of an oracle-pinned single-system workload (tests/golden/pinned.py, numpy-seeded):
+    rank 0 gets the pinned system itself (the fixture's rescale factor and grid, and the oracle's
+    E_c to compare with), other ranks another system of the same shape, rescaled here.
+    Returns (SyntheticSystem with R on the device, R rows on the host, oracle E_c or None)."""
+    import torch
+    from beyond_rpa_b200.workloads import SyntheticSystem, lambda_max_pi0
+    sys.path.insert(0, str(ROOT))
+    from tests.golden import pinned as P
+    fix = json.loads(PINNED.read_text()).get(name) if PINNED.exists() else None
+    K = P.SINGLE[name][3]
+    if rank == 0 and fix is not None:
+        Rt, eo, ev = P.single_system(name, fix["factor"])
+        x, w, ref = np.array(fix["freqs"]), np.array(fix["weights"]), fix["Ec"]
+    else:
+        Rt, eo, ev = P.single_system(name, variant=rank)
+        Rd = torch.from_numpy(Rt).cuda()
+        d = torch.from_numpy((ev[:, None] - eo[None, :]).reshape(-1, order="F")).cuda()
+        Rt *= math.sqrt(0.8 / lambda_max_pi0(Rd.T, d))
+        del Rd, d
+        x, w = pkg.freq_grid(np.concatenate([eo, ev]), len(eo), len(ev), nfixed=K)
+        ref = None
+    R = torch.from_numpy(Rt).cuda().T  # (NQ, nov) column-major, ld = NQ
+    return SyntheticSystem(R=R, eps_o=eo, eps_v=ev, freqs=x, weights=w), Rt, ref
 
 
 # ----------------------------------------------------------------------------- ours
@@ -178,7 +260,11 @@ def run_ours(args):
     stream = torch.cuda.Stream()  # the library and the timing events share this stream
     torch.cuda.set_stream(stream)
     h.set_stream(stream.cuda_stream)
-    s = make_single_system(WORKLOAD, seed=1000 + rank)
+    from tests.golden import pinned as P
+    if WORKLOAD in P.SINGLE:
+        s, R_host_rows, ec_oracle = pinned_system(pkg, WORKLOAD, rank)
+    else:
+        s, R_host_rows, ec_oracle = make_single_system(WORKLOAD, seed=1000 + rank), None, None
     torch.cuda.synchronize()
 
     def barrier():
@@ -237,7 +323,11 @@ def run_ours(args):
         return
     # end-to-end through the public API with host (pinned) inputs
     Rh_t = torch.empty((nov, nq), dtype=torch.float64, pin_memory=True)
-    Rh_t.copy_(s.R.T)
+    if R_host_rows is not None:
+        Rh_t.copy_(torch.from_numpy(R_host_rows))
+        del R_host_rows
+    else:
+        Rh_t.copy_(s.R.T)
     Rh = Rh_t.T
     h.ec_rpa(Rh, s.eps_o, s.eps_v, s.freqs, s.weights, prec="split")
     e2e_steps = max(1, min(args.steps, 5))
@@ -311,13 +401,103 @@ def run_ours(args):
         "energy": {"Ec_split": ecs[-1], "Ec_fp64": ec64, "abs_diff_split_vs_fp64": abs(ecs[-1] - ec64)},
         "clocks": clocks,
     }
+    ld_ms = statistics.mean(logdet)
+    ld_flops = float(nq) ** 3 / 3.0 * K
+    split_bytes = 8.0 * nq * nov + 4.0 * nq * nov * K  # R read once, bf16 hi + lo written per frequency
+    out["scale_split_roofline"] = {"bound": "hbm", "achieved": split_bytes / (statistics.mean(split) / 1e3) / 1e9,
+                                   "peak": hbm, "unit": "GB/s",
+                                   "frac": split_bytes / (statistics.mean(split) / 1e3) / 1e9 / hbm,
+                                   "kernel": "scale_split_kernel",
+                                   "note": "algorithmic bytes 8 NQ nov + 4 NQ nov K over the pass time"}
+    if ec_oracle is not None:
+        out["oracle_check"] = {"Ec_oracle": ec_oracle, "abs_err_split": abs(ecs[-1] - ec_oracle),
+                               "abs_err_fp64": abs(ec64 - ec_oracle),
+                               "source": "tests/golden/pinned_golden.json: the oracle (numpy/LAPACK FP64) on "
+                                         "the same seeded inputs"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_sample(nq, no, nv, K)
+    if world == 1 and not args.no_mbe:
+        # FP64 (DMMA) peak of this GPU, the denominator of the FP64 kernels' fractions
+        fp = fp64_peak(stream)
+        out["fp64_peak"] = fp
+        out["logdet_roofline"] = {"bound": "fp64", "achieved": ld_flops / (ld_ms / 1e3) / 1e12,
+                                  "peak": fp["sustained_tflops"], "unit": "TFLOP/s",
+                                  "frac": ld_flops / (ld_ms / 1e3) / 1e12 / fp["sustained_tflops"],
+                                  "note": "NQ^3/3 K Cholesky flops over the log-det phase; peak = measured "
+                                          "sustained cuBLAS DGEMM"}
+        out["fp64_form"]["pi_fp64_tflops"] = pi_flops / (t64["contraction_ms"] / 1e3) / 1e12
+        # the batched many-body-expansion workload (512 fragments), split-BF16 vs FP64
+        del s
+        h.close()
+        torch.cuda.empty_cache()
+        h = pkg.Handle(local)
+        h.set_stream(stream.cuda_stream)
+        out["mbe_512"] = mbe_measure(pkg, h, stream, 512, steps=2, warmup=1)
     if rank == 0:
         print(json.dumps(out), flush=True)
     h.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def mbe_measure(pkg, h, stream, n_inst, steps, warmup, rank=0, world=1, fp64_steps=1):
+    """Batched many-fragment workload on this rank's share: instances/s of rpa_b200_ec_batched,
+    split-BF16 vs FP64 (same batched path), energies gathered over ranks."""
+    import torch
+    from beyond_rpa_b200.workloads import make_mbe_batch, mbe_specs
+    from beyond_rpa_b200 import distributed as D
+    specs = mbe_specs(n_inst, seed=4000)
+    mine = D.shard([D.instance_cost(nq, no * nv, K) for no, nv, nq, K in specs], rank, world)
+    systems, kinds = make_mbe_batch(n_inst, seed=4000, only=mine)
+    torch.cuda.synchronize()
+    flops = sum(float(R.shape[0]) ** 2 * len(eo) * len(ev) * len(x) for R, eo, ev, x, w in systems)
+    ld_flops = sum(float(R.shape[0]) ** 3 / 3 * len(x) for R, eo, ev, x, w in systems)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    for _ in range(warmup):
+        h.ec_batched(systems, prec="split")
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        ec, _ = h.ec_batched(systems, prec="split")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    t_ms = D.max_over_ranks(e0.elapsed_time(e1) / steps, device="cuda")
+    launches = h.launches()
+    h.ec_batched(systems, prec="fp64")
+    barrier()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(fp64_steps):
+        ec64, _ = h.ec_batched(systems, prec="fp64")
+    e3.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    t64 = D.max_over_ranks(e2.elapsed_time(e3) / fp64_steps, device="cuda")
+    all_ec = D.gather_energies(mine, ec, n_inst, device="cuda")
+    all_ec64 = D.gather_energies(mine, ec64, n_inst, device="cuda")
+    del systems
+    return {
+        "metric": "RPA E_c of a batched many-body-expansion workload",
+        "value": n_inst / (t_ms / 1e3), "unit": "instances/s", "ms_per_step": t_ms, "steps": steps,
+        "n_gpus": world, "scaling": "strong", "instances": n_inst, "dimers": kinds.count("dimer"),
+        "trimers": kinds.count("trimer"),
+        "pi_fp64_equiv_tflops_rank0": flops / (t_ms / 1e3) / 1e12, "pi_flops_rank0": flops,
+        "logdet_flops_rank0": ld_flops, "gpu_launches_per_step_rank0": launches,
+        "fp64_form": {"ms_per_step": t64, "instances_per_s": n_inst / (t64 / 1e3),
+                      "speedup_split_vs_fp64": t64 / t_ms},
+        "max_abs_dEc_split_vs_fp64": float(np.max(np.abs(all_ec - all_ec64))),
+        "dEint_note": "fragments are independent synthetic systems; interaction energies of 16 of them "
+                      "are checked against the oracle by tests/test_gpu_pinned.py (<= 1e-7 Eh)",
+    }
 
 
 def run_mbe(args):
@@ -333,61 +513,14 @@ def run_mbe(args):
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     pkg = load_package()
-    from beyond_rpa_b200.workloads import make_mbe_batch, mbe_specs
-    from beyond_rpa_b200 import distributed as D
     n_inst = int(args.workload.split("_")[1]) if "_" in args.workload else 512
-    specs = mbe_specs(n_inst, seed=4000)
-    mine = D.shard([D.instance_cost(nq, no * nv, K) for no, nv, nq, K in specs], rank, world)
     h = pkg.Handle(local)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     h.set_stream(stream.cuda_stream)
-    systems, kinds = make_mbe_batch(n_inst, seed=4000, only=mine)
-    torch.cuda.synchronize()
-    flops = sum(float(R.shape[0]) ** 2 * len(eo) * len(ev) * len(x) for R, eo, ev, x, w in systems)
-    ld_flops = sum(float(R.shape[0]) ** 3 / 3 * len(x) for R, eo, ev, x, w in systems)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    for _ in range(args.warmup):
-        h.ec_batched(systems, prec="split")
-    barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        ec, _ = h.ec_batched(systems, prec="split")
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    t_ms = D.max_over_ranks(e0.elapsed_time(e1) / args.steps, device="cuda")
-    launches = h.launches()
-    h.ec_batched(systems, prec="fp64")
-    barrier()
-    e2 = torch.cuda.Event(enable_timing=True)
-    e3 = torch.cuda.Event(enable_timing=True)
-    e2.record(stream)
-    ec64, _ = h.ec_batched(systems, prec="fp64")
-    e3.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    t64 = D.max_over_ranks(e2.elapsed_time(e3), device="cuda")
-    all_ec = D.gather_energies(mine, ec, n_inst, device="cuda")
-    all_ec64 = D.gather_energies(mine, ec64, n_inst, device="cuda")
+    res = mbe_measure(pkg, h, stream, n_inst, args.steps, args.warmup, rank, world)
     if rank == 0:
-        print(json.dumps({
-            "metric": "RPA E_c of a batched many-body-expansion workload", "workload": args.workload,
-            "value": n_inst / (t_ms / 1e3), "unit": "instances/s", "ms_per_step": t_ms, "steps": args.steps,
-            "n_gpus": world, "scaling": "strong", "instances": n_inst, "dimers": kinds.count("dimer"),
-            "trimers": kinds.count("trimer"),
-            "pi_fp64_equiv_tflops_rank0": flops / (t_ms / 1e3) / 1e12, "pi_flops_rank0": flops,
-            "logdet_flops_rank0": ld_flops, "gpu_launches_per_step_rank0": launches,
-            "fp64_form": {"ms_per_step": t64, "speedup_split_vs_fp64": t64 / t_ms},
-            "max_abs_dEc_split_vs_fp64": float(np.max(np.abs(all_ec - all_ec64))),
-        }), flush=True)
+        print(json.dumps({**res, "workload": args.workload}), flush=True)
     h.close()
     if world > 1:
         dist.destroy_process_group()
@@ -696,12 +829,27 @@ def run_reference(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"{WORKLOAD}: NQ={nq} NOcc={no} NVirt={nv} nov={no * nv} K={K}",
                        "parallelism": "host threads (OpenBLAS)"},
-            "cpu_baseline": {"value": value, "unit": "E_c/s", "cores": os.cpu_count(), "kind": "port",
+            "cpu_baseline": {"value": value, "unit": "E_c/s", "cores": host_cores()[0],
+                             "threads": host_cores()[1], "kind": "port",
                              "sample": "per step: DGEMM blocks of 500 ai for ~6 s (1 frequency) + 1 DGEQRF "
                                        "log-det, extrapolated to the full E_c (reference binary cannot be "
                                        "built: Fortran, no gfortran)"},
             "e2e": {"value": value, "unit": "E_c/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}
+    if args.full_cpu_check:
+        # one complete CPU E_c of the same workload (the oracle on the pinned inputs), to validate the
+        # per-step extrapolation above
+        sys.path.insert(0, str(ROOT))
+        from oracle import rpa_oracle as O
+        from tests.golden import pinned as P
+        fix = json.loads(PINNED.read_text())["single_4096"]
+        Rt, eo, ev = P.single_system("single_4096", fix["factor"])
+        t0 = time.perf_counter()
+        ec, _ = O.ec_rpa(Rt.T, eo, ev, np.array(fix["freqs"]), np.array(fix["weights"]))
+        t_full = time.perf_counter() - t0
+        line["full_cpu_check"] = {"seconds_per_Ec_measured": t_full, "seconds_per_Ec_extrapolated": spe,
+                                  "ratio_measured_over_extrapolated": t_full / spe,
+                                  "abs_err_vs_fixture": abs(ec - fix["Ec"])}
     print(json.dumps(line), flush=True)
 
 
@@ -713,6 +861,10 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default=WORKLOAD, help="single-system workload name (beyond-rpa_b200/workloads.py)")
+    ap.add_argument("--full-cpu-check", action="store_true",
+                    help="--impl reference: also time one complete CPU E_c to validate the extrapolation")
+    ap.add_argument("--no-mbe", action="store_true",
+                    help="skip the FP64 peak and the batched many-fragment legs of the default line")
     ap.add_argument("--no-extras", action="store_true",
                     help="profiling runs: print only the timed leg (no e2e, FP64-form or CPU legs)")
     args = ap.parse_args()

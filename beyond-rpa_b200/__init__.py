@@ -367,26 +367,76 @@ class Handle:
                                               float(alpha), _PREC[prec], ctypes.byref(ec), p_dR, ld_dR, p_dO, p_dV))
         return ec.value, dR, dO, dV
 
-    def mbe_energies(self, subsystems, nbody, prec="split", limit_dai=True, nfixed=0, core_thresh=-3.0):
+    def mbe_energies(self, subsystems, nbody, prec="split", limit_dai=True, nfixed=0, core_thresh=-3.0,
+                     basis=None, basis_target_error=math.sqrt(1e-5)):
         """Many-body-expansion driver (the energy part of rpa_PostSCF, src/rpa/rpa_driver.f90:25-433):
         one frequency grid shared by all subsystems (freq_grid_mbe), every subsystem's E_c in one
         batched call, then the interaction (nbody 2) or nonadditive (3, 4) energy (mbe_energy).
 
         subsystems: (R, eps_occ, eps_virt) per subsystem in the order of SUBSYSTEMS (3, 7 or 15 of
         them), R over the active occupied orbitals (those with eps >= core_thresh), eps_occ all
-        occupied energies ascending.  Returns (E_c per subsystem, interaction energy, freqs, weights)."""
+        occupied energies ascending.
+        basis: None uses each R as given.  "eigen" or "random" compresses the Pi basis once, for the
+        whole system (subsystems[0]) at the lowest frequency of the shared grid (piu_basis), and
+        projects every subsystem onto it, R' = G^T R (project_basis), as the reference shares
+        THC_ZgkPiU between all subsystems for size consistency (src/rpa/rpa.f90:2305-2322); all R
+        must then have the same NQ rows (the cluster's Cholesky basis).
+        Returns (E_c per subsystem, interaction energy, freqs, weights)."""
+        ec, eint, x, w, _ = self._mbe_rpa(subsystems, nbody, prec, limit_dai, nfixed, core_thresh, basis,
+                                          basis_target_error)
+        return ec, eint, x, w
+
+    def _mbe_rpa(self, subsystems, nbody, prec, limit_dai, nfixed, core_thresh, basis, basis_target_error):
         need = {2: 3, 3: 7, 4: 15}.get(int(nbody))
         if need is None or len(subsystems) != need:
             raise ValueError("nbody 2, 3 or 4 needs 3, 7 or 15 subsystems")
         sets = [(np.concatenate([np.asarray(eo, np.float64), np.asarray(ev, np.float64)]), len(eo), len(ev))
                 for _, eo, ev in subsystems]
         x, w = freq_grid_mbe(sets, limit_dai=limit_dai, nfixed=nfixed, core_thresh=core_thresh)
-        systems = []
+        active = []
         for R, eo, ev in subsystems:
             eo = np.asarray(eo, np.float64)
-            systems.append((R, eo[eo >= core_thresh], ev, x, w))
-        ec, _ = self.ec_batched(systems, prec=prec)
-        return ec, mbe_energy(ec, nbody), x, w
+            active.append((R, eo[eo >= core_thresh], np.asarray(ev, np.float64)))
+        G = None
+        if basis is not None:
+            nq = int(active[0][0].shape[0])
+            if any(int(R.shape[0]) != nq for R, _, _ in active):
+                raise ValueError("a shared Pi basis needs every subsystem's R over the same NQ Cholesky vectors")
+            R0, eo0, ev0 = active[0]
+            G, _, _ = self.piu_basis(R0, eo0, ev0, float(x[0]), target_error=basis_target_error, basis=basis)
+            active = [(self.project_basis(G, R), eo, ev) for R, eo, ev in active]
+        ec, _ = self.ec_batched([(R, eo, ev, x, w) for R, eo, ev in active], prec=prec)
+        return ec, mbe_energy(ec, nbody), x, w, (active, G)
+
+    def mbe_beyond_rpa(self, subsystems, nbody, prec="split", limit_dai=True, nfixed=0, core_thresh=-3.0,
+                       basis=None, basis_target_error=math.sqrt(1e-5), cutoff_thresh=1e-4, cutoff_type=0,
+                       n_guess=None, seed=0):
+        """Many-body expansion of RPA plus the SOSEX exchange energy (the beyond-RPA subsystem loop of
+        rpa_PostSCF, src/rpa/rpa_driver.f90:83-91, 175-240): the shared grid and (optionally) the shared
+        Pi basis of mbe_energies, then for every subsystem the direct-ring T2 amplitudes and the SOSEX
+        energy.  The T2 eigenvalue cutoff threshold is fixed once by the whole system (dring_t2 with
+        common_thresh < 0) and reused by every subsystem, as the reference shares
+        T2CutoffCommonThresh for size-consistent interaction energies.  n_guess: guess vectors of the
+        range finder (None: the reference's ceil(3 NQ), capped at NOcc NVirt).  The range finder drops
+        Gram directions below its linear-dependency cutoff, so even with a shared threshold the
+        exchange energies of non-interacting fragments add up only to the accuracy of the retained
+        subspace (in the reference as here), while the RPA energies add up to rounding.
+        Returns a dict: freqs, weights, ec and eint (RPA), ex and ex_int (SOSEX), eig_rpa (the T2
+        eigenvalue energies), nt (amplitude counts) and common_thresh."""
+        ec, eint, x, w, (active, _) = self._mbe_rpa(subsystems, nbody, prec, limit_dai, nfixed, core_thresh, basis,
+                                                    basis_target_error)
+        common = -1.0
+        ex, eig, nts = [], [], []
+        for R, eo, ev in active:
+            t2 = self.dring_t2(R, eo, ev, x, w, prec=prec, seed=seed, n_guess=n_guess, cutoff_thresh=cutoff_thresh,
+                               cutoff_type=cutoff_type, common_thresh=common)
+            common = t2["common_thresh"]
+            nts.append(t2["NT"])
+            eig.append(float(np.sum(t2["EigRPA"])))
+            ex.append(self.exchange_sosex(R, len(eo), len(ev), t2["U"], t2["A"], prec=prec))
+        ex = np.array(ex)
+        return {"freqs": x, "weights": w, "ec": ec, "eint": eint, "ex": ex, "ex_int": mbe_energy(ex, nbody),
+                "eig_rpa": np.array(eig), "nt": nts, "common_thresh": common}
 
     def ec_batched(self, systems, prec="split"):
         """Energies of many systems in one call (rpa_b200_ec_batched).

@@ -119,6 +119,7 @@ struct rpa_b200_handle {
   uint64_t plans_version = 0;  // bumped on every change (part of the batched graph key)
   int autotune = 1;            // tune unseen order buckets on their first batched use (RPA_B200_AUTOTUNE=0: off)
   size_t batch_bytes = 0;      // device bytes per batch of the batched entry (0: 60% of free memory)
+  size_t thc_piece_bytes = (size_t)2 << 30;  // device bytes of one piece of the THC Pi build (R, YX, hi + lo)
   int sosex_seg = 2;           // 32-column chunks per accumulation segment of the split exchange contraction
   int ring_seg = 2;            // the same for the split ring contractions of the T2 range finder
   DevBuf tune;                 // tuner workspace: descriptors and pivots of its test matrices
@@ -332,6 +333,15 @@ int encode_map(rpa_b200_handle* h, CUtensorMap* m, void* base, int64_t nov, int 
   return RPA_OK;
 }
 
+// Store views of X_hi / X_lo for the scale/split pass (boxes of 64 ai x 32 Q, 128-byte swizzle).
+int encode_store_maps(rpa_b200_handle* h, CUtensorMap* hi, CUtensorMap* lo, void* xhi, void* xlo, int64_t nov, int NQ,
+                      int kg, int64_t pitch) {
+  if (rpa::encode_split_store_map(h->encode, hi, xhi, nov, NQ, kg, pitch) != cudaSuccess ||
+      rpa::encode_split_store_map(h->encode, lo, xlo, nov, NQ, kg, pitch) != cudaSuccess)
+    return fail(h, RPA_ERR_CUDA, "cuTensorMapEncodeTiled failed for the split operands' store views");
+  return RPA_OK;
+}
+
 // Build the lower triangles of Pi_k (k = 0..K-1) into h->Pi (ld = NQ).
 // Frequencies per split-BF16 group (all of them unless the device is short of memory).  The
 // free-memory query can stall the host for tens of ms while the GPU idles: ask only when the
@@ -405,15 +415,15 @@ int build_pi(rpa_b200_handle* h, const Validated& v, const double* Rd, int64_t l
     fg.n = n;
     for (int k = 0; k < n; ++k) fg.u2[k] = v.freqs[g0 + k] * v.freqs[g0 + k];
     double* diag = static_cast<double*>(h->diag.p) + (int64_t)g0 * NQ;
+    CUtensorMap mAh, mAl, mBh, mBl, sHi, sLo;
+    int s;
+    if ((s = encode_store_maps(h, &sHi, &sLo, h->Xhi.p, h->Xlo.p, nov, NQ, n, pitch)) != RPA_OK) return s;
     cudaEvent_t e0 = pool_event(h), e1 = pool_event(h), e2 = pool_event(h);
     RPA_CUDA(h, cudaEventRecord(e0, h->stream));
-    RPA_CUDA(h, rpa::launch_scale_split(Rd, ldR, NQ, nov, D, fg, alpha, static_cast<__nv_bfloat16*>(h->Xhi.p),
-                                        static_cast<__nv_bfloat16*>(h->Xlo.p), pitch, (int64_t)NQ * pitch,
-                                        static_cast<double*>(h->diag_part.p), diag, plan, h->stream));
+    RPA_CUDA(h, rpa::launch_scale_split(Rd, ldR, NQ, nov, D, fg, alpha, &sHi, &sLo,
+                                        static_cast<double*>(h->diag_part.p), diag, plan, h->err_dev, h->stream));
     RPA_CUDA(h, cudaEventRecord(e1, h->stream));
     h->split_ev.push_back({e0, e1});
-    CUtensorMap mAh, mAl, mBh, mBl;
-    int s;
     if ((s = encode_map(h, &mAh, h->Xhi.p, nov, NQ, n, pitch, rpa::kSyrkTcTM)) != RPA_OK) return s;
     if ((s = encode_map(h, &mAl, h->Xlo.p, nov, NQ, n, pitch, rpa::kSyrkTcTM)) != RPA_OK) return s;
     if ((s = encode_map(h, &mBh, h->Xhi.p, nov, NQ, n, pitch, rpa::kSyrkTcTN)) != RPA_OK) return s;
@@ -489,8 +499,9 @@ int build_pi_pipelined(rpa_b200_handle* h, const Validated& v, const double* Rh,
   rpa::FreqGroup fg{};
   fg.n = v.K;
   for (int k = 0; k < v.K; ++k) fg.u2[k] = v.freqs[k] * v.freqs[k];
-  CUtensorMap mAh, mAl, mBh, mBl;
+  CUtensorMap mAh, mAl, mBh, mBl, sHi, sLo;
   int s;
+  if ((s = encode_store_maps(h, &sHi, &sLo, h->Xhi.p, h->Xlo.p, nov, NQ, v.K, pitch)) != RPA_OK) return s;
   if ((s = encode_map(h, &mAh, h->Xhi.p, nov, NQ, v.K, pitch, rpa::kSyrkTcTM)) != RPA_OK) return s;
   if ((s = encode_map(h, &mAl, h->Xlo.p, nov, NQ, v.K, pitch, rpa::kSyrkTcTM)) != RPA_OK) return s;
   if ((s = encode_map(h, &mBh, h->Xhi.p, nov, NQ, v.K, pitch, rpa::kSyrkTcTN)) != RPA_OK) return s;
@@ -514,9 +525,9 @@ int build_pi_pipelined(rpa_b200_handle* h, const Validated& v, const double* Rh,
     RPA_CUDA(h, rpa::launch_count_nonfinite(Rd + a0 * NQ, (a1 - a0) * NQ, h->count_dev, h->stream));
     cudaEvent_t e0 = pool_event(h), e1 = pool_event(h), e2 = pool_event(h);
     RPA_CUDA(h, cudaEventRecord(e0, h->stream));
-    RPA_CUDA(h, rpa::launch_scale_split_part(Rd, NQ, NQ, nov, D, fg, alpha, static_cast<__nv_bfloat16*>(h->Xhi.p),
-                                             static_cast<__nv_bfloat16*>(h->Xlo.p), pitch, (int64_t)NQ * pitch,
-                                             static_cast<double*>(h->diag_part.p), plan, s0, s1, h->stream));
+    RPA_CUDA(h, rpa::launch_scale_split_part(Rd, NQ, NQ, nov, D, fg, alpha, &sHi, &sLo,
+                                             static_cast<double*>(h->diag_part.p), plan, s0, s1, h->err_dev,
+                                             h->stream));
     const bool last = (s1 == plan.nsplit);
     if (last)
       RPA_CUDA(h, rpa::launch_diag_reduce(static_cast<double*>(h->diag_part.p), plan, v.K, NQ, diag, h->stream));
@@ -1029,6 +1040,7 @@ int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) try
   if (const char* se = std::getenv("RPA_B200_SYNC_EVERY")) h->sync_every = std::atoi(se);
   if (const char* at = std::getenv("RPA_B200_AUTOTUNE")) h->autotune = std::atoi(at) != 0;
   if (const char* bb = std::getenv("RPA_B200_BATCH_BYTES")) h->batch_bytes = (size_t)std::atoll(bb);
+  if (const char* tp = std::getenv("RPA_B200_THC_PIECE_BYTES")) h->thc_piece_bytes = (size_t)std::max(1ll, std::atoll(tp));
   if (const char* sg = std::getenv("RPA_B200_SOSEX_SEG")) h->sosex_seg = std::max(1, std::atoi(sg));
   if (const char* rg = std::getenv("RPA_B200_RING_SEG")) h->ring_seg = std::max(1, std::atoi(rg));
   for (auto& e : h->ev) cudaEventCreate(&e);
@@ -2171,8 +2183,91 @@ int rpa_b200_thc_r(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, 
   return exception_status(h);
 }
 
-// RPA energy from THC factors (the FullRkai branch of rpa_THC_PiU, src/rpa/rpa_THC.f90:215-329):
-// R is formed on the device and handed to the energy path; it never leaves the GPU.
+// Split-BF16 Pi build straight from THC factors, the way rpa_THC_PiU_BlockAlgo forms and
+// contracts R block by block (src/rpa/rpa_THC.f90:285-340, 374-403): the ai columns are taken in
+// pieces; for each piece the Khatri-Rao block YX = Xa * Xi of its columns, one FP64 DMMA GEMM
+// R_piece = Z^T YX, the scale/split pass into piece-sized bf16 operands and the tensor-core SYRK
+// adding the piece into Pi (FP64).  Neither the whole R nor the whole split operands are held:
+// the device holds one piece of each (the piece width is sized to h->thc_piece_bytes).  The exact
+// diagonal is summed over the pieces and written by the last piece's SYRK.
+int build_pi_thc(rpa_b200_handle* h, const Validated& v, int64_t NGrid, const double* Zd, int64_t ldz,
+                 const double* Xad, int64_t ldxa, const double* Xid, int64_t ldxi, double alpha) {
+  const int NQ = v.NQ, K = v.K;
+  const int64_t nov = v.nov;
+  const size_t per_col = (size_t)NQ * 8 + (size_t)NGrid * 8 + (size_t)4 * K * NQ;  // R, YX, hi + lo
+  int64_t w = (int64_t)(h->thc_piece_bytes / per_col) / 128 * 128;
+  w = std::max<int64_t>(128, std::min<int64_t>(w, (nov + 127) / 128 * 128));
+  const int64_t pitch = w;  // a multiple of 8 bf16 (16 bytes)
+  RPA_CUDA(h, ensure(h->thR, (size_t)NQ * w * 8));
+  RPA_CUDA(h, ensure(h->thYX, (size_t)NGrid * w * 8));
+  RPA_CUDA(h, ensure(h->Xhi, (size_t)K * NQ * pitch * 2));
+  RPA_CUDA(h, ensure(h->Xlo, (size_t)K * NQ * pitch * 2));
+  RPA_CUDA(h, ensure(h->Pi, (size_t)K * NQ * NQ * 8));
+  RPA_CUDA(h, ensure(h->diag, (size_t)2 * K * NQ * 8));
+  double* Rp = static_cast<double*>(h->thR.p);
+  double* YX = static_cast<double*>(h->thYX.p);
+  double* Pi = static_cast<double*>(h->Pi.p);
+  double* dsum = static_cast<double*>(h->diag.p);        // exact diagonal summed over the pieces
+  double* dpiece = dsum + (size_t)K * NQ;                 // this piece's exact diagonal
+  const double* D = static_cast<const double*>(h->D.p);
+  rpa::FreqGroup fg{};
+  fg.n = K;
+  for (int k = 0; k < K; ++k) fg.u2[k] = v.freqs[k] * v.freqs[k];
+  RPA_CUDA(h, cudaMemsetAsync(h->count_dev, 0, sizeof(int), h->stream));
+  int s;
+  for (int64_t a0 = 0; a0 < nov; a0 += w) {
+    const int64_t wp = std::min(w, nov - a0);
+    const bool first = a0 == 0, last = a0 + wp == nov;
+    cudaEvent_t e0 = pool_event(h), e1 = pool_event(h), e2 = pool_event(h);
+    RPA_CUDA(h, rpa::launch_khatri_rao_cols(Xad, ldxa, Xid, ldxi, (int)NGrid, (int)v.nv, a0, wp, YX, h->stream));
+    RPA_CUDA(h, rpa::launch_gemm_f64(gemm_tn(NQ, (int)wp, NGrid, Zd, ldz, YX, NGrid, Rp, NQ), h->stream));
+    RPA_CUDA(h, rpa::launch_count_nonfinite(Rp, (int64_t)NQ * wp, h->count_dev, h->stream));
+    const rpa::SplitPlan plan = rpa::plan_scale_split(NQ, wp, h->num_sms);
+    RPA_CUDA(h, ensure(h->diag_part, (size_t)plan.nsplit * K * NQ * 8));
+    CUtensorMap sHi, sLo, mAh, mAl, mBh, mBl;
+    if ((s = encode_store_maps(h, &sHi, &sLo, h->Xhi.p, h->Xlo.p, wp, NQ, K, pitch)) != RPA_OK) return s;
+    if ((s = encode_map(h, &mAh, h->Xhi.p, wp, NQ, K, pitch, rpa::kSyrkTcTM)) != RPA_OK) return s;
+    if ((s = encode_map(h, &mAl, h->Xlo.p, wp, NQ, K, pitch, rpa::kSyrkTcTM)) != RPA_OK) return s;
+    if ((s = encode_map(h, &mBh, h->Xhi.p, wp, NQ, K, pitch, rpa::kSyrkTcTN)) != RPA_OK) return s;
+    if ((s = encode_map(h, &mBl, h->Xlo.p, wp, NQ, K, pitch, rpa::kSyrkTcTN)) != RPA_OK) return s;
+    RPA_CUDA(h, cudaEventRecord(e0, h->stream));
+    RPA_CUDA(h, rpa::launch_scale_split(Rp, NQ, NQ, wp, D + a0, fg, alpha, &sHi, &sLo,
+                                        static_cast<double*>(h->diag_part.p), dpiece, plan, h->err_dev, h->stream));
+    RPA_CUDA(h, rpa::launch_add_into(dsum, dpiece, (int64_t)K * NQ, first, h->stream));
+    RPA_CUDA(h, cudaEventRecord(e1, h->stream));
+    h->split_ev.push_back({e0, e1});
+    rpa::SyrkTcArgs a{};
+    a.NQ = NQ;
+    a.nov = wp;
+    a.kg = K;
+    a.Pi = Pi;
+    a.ldPi = NQ;
+    a.piStride = (int64_t)NQ * NQ;
+    a.diag = last ? dsum : nullptr;
+    a.err = h->err_dev;
+    a.seg_chunks = h->seg_chunks;
+    a.chunk0 = 0;
+    a.nov_part = wp;
+    a.accumulate = first ? 0 : 1;
+    if ((s = prepare_sync(h, NQ, K, wp, &a.sync)) != RPA_OK) return s;
+    a.sync_every = h->sync_every;
+    a.sync_lag = 2;
+    RPA_CUDA(h, rpa::launch_syrk_split_bf16(&mAh, &mAl, &mBh, &mBl, a, h->num_sms, h->stream));
+    RPA_CUDA(h, cudaEventRecord(e2, h->stream));
+    h->tc_ev.push_back({e1, e2});
+  }
+  int cnt = 0;
+  RPA_CUDA(h, cudaMemcpyAsync(&cnt, h->count_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (cnt) return fail(h, RPA_ERR_NONFINITE, "%d non-finite entries in the Cholesky vectors formed from the THC factors",
+                       cnt);
+  return RPA_OK;
+}
+
+// RPA energy from THC factors (the FullRkai branch of rpa_THC_PiU, src/rpa/rpa_THC.f90:215-329).
+// Split precision with up to 16 frequencies: R is formed and contracted piece by piece
+// (build_pi_thc).  Otherwise (FP64 form, or more frequencies than one split group) R is formed
+// whole on the device and handed to the energy path; it never leaves the GPU.
 int rpa_b200_ec_thc(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, int64_t NVirt, const double* Zgk,
                     int64_t ldZ, const double* Xga, int64_t ldXa, const double* Xgi, int64_t ldXi,
                     const double* OccEnergies, const double* VirtEnergies, int64_t NFreqs, const double* Freqs,
@@ -2187,6 +2282,21 @@ int rpa_b200_ec_thc(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc,
   if ((s = stage_matrix(h, h->thZ, Zgk, ldZ, NGrid, NQ, &Zd, &ldz))) return s;
   if ((s = stage_matrix(h, h->thXa, Xga, ldXa, NGrid, NVirt, &Xad, &ldxa))) return s;
   if ((s = stage_matrix(h, h->thXi, Xgi, ldXi, NGrid, NOcc, &Xid, &ldxi))) return s;
+  if (prec == RPA_PREC_SPLIT_BF16 && NFreqs >= 1 && NFreqs <= rpa::kMaxKgLaunch) {
+    Validated v;
+    // R itself is formed below: the factor Z stands in for the R argument of the common checks
+    if ((s = validate_common(h, NQ, NOcc, NVirt, Zd, NQ, OccEnergies, VirtEnergies, NFreqs, Freqs, alpha, prec, v)))
+      return s;
+    if (!FreqWeights || !Ec) return fail(h, RPA_ERR_INVALID_ARG, "FreqWeights or Ec is NULL");
+    if ((s = fetch_small(h, FreqWeights, NFreqs, v.weights))) return s;
+    if ((s = stage_eps(h, v))) return s;
+    RPA_CUDA(h, cudaEventRecord(h->ev[1], h->stream));
+    if ((s = build_pi_thc(h, v, NGrid, Zd, ldz, Xad, ldxa, Xid, ldxi, alpha))) return s;
+    if ((s = energy_from_workspace(h, v.NQ, v.K, v.weights, Ec, Eu))) return s;
+    RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+    finish_timings(h);
+    return RPA_OK;
+  }
   RPA_CUDA(h, ensure(h->thR, (size_t)NQ * nov * 8));
   double* Rd = static_cast<double*>(h->thR.p);
   if ((s = form_thc_r(h, NGrid, NQ, NOcc, NVirt, Zd, ldz, Xad, ldxa, Xid, ldxi, Rd, NQ))) return s;
@@ -2637,27 +2747,20 @@ int rpa_b200_jctc2024(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOc
   return exception_status(h);
 }
 
-int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* inst, int64_t prec, double* Ec,
-                        double* Eu) try {
-  int s = begin_call(h);
-  if (s != RPA_OK) return s;
-  if (ninst < 1 || ninst > (1 << 24) || !inst || !Ec)
-    return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_ec_batched");
-  if (prec != RPA_PREC_FP64 && prec != RPA_PREC_SPLIT_BF16)
-    return fail(h, RPA_ERR_INVALID_ARG, "unknown precision mode %lld", (long long)prec);
+// The batched energies of instances with at most kMaxKgLaunch frequencies each (one frequency group
+// per instance).  Called by rpa_b200_ec_batched after begin_call and the argument checks.
+static int ec_batched_groups(rpa_b200_handle* h, int64_t ninst, const rpa_instance* inst, int64_t prec, double* Ec,
+                             double* Eu) {
+  int s = RPA_OK;
   const int n = (int)ninst;
   std::vector<Validated> v(n);
   std::vector<int64_t> eu_off(n + 1, 0);
   size_t host_R = 0, total_nov = 0;
   for (int i = 0; i < n; ++i) {
     const rpa_instance& I = inst[i];
-    if ((s = check_arrays(h, {I.R, I.OccEnergies, I.VirtEnergies, I.Freqs, I.FreqWeights})))
-      return fail(h, s, "instance %d: %s", i, h->last_error.c_str());
     if ((s = validate_common(h, I.NQ, I.NOcc, I.NVirt, I.R, I.ldR, I.OccEnergies, I.VirtEnergies, I.NFreqs, I.Freqs,
                              I.alpha, prec, v[i])))
       return fail(h, s, "instance %d: %s", i, h->last_error.c_str());
-    if (I.NFreqs > rpa::kMaxKgLaunch)
-      return fail(h, RPA_ERR_INVALID_ARG, "instance %d: NFreqs > %d in a batched call", i, rpa::kMaxKgLaunch);
     if (!I.FreqWeights) return fail(h, RPA_ERR_INVALID_ARG, "instance %d: FreqWeights is NULL", i);
     if ((s = fetch_small(h, I.FreqWeights, I.NFreqs, v[i].weights))) return s;
     eu_off[i + 1] = eu_off[i] + I.NFreqs;
@@ -2908,10 +3011,7 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
           j.fg.n = K;
           for (int k = 0; k < K; ++k) j.fg.u2[k] = v[i].freqs[k] * v[i].freqs[k];
           j.alpha = inst[i].alpha;
-          j.Xhi = xh;
-          j.Xlo = xl;
-          j.pitch = per[i].pitch;
-          j.kstride = (int64_t)NQ * per[i].pitch;
+          if ((s = encode_store_maps(h, &j.tm_hi, &j.tm_lo, xh, xl, nov, NQ, K, per[i].pitch))) return s;
           j.diag_part = dpart;
           j.ai_per_split = per[i].plan.ai_per_split;
           j.nsplit = per[i].plan.nsplit;
@@ -3020,7 +3120,8 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
     auto split_pass = [&](const BatchDev& dv, cudaStream_t st) {
       cudaError_t r = cudaSuccess;
       if (dv.sync_words > 0) r = cudaMemsetAsync(dv.msync, 0, (size_t)dv.sync_words * sizeof(int), st);
-      if (r == cudaSuccess) r = rpa::launch_scale_split_multi(dv.jobs, dv.work, dv.nwork, dv.offs, dv.ni, dv.offs_total, st);
+      if (r == cudaSuccess) r = rpa::launch_scale_split_multi(dv.jobs, dv.work, dv.nwork, dv.offs, dv.ni, dv.offs_total,
+                                                           h->err_dev, st);
       return r;
     };
     auto logdet = [&](const BatchDev& dv) {
@@ -3127,6 +3228,51 @@ int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* i
     Ec[i] = ec.hi + ec.lo;
   }
   finish_timings(h);
+  return RPA_OK;
+}
+
+// Instances with more than kMaxKgLaunch frequencies (the reference allows up to 64 points,
+// src/rpa/rpa_definitions.f90:109-110) run as consecutive frequency groups of at most
+// kMaxKgLaunch points, each group a sub-instance on the same R; E(u) of the groups are already in
+// the caller's order, and an instance's E_c is the sum of its groups' (a sum over frequencies).
+int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* inst, int64_t prec, double* Ec,
+                        double* Eu) try {
+  int s = begin_call(h);
+  if (s != RPA_OK) return s;
+  if (ninst < 1 || ninst > (1 << 24) || !inst || !Ec)
+    return fail(h, RPA_ERR_INVALID_ARG, "invalid argument to rpa_b200_ec_batched");
+  if (prec != RPA_PREC_FP64 && prec != RPA_PREC_SPLIT_BF16)
+    return fail(h, RPA_ERR_INVALID_ARG, "unknown precision mode %lld", (long long)prec);
+  bool wide = false;
+  for (int64_t i = 0; i < ninst; ++i) {
+    if (inst[i].NFreqs < 1 || inst[i].NFreqs > 64)
+      return fail(h, RPA_ERR_INVALID_ARG, "instance %lld: NFreqs=%lld not in [1,64]", (long long)i,
+                  (long long)inst[i].NFreqs);
+    if (!inst[i].Freqs || !inst[i].FreqWeights)
+      return fail(h, RPA_ERR_INVALID_ARG, "instance %lld: Freqs or FreqWeights is NULL", (long long)i);
+    const rpa_instance& I = inst[i];
+    if ((s = check_arrays(h, {I.R, I.OccEnergies, I.VirtEnergies, I.Freqs, I.FreqWeights})))
+      return fail(h, s, "instance %lld: %s", (long long)i, h->last_error.c_str());
+    wide = wide || inst[i].NFreqs > rpa::kMaxKgLaunch;
+  }
+  if (!wide) return ec_batched_groups(h, ninst, inst, prec, Ec, Eu);
+  std::vector<rpa_instance> groups;
+  std::vector<int64_t> owner;
+  for (int64_t i = 0; i < ninst; ++i)
+    for (int64_t k0 = 0; k0 < inst[i].NFreqs; k0 += rpa::kMaxKgLaunch) {
+      rpa_instance g = inst[i];
+      g.NFreqs = std::min<int64_t>(rpa::kMaxKgLaunch, inst[i].NFreqs - k0);
+      g.Freqs = inst[i].Freqs + k0;
+      g.FreqWeights = inst[i].FreqWeights + k0;
+      groups.push_back(g);
+      owner.push_back(i);
+    }
+  if (groups.size() > (size_t)(1 << 24)) return fail(h, RPA_ERR_INVALID_ARG, "too many frequency groups");
+  std::vector<double> eg(groups.size());
+  if ((s = ec_batched_groups(h, (int64_t)groups.size(), groups.data(), prec, eg.data(), Eu))) return s;
+  std::vector<dd> acc((size_t)ninst, dd{0.0, 0.0});
+  for (size_t j = 0; j < groups.size(); ++j) acc[owner[j]] = rpa::dd_add(acc[owner[j]], eg[j]);
+  for (int64_t i = 0; i < ninst; ++i) Ec[i] = acc[i].hi + acc[i].lo;
   return RPA_OK;
 } catch (...) {
   return exception_status(h);

@@ -4,6 +4,7 @@
 #include <cstdint>
 #include <vector>
 #include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 
@@ -30,8 +31,15 @@ struct SplitPlan {
 
 SplitPlan plan_scale_split(int NQ, int64_t nov, int num_sms);
 
+// Store views of the split operands X_hi / X_lo written by the scale/split pass: 3-D (ai, Q, k)
+// bf16 with row pitch `pitch` (a multiple of 8) and frequency stride pitch * NQ, boxes of 64 ai x
+// 32 Q, 128-byte swizzle.  Returns cudaErrorInvalidValue when the driver rejects the map.
+cudaError_t encode_split_store_map(PFN_cuTensorMapEncodeTiled_v12000 encode, CUtensorMap* m, void* base,
+                                   int64_t nov, int NQ, int kg, int64_t pitch);
+
 // One instance of a multi-instance scale/split launch.
 struct SplitJob {
+  CUtensorMap tm_hi, tm_lo;  // store views of this instance's X_hi / X_lo (encode_split_store_map)
   const double* R;
   int64_t ldR;
   int NQ;
@@ -39,31 +47,28 @@ struct SplitJob {
   const double* D;
   FreqGroup fg;
   double alpha;
-  __nv_bfloat16* Xhi;
-  __nv_bfloat16* Xlo;
-  int64_t pitch, kstride;
   double* diag_part;
   int64_t ai_per_split;
   int nsplit;
   double* diag;  // [fg.n][NQ]
 };
 // work[b] = (job, q tile, ai split, 0); offsets[j] = sum_{i<j} fg.n * NQ of job i, total = sum.
+// A bounded wait that expires records its code in *err.
 cudaError_t launch_scale_split_multi(const SplitJob* jobs, const int4* work, int nwork, const int64_t* offsets,
-                                     int njobs, int64_t total, cudaStream_t stream);
+                                     int njobs, int64_t total, int* err, cudaStream_t stream);
 
-// X_k = sqrt(alpha c_k) R split into bf16 hi/lo rows (Q-major rows, ai
-// contiguous, row pitch `pitch`, frequency stride `kstride` elements), plus
-// the exact FP64 diagonal diag[k*NQ + Q] = sum_ai X_k(Q,ai)^2.
+// X_k = sqrt(alpha c_k) R split into bf16 hi/lo rows (Q-major rows, ai contiguous, written
+// through the store views tm_hi / tm_lo), plus the exact FP64 diagonal
+// diag[k*NQ + Q] = sum_ai X_k(Q,ai)^2.
 cudaError_t launch_scale_split(const double* R, int64_t ldR, int NQ, int64_t nov, const double* D,
-                               const FreqGroup& fg, double alpha, __nv_bfloat16* Xhi, __nv_bfloat16* Xlo,
-                               int64_t pitch, int64_t kstride, double* diag_part, double* diag,
-                               const SplitPlan& plan, cudaStream_t stream);
+                               const FreqGroup& fg, double alpha, const CUtensorMap* tm_hi, const CUtensorMap* tm_lo,
+                               double* diag_part, double* diag, const SplitPlan& plan, int* err, cudaStream_t stream);
 // The splits split0 .. split1-1 of the same pass (ai columns split*ai_per_split ..), without the
 // diagonal reduction; launch_diag_reduce completes the diagonal once every split has run.
 cudaError_t launch_scale_split_part(const double* R, int64_t ldR, int NQ, int64_t nov, const double* D,
-                                    const FreqGroup& fg, double alpha, __nv_bfloat16* Xhi, __nv_bfloat16* Xlo,
-                                    int64_t pitch, int64_t kstride, double* diag_part, const SplitPlan& plan,
-                                    int split0, int split1, cudaStream_t stream);
+                                    const FreqGroup& fg, double alpha, const CUtensorMap* tm_hi,
+                                    const CUtensorMap* tm_lo, double* diag_part, const SplitPlan& plan, int split0,
+                                    int split1, int* err, cudaStream_t stream);
 cudaError_t launch_diag_reduce(const double* diag_part, const SplitPlan& plan, int kg, int NQ, double* diag,
                                cudaStream_t stream);
 
@@ -299,6 +304,11 @@ constexpr int kDotPartials = 64;
 cudaError_t launch_dot_partials(const double* A, int64_t lda, const double* B, int64_t ldb, int rows, int cols,
                                 const double* w, double* out, cudaStream_t stream);
 // YX(g, a + nv*ii) = Xa(g, a) Xi(g, i0 + ii) for ii < ni (YX: ngrid x nv*ni, ld ngrid).
+// YX(g, c) = Xa(g, a) Xi(g, i) for the ai columns ai0 .. ai0 + ncols - 1 (ai = a + nv i), ld ngrid.
+cudaError_t launch_khatri_rao_cols(const double* Xa, int64_t ldXa, const double* Xi, int64_t ldXi, int ngrid, int nv,
+                                   int64_t ai0, int64_t ncols, double* YX, cudaStream_t stream);
+// dst[j] += src[j] for j < n (first: dst[j] = src[j]).
+cudaError_t launch_add_into(double* dst, const double* src, int64_t n, bool first, cudaStream_t stream);
 cudaError_t launch_khatri_rao(const double* Xa, int64_t ldXa, const double* Xi, int64_t ldXi, int ngrid, int nv,
                               int i0, int ni, double* YX, cudaStream_t stream);
 // A(i, i) += s * fro2[0]  (shift of a Gram matrix by a multiple of a device-side norm).

@@ -329,6 +329,22 @@ __global__ void khatri_rao_kernel(const double* Xa, int64_t ldXa, const double* 
   YX[idx] = Xa[g + ldXa * a] * Xi[g + ldXi * (i0 + ii)];
 }
 
+// Khatri-Rao block of an ai column range: YX(g, c) = Xa(g, a) Xi(g, i) for ai = ai0 + c = a + nv i.
+__global__ void khatri_rao_cols_kernel(const double* Xa, int64_t ldXa, const double* Xi, int64_t ldXi, int ngrid,
+                                       int nv, int64_t ai0, int64_t ncols, double* YX) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)ngrid * ncols) return;
+  const int64_t g = idx % ngrid, ai = ai0 + idx / ngrid;
+  const int64_t a = ai % nv, i = ai / nv;
+  YX[idx] = Xa[g + ldXa * a] * Xi[g + ldXi * i];
+}
+
+// dst[j] += src[j] (first: dst[j] = src[j])
+__global__ void add_into_kernel(double* dst, const double* src, int64_t n, int first) {
+  const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < n) dst[j] = first ? src[j] : dst[j] + src[j];
+}
+
 // A(i, i) += s * (*fro2) for i < n  (fro2: a device scalar, e.g. ||Y||_F^2)
 __global__ void add_diag_scaled_kernel(double* A, int64_t lda, int n, double s, const double* fro2) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -475,6 +491,20 @@ cudaError_t launch_khatri_rao(const double* Xa, int64_t ldXa, const double* Xi, 
                               int i0, int ni, double* YX, cudaStream_t stream) {
   const int64_t total = (int64_t)ngrid * nv * ni;
   khatri_rao_kernel<<<blocks_for(total), 256, 0, stream>>>(Xa, ldXa, Xi, ldXi, ngrid, nv, i0, ni, YX);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_khatri_rao_cols(const double* Xa, int64_t ldXa, const double* Xi, int64_t ldXi, int ngrid, int nv,
+                                   int64_t ai0, int64_t ncols, double* YX, cudaStream_t stream) {
+  const int64_t total = (int64_t)ngrid * ncols;
+  khatri_rao_cols_kernel<<<blocks_for(total), 256, 0, stream>>>(Xa, ldXa, Xi, ldXi, ngrid, nv, ai0, ncols, YX);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_add_into(double* dst, const double* src, int64_t n, bool first, cudaStream_t stream) {
+  add_into_kernel<<<blocks_for(n), 256, 0, stream>>>(dst, src, n, first ? 1 : 0);
   ++g_launches;
   return cudaGetLastError();
 }

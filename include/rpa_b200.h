@@ -23,8 +23,9 @@
  * Limits (checked before any GPU work):
  *   - 1 <= NQ <= 2^20 and 1 <= NFreqs <= 64 (RPA_ERR_INVALID_ARG otherwise);
  *   - NOcc * NVirt <= 2^31 - 1 (RPA_ERR_TOO_LARGE);
- *   - at most 16 frequencies per instance in rpa_b200_ec_batched, at most 2^24
- *     instances per call (RPA_ERR_INVALID_ARG);
+ *   - at most 64 frequencies per instance in rpa_b200_ec_batched (the
+ *     reference's limit), at most 2^24 instances (and frequency groups of 16)
+ *     per call (RPA_ERR_INVALID_ARG);
  *   - N <= 46340 in rpa_b200_syevd and NQ <= 46340 in rpa_b200_piu_basis (an
  *     N x N FP64 matrix indexed in 32-bit); GEMM dimensions of the T2, exchange,
  *     THC and JCTC paths <= 2^31 - 1 (RPA_ERR_TOO_LARGE);
@@ -250,7 +251,7 @@ typedef struct rpa_instance {
   int64_t ldR;
   const double* OccEnergies;
   const double* VirtEnergies;
-  int64_t NFreqs; /* <= 16 */
+  int64_t NFreqs; /* 1 .. 64 */
   const double* Freqs;
   const double* FreqWeights;
   double alpha;
@@ -263,7 +264,9 @@ typedef struct rpa_instance {
  * memory-bounded batches; per batch one multi-instance scale/split launch, one
  * persistent multi-instance tensor-core SYRK launch and one variable-order
  * batched Cholesky run as a single CUDA graph.  Ec[i] receives the energy of
- * instance i; Eu (may be NULL) the E(u) of all instances concatenated.
+ * instance i; Eu (may be NULL) the E(u) of all instances concatenated.  An
+ * instance with more than 16 frequencies runs as consecutive groups of at
+ * most 16 frequencies on the same R (E_c summed over its groups).
  */
 int rpa_b200_ec_batched(rpa_b200_handle* h, int64_t ninst, const rpa_instance* inst, int64_t prec, double* Ec,
                         double* Eu);

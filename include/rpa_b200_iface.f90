@@ -19,7 +19,7 @@ module rpa_b200_iface
             type(c_ptr) :: R                 ! c_loc(Rkai): NQ x NOcc*NVirt, leading dimension ldR
             integer(c_int64_t) :: ldR
             type(c_ptr) :: OccEnergies, VirtEnergies
-            integer(c_int64_t) :: NFreqs     ! <= 16
+            integer(c_int64_t) :: NFreqs     ! 1 .. 64
             type(c_ptr) :: Freqs, FreqWeights
             real(c_double) :: alpha
       end type rpa_instance

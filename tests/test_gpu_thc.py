@@ -30,3 +30,24 @@ def test_ec_thc_matches_oracle(handle, prec, tol):
     ec, eu = handle.ec_thc(Z, Xa, Xi, eo, ev, x, w, prec=prec)
     assert abs(ec - ref) < tol
     assert np.max(np.abs(eu - ref_eu)) < 10 * tol
+
+
+@pytest.mark.parametrize("piece_bytes", [None, 3 * 1024 * 1024])
+def test_ec_thc_pieces_never_hold_whole_R(pkg, monkeypatch, piece_bytes):
+    # split precision: R is formed and contracted piece by piece (Khatri-Rao block, FP64 GEMM,
+    # scale/split, tensor-core SYRK adding into Pi); with a small piece budget the build runs in
+    # many pieces and the device holds far less than R plus its split operands
+    Z, Xa, Xi, eo, ev = O.make_thc_factors(512, 128, 16, 200, 13)
+    R = O.thc_r(Z, Xa, Xi)
+    x, w = O.casimir_polder(12, 0.7)
+    ref, _ = O.ec_rpa(R, eo, ev, x, w)
+    if piece_bytes:
+        monkeypatch.setenv("RPA_B200_THC_PIECE_BYTES", str(piece_bytes))
+    with pkg.Handle(0) as h:
+        ec, _ = h.ec_thc(Z, Xa, Xi, eo, ev, x, w, prec="split")
+        used, _ = h.workspace_bytes()
+    assert abs(ec - ref) < 1e-6
+    whole = R.nbytes + 4 * len(x) * R.size  # R in FP64 + its hi/lo operands for every frequency
+    if piece_bytes:
+        # 3200 ai columns in pieces of 256: the pieces' buffers, Pi and the staged factors only
+        assert used < 0.5 * whole, (used, whole)
