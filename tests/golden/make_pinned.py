@@ -81,13 +81,16 @@ def make_mbe_sample():
         Rt *= f
         x, w = grid(eo, ev, K)
         nfrag = P.fragments(i)
-        energies = []
+        energies, energies_chol = [], []
         for frags in P.subsystems(nfrag):
             Rs, eos, evs = P.subsystem(Rt, eo, ev, frags, nfrag)
-            energies.append(O.ec_rpa(Rs.T, eos, evs, x, w)[0])
+            pi = O.pi_matrices(Rs.T, eos, evs, x)
+            energies.append(O.ec_rpa_analytic(pi, w)[0])
+            energies_chol.append(O.ec_rpa_analytic(pi, w, logdet=O.logdet_cholesky)[0])
         eint = O.mbe_energy(nfrag, np.array(energies))
         out[str(i)] = dict(factor=f, freqs=x.tolist(), weights=w.tolist(), nfrag=nfrag, energies=energies,
-                           Eint=eint, R=checksum(Rt))
+                           Eint=eint, energies_cholesky=energies_chol,
+                           Eint_cholesky=O.mbe_energy(nfrag, np.array(energies_chol)), R=checksum(Rt))
         print(f"mbe {i}: NQ={Rt.shape[1]} nov={Rt.shape[0]} K={K} frags={nfrag} Eint={eint:.3e} "
               f"({time.time() - t:.0f} s)", flush=True)
     return out
