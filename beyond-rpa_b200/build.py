@@ -18,7 +18,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 INCLUDE = HERE.parent / "include"
 LIB = HERE / "librpa_b200.so"
-SOURCES = ["capi.cu", "scale_split.cu", "syrk_tc.cu", "dsyrk_f64.cu", "logdet.cu", "freq_grid.cu", "noalloc.cu", "gemm_f64.cu", "t2_kernels.cu", "sosex.cu", "sosex_tc.cu", "syevd.cu", "selftest.cu"]
+SOURCES = ["capi.cu", "scale_split.cu", "syrk_tc.cu", "dsyrk_f64.cu", "logdet.cu", "freq_grid.cu", "noalloc.cu", "gemm_f64.cu", "t2_kernels.cu", "sosex.cu", "sosex_tc.cu", "syevd.cu", "selftest.cu", "ozaki.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

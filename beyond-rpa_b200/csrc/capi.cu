@@ -110,10 +110,17 @@ struct rpa_b200_handle {
     double* Ldiag;
     cudaStream_t stream;
     int nb2, tile_w;
+    int oz;  // digits of the int8 trailing updates (0: DMMA)
     cudaGraphExec_t exec;
     int64_t launches;
   };
   std::vector<CholGraph> chol_graphs;
+  // int8 tensor-core trailing updates of the log-det (ozaki.cu): two digit-plane buffers and
+  // their tensor maps, set up for one (order, matrices, panel width) at a time
+  DevBuf ozBuf[2];
+  rpa::OzakiWork ozw;
+  int oz_n = 0, oz_nmat = 0;
+  int ozaki_slices = 0;  // digits per entry of the int8 updates (RPA_B200_OZAKI_SLICES: 7 or 8; 0: DMMA)
   // tile plans of the FP64 log-det per bucket of 256 matrix orders (tuned or set)
   std::map<int, rpa::LogdetPlan> logdet_plans;
   uint64_t plans_version = 0;  // bumped on every change (part of the batched graph key)
@@ -647,12 +654,47 @@ int tune_single(rpa_b200_handle* h, int n, int nmat) {
 // Blocked Cholesky of nmat matrices through a cached CUDA graph (the launch
 // sequence depends only on the arguments; ~6 launches per 64 columns would
 // otherwise leave the GPU idle between the small late-step kernels).
+// The int8 digit-plane buffers for nmat matrices of order n and the plan's panel width (nullptr:
+// the trailing updates stay on DMMA).  Reallocating them invalidates the captured Cholesky graphs,
+// which hold their addresses.
+const rpa::OzakiWork* ozaki_for(rpa_b200_handle* h, int n, int nmat, const rpa::LogdetPlan& plan) {
+  const int S = h->ozaki_slices;
+  if (S == 0 || n < 2 * plan.nb2 || plan.nb2 > 512) return nullptr;
+  if (h->ozw.S == S && h->ozw.K == plan.nb2 && h->oz_n == n && h->oz_nmat == nmat) return &h->ozw;
+  const size_t bytes = rpa::ozaki_buffer_bytes(n, nmat, plan.nb2, S);
+  bool grew = false;
+  for (DevBuf& b : h->ozBuf)
+    if (b.bytes < bytes) {
+      cudaStreamSynchronize(h->stream);
+      if (ensure(b, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        h->ozw.S = 0;
+        return nullptr;  // no room: DMMA updates
+      }
+      grew = true;
+    }
+  if (grew) {
+    for (auto& g : h->chol_graphs) cudaGraphExecDestroy(g.exec);
+    h->chol_graphs.clear();
+  }
+  void* bufs[2] = {h->ozBuf[0].p, h->ozBuf[1].p};
+  if (rpa::ozaki_setup(h->ozw, h->encode, bufs, n, nmat, plan.nb2, S) != cudaSuccess) {
+    h->ozw.S = 0;
+    return nullptr;
+  }
+  h->ozw.num_sms = h->num_sms;
+  h->oz_n = n;
+  h->oz_nmat = nmat;
+  return &h->ozw;
+}
+
 int cholesky(rpa_b200_handle* h, double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag) {
   if (int ts = tune_single(h, n, nmat)) return ts;
   const rpa::LogdetPlan plan = plan_for(h, n);
+  const rpa::OzakiWork* oz = ozaki_for(h, n, nmat, plan);
   for (auto& g : h->chol_graphs) {
     if (g.A == A && g.ld == ld && g.stride == stride && g.n == n && g.nmat == nmat && g.Ldiag == Ldiag &&
-        g.stream == h->stream && g.nb2 == plan.nb2 && g.tile_w == plan.tile_w) {
+        g.stream == h->stream && g.nb2 == plan.nb2 && g.tile_w == plan.tile_w && g.oz == (oz ? oz->S : 0)) {
       RPA_CUDA(h, cudaGraphLaunch(g.exec, h->stream));
       rpa::g_launches += g.launches;
       return RPA_OK;
@@ -662,7 +704,7 @@ int cholesky(rpa_b200_handle* h, double* A, int64_t ld, int64_t stride, int n, i
   cudaGraph_t graph = nullptr;
   if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
     cudaError_t e = rpa::launch_cholesky_lower(A, ld, stride, n, nmat, Ldiag, h->err_dev, h->stream, plan,
-                                               h->lookahead ? &h->la[0] : nullptr);
+                                               h->lookahead ? &h->la[0] : nullptr, oz);
     cudaError_t e2 = cudaStreamEndCapture(h->stream, &graph);
     const int64_t count = rpa::g_launches - before;
     rpa::g_launches = before;
@@ -674,7 +716,8 @@ int cholesky(rpa_b200_handle* h, double* A, int64_t ld, int64_t stride, int n, i
         cudaGraphExecDestroy(h->chol_graphs.front().exec);
         h->chol_graphs.erase(h->chol_graphs.begin());
       }
-      h->chol_graphs.push_back({A, ld, stride, n, nmat, Ldiag, h->stream, plan.nb2, plan.tile_w, exec, count});
+      h->chol_graphs.push_back(
+          {A, ld, stride, n, nmat, Ldiag, h->stream, plan.nb2, plan.tile_w, oz ? oz->S : 0, exec, count});
       RPA_CUDA(h, cudaGraphLaunch(exec, h->stream));
       rpa::g_launches += count;
       return RPA_OK;
@@ -685,7 +728,7 @@ int cholesky(rpa_b200_handle* h, double* A, int64_t ld, int64_t stride, int n, i
     cudaGetLastError();
   }
   // capture unavailable on this stream: launch the same kernels directly
-  RPA_CUDA(h, rpa::launch_cholesky_lower(A, ld, stride, n, nmat, Ldiag, h->err_dev, h->stream, plan));
+  RPA_CUDA(h, rpa::launch_cholesky_lower(A, ld, stride, n, nmat, Ldiag, h->err_dev, h->stream, plan, nullptr, oz));
   return RPA_OK;
 }
 
@@ -1046,6 +1089,7 @@ int rpa_b200_create(rpa_b200_handle** handle, int64_t device, int64_t flags) try
   for (auto& e : h->ev) cudaEventCreate(&e);
   for (auto& e : h->fork_ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
   if (const char* la = std::getenv("RPA_B200_LOOKAHEAD")) h->lookahead = std::atoi(la) != 0;
+  h->ozaki_slices = rpa::ozaki_slices_default();
   {
     int least = 0, greatest = 0;
     cudaDeviceGetStreamPriorityRange(&least, &greatest);
@@ -1086,7 +1130,7 @@ int rpa_b200_destroy(rpa_b200_handle* h) try {
                     &h->jU, &h->jL, &h->jX, &h->jPno, &h->jWork,
                     &h->jPack, &h->jQS, &h->jS, &h->jD, &h->syncBuf,
                     &h->jT, &h->jM, &h->jV, &h->jMap, &h->jSK, &h->tune, &h->sxR, &h->sxU, &h->sxP,
-                    &h->t2Z, &h->t2M, &h->t2Sync})
+                    &h->t2Z, &h->t2M, &h->t2Sync, &h->ozBuf[0], &h->ozBuf[1]})
     release(*b);
   for (auto e : h->bgraph.execs) cudaGraphExecDestroy(e);
   if (h->err_dev) cudaFree(h->err_dev);

@@ -187,8 +187,32 @@ struct Lookahead {
   cudaStream_t crit, rest;
   cudaEvent_t ev[4];
 };
+// FP64-accurate trailing updates on the int8 tensor cores (ozaki.cu): digit planes of the current
+// panel (two buffers, alternating by outer block) and their tensor maps.
+struct OzakiWork {
+  int S = 0;  // digits per entry (7 or 8); 0: updates stay on DMMA
+  int K = 0;  // panel width (the plan's outer block)
+  int8_t* slices[2] = {nullptr, nullptr};
+  int* expo[2] = {nullptr, nullptr};
+  CUtensorMap mapA[2], mapB[2];
+  int num_sms = 0;
+};
+int ozaki_slices_default();  // 0 (DMMA updates) unless RPA_B200_OZAKI_SLICES = 7 or 8
+// Bytes of one of the two buffers for nmat matrices of order n, panel width K, S digits.
+size_t ozaki_buffer_bytes(int n, int nmat, int K, int S);
+cudaError_t ozaki_setup(OzakiWork& w, PFN_cuTensorMapEncodeTiled_v12000 encode, void* const buf[2], int n, int nmat,
+                        int K, int S);
+// Exponents and digit planes of rows r0 .. n-1 of the panel A(:, c0 .. c0 + K - 1), into buffer buf.
+cudaError_t launch_ozaki_slices(const OzakiWork& w, int buf, const double* A, int64_t ld, int64_t stride, int n,
+                                int nmat, int r0, int c0, cudaStream_t stream);
+// C(r, c) -= sum_k P(r, k) P(c, k) over the C block rows row0 .. row0 + nrows - 1, columns col0 ..
+// col0 + ncols - 1, entries with r >= c, P from buffer buf.
+cudaError_t launch_ozaki_update(const OzakiWork& w, int buf, double* A, int64_t ld, int64_t stride, int n, int nmat,
+                                int row0, int col0, int nrows, int ncols, int* err, int num_sms, cudaStream_t stream);
+
 cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag, int* err,
-                                  cudaStream_t stream, const LogdetPlan& plan, const Lookahead* la = nullptr);
+                                  cudaStream_t stream, const LogdetPlan& plan, const Lookahead* la = nullptr,
+                                  const OzakiWork* oz = nullptr);
 // tr[z] = sum_i A_z(i,i) (double-double, deterministic); then A_z(i,i) += 1.
 // If `diag` is non-null the diagonal is first overwritten with diag[z*n+i].
 cudaError_t launch_trace_shift(double* A, int64_t ld, int64_t stride, int n, int nmat, const double* diag,

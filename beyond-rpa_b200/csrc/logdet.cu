@@ -381,9 +381,13 @@ DsyrkArgs update_args(double* A, int64_t ld, int64_t stride, int nmat, int row0,
 }  // namespace
 
 cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, int nmat, double* Ldiag, int* err,
-                                  cudaStream_t stream, const LogdetPlan& plan, const Lookahead* la) {
+                                  cudaStream_t stream, const LogdetPlan& plan, const Lookahead* la,
+                                  const OzakiWork* oz) {
   if (!valid_logdet_plan(plan)) return cudaErrorInvalidValue;
   const int nb2 = plan.nb2;
+  if (oz && (oz->S == 0 || oz->K != nb2)) oz = nullptr;
+  int obuf = 0;  // digit-plane buffer of the current outer block (alternates: the rest of block t's
+                 // update may still read its planes while block t+1 is sliced)
   LookaheadState st{la, stream};
   cudaError_t e = st.begin(stream);
   if (e != cudaSuccess) return e;
@@ -408,22 +412,29 @@ cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, 
     }
     const int trail = n - J1;
     if (trail <= 0) break;
+    // full-width panels take the int8 route; a narrower last panel (n not a multiple of nb2) stays on DMMA
+    const bool use_oz = oz && J1 - J0 == oz->K;
+    if (use_oz && (e = launch_ozaki_slices(*oz, obuf, A, ld, stride, n, nmat, J1, J0, S)) != cudaSuccess) return e;
+    auto update = [&](int row0, int nrows, int ncols, cudaStream_t s) {
+      return use_oz ? launch_ozaki_update(*oz, obuf, A, ld, stride, n, nmat, row0, row0, nrows, ncols, err,
+                                          oz->num_sms, s)
+                    : launch_dsyrk_lower(update_args(A, ld, stride, nmat, row0, J0, nrows, ncols, J1 - J0,
+                                                     plan.tile_w), s);
+    };
     if (!la) {
-      e = launch_dsyrk_lower(update_args(A, ld, stride, nmat, J1, J0, trail, trail, J1 - J0, plan.tile_w), S);
-      if (e != cudaSuccess) return e;
+      if ((e = update(J1, trail, trail, S)) != cudaSuccess) return e;
+      obuf ^= 1;
       continue;
     }
     const int J2 = min(n, J1 + nb2);
     if ((e = st.before_next_block()) != cudaSuccess) return e;
-    e = launch_dsyrk_lower(update_args(A, ld, stride, nmat, J1, J0, trail, J2 - J1, J1 - J0, plan.tile_w), S);
-    if (e != cudaSuccess) return e;
+    if ((e = update(J1, trail, J2 - J1, S)) != cudaSuccess) return e;
     if (n - J2 > 0) {
       if ((e = st.fork_rest()) != cudaSuccess) return e;
-      e = launch_dsyrk_lower(update_args(A, ld, stride, nmat, J2, J0, n - J2, n - J2, J1 - J0, plan.tile_w),
-                             la->rest);
-      if (e != cudaSuccess) return e;
+      if ((e = update(J2, n - J2, n - J2, la->rest)) != cudaSuccess) return e;
       if ((e = st.rest_done()) != cudaSuccess) return e;
     }
+    obuf ^= 1;
   }
   return st.end(stream);
 }

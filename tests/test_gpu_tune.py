@@ -139,3 +139,27 @@ def test_lookahead_schedule_is_bit_identical(pkg, prec, monkeypatch):
     assert np.array_equal(out["0"][2], out["1"][2])
     ref, _ = O.ec_rpa(s.R, s.eps_o, s.eps_v, x, w)
     assert abs(out["1"][0] - ref) < (1e-10 if prec == "fp64" else 1e-6)
+
+
+@pytest.mark.parametrize("digits", ["7", "8"])
+def test_int8_trailing_updates_match_the_dmma_log_det(pkg, monkeypatch, digits):
+    # opt-in int8 tensor-core trailing updates (digit planes, exact integer products, FP64
+    # recombination): E(u) equal to the DMMA updates' to 1e-13 relative, for the lookahead and the
+    # plain schedule (which are bit-identical to each other), with a ragged last panel (order 1100)
+    import torch
+    s = O.make_system(1100, 10, 90, 77, decay=140.0, lam0=0.8)
+    x, w = O.grid_for(s, 6)
+    with pkg.Handle(0) as h0:
+        pi = torch.from_numpy(h0.pi_u(s.R, s.eps_o, s.eps_v, x, prec="fp64")).cuda()
+        h0.set_autotune(False)
+        _, ref = h0.ec_from_pi(pi, w)
+    out = []
+    for la in ("1", "0"):
+        monkeypatch.setenv("RPA_B200_OZAKI_SLICES", digits)
+        monkeypatch.setenv("RPA_B200_LOOKAHEAD", la)
+        with pkg.Handle(0) as h:
+            h.set_autotune(False)
+            _, eu = h.ec_from_pi(pi, w)
+        out.append(eu)
+        assert np.max(np.abs(eu - ref) / np.abs(ref)) < 1e-13
+    assert np.array_equal(out[0], out[1])
