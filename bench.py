@@ -650,6 +650,96 @@ def run_cc(args):
     h.close()
 
 
+def run_exchange_large(args):
+    """Beyond-RPA large case, exchange part (exchange_8192: NQ = 8192, NOcc = 128, NVirt = 2048,
+    nov = 262144, R = 17.2 GB FP64): the SOSEX exchange contraction -sum (ai|bj) T_aj,bi on ring
+    amplitudes of NT = --nt vectors (default 4096), split-BF16 on the tensor cores and FP64 (DMMA)
+    on the same amplitudes.  The amplitudes are synthetic (Gaussian vectors, A_mu = -0.1 exp(-mu/400)):
+    the direct-ring range finder at this shape (G = 3 NQ = 24576 guess vectors, K = 20) does not fit
+    one GPU (its resident split operands alone are 344 GB)."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    pkg = load_package()
+    from beyond_rpa_b200.workloads import make_single_system, SINGLE_SYSTEM
+    nq, no, nv, K, _ = SINGLE_SYSTEM["large_8192"]
+    nov = no * nv
+    NT = args.nt
+    h = pkg.Handle(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    h.set_stream(stream.cuda_stream)
+    s = make_single_system("large_8192", seed=131)
+    g = torch.Generator(device="cuda").manual_seed(7)
+    U = (torch.randn((NT, nov), generator=g, device="cuda", dtype=torch.float64) / math.sqrt(nov)).T
+    A = -0.1 * np.exp(-np.arange(NT) / 400.0)
+    torch.cuda.synchronize()
+    out = {}
+    for prec, reps in (("split", max(1, args.steps)), ("fp64", 1)):
+        h.exchange_sosex(s.R, no, nv, U, A, prec=prec) if prec == "split" else None  # warm-up (split only)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            ex = h.exchange_sosex(s.R, no, nv, U, A, prec=prec)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        out[prec] = {"ms": e0.elapsed_time(e1) / reps, "Ex": ex}
+    pair = 2.0 * no * no * nq * nv * NT  # FP64-equivalent flops of the pair contraction
+    burst, sustained, hbm, src = peaks()
+    tf_split = pair / (out["split"]["ms"] * 1e-3) / 1e12
+    print(json.dumps({
+        "metric": "SOSEX exchange contraction at the beyond-RPA large shape",
+        "workload": f"exchange_8192: NQ={nq} NOcc={no} NVirt={nv} nov={nov} NT={NT} (synthetic amplitudes)",
+        "ms_split": out["split"]["ms"], "ms_fp64": out["fp64"]["ms"],
+        "speedup_split_vs_fp64": out["fp64"]["ms"] / out["split"]["ms"],
+        "pair_flops_fp64_equiv": pair, "tflops_fp64_equiv_split": tf_split,
+        "tensor_pipe_fraction_of_sustained_bf16": 3.0 * tf_split / sustained,
+        "tflops_fp64": pair / (out["fp64"]["ms"] * 1e-3) / 1e12,
+        "Ex_split": out["split"]["Ex"], "Ex_fp64": out["fp64"]["Ex"],
+        "dEx_split_vs_fp64": out["split"]["Ex"] - out["fp64"]["Ex"],
+        "note": "tensor-pipe fraction = 3 bf16 products x FP64-equivalent flops / CUDA-event time / "
+                f"bf16_tflops_sustained ({src})"}), flush=True)
+    h.close()
+
+
+def run_logdet(args):
+    """The FP64 log-det alone (logdet_2048 / logdet_4096: the 16 matrices 1 + Pi(u) of the
+    single_2048 / single_4096 workloads, Pi built once in FP64 on the device): time of
+    rpa_b200_ec_from_pi's Cholesky phase, its FP64 rate (NQ^3/3 K flops) and the fraction of the
+    measured DGEMM peak.  RPA_B200_OZAKI_SLICES=7 or 8 runs the trailing updates on the int8 tensor
+    cores instead of DMMA."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    pkg = load_package()
+    from beyond_rpa_b200.workloads import make_single_system, SINGLE_SYSTEM
+    name = "single_" + args.workload.split("_")[1]
+    nq, no, nv, K, _ = SINGLE_SYSTEM[name]
+    h = pkg.Handle(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    h.set_stream(stream.cuda_stream)
+    s = make_single_system(name, seed=17)
+    pi = torch.empty((K, nq, nq), dtype=torch.float64, device="cuda")
+    h.pi_u(s.R, s.eps_o, s.eps_v, s.freqs, prec="fp64", out=pi)
+    del s
+    torch.cuda.synchronize()
+    ms = []
+    for it in range(args.warmup + args.steps):
+        ec, _ = h.ec_from_pi(pi, np.ones(K))
+        if it >= args.warmup:
+            ms.append(h.timings()["logdet_ms"])
+    flops = float(nq) ** 3 / 3.0 * K
+    fp = fp64_peak(stream, seconds=2.0)
+    t = statistics.mean(ms)
+    print(json.dumps({"metric": "FP64 log-det of 1 + Pi(u)", "workload": f"{args.workload}: {K} matrices of order {nq}",
+                      "logdet_ms": t, "logdet_ms_all": ms, "tflops": flops / (t * 1e-3) / 1e12,
+                      "fraction_of_dgemm_sustained": flops / (t * 1e-3) / 1e12 / fp["sustained_tflops"],
+                      "fp64_peak": fp, "int8_updates": os.environ.get("RPA_B200_OZAKI_SLICES", "0"),
+                      "launches_per_call": h.launches()}), flush=True)
+    h.close()
+
+
 def run_split(args):
     """One system split over the N GPUs (ai columns per rank, reduce-scatter of Pi over the
     frequency index, distributed log-dets): E_c/s of the whole job, strong scaling.
@@ -863,6 +953,7 @@ def main():
     ap.add_argument("--workload", default=WORKLOAD, help="single-system workload name (beyond-rpa_b200/workloads.py)")
     ap.add_argument("--full-cpu-check", action="store_true",
                     help="--impl reference: also time one complete CPU E_c to validate the extrapolation")
+    ap.add_argument("--nt", type=int, default=4096, help="exchange_8192: ring amplitudes NT")
     ap.add_argument("--no-mbe", action="store_true",
                     help="skip the FP64 peak and the batched many-fragment legs of the default line")
     ap.add_argument("--no-extras", action="store_true",
@@ -876,6 +967,10 @@ def main():
         run_adjoint(args)
     elif args.workload.startswith("cc"):
         run_cc(args)
+    elif args.workload == "exchange_8192":
+        run_exchange_large(args)
+    elif args.workload.startswith("logdet_"):
+        run_logdet(args)
     elif args.workload.startswith("split_"):
         run_split(args)
     elif args.workload.startswith("thc_"):
