@@ -433,11 +433,97 @@ def run_ours(args):
         h = pkg.Handle(local)
         h.set_stream(stream.cuda_stream)
         out["mbe_512"] = mbe_measure(pkg, h, stream, 512, steps=2, warmup=1)
+        h.close()
+        torch.cuda.empty_cache()
+        h = pkg.Handle(local)
+        # the adjoint and the large single-system shapes of the configuration list, compact legs
+        out["adjoint_2560"] = adjoint_leg(pkg, stream)
+        out["large_8192"] = single_leg(pkg, stream, "large_8192")
     if rank == 0:
         print(json.dumps(out), flush=True)
     h.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+def single_leg(pkg, stream, name, steps=2):
+    """A compact split-vs-FP64 measurement of one more single-system workload for the default line:
+    one warm-up, `steps` timed split-BF16 energies, one timed FP64 energy (R resident)."""
+    import torch
+    from beyond_rpa_b200.workloads import make_single_system, SINGLE_SYSTEM
+    nq, no, nv, K, _ = SINGLE_SYSTEM[name]
+    h = pkg.Handle(torch.cuda.current_device())
+    h.set_stream(stream.cuda_stream)
+    s = make_single_system(name, seed=131)
+    torch.cuda.synchronize()
+    h.ec_rpa(s.R, s.eps_o, s.eps_v, s.freqs, s.weights, prec="split")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tc = []
+    e0.record(stream)
+    for _ in range(steps):
+        ec, _ = h.ec_rpa(s.R, s.eps_o, s.eps_v, s.freqs, s.weights, prec="split")
+        tc.append(h.timings()["contraction_ms"])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_split = e0.elapsed_time(e1) / steps
+    e0.record(stream)
+    ec64, _ = h.ec_rpa(s.R, s.eps_o, s.eps_v, s.freqs, s.weights, prec="fp64")
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t64 = e0.elapsed_time(e1)
+    h.close()
+    del s
+    torch.cuda.empty_cache()
+    burst, sustained, hbm, src = peaks()
+    tf = 3.0 * nq * nq * no * nv * K / (statistics.mean(tc) * 1e-3) / 1e12
+    return {"workload": f"{name}: NQ={nq} NOcc={no} NVirt={nv} K={K}", "ms_split": t_split, "ms_fp64": t64,
+            "speedup_split_vs_fp64": t64 / t_split, "Ec_split": ec, "Ec_fp64": ec64,
+            "abs_diff_split_vs_fp64": abs(ec - ec64), "contraction_tflops_bf16": tf,
+            "contraction_frac_of_sustained": tf / sustained}
+
+
+def adjoint_leg(pkg, stream, steps=2):
+    """The adjoint workload on its oracle-pinned inputs (adjoint_2560): E_c + dE/dR + dE/de per
+    step, split-BF16 Pi and FP64 Pi, errors against the oracle fixture."""
+    import torch
+    sys.path.insert(0, str(ROOT))
+    from tests.golden import pinned as P
+    fix = json.loads(PINNED.read_text())["adjoint_2560"]
+    Rt, eo, ev = P.single_system("adjoint_2560", fix["factor"])
+    x, w = np.array(fix["freqs"]), np.array(fix["weights"])
+    g = fix["grad"]
+    R = torch.from_numpy(Rt).cuda().T
+    del Rt
+    nq, nov = int(R.shape[0]), int(R.shape[1])
+    dR = torch.empty((nov, nq), dtype=torch.float64, device="cuda").T
+    dO = torch.empty(len(eo), dtype=torch.float64, device="cuda")
+    dV = torch.empty(len(ev), dtype=torch.float64, device="cuda")
+    h = pkg.Handle(torch.cuda.current_device())
+    h.set_stream(stream.cuda_stream)
+    out = {"workload": f"adjoint_2560: NQ={nq} NOcc={len(eo)} NVirt={len(ev)} K={len(x)} (oracle-pinned inputs)"}
+    qi = torch.as_tensor(g["q"], device="cuda")
+    ai = torch.as_tensor(g["ai"], device="cuda")
+    for prec, reps in (("split", steps), ("fp64", 1)):
+        h.ec_grad(R, eo, ev, x, w, prec=prec, out=(dR, dO, dV))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            ec, *_ = h.ec_grad(R, eo, ev, x, w, prec=prec, out=(dR, dO, dV))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        samp = dR[qi, ai].cpu().numpy()
+        out[prec] = {"ms_per_gradient": e0.elapsed_time(e1) / reps, "Ec": ec,
+                     "abs_err_Ec_vs_oracle_qr": abs(ec - fix["Ec"]),
+                     "abs_err_Ec_vs_oracle_cholesky": abs(ec - fix["Ec_cholesky"]),
+                     "rel_err_dR_vs_oracle": float(np.max(np.abs(samp - np.array(g["dR"]))) / g["dR_max"]),
+                     "rel_err_deps_vs_oracle": float(max(
+                         np.max(np.abs(dO.cpu().numpy() - np.array(g["deps_o"]))) / np.max(np.abs(g["deps_o"])),
+                         np.max(np.abs(dV.cpu().numpy() - np.array(g["deps_v"]))) / np.max(np.abs(g["deps_v"]))))}
+    h.close()
+    del R, dR
+    torch.cuda.empty_cache()
+    out["gradients_per_s_split"] = 1e3 / out["split"]["ms_per_gradient"]
+    return out
 
 
 def mbe_measure(pkg, h, stream, n_inst, steps, warmup, rank=0, world=1, fp64_steps=1):
@@ -955,7 +1041,8 @@ def main():
                     help="--impl reference: also time one complete CPU E_c to validate the extrapolation")
     ap.add_argument("--nt", type=int, default=4096, help="exchange_8192: ring amplitudes NT")
     ap.add_argument("--no-mbe", action="store_true",
-                    help="skip the FP64 peak and the batched many-fragment legs of the default line")
+                    help="skip the extra legs of the default line (FP64 peak, batched fragments, adjoint, "
+                         "large system)")
     ap.add_argument("--no-extras", action="store_true",
                     help="profiling runs: print only the timed leg (no e2e, FP64-form or CPU legs)")
     args = ap.parse_args()
