@@ -526,15 +526,18 @@ def adjoint_leg(pkg, stream, steps=2):
     return out
 
 
-def mbe_measure(pkg, h, stream, n_inst, steps, warmup, rank=0, world=1, fp64_steps=1):
+def mbe_measure(pkg, h, stream, n_inst, steps, warmup, rank=0, world=1, fp64_steps=1, gen_cpu=False):
     """Batched many-fragment workload on this rank's share: instances/s of rpa_b200_ec_batched,
-    split-BF16 vs FP64 (same batched path), energies gathered over ranks."""
+    split-BF16 vs FP64 (same batched path), energies gathered over ranks.  gen_cpu: draw the inputs
+    on the host and copy them (for profiling runs, whose device launches should be the library's)."""
     import torch
     from beyond_rpa_b200.workloads import make_mbe_batch, mbe_specs
     from beyond_rpa_b200 import distributed as D
     specs = mbe_specs(n_inst, seed=4000)
     mine = D.shard([D.instance_cost(nq, no * nv, K) for no, nv, nq, K in specs], rank, world)
-    systems, kinds = make_mbe_batch(n_inst, seed=4000, only=mine)
+    systems, kinds = make_mbe_batch(n_inst, seed=4000, only=mine, device="cpu" if gen_cpu else "cuda")
+    if gen_cpu:
+        systems = [(R.T.contiguous().cuda().T, eo, ev, x, w) for R, eo, ev, x, w in systems]
     torch.cuda.synchronize()
     flops = sum(float(R.shape[0]) ** 2 * len(eo) * len(ev) * len(x) for R, eo, ev, x, w in systems)
     ld_flops = sum(float(R.shape[0]) ** 3 / 3 * len(x) for R, eo, ev, x, w in systems)
@@ -604,7 +607,7 @@ def run_mbe(args):
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     h.set_stream(stream.cuda_stream)
-    res = mbe_measure(pkg, h, stream, n_inst, args.steps, args.warmup, rank, world)
+    res = mbe_measure(pkg, h, stream, n_inst, args.steps, args.warmup, rank, world, gen_cpu=args.gen_cpu)
     if rank == 0:
         print(json.dumps({**res, "workload": args.workload}), flush=True)
     h.close()
@@ -1040,6 +1043,7 @@ def main():
     ap.add_argument("--full-cpu-check", action="store_true",
                     help="--impl reference: also time one complete CPU E_c to validate the extrapolation")
     ap.add_argument("--nt", type=int, default=4096, help="exchange_8192: ring amplitudes NT")
+    ap.add_argument("--gen-cpu", action="store_true", help="mbe workloads: draw the inputs on the host")
     ap.add_argument("--no-mbe", action="store_true",
                     help="skip the extra legs of the default line (FP64 peak, batched fragments, adjoint, "
                          "large system)")
