@@ -17,137 +17,238 @@
 namespace rpa {
 
 namespace {
-constexpr int NB = 64;  // Cholesky block size
-constexpr int NB2 = 256;  // outer block of the two-level schedule
+constexpr int NB = kCholNB;  // Cholesky block size (64)
+constexpr int NB2 = 256;     // outer block of the two-level schedule
 
 // Factor the NB x NB diagonal block of each matrix (blockDim = 256): thread (r, q) = (t / 4,
-// t % 4) keeps columns q, q+4, ..., q+60 of row r in registers.  Step j: the owners of column j
-// scale it by 1/sqrt(pivot) and publish it in shared memory (double-buffered); every thread
-// subtracts l_rj l_cj from its columns c in (j, r]; the owner of entry (j+1, j+1) then takes its
-// square root.  Two barriers per column and no shared-memory copy of the block.
-__device__ __forceinline__ double reg_get(const double (&v)[NB / 4], int i) {
-  double x = 0.0;
-#pragma unroll
-  for (int k = 0; k < NB / 4; ++k)
-    if (k == i) x = v[k];
-  return x;
-}
-__device__ __forceinline__ void reg_set(double (&v)[NB / 4], int i, double x) {
-#pragma unroll
-  for (int k = 0; k < NB / 4; ++k)
-    if (k == i) v[k] = x;
-}
+// t % 4) keeps columns 16q .. 16q+15 of row r in registers; the column loop is unrolled by 16, so
+// every register index is static.  Step j (one barrier): every thread forms the pivot d_j itself
+// from what step j-1 published (the diagonal entry a_jj and l_{j,j-1}: d_j = a_jj - l_{j,j-1}^2,
+// the same FMA the entry's owner applies), and the owners of column j publish the whole column,
+// l_rj = a_rj / sqrt(d_j) below the pivot and zeros on and above it (double-buffered); every thread
+// then subtracts l_rj l_cj from all 16 of its entries without a branch: the zeros leave the
+// finished columns and the rows above the pivot unchanged, and entries above the diagonal (never
+// stored) take whatever they get.  A block smaller than NB (the last of a matrix) is padded with
+// the identity.  A non-positive or NaN pivot is replaced by 1 so that the factorization finishes,
+// and reported.
+//
+// The inverse W = L^-1 of the block is then formed by columns, right-looking: thread (c, q) holds
+// rows 16q .. 16q+15 of column c of W, the owner of row k scales it by 1 / L_kk and hands it to the
+// column's other three threads by a shuffle.  W is stored transposed in the block's strict upper
+// triangle, which the lower factorization never reads: W(k, c) at (c, k) for k > c.  The panel
+// solve below reads it there; the diagonal of W, 1 / L_cc, it recomputes from the pivots.
+constexpr int kPotrfThreads = 256;
+constexpr int kLP = NB + 4;  // skewed pitch: index m at m + m / 16, so the four column blocks of a
+                             // warp's rows fall in different banks
+__device__ __forceinline__ int sk(int m) { return m + (m >> 4); }
 
 __device__ __forceinline__ void potrf_diag_body(double* Az, int64_t ld, int n, int j0, double* Ldz, int* err) {
-  __shared__ double col[2][NB];
-  __shared__ double piv[NB], pinv[NB];
+  __shared__ double col[2][kLP];
+  __shared__ double dnx[2];
+  __shared__ double LsT[NB][kLP];  // LsT[c][sk(r)] = L(r, c) below the diagonal, 0 elsewhere
+  __shared__ double inv[NB];
   const int nbe = min(NB, n - j0);
   const int t = threadIdx.x;
   const int r = t >> 2, q = t & 3;
-  const bool live = r < nbe;
-  double v[NB / 4];
+  double v[16];
 #pragma unroll
-  for (int i = 0; i < NB / 4; ++i) {
-    const int c = q + 4 * i;
-    v[i] = (live && c <= r) ? Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] : 0.0;
+  for (int i = 0; i < 16; ++i) {
+    const int c = 16 * q + i;
+    v[i] = (c <= r && r < nbe) ? Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] : (c == r ? 1.0 : 0.0);
   }
-  bool bad = false;
-  // owner of (j, j): square root of the updated pivot (a non-positive or NaN pivot is replaced
-  // by 1 so that the factorization finishes; the error is reported)
-  auto take_pivot = [&](int j) {
-    double d = reg_get(v, j >> 2);
-    if (!(d > 0.0)) {
-      bad = true;
-      d = 1.0;
-    }
-    // one reciprocal square root (1 ulp) instead of a square root and a division: the
-    // pivot chain is the kernel's critical path
-    const double ri = rsqrt(d);
-    const double sq = d * ri;
-    reg_set(v, j >> 2, sq);
-    piv[j] = sq;
-    pinv[j] = ri;
-  };
-  if (t == 0 && nbe > 0) take_pivot(0);
+  if (t == 0) dnx[1] = v[0];
   __syncthreads();
-  for (int j = 0; j < nbe; ++j) {
-    const int buf = j & 1;
-    if (live && r > j && q == (j & 3)) {
-      const double l = reg_get(v, j >> 2) * pinv[j];
-      reg_set(v, j >> 2, l);
-      col[buf][r] = l;
-    }
-    __syncthreads();
-    if (live && r > j) {
-      const double lr = col[buf][r];
+  double dj = dnx[1];  // pivot of column 0
+  double piv = 1.0;
+  bool bad = false;
+  for (int g = 0; g < 4; ++g) {
 #pragma unroll
-      for (int i = 0; i < NB / 4; ++i) {
-        const int c = q + 4 * i;
-        if (c > j && c <= r) v[i] -= lr * col[buf][c];
+    for (int jj = 0; jj < 16; ++jj) {
+      const int j = 16 * g + jj;
+      const int buf = jj & 1;
+      double d = dj;
+      if (!(d > 0.0)) {  // the same value in every thread
+        bad = true;
+        d = 1.0;
       }
-      if (r == j + 1 && q == ((j + 1) & 3)) take_pivot(j + 1);
-    }
-    __syncthreads();
-  }
-  if (bad) atomicCAS(err, 0, (int)kDevNotSPD);
+      // one reciprocal square root (1 ulp) instead of a square root and a division: the pivot
+      // chain is the kernel's critical path
+      const double ri = rsqrt(d);
+      if (q == g) {
+        double l = 0.0;
+        if (r == j) {
+          v[jj] = d * ri;
+          piv = v[jj];
+        } else if (r > j) {
+          v[jj] *= ri;
+          l = v[jj];
+        }
+        col[buf][sk(r)] = l;
+      }
+      if (r == j + 1 && q == ((j + 1) >> 4)) dnx[buf] = v[(jj + 1) & 15];
+      __syncthreads();
+      if (j + 1 < NB) {
+        const double l1 = col[buf][sk(j + 1)];
+        dj = fma(-l1, l1, dnx[buf]);
+      }
+      const double lr = col[buf][sk(r)];
 #pragma unroll
-  for (int i = 0; i < NB / 4; ++i) {
-    const int c = q + 4 * i;
-    if (live && c <= r) Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] = v[i];
+      for (int i = 0; i < 16; ++i) v[i] = fma(-lr, col[buf][sk(16 * q + i)], v[i]);
+    }
   }
-  if (t < nbe) Ldz[j0 + t] = piv[t];
+  if (bad && t == 0) atomicCAS(err, 0, (int)kDevNotSPD);
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const int c = 16 * q + i;
+    LsT[c][sk(r)] = c < r ? v[i] : 0.0;
+    if (c <= r && r < nbe) Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] = v[i];
+  }
+  if (q == (r >> 4)) {  // the owner of the diagonal entry
+    inv[r] = 1.0 / piv;
+    if (r < nbe) Ldz[j0 + r] = piv;
+  }
+  __syncthreads();
+  // column c = r of W: s[i] = W(16q + i, c), zero above the diagonal
+  const int lane = t & 31;
+  double s[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) s[i] = (16 * q + i == r) ? 1.0 : 0.0;
+  for (int g = 0; g < 4; ++g) {
+#pragma unroll
+    for (int kk = 0; kk < 16; ++kk) {
+      const int k = 16 * g + kk;
+      double wk = s[kk] * inv[k];
+      if (q == g) s[kk] = wk;
+      wk = __shfl_sync(0xffffffffu, wk, (lane & ~3) | g);
+#pragma unroll
+      for (int i = 0; i < 16; ++i) s[i] = fma(-LsT[k][sk(16 * q + i)], wk, s[i]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const int m = 16 * q + i;
+    if (m > r && m < nbe) Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + m)] = s[i];
+  }
 }
 
-__global__ void __launch_bounds__(256) potrf_diag_kernel(double* A, int64_t ld, int64_t stride, int n, int j0,
-                                                         double* Ldiag, int* err) {
+__global__ void __launch_bounds__(kPotrfThreads) potrf_diag_kernel(double* A, int64_t ld, int64_t stride, int n,
+                                                                   int j0, double* Ldiag, int* err) {
   const int z = blockIdx.x;
   potrf_diag_body(A + (int64_t)z * stride, ld, n, j0, Ldiag + (int64_t)z * n, err);
 }
 
-// Panel solve: rows below the diagonal block, X L_jj^T = A_panel, one row per thread.  Column c
-// of X is final once it is scaled by 1/L_cc; it is then subtracted from the later columns of the
-// row (right-looking within the row: 64 short dependency chains instead of one long one).
-__device__ __forceinline__ void trsm_panel_body(double* Az, int64_t ld, int n, int j0, int rblock) {
-  __shared__ double Ls[NB][NB + 1];
-  __shared__ double inv[NB];
-  const int t = threadIdx.x;
-  for (int idx = t; idx < NB * NB; idx += blockDim.x) {
-    const int r = idx % NB, c = idx / NB;
-    Ls[r][c] = (r >= c) ? Az[(int64_t)(j0 + r) + ld * (int64_t)(j0 + c)] : 0.0;
-  }
-  __syncthreads();
-  if (t < NB) inv[t] = 1.0 / Ls[t][t];
-  __syncthreads();
-  const int r = j0 + NB + rblock * blockDim.x + t;
-  if (r >= n) return;
-  double x[NB];
-#pragma unroll
-  for (int c = 0; c < NB; ++c) x[c] = Az[(int64_t)r + ld * (int64_t)(j0 + c)];
-#pragma unroll
-  for (int c = 0; c < NB; ++c) {
-    x[c] *= inv[c];
-#pragma unroll
-    for (int m = c + 1; m < NB; ++m) x[m] -= x[c] * Ls[m][c];
-  }
-#pragma unroll
-  for (int c = 0; c < NB; ++c) Az[(int64_t)r + ld * (int64_t)(j0 + c)] = x[c];
+// Panel solve: the rows below the diagonal block, X = A_p L^-T = A_p B with B = W^T upper
+// triangular (strict part from the block's upper triangle, diagonal 1 / L_cc), on the FP64 tensor
+// cores (DMMA m8n8k4, the fragment layout of dsyrk_f64.cu): 64 rows per CTA, 4 warps of 32 x 32
+// outputs; warps of the first 32 columns stop at k = 32 (B(k, c) = 0 for k > c).  Every CTA reads
+// all of its rows before it writes any, and no other CTA touches them.
+constexpr int kTrsmRows = 64;
+constexpr int kTrsmThreads = 128;
+constexpr int kLdA = NB + 8;  // As[k][m]: fragment loads hit each bank pair twice
+constexpr int kLdB = NB + 4;  // BsT[c][k]: likewise, and conflict-free fills
+constexpr size_t kTrsmSmem = sizeof(double) * (size_t)NB * (kLdA + kLdB);
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
 }
 
-__global__ void __launch_bounds__(128) trsm_panel_kernel(double* A, int64_t ld, int64_t stride, int n, int j0) {
-  trsm_panel_body(A + (int64_t)blockIdx.y * stride, ld, n, j0, blockIdx.x);
+__device__ __forceinline__ void trsm_panel_body(double* Az, int64_t ld, int n, int j0, int rblock, const double* Ldz) {
+  extern __shared__ __align__(16) double trsm_smem[];
+  auto As = reinterpret_cast<double(*)[kLdA]>(trsm_smem);               // As[k][m] = A_p(m, k)
+  auto BsT = reinterpret_cast<double(*)[kLdB]>(trsm_smem + NB * kLdA);  // BsT[c][k] = B(k, c)
+  const int t = threadIdx.x;
+  const int r0 = j0 + NB + rblock * kTrsmRows;
+  const int rows = min(kTrsmRows, n - r0);
+  // operands by asynchronous 8-byte copies (every load in flight at once), zeros and the
+  // diagonal of B by plain stores to other addresses
+  const int fi = t & (NB - 1), fc0 = t >> 6;
+#pragma unroll
+  for (int m = 0; m < NB / 2; ++m) {
+    const int c = fc0 + 2 * m;
+    if (fi < rows) cp_async8(&As[c][fi], Az + (int64_t)(r0 + fi) + ld * (int64_t)(j0 + c));
+    else As[c][fi] = 0.0;
+    if (fi < c) cp_async8(&BsT[c][fi], Az + (int64_t)(j0 + fi) + ld * (int64_t)(j0 + c));
+    else if (fi > c) BsT[c][fi] = 0.0;
+  }
+  if (t < NB) BsT[t][t] = 1.0 / Ldz[j0 + t];
+  cp_async_wait_all();
+  __syncthreads();
+  const int lane = t & 31, warp = t >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  auto kstep = [&](int ks) {
+    const int kr = 4 * ks + (lane & 3);
+    double af[4], bf[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) af[i] = As[kr][wm * 32 + i * 8 + (lane >> 2)];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) bf[j] = BsT[wn * 32 + j * 8 + (lane >> 2)][kr];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+  };
+#pragma unroll
+  for (int ks = 0; ks < 8; ++ks) kstep(ks);
+  if (wn == 1) {  // B(k, c) = 0 for k > c: the first 32 columns stop at k = 32
+#pragma unroll
+    for (int ks = 8; ks < 16; ++ks) kstep(ks);
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int row = wm * 32 + i * 8 + (lane >> 2);
+    if (row >= rows) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int v = 0; v < 2; ++v) {
+        const int c = wn * 32 + j * 8 + 2 * (lane & 3) + v;
+        Az[(int64_t)(r0 + row) + ld * (int64_t)(j0 + c)] = acc[i][j][v];
+      }
+  }
+}
+
+__global__ void __launch_bounds__(kTrsmThreads) trsm_panel_kernel(double* A, int64_t ld, int64_t stride, int n,
+                                                                  int j0, const double* Ldiag) {
+  const int z = blockIdx.y;
+  trsm_panel_body(A + (int64_t)z * stride, ld, n, j0, blockIdx.x, Ldiag + (int64_t)z * n);
 }
 
 // ----------------------------------------------------------------- variable-size batches
-__global__ void __launch_bounds__(256) potrf_varlen_kernel(const MatDesc* mats, int j0, int* err) {
+__global__ void __launch_bounds__(kPotrfThreads) potrf_varlen_kernel(const MatDesc* mats, int j0, int* err) {
   const MatDesc md = mats[blockIdx.x];
   if (j0 >= md.n) return;
   potrf_diag_body(md.A, md.ld, md.n, j0, md.Ldiag, err);
 }
 
-__global__ void __launch_bounds__(128) trsm_varlen_kernel(const MatDesc* mats, int j0) {
+__global__ void __launch_bounds__(kTrsmThreads) trsm_varlen_kernel(const MatDesc* mats, int j0) {
   const MatDesc md = mats[blockIdx.y];
-  if (md.n - j0 - NB <= 0 || (int)(blockIdx.x * blockDim.x) >= md.n - j0 - NB) return;
-  trsm_panel_body(md.A, md.ld, md.n, j0, blockIdx.x);
+  if (md.n - j0 - NB <= 0 || (int)blockIdx.x * kTrsmRows >= md.n - j0 - NB) return;
+  trsm_panel_body(md.A, md.ld, md.n, j0, blockIdx.x, md.Ldiag);
+}
+
+// Shared-memory opt-in of the panel solve (> 48 KB), once per process.
+cudaError_t trsm_smem_optin() {
+  static const cudaError_t e = [] {
+    cudaError_t r = cudaFuncSetAttribute(trsm_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem);
+    if (r == cudaSuccess)
+      r = cudaFuncSetAttribute(trsm_varlen_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem);
+    return r;
+  }();
+  return e;
 }
 
 // Deterministic block reduction of double-double values (blockDim = 256).
@@ -386,6 +487,7 @@ cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, 
   if (!valid_logdet_plan(plan)) return cudaErrorInvalidValue;
   const int nb2 = plan.nb2;
   if (oz && (oz->S == 0 || oz->K != nb2)) oz = nullptr;
+  if (cudaError_t e0 = trsm_smem_optin()) return e0;
   int obuf = 0;  // digit-plane buffer of the current outer block (alternates: the rest of block t's
                  // update may still read its planes while block t+1 is sliced)
   LookaheadState st{la, stream};
@@ -395,13 +497,14 @@ cudaError_t launch_cholesky_lower(double* A, int64_t ld, int64_t stride, int n, 
   for (int J0 = 0; J0 < n; J0 += nb2) {
     const int J1 = min(n, J0 + nb2);
     for (int j0 = J0; j0 < J1; j0 += NB) {
-      potrf_diag_kernel<<<nmat, 256, 0, S>>>(A, ld, stride, n, j0, Ldiag, err);
+      potrf_diag_kernel<<<nmat, kPotrfThreads, 0, S>>>(A, ld, stride, n, j0, Ldiag, err);
       ++g_launches;
       e = cudaGetLastError();
       if (e != cudaSuccess) return e;
       const int below = n - j0 - NB;
       if (below <= 0) break;
-      trsm_panel_kernel<<<dim3((below + 127) / 128, nmat), 128, 0, S>>>(A, ld, stride, n, j0);
+      trsm_panel_kernel<<<dim3((below + kTrsmRows - 1) / kTrsmRows, nmat), kTrsmThreads, kTrsmSmem, S>>>(
+          A, ld, stride, n, j0, Ldiag);
       ++g_launches;
       e = cudaGetLastError();
       if (e != cudaSuccess) return e;
@@ -446,6 +549,7 @@ cudaError_t launch_logdet_varlen(const MatDesc* mats, int nmat, int nmax, int* e
                                  const LogdetPlan& plan, const Lookahead* la) {
   if (nmat <= 0) return cudaSuccess;
   if (!valid_logdet_plan(plan)) return cudaErrorInvalidValue;
+  if (cudaError_t e0 = trsm_smem_optin()) return e0;
   trace_shift_varlen_kernel<<<nmat, 256, 0, stream>>>(mats);
   ++g_launches;
   cudaError_t e = cudaGetLastError();
@@ -457,11 +561,11 @@ cudaError_t launch_logdet_varlen(const MatDesc* mats, int nmat, int nmax, int* e
   for (int J0 = 0; J0 < nmax; J0 += nb2) {
     const int J1 = std::min(nmax, J0 + nb2);
     for (int j0 = J0; j0 < J1; j0 += NB) {
-      potrf_varlen_kernel<<<nmat, 256, 0, S>>>(mats, j0, err);
+      potrf_varlen_kernel<<<nmat, kPotrfThreads, 0, S>>>(mats, j0, err);
       ++g_launches;
       const int below = nmax - j0 - NB;
       if (below <= 0) break;
-      trsm_varlen_kernel<<<dim3((below + 127) / 128, nmat), 128, 0, S>>>(mats, j0);
+      trsm_varlen_kernel<<<dim3((below + kTrsmRows - 1) / kTrsmRows, nmat), kTrsmThreads, kTrsmSmem, S>>>(mats, j0);
       ++g_launches;
       e = launch_dsyrk_varlen(mats, nmat, 0, J0, j0, nb2, plan.tile_w, nmax, S);
       if (e != cudaSuccess) return e;
