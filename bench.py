@@ -796,11 +796,32 @@ def run_logdet(args):
     single_2048 / single_4096 workloads, Pi built once in FP64 on the device): time of
     rpa_b200_ec_from_pi's Cholesky phase, its FP64 rate (NQ^3/3 K flops) and the fraction of the
     measured DGEMM peak.  RPA_B200_OZAKI_SLICES=7 or 8 runs the trailing updates on the int8 tensor
-    cores instead of DMMA."""
+    cores instead of DMMA.
+
+    logdet_batch_<n>x<m>: the batched log-det of the many-fragment path (m seeded SPD matrices of
+    order n in one variable-size batch, every tile plan timed by rpa_b200_tune_logdet); reports the
+    fastest plan's time per step (best of the steps) and its FP64 rate."""
     import torch
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     pkg = load_package()
+    if args.workload.startswith("logdet_batch_"):
+        n, m = (int(x) for x in args.workload[len("logdet_batch_"):].split("x"))
+        h = pkg.Handle(local)
+        best, plans = None, {}
+        for it in range(args.warmup + args.steps):
+            plan, ms = h.tune_logdet(n, m)
+            if it >= args.warmup:
+                for k, t in ms.items():
+                    plans[str(k)] = min(plans.get(str(k), t), t)
+                t = min(ms.values())
+                best = t if best is None else min(best, t)
+        flops = float(n) ** 3 / 3.0 * m
+        print(json.dumps({"metric": "FP64 log-det of a variable-size batch", "workload": f"{m} matrices of order {n}",
+                          "logdet_ms": best, "tflops": flops / (best * 1e-3) / 1e12, "plan_ms": plans,
+                          "best_plan": list(h.logdet_plan(n))}), flush=True)
+        h.close()
+        return
     from beyond_rpa_b200.workloads import make_single_system, SINGLE_SYSTEM
     name = "single_" + args.workload.split("_")[1]
     nq, no, nv, K, _ = SINGLE_SYSTEM[name]
