@@ -240,6 +240,13 @@ __device__ __forceinline__ void syrk_body(const Source& src, int* err, const int
         }
         const int wave = (u - (int)blockIdx.x) / (int)gridDim.x;
         const int members = min((int)gridDim.x, nunits - wave * (int)gridDim.x);
+        // a lower-triangle unit whose live columns fit 128 rows (the first 128-row tile of a
+        // 256-column block on the diagonal, a ragged last block) loads B through the 128-row box
+        // of the same tensor (the A maps): half the B bytes, and the MMA reads only those rows
+        const bool narrowB = x.tri && min(x.NQ, (x.tm + 1) * TM) - x.tn * TN <= TM;
+        const CUtensorMap* mbh = narrowB ? x.map[0] : x.map[2];
+        const CUtensorMap* mbl = narrowB ? x.map[1] : x.map[3];
+        const uint32_t stage_bytes = narrowB ? 4 * kATileBytes : kStageBytes;
         for (int ch = 0; ch < x.nchunks; ++ch) {
           if (sync && ch % sync_every == 0) {
             const int mi = ch / sync_every;
@@ -251,12 +258,12 @@ __device__ __forceinline__ void syrk_body(const Source& src, int* err, const int
             ok = false;
             break;
           }
-          mbar_arrive_expect_tx(&full[stage], kStageBytes);
+          mbar_arrive_expect_tx(&full[stage], stage_bytes);
           const int c0 = (x.chunk0 + ch) * TK;
           tma_load_3d(a_hi(stage), x.map[0], &full[stage], c0, x.tm * TM, x.k);
           tma_load_3d(a_lo(stage), x.map[1], &full[stage], c0, x.tm * TM, x.k);
-          tma_load_3d(b_hi(stage), x.map[2], &full[stage], c0, x.tn * TN, x.k);
-          tma_load_3d(b_lo(stage), x.map[3], &full[stage], c0, x.tn * TN, x.k);
+          tma_load_3d(b_hi(stage), mbh, &full[stage], c0, x.tn * TN, x.k);
+          tma_load_3d(b_lo(stage), mbl, &full[stage], c0, x.tn * TN, x.k);
           issued |= 1u << stage;
           issued_par = (issued_par & ~(1u << stage)) | (phase << stage);
           if (++stage == kStages) {
