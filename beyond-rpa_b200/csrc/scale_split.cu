@@ -119,24 +119,24 @@ __device__ __forceinline__ void scale_split_body(const double* __restrict__ R, i
     bool ok = true;
     for (int c = 0; c < nchunks && ok; ++c) {
       const int64_t a0 = a_begin + (int64_t)c * kTA + warp * kCols;
-      // scale factors of this warp's 16 columns for every frequency (FP64), into its own slice
-      __syncwarp();
-      for (int idx = lane; idx < kg * kCols; idx += 32) {
-        const int k = idx / kCols, j = idx % kCols;
-        const int64_t a = a0 + j;
-        double f = 0.0;
-        if (a < a_end) {
-          const double d = D[a];
-          f = sqrt(alpha * d / (d * d + fg.u2[k]));
-        }
-        fac[k * kCols + j] = f;
-      }
-      // R(q, a0 + j): for each j the warp reads 32 consecutive Q of one column (256 bytes)
+      // R(q, a0 + j): for each j the warp reads 32 consecutive Q of one column (256 bytes).  Issued
+      // before the scale-factor arithmetic, whose latency covers part of theirs.
       double r[kCols];
 #pragma unroll
       for (int j = 0; j < kCols; ++j) {
         const int64_t a = a0 + j;
         r[j] = (q < NQ && a < a_end) ? __ldg(R + (int64_t)q + ldR * a) : 0.0;
+      }
+      // scale factors of this warp's 16 columns for every frequency (FP64), into its own slice:
+      // sqrt(alpha d / (d^2 + u^2)) = sqrt(alpha d) / sqrt(d^2 + u^2), the first per column (lanes
+      // j and j + 16 each take column j), the second one reciprocal square root per (k, j)
+      __syncwarp();
+      const int jl = lane & (kCols - 1);
+      const double dl = (a0 + jl < a_end) ? D[a0 + jl] : 0.0;
+      const double sad = sqrt(alpha * dl);
+      for (int idx = lane; idx < kg * kCols; idx += 32) {
+        const int k = idx / kCols;  // idx % kCols == jl: this lane's column
+        fac[k * kCols + jl] = (a0 + jl < a_end) ? sad * rsqrt(fma(dl, dl, fg.u2[k])) : 0.0;
       }
       // warm L2 with the next chunk's 16 columns (two 128-byte lines each) while this one is split
       {
