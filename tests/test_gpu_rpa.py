@@ -167,6 +167,38 @@ def test_invalid_gap_is_reported(handle, pkg):
     assert e.value.status == pkg.RPA_ERR_INVALID_ARG
 
 
+@pytest.mark.parametrize("n", [1, 2, 63, 64, 65, 127, 128, 129, 191, 257, 320])
+def test_ec_from_pi_at_block_boundaries(handle, n):
+    # orders around the 64-column diagonal blocks (factored with their inverses, a panel solve only
+    # below a full block) and the 256-column outer blocks of the blocked Cholesky: E(u) = ln det(1 +
+    # Pi) - Tr Pi against LAPACK on the same symmetric positive semidefinite Pi
+    rng = np.random.default_rng(1000 + n)
+    w = np.array([0.7, 1.1, 0.4])
+    pis = []
+    for k in range(len(w)):
+        B = rng.standard_normal((n, n // 2 + 3))
+        P = B @ B.T
+        pis.append(P * ((0.3 + 0.25 * k) / np.linalg.eigvalsh(P)[-1]))
+    pi = np.stack(pis)
+    ref = np.array([np.linalg.slogdet(np.eye(n) + p)[1] - np.trace(p) for p in pis])
+    ec, eu = handle.ec_from_pi(pi, w)
+    assert np.max(np.abs(eu - ref)) <= 1e-12 * max(1.0, np.max(np.abs(ref))), (eu, ref)
+    assert abs(ec - float(np.sum(w * ref)) / (2 * np.pi)) <= 1e-12 * max(1.0, np.max(np.abs(ref)))
+
+
+def test_batched_log_det_at_block_boundaries(handle):
+    # the variable-order batched Cholesky (orders 63 .. 257 in one order bucket and the next)
+    # against the single-system path on the same FP64 Pi
+    systems, refs = [], []
+    for i, nq in enumerate((63, 64, 65, 129, 257)):
+        s = O.make_system(nq, 3, 12 + i, 600 + i, lam0=0.8)
+        x, w = O.grid_for(s, 4)
+        systems.append((s.R, s.eps_o, s.eps_v, x, w))
+        refs.append(handle.ec_rpa(s.R, s.eps_o, s.eps_v, x, w, prec="fp64")[0])
+    ec, _ = handle.ec_batched(systems, prec="fp64")
+    assert np.max(np.abs(np.array(ec) - np.array(refs))) <= 1e-11, (ec, refs)
+
+
 def test_not_spd_is_reported(handle, pkg):
     pi = np.zeros((2, 70, 70))
     pi[0] = np.eye(70) * 0.1
