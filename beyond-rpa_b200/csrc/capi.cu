@@ -316,9 +316,10 @@ int stage_R(rpa_b200_handle* h, const Validated& v, const double* R, int64_t ldR
     *Rd = static_cast<const double*>(h->R.p);
     *ldd = v.NQ;
   }
-  // NaN/Inf screen of the Cholesky vectors (ld may exceed NQ: screen the span)
+  // NaN/Inf screen of the Cholesky vectors: the NQ rows of every column (rows between NQ and ld
+  // are the caller's padding, which no kernel reads)
   RPA_CUDA(h, cudaMemsetAsync(h->count_dev, 0, sizeof(int), h->stream));
-  RPA_CUDA(h, rpa::launch_count_nonfinite(*Rd, (*ldd) * (v.nov - 1) + v.NQ, h->count_dev, h->stream));
+  RPA_CUDA(h, rpa::launch_count_nonfinite_cols(*Rd, *ldd, v.NQ, v.nov, h->count_dev, h->stream));
   int s = stage_eps(h, v);
   if (s != RPA_OK) return s;
   int cnt = 0;
@@ -2839,24 +2840,26 @@ static int ec_batched_groups(rpa_b200_handle* h, int64_t ninst, const rpa_instan
     }
     RPA_CUDA(h, cudaMemcpyAsync(h->D.p, Dh.data(), total_nov * 8, cudaMemcpyHostToDevice, h->stream));
     RPA_CUDA(h, cudaMemsetAsync(h->count_dev, 0, sizeof(int), h->stream));
-    {  // one screening launch for every instance
+    {  // one screening launch for every instance: the NQ rows of each column (not an ld > NQ padding)
       std::vector<const double*> ptrs(n);
-      std::vector<int64_t> lens(n);
-      int64_t longest = 0;
+      std::vector<int64_t> dims(3 * (size_t)n);
+      int64_t widest = 0;
       for (int i = 0; i < n; ++i) {
         ptrs[i] = Rd[i];
-        lens[i] = ldR[i] * (v[i].nov - 1) + v[i].NQ;
-        longest = std::max(longest, lens[i]);
+        dims[3 * i] = ldR[i];
+        dims[3 * i + 1] = v[i].NQ;
+        dims[3 * i + 2] = v[i].nov;
+        widest = std::max(widest, v[i].nov);
       }
-      RPA_CUDA(h, ensure(h->bRes, (size_t)n * 16 + 64));
+      RPA_CUDA(h, ensure(h->bRes, (size_t)n * 32 + 64));
       char* scr = static_cast<char*>(h->bRes.p);
       RPA_CUDA(h, cudaMemcpyAsync(scr, ptrs.data(), (size_t)n * 8, cudaMemcpyHostToDevice, h->stream));
-      RPA_CUDA(h, cudaMemcpyAsync(scr + (size_t)n * 8, lens.data(), (size_t)n * 8, cudaMemcpyHostToDevice, h->stream));
-      const int per = (int)std::min<int64_t>(1024, std::max<int64_t>(1, (longest + 256 * 8 - 1) / (256 * 8)));
+      RPA_CUDA(h, cudaMemcpyAsync(scr + (size_t)n * 8, dims.data(), (size_t)n * 24, cudaMemcpyHostToDevice, h->stream));
+      const int per = (int)std::min<int64_t>(1024, std::max<int64_t>(1, (widest + 15) / 16));
       RPA_CUDA(h, rpa::launch_count_nonfinite_multi(reinterpret_cast<const double* const*>(scr),
                                                     reinterpret_cast<const int64_t*>(scr + (size_t)n * 8), n, per,
                                                     h->count_dev, h->stream));
-      RPA_CUDA(h, cudaStreamSynchronize(h->stream));  // ptrs and lens must outlive their copies
+      RPA_CUDA(h, cudaStreamSynchronize(h->stream));  // ptrs and dims must outlive their copies
     }
     int cnt = 0;
     RPA_CUDA(h, cudaMemcpyAsync(&cnt, h->count_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));

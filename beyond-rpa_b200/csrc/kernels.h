@@ -232,8 +232,13 @@ cudaError_t launch_count_nonfinite(const double* x, int64_t n, int* count, cudaS
 // The same over the lower triangles (diagonal included) of nmat n x n matrices, ld and stride apart.
 cudaError_t launch_count_nonfinite_lower(const double* A, int64_t ld, int64_t stride, int n, int nmat, int* count,
                                          cudaStream_t stream);
-// The same over narr arrays (device arrays of pointers and lengths), blocks_per CTAs each.
-cudaError_t launch_count_nonfinite_multi(const double* const* ptrs, const int64_t* counts, int narr, int blocks_per,
+// The same over rows 0 .. rows-1 of cols columns of a column-major array, ld apart (rows from rows to
+// ld - 1 are a caller's padding and are never read).
+cudaError_t launch_count_nonfinite_cols(const double* A, int64_t ld, int64_t rows, int64_t cols, int* count,
+                                        cudaStream_t stream);
+// The same over narr such arrays: device arrays of pointers and of (ld, rows, cols) triples,
+// blocks_per CTAs each.
+cudaError_t launch_count_nonfinite_multi(const double* const* ptrs, const int64_t* dims, int narr, int blocks_per,
                                          int* count, cudaStream_t stream);
 // Strided 2-D copy of a column-major matrix block (device to device).
 cudaError_t launch_copy_lower(const double* src, int64_t lds, int64_t strideS, double* dst, int64_t ldd,

@@ -370,13 +370,27 @@ __global__ void count_nonfinite_lower_kernel(const double* A, int64_t ld, int64_
   if (local) atomicAdd(count, local);
 }
 
-// Many arrays at once: blockIdx.y selects array (ptrs[y], counts[y]).
-__global__ void count_nonfinite_multi_kernel(const double* const* ptrs, const int64_t* counts, int* count) {
-  const double* x = ptrs[blockIdx.y];
-  const int64_t n = counts[blockIdx.y];
+// Rows 0 .. rows-1 of each column of a column-major array (blockIdx.x strides over the columns):
+// a caller's padding rows between rows and ld are never read, so they cannot raise a false count.
+__device__ __forceinline__ int count_nonfinite_cols_body(const double* A, int64_t ld, int64_t rows, int64_t cols) {
   int local = 0;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    if (!isfinite(x[i])) ++local;
+  for (int64_t c = blockIdx.x; c < cols; c += gridDim.x) {
+    const double* col = A + ld * c;
+    for (int64_t r = threadIdx.x; r < rows; r += blockDim.x)
+      if (!isfinite(col[r])) ++local;
+  }
+  return local;
+}
+
+__global__ void count_nonfinite_cols_kernel(const double* A, int64_t ld, int64_t rows, int64_t cols, int* count) {
+  const int local = count_nonfinite_cols_body(A, ld, rows, cols);
+  if (local) atomicAdd(count, local);
+}
+
+// Many arrays at once: blockIdx.y selects array ptrs[y] with (ld, rows, cols) = dims[3y .. 3y+2].
+__global__ void count_nonfinite_multi_kernel(const double* const* ptrs, const int64_t* dims, int* count) {
+  const int64_t* d = dims + 3 * (int64_t)blockIdx.y;
+  const int local = count_nonfinite_cols_body(ptrs[blockIdx.y], d[0], d[1], d[2]);
   if (local) atomicAdd(count, local);
 }
 
@@ -646,10 +660,19 @@ cudaError_t launch_count_nonfinite_lower(const double* A, int64_t ld, int64_t st
   return cudaGetLastError();
 }
 
-cudaError_t launch_count_nonfinite_multi(const double* const* ptrs, const int64_t* counts, int narr, int blocks_per,
+cudaError_t launch_count_nonfinite_cols(const double* A, int64_t ld, int64_t rows, int64_t cols, int* count,
+                                        cudaStream_t stream) {
+  if (rows <= 0 || cols <= 0) return cudaSuccess;
+  const int64_t blocks = std::min<int64_t>(cols, 4096);
+  count_nonfinite_cols_kernel<<<(unsigned)blocks, 256, 0, stream>>>(A, ld, rows, cols, count);
+  ++g_launches;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_count_nonfinite_multi(const double* const* ptrs, const int64_t* dims, int narr, int blocks_per,
                                          int* count, cudaStream_t stream) {
   if (narr <= 0) return cudaSuccess;
-  count_nonfinite_multi_kernel<<<dim3((unsigned)std::max(1, blocks_per), (unsigned)narr), 256, 0, stream>>>(ptrs, counts,
+  count_nonfinite_multi_kernel<<<dim3((unsigned)std::max(1, blocks_per), (unsigned)narr), 256, 0, stream>>>(ptrs, dims,
                                                                                                          count);
   ++g_launches;
   return cudaGetLastError();

@@ -81,14 +81,20 @@ def test_device_pointers_match_host(handle):
 
 
 def test_leading_dimension_larger_than_nq(handle):
+    # the rows between NQ and the leading dimension are the caller's padding: never read, never
+    # screened (NaN there must not raise RPA_ERR_NONFINITE), in the single and the batched path
     s, x, w = golden_system("ragged")
-    big = np.zeros((s.nq + 13, s.R.shape[1]), order="F")
+    big = np.full((s.nq + 13, s.R.shape[1]), np.nan, order="F")
     big[: s.nq] = s.R
     import torch
     Rt = torch.from_numpy(np.ascontiguousarray(big.T)).cuda()
     view = Rt.T[: s.nq]  # stride(1) = NQ + 13
     ec, _ = handle.ec_rpa(view, s.eps_o, s.eps_v, x, w, prec="fp64")
     assert abs(ec - GOLDEN["ragged"]["Ec"]) < 1e-10
+    esp, _ = handle.ec_rpa(view, s.eps_o, s.eps_v, x, w, prec="split")
+    assert abs(esp - GOLDEN["ragged"]["Ec"]) < 1e-6
+    eb, _ = handle.ec_batched([(view, s.eps_o, s.eps_v, x, w)], prec="fp64")
+    assert abs(eb[0] - GOLDEN["ragged"]["Ec"]) < 1e-10
 
 
 def test_repeated_calls_are_deterministic(handle):
