@@ -155,6 +155,14 @@ int fail(rpa_b200_handle* h, int status, const char* fmt, ...) {
   return status;
 }
 
+// RPA_ERR_NONFINITE for a NaN or Inf energy: entry points that do not screen every input array
+// (the exchange and PNO energies) report a non-finite input through their result.
+int finite_or_fail(rpa_b200_handle* h, std::initializer_list<double> xs, const char* what) {
+  for (double x : xs)
+    if (!std::isfinite(x)) return fail(h, RPA_ERR_NONFINITE, "non-finite %s (NaN or Inf in an input)", what);
+  return RPA_OK;
+}
+
 #define RPA_CUDA(h, call)                                                                                   \
   do {                                                                                                      \
     cudaError_t e_ = (call);                                                                                \
@@ -1682,6 +1690,7 @@ int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
     RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
     RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
     RPA_CUDA(h, cudaEventRecord(h->ev[4], h->stream));
+    if ((s = finite_or_fail(h, {sum}, "exchange energy"))) return s;
     *Ex = -Alpha * sum;
     finish_timings(h);
     return RPA_OK;
@@ -1697,6 +1706,7 @@ int rpa_b200_exchange_sosex(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
   RPA_CUDA(h, cudaStreamSynchronize(h->stream));
   dd acc{0.0, 0.0};
   for (double x : hp) acc = rpa::dd_add(acc, x);
+  if ((s = finite_or_fail(h, {acc.hi}, "exchange energy"))) return s;
   *Ex = -Alpha * (acc.hi + acc.lo);
   finish_timings(h);
   return RPA_OK;
@@ -1890,6 +1900,7 @@ int rpa_b200_exchange_mbpt3(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_
   RPA_CUDA(h, cudaStreamSynchronize(h->stream));
   dd acc{split_sum, 0.0};
   for (double x : hp) acc = rpa::dd_add(acc, x);
+  if ((s = finite_or_fail(h, {acc.hi}, "MBPT3 exchange energy"))) return s;
   *Ex = -(acc.hi + acc.lo);
   finish_timings(h);
   return RPA_OK;
@@ -2782,6 +2793,7 @@ int rpa_b200_jctc2024(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOc
     if (contrib) e2ghij = rpa::dd_add(e2ghij, total(p, 2));
     e2bcd = rpa::dd_add(e2bcd, total(p, 3));
   }
+  if ((s = finite_or_fail(h, {erpa.hi, e1b.hi, e2bcd.hi, e2ghij.hi}, "PNO correction energy"))) return s;
   Energies[0] = erpa.hi + erpa.lo;
   Energies[1] = e1b.hi + e1b.lo;
   Energies[2] = e2bcd.hi + e2bcd.lo;

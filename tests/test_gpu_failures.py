@@ -83,3 +83,33 @@ def test_upper_triangle_of_pi_is_never_read(pkg, handle):
     with pytest.raises(pkg.RPAError) as err:
         handle.ec_from_pi(torch.from_numpy(low).cuda(), w)
     assert err.value.status == pkg.RPA_ERR_NONFINITE
+
+
+@pytest.mark.parametrize("prec", ["fp64", "split"])
+def test_nonfinite_exchange_inputs_are_reported(pkg, handle, prec):
+    # the exchange entry points do not screen R and U: a non-finite input shows in the energy, which
+    # is reported as RPA_ERR_NONFINITE (not returned as NaN), and the handle stays usable
+    rng = np.random.default_rng(5)
+    nq, no, nv, nt = 77, 5, 19, 45
+    R = rng.standard_normal((nq, no * nv)) * 0.1
+    U = rng.standard_normal((no * nv, nt)) * 0.2
+    A = -0.05 * rng.uniform(size=nt)
+    good = handle.exchange_sosex(R, no, nv, U, A, alpha=2.0, prec=prec)
+    bad = U.copy()
+    bad[17, 3] = np.nan
+    with pytest.raises(pkg.RPAError) as err:
+        handle.exchange_sosex(R, no, nv, bad, A, alpha=2.0, prec=prec)
+    assert err.value.status == pkg.RPA_ERR_NONFINITE
+    assert handle.exchange_sosex(R, no, nv, U, A, alpha=2.0, prec=prec) == good
+
+
+def test_nonfinite_pno_inputs_are_reported(pkg, handle):
+    Z, Xa, Xi, eo, ev = O.make_thc_factors(120, 30, 4, 16, 41)
+    rng = np.random.default_rng(141)
+    U, _ = np.linalg.qr(rng.standard_normal((4 * 16, 24)))
+    A = -0.2 * rng.uniform(size=24)
+    Z = Z.copy()
+    Z[7, 2] = np.inf
+    with pytest.raises(pkg.RPAError) as err:
+        handle.jctc2024(Z, Xi, Xa, U, A, cutoff_pno=1e-8)
+    assert err.value.status == pkg.RPA_ERR_NONFINITE
