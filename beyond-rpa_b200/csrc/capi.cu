@@ -172,6 +172,19 @@ int finite_or_fail(rpa_b200_handle* h, std::initializer_list<double> xs, const c
     }                                                                                                       \
   } while (0)
 
+// RPA_ERR_NONFINITE when a device result (rows x cols, column-major, ld) holds NaN or Inf: the array
+// entry points that do not screen their inputs report a non-finite input through their output.
+// Synchronises the stream.
+int screen_result(rpa_b200_handle* h, const double* A, int64_t ld, int64_t rows, int64_t cols, const char* what) {
+  RPA_CUDA(h, cudaMemsetAsync(h->count_dev, 0, sizeof(int), h->stream));
+  RPA_CUDA(h, rpa::launch_count_nonfinite_cols(A, ld, rows, cols, h->count_dev, h->stream));
+  int cnt = 0;
+  RPA_CUDA(h, cudaMemcpyAsync(&cnt, h->count_dev, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+  RPA_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (cnt) return fail(h, RPA_ERR_NONFINITE, "%d non-finite entries in %s (NaN or Inf in an input)", cnt, what);
+  return RPA_OK;
+}
+
 cudaError_t ensure(DevBuf& b, size_t bytes) {
   if (b.bytes >= bytes && b.p) return cudaSuccess;
   if (b.p) {
@@ -2144,6 +2157,7 @@ int rpa_b200_project_basis(rpa_b200_handle* h, int64_t NQ, int64_t NVecs, int64_
   RPA_CUDA(h, rpa::launch_gemm_f64(gemm_tn((int)NVecs, (int)nov, NQ, Gd, ldg, Rd, ldr, out, ldo), h->stream));
   RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
   RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
+  if ((s = screen_result(h, out, ldo, NVecs, nov, "the projected Cholesky vectors"))) return s;
   if (!dev_out)
     RPA_CUDA(h, cudaMemcpy2DAsync(Rp, (size_t)ldRp * 8, out, (size_t)NVecs * 8, (size_t)NVecs * 8, (size_t)nov,
                                   cudaMemcpyDeviceToHost, h->stream));
@@ -2228,6 +2242,7 @@ int rpa_b200_thc_r(rpa_b200_handle* h, int64_t NGrid, int64_t NQ, int64_t NOcc, 
   if ((s = form_thc_r(h, NGrid, NQ, NOcc, NVirt, Zd, ldz, Xad, ldxa, Xid, ldxi, Rd, ldr))) return s;
   RPA_CUDA(h, cudaEventRecord(h->ev[2], h->stream));
   RPA_CUDA(h, cudaEventRecord(h->ev[3], h->stream));
+  if ((s = screen_result(h, Rd, ldr, NQ, nov, "the formed Cholesky vectors"))) return s;
   if (!dev)
     RPA_CUDA(h, cudaMemcpy2DAsync(R, (size_t)ldR * 8, Rd, (size_t)NQ * 8, (size_t)NQ * 8, (size_t)nov,
                                   cudaMemcpyDeviceToHost, h->stream));

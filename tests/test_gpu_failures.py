@@ -113,3 +113,22 @@ def test_nonfinite_pno_inputs_are_reported(pkg, handle):
     with pytest.raises(pkg.RPAError) as err:
         handle.jctc2024(Z, Xi, Xa, U, A, cutoff_pno=1e-8)
     assert err.value.status == pkg.RPA_ERR_NONFINITE
+
+
+def test_nonfinite_thc_and_projection_inputs_are_reported(pkg, handle):
+    # array entry points that do not screen their inputs screen their output instead
+    Z, Xa, Xi, eo, ev = O.make_thc_factors(90, 20, 3, 11, 43)
+    good = handle.thc_r(Z, Xa, Xi)
+    bad = Z.copy()
+    bad[5, 4] = np.nan
+    with pytest.raises(pkg.RPAError) as err:
+        handle.thc_r(bad, Xa, Xi)
+    assert err.value.status == pkg.RPA_ERR_NONFINITE
+    G = np.linalg.qr(np.random.default_rng(9).standard_normal((20, 8)))[0]
+    Rp = handle.project_basis(G, good)
+    assert np.allclose(Rp, G.T @ good, rtol=1e-12, atol=1e-14)
+    Gb = G.copy()
+    Gb[3, 2] = np.inf
+    with pytest.raises(pkg.RPAError) as err:
+        handle.project_basis(Gb, good)
+    assert err.value.status == pkg.RPA_ERR_NONFINITE
