@@ -1479,6 +1479,7 @@ int rpa_b200_dring_t2(rpa_b200_handle* h, int64_t NQ, int64_t NOcc, int64_t NVir
   double* IOm = static_cast<double*>(h->tIOm.p);
   if (Omega) {
     RPA_CUDA(h, cudaMemcpyAsync(Om, Omega, (size_t)nov * G * 8, cudaMemcpyDefault, h->stream));
+    if ((s = screen_result(h, Om, nov, nov, G, "the given guess vectors"))) return s;
   } else {
     RPA_CUDA(h, rpa::launch_fill_uniform(Om, nov, G, nov, seed, h->stream));
   }

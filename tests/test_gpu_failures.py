@@ -132,3 +132,13 @@ def test_nonfinite_thc_and_projection_inputs_are_reported(pkg, handle):
     with pytest.raises(pkg.RPAError) as err:
         handle.project_basis(Gb, good)
     assert err.value.status == pkg.RPA_ERR_NONFINITE
+
+
+def test_nonfinite_t2_guess_vectors_are_reported(pkg, handle):
+    s = O.make_system(60, 3, 10, 77, lam0=0.8)
+    x, w = O.grid_for(s, 4)
+    omega = np.random.default_rng(2).uniform(-0.5, 0.5, size=(3 * 10, 24))
+    omega[4, 7] = np.nan
+    with pytest.raises(pkg.RPAError) as err:
+        handle.dring_t2(s.R, s.eps_o, s.eps_v, x, w, prec="fp64", guess=omega)
+    assert err.value.status == pkg.RPA_ERR_NONFINITE
