@@ -32,7 +32,10 @@ constexpr int kCols = kTA / kComputeWarps;
 constexpr int kComputeThreads = 32 * kComputeWarps;
 constexpr int kThreads = kComputeThreads + 32;  // + the store warp
 constexpr int kStages = 4;
-constexpr int kStoreLag = 2;  // bulk-store groups still reading shared memory while the next is issued
+// bulk-store groups still reading shared memory while the next is issued: a stage is freed as soon
+// as the group after it has been committed (1: 4.23-4.31 ms at NQ 4096 / 65536 ai / 16 frequencies;
+// 2: 4.28-4.34 ms; 3: 4.74-4.84 ms, each later free stalls the compute warps)
+constexpr int kStoreLag = 1;
 constexpr int kBoxBytes = kTQ * 128;            // 32 rows x 64 bf16
 constexpr int kStageBytes = 4 * kBoxBytes;      // hi box 0, hi box 1, lo box 0, lo box 1
 constexpr int kFacBytes = kComputeWarps * kCols * kMaxKgLaunch * 8;
